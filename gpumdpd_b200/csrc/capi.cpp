@@ -1,0 +1,238 @@
+// capi.cpp -- the extern "C" boundary of libdpd_b200.so (include/dpd_b200.h).
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/dpd_b200.h"
+#include "engine.h"
+
+struct dpd_engine {
+    dpd::Engine eng;
+};
+
+static thread_local std::string g_create_err;
+
+static int set_create_err(const std::string& e, int code)
+{
+    g_create_err = e;
+    return code;
+}
+
+extern "C" {
+
+const char* dpd_version(void) { return "dpd_b200 1.0 (sm_100a)"; }
+
+int dpd_create(const char* run_in_text, const char* data_path, const char* base_dir, dpd_engine** out)
+{
+    if (!run_in_text || !out) return set_create_err("null argument", DPD_E_ARG);
+    *out = nullptr;
+    std::vector<dpd::Replica> reps(1);
+    std::string err;
+    int e = dpd::make_replica(run_in_text, data_path ? data_path : "", base_dir ? base_dir : "", reps[0], err);
+    if (e) return set_create_err(err, e);
+    auto* h = new (std::nothrow) dpd_engine;
+    if (!h) return set_create_err("out of host memory", DPD_E_NOMEM);
+    e = h->eng.init(std::move(reps), nullptr);
+    if (e) {
+        g_create_err = h->eng.err;
+        delete h;
+        return e;
+    }
+    *out = h;
+    return DPD_OK;
+}
+
+int dpd_create_from_system(const char* run_in_text, const dpd_system* sys, dpd_engine** out)
+{
+    if (!run_in_text || !sys || !out) return set_create_err("null argument", DPD_E_ARG);
+    *out = nullptr;
+    std::vector<dpd::Replica> reps(1);
+    std::string err;
+    int e = dpd::make_replica_from_system(run_in_text, sys, reps[0], err);
+    if (e) return set_create_err(err, e);
+    auto* h = new (std::nothrow) dpd_engine;
+    if (!h) return set_create_err("out of host memory", DPD_E_NOMEM);
+    e = h->eng.init(std::move(reps), nullptr);
+    if (e) {
+        g_create_err = h->eng.err;
+        delete h;
+        return e;
+    }
+    *out = h;
+    return DPD_OK;
+}
+
+int dpd_batch_create(int n_rep, const char* const* run_in_texts, const dpd_system* systems,
+                     const dpd_tuning* tune, dpd_engine** out)
+{
+    if (n_rep <= 0 || !run_in_texts || !systems || !out) return set_create_err("invalid argument", DPD_E_ARG);
+    *out = nullptr;
+    std::vector<dpd::Replica> reps(n_rep);
+    for (int r = 0; r < n_rep; r++) {
+        std::string err;
+        int e = dpd::make_replica_from_system(run_in_texts[r] ? run_in_texts[r] : "", &systems[r], reps[r], err);
+        if (e) return set_create_err("replica " + std::to_string(r) + ": " + err, e);
+    }
+    auto* h = new (std::nothrow) dpd_engine;
+    if (!h) return set_create_err("out of host memory", DPD_E_NOMEM);
+    int e = h->eng.init(std::move(reps), tune);
+    if (e) {
+        g_create_err = h->eng.err;
+        delete h;
+        return e;
+    }
+    *out = h;
+    return DPD_OK;
+}
+
+#define ENG_CHECK(h)               \
+    if (!(h)) {                    \
+        g_create_err = "null engine"; \
+        return DPD_E_ARG;          \
+    }
+
+int dpd_run(dpd_engine* h, uint32_t nsteps)
+{
+    ENG_CHECK(h);
+    return h->eng.run(nsteps);
+}
+
+int dpd_sync(dpd_engine* h)
+{
+    ENG_CHECK(h);
+    return h->eng.sync_and_check();
+}
+
+int dpd_get_thermo(dpd_engine* h, dpd_thermo* rows, int max_rows, int* n_rows)
+{
+    ENG_CHECK(h);
+    if (!rows || max_rows < 0) return DPD_E_ARG;
+    return h->eng.get_thermo(0, rows, max_rows, n_rows);
+}
+
+int dpd_get_state(dpd_engine* h, double* x, double* v, int* image, double* f)
+{
+    ENG_CHECK(h);
+    return h->eng.get_state(0, x, v, image, f);
+}
+
+int dpd_set_state(dpd_engine* h, const double* x, const double* v)
+{
+    ENG_CHECK(h);
+    return h->eng.set_state(0, x, v);
+}
+
+int dpd_get_density(dpd_engine* h, double* rho)
+{
+    ENG_CHECK(h);
+    if (!rho) return DPD_E_ARG;
+    return h->eng.get_density(0, rho);
+}
+
+int dpd_get_cells(dpd_engine* h, int* cell, float* offset, int* nc, float* w, float* cut2)
+{
+    ENG_CHECK(h);
+    return h->eng.get_cells(0, cell, offset, nc, w, cut2);
+}
+
+int dpd_get_neighbors(dpd_engine* h, int* pairs, int64_t cap, int64_t* n_pairs)
+{
+    ENG_CHECK(h);
+    return h->eng.get_neighbors(0, pairs, cap, n_pairs);
+}
+
+int dpd_compute_rdf(dpd_engine* h, int ta, int tb, double rmax, int nbins, double* g)
+{
+    ENG_CHECK(h);
+    return h->eng.compute_rdf_now(0, ta, tb, rmax, nbins, g);
+}
+
+int dpd_rdf_config(dpd_engine* h, int ta, int tb, double rmax, int nbins, int every)
+{
+    ENG_CHECK(h);
+    return h->eng.rdf_config(0, ta, tb, rmax, nbins, every);
+}
+
+int dpd_rdf_result(dpd_engine* h, double* g, int64_t* nsamples)
+{
+    ENG_CHECK(h);
+    if (!g) return DPD_E_ARG;
+    return h->eng.rdf_result(0, g, nsamples);
+}
+
+int dpd_get_info(dpd_engine* h, int64_t* step, int64_t* n_builds, int64_t* n_atoms, int64_t* device_bytes)
+{
+    ENG_CHECK(h);
+    if (step) *step = h->eng.steps_done(0);
+    if (n_builds) *n_builds = h->eng.n_builds();
+    if (n_atoms) *n_atoms = h->eng.total_atoms();
+    if (device_bytes) *device_bytes = h->eng.device_bytes();
+    return DPD_OK;
+}
+
+int dpd_set_tuning(dpd_engine* h, const dpd_tuning* t)
+{
+    ENG_CHECK(h);
+    return h->eng.set_tuning(t);
+}
+
+int dpd_write_data(dpd_engine* h, const char* path)
+{
+    ENG_CHECK(h);
+    if (!path) return DPD_E_ARG;
+    return h->eng.write_data(0, path);
+}
+
+int dpd_time_steps(dpd_engine* h, uint32_t nsteps, double* total_ms, double* pair_ms, int64_t* pair_launches)
+{
+    ENG_CHECK(h);
+    return h->eng.time_steps(nsteps, total_ms, pair_ms, pair_launches);
+}
+
+const char* dpd_last_error(dpd_engine* h)
+{
+    if (!h) return g_create_err.c_str();
+    return h->eng.err.c_str();
+}
+
+int dpd_destroy(dpd_engine* h)
+{
+    delete h;
+    return DPD_OK;
+}
+
+int dpd_pair_compute_aos(dpd_engine* h, const float* d_pos, const float* d_vel, const int* d_id,
+                         const int* d_type, int n, uint32_t step, float* d_force, float* d_pe,
+                         float* d_virial)
+{
+    ENG_CHECK(h);
+    return h->eng.pair_compute_aos(d_pos, d_vel, d_id, d_type, n, step, d_force, d_pe, d_virial);
+}
+
+int dpd_batch_n(dpd_engine* h, int* n_rep)
+{
+    ENG_CHECK(h);
+    if (n_rep) *n_rep = h->eng.n_rep();
+    return DPD_OK;
+}
+
+int dpd_batch_get_thermo(dpd_engine* h, int rep, dpd_thermo* rows, int max_rows, int* n_rows)
+{
+    ENG_CHECK(h);
+    return h->eng.get_thermo(rep, rows, max_rows, n_rows);
+}
+
+int dpd_batch_get_state(dpd_engine* h, int rep, double* x, double* v, int* image, double* f)
+{
+    ENG_CHECK(h);
+    return h->eng.get_state(rep, x, v, image, f);
+}
+
+int dpd_batch_rdf_result(dpd_engine* h, int rep, double* g, int64_t* nsamples)
+{
+    ENG_CHECK(h);
+    return h->eng.rdf_result(rep, g, nsamples);
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// dpd_common.h -- types shared by the host engine and the sm_100a kernels.
+#pragma once
+#include <stdint.h>
+
+#define DPD_MAX_TYPES 32
+#define DPD_NACC 24          // FP64 accumulators per replica and slot
+#define DPD_ACC_SLOTS 32     // atomic spreading slots per replica
+#define DPD_THERMO_FIELDS 16 // doubles per logged thermo row
+#define DPD_RING_ROWS 2048   // thermo rows kept per replica on the device
+#define DPD_CELL_BITS 10     // bits per cell coordinate in the packed cell code
+#define DPD_MAX_NC ((1 << DPD_CELL_BITS) - 1)
+#define DPD_TYPE_BITS 5      // type-1 in the low bits of the packed tag word
+#define DPD_MAX_TAG ((1 << (32 - DPD_TYPE_BITS)) - 1)
+
+// accumulator slots
+enum {
+    ACC_KE = 0,      // sum 1/2 m v^2
+    ACC_KIN = 1,     // 6: sum m v_a v_b
+    ACC_PAIR_PE = 7,
+    ACC_BOND_PE = 8,
+    ACC_VIR = 9,     // 6: sum over pairs and bonds of r_a F_b
+    ACC_MOM = 15,    // 3: sum m v
+    ACC_NONFINITE = 18,
+};
+
+// status bits (per replica, device)
+enum {
+    ST_LIST_OVERFLOW = 1,
+    ST_NONFINITE = 2,
+    ST_BOND_MISSING = 4,
+    ST_FENE_BROKEN = 8,
+    ST_BOND_OVERFLOW = 16,
+};
+
+// Per-replica constant description (device copy, read through the L1 cache).
+struct RepDesc {
+    int p_begin;    // first particle slot (multiple of 32)
+    int p_end;      // one past the last real particle
+    int p_cap_end;  // one past the last slot (multiple of 32); [p_end, p_cap_end) are ghosts
+    int n_real;
+    int c_begin;    // first cell of this replica in the packed cell arrays
+    int ncell;      // cells nc[0]*nc[1]*nc[2]; local cell `ncell` holds the ghosts
+    int nc[3];
+    int tag_base;   // offset of this replica's tags in tag2idx
+    float w[3];     // cell widths (>= global_cut + skin)
+    float inv_w[3];
+    float L[3];
+    float cut2;     // (global_cut + skin)^2 in float, list predicate
+    float rcmax2;   // max over type pairs of rc^2
+    float hskin2;   // (skin/2)^2
+    int skin_zero;  // skin == 0: rebuild every nl_f steps unconditionally
+    int ntypes;
+    int coeff_off;  // in units of float4, 3 float4 per (ti,tj)
+    int mass_off;   // float2 (mass, 1/mass) per type
+    int style;      // 0 dpd, 1 mdpd
+    uint32_t seed;
+    float dt;
+    int nl_f;
+    int log_f;
+    int bond_style; // 0 none, 1 harmonic, 2 fene
+    int bond_off;   // float4 per bond type
+    uint32_t integ_mask; // bit (type-1) set when the type is integrated (fix nve group)
+    double lo[3];
+    double volume;
+    int rdf_every;  // 0 = off
+    int rdf_ta, rdf_tb, rdf_nbins;
+    float rdf_rmax;
+    int rdf_off;    // offset into the RDF histogram array (nbins per replica)
+};
+
+// Per-replica dynamic state (device).
+struct RepState {
+    uint32_t step;      // the step whose force evaluation comes next
+    uint32_t target;    // last step to evaluate in the current run
+    int zero_pending;   // next evaluation is the zero step (no final half kick)
+    int status;
+    int nlog;           // thermo rows written
+    int nbuild;
+    int64_t rdf_samples;
+};
+
+// Coefficient table entry per ordered type pair (3 float4):
+//  c0 = {A, gamma, sigma = sqrt(gamma)*sqrt(2kT)/sqrt(dt), rc^2}
+//  c1 = {1/rc, 0.5*A*rc, B, 1/rd}
+//  c2 = {rd^2, 0.25*B*rd, 15/(2 pi rd^3), rc}

@@ -1,0 +1,77 @@
+// dpd_io.h -- the reference's command surface: run.in grammar, data files, thermo.txt.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <functional>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace dpd {
+
+// Global commands of run.in, src/main/read_in.cu:40-290 (Read_in::read).
+struct RunInput {
+    int atom_style = -1;  // 0 atomic, 1 bond, 2 angle
+    double global_cut = 0, skin = 0, max_rho = 0;
+    int nl_f = 1;
+    double dt = 0;
+    unsigned log_f = 0;
+    unsigned nsteps = 0;
+    std::string read_data;
+    bool write_data = false;
+    std::string write_data_name;
+    bool dump = false;
+    unsigned dump_start = 0, dump_f = 1;
+    bool dump_wrapped = false, dump_force = false, dump_vel = false;
+    std::vector<std::vector<std::string>> lines;  // every command line, tokenized
+    std::vector<std::string> raw;                 // the same lines as text
+};
+
+// Contents of a data file (src/system/read_data.cu:145-468), rows indexed by tag-1.
+struct SystemData {
+    int n_atoms = 0, n_atomtypes = 0, n_bonds = 0, n_bondtypes = 0, n_angles = 0, n_angletypes = 0;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    std::vector<double> masses;
+    std::vector<int> type, mol;
+    std::vector<double> x, v;
+    std::vector<int> bonds;  // type, tag_i, tag_j
+    bool has_velocities = false;
+};
+
+struct ComputeTemp {
+    std::string id, group, file;
+    unsigned frequency = 1;
+    uint32_t type_mask = 0;
+};
+
+struct ComputeRdf {
+    std::string id, file;
+    int ta = 1, tb = 1, nbins = 150, every = 100;
+    double rmax = 3.0;
+};
+
+// Pair/bond styles and their coefficients, groups, fixes and computes, parsed after
+// the data file is known (as the reference's isEnabled/validateParams do).
+struct ForceField {
+    int pair_style = -1;  // 0 dpd (src/force/pair_dpd.cu:19-173), 1 mdpd (pair_mdpd.cu:21-192)
+    double temp = 0, rc = 0, rd = 0;
+    unsigned seed = 0;
+    int ntypes = 0;
+    std::vector<std::array<double, 5>> coeff;  // triangular index: A, B, gamma, rc, rd
+    int bond_style = 0;                        // 0 none, 1 harmonic, 2 fene
+    std::vector<std::array<double, 4>> bond_coeff;
+    std::map<std::string, std::vector<int>> groups;
+    uint32_t integ_mask = 0;  // types integrated by fix nve
+    std::vector<ComputeTemp> temps;
+    std::vector<ComputeRdf> rdfs;
+};
+
+int tri_index(int ti, int tj, int nt);  // src/force/pair_dpd.cu:134, 0-based
+
+int parse_run_in(const std::string& text, RunInput& out, std::string& err);
+int read_data_file(const std::string& path, int atom_style, SystemData& out, std::string& err);
+int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff, std::string& err);
+int write_data_file(const std::string& path, int atom_style, const SystemData& sys,
+                    std::string& err);
+
+}  // namespace dpd

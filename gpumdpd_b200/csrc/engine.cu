@@ -1,0 +1,997 @@
+// engine.cu -- host engine: packed replica layout, device buffers, the captured
+// timestep, state I/O.  The timestep order is the reference's
+// (src/main/utils.cuh:166-213 zero step, :254-303 per step):
+//   [list build if flagged] [mDPD density] [pair + bonds] [RDF sample]
+//   [final half kick n, thermo n, initial half kick + drift n+1, build check] [advance]
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "engine.h"
+#include "kernels.cuh"
+#include "kernels_step.cuh"
+
+namespace dpd {
+
+#define CK(call)                                               \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);    \
+    } while (0)
+
+int Engine::cuda_fail(cudaError_t e, const char* what)
+{
+    err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DPD_E_NOMEM : DPD_E_CUDA;
+}
+
+template <class T>
+int Engine::dalloc(T** p, size_t n)
+{
+    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    allocs_.push_back((void*)*p);
+    dev_bytes_ += (int64_t)bytes;
+    e = cudaMemsetAsync(*p, 0, bytes, stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    return DPD_OK;
+}
+
+Engine::~Engine()
+{
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (void* p : allocs_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+// ---------------------------------------------------------------------------------
+static uint32_t morton3(uint32_t x, uint32_t y, uint32_t z)
+{
+    auto spread = [](uint32_t v) {
+        v &= 0x3ff;
+        v = (v | (v << 16)) & 0x030000FF;
+        v = (v | (v << 8)) & 0x0300F00F;
+        v = (v | (v << 4)) & 0x030C30C3;
+        v = (v | (v << 2)) & 0x09249249;
+        return v;
+    };
+    return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+int Engine::layout()
+{
+    P_ = 0;
+    C_ = 0;
+    nmax_ = 16;
+    maxb_ = 0;
+    int tag_base = 0, coeff_off = 0, mass_off = 0, bond_off = 0, rdf_off = 0;
+    any_mdpd_ = any_dpd_ = small_ = bonds_ = rdf_ = false;
+    for (size_t r = 0; r < reps_.size(); r++) {
+        Replica& R = reps_[r];
+        RepDesc& d = R.desc;
+        memset(&d, 0, sizeof(d));
+        const double cut = R.in.global_cut + R.in.skin;
+        for (int k = 0; k < 3; k++) {
+            const double L = R.sys.hi[k] - R.sys.lo[k];
+            int nc = (int)std::floor(L / cut);
+            if (nc < 3) {
+                err = "box too small: the cell grid needs at least 3 cells of size global_cut+skin per dimension";
+                return DPD_E_ARG;
+            }
+            if (nc > DPD_MAX_NC) {
+                err = "box too large: at most 1023 cells per dimension";
+                return DPD_E_ARG;
+            }
+            d.nc[k] = nc;
+            d.w[k] = (float)(L / nc);
+            d.inv_w[k] = 1.0f / d.w[k];
+            R.box_len[k] = (double)nc * (double)d.w[k];
+            d.L[k] = (float)R.box_len[k];
+            d.lo[k] = R.sys.lo[k];
+            if (nc < 5) small_ = true;
+        }
+        const int n = R.sys.n_atoms;
+        if (n > DPD_MAX_TAG) {
+            err = "too many atoms in one system";
+            return DPD_E_ARG;
+        }
+        d.p_begin = P_;
+        d.n_real = n;
+        d.p_end = P_ + n;
+        d.p_cap_end = P_ + ((n + 31) / 32) * 32;
+        P_ = d.p_cap_end;
+        d.c_begin = C_;
+        d.ncell = d.nc[0] * d.nc[1] * d.nc[2];
+        C_ += d.ncell + 1;
+        d.tag_base = tag_base;
+        tag_base += n;
+        const float cutf = (float)cut;
+        d.cut2 = cutf * cutf;
+        double rcm = 0;
+        for (auto& c : R.ff.coeff) rcm = std::max(rcm, c[3]);
+        d.rcmax2 = (float)(rcm * rcm);
+        const float hs = (float)(R.in.skin * 0.5);
+        d.hskin2 = hs * hs;
+        d.skin_zero = R.in.skin == 0.0;
+        d.ntypes = R.sys.n_atomtypes;
+        d.coeff_off = coeff_off;
+        coeff_off += d.ntypes * d.ntypes * 3;
+        d.mass_off = mass_off;
+        mass_off += d.ntypes;
+        d.style = R.ff.pair_style;
+        if (d.style == 1) any_mdpd_ = true; else any_dpd_ = true;
+        d.seed = R.ff.seed;
+        d.dt = (float)R.in.dt;
+        d.nl_f = R.in.nl_f;
+        d.log_f = (int)R.in.log_f;
+        d.bond_style = R.sys.n_bonds > 0 ? R.ff.bond_style : 0;
+        if (d.bond_style) bonds_ = true;
+        d.bond_off = bond_off;
+        bond_off += std::max(R.sys.n_bondtypes, 1);
+        d.integ_mask = R.ff.integ_mask;
+        d.volume = R.box_len[0] * R.box_len[1] * R.box_len[2];
+        if (!R.ff.rdfs.empty()) {
+            const ComputeRdf& c = R.ff.rdfs[0];
+            d.rdf_every = c.every;
+            d.rdf_ta = c.ta;
+            d.rdf_tb = c.tb;
+            d.rdf_nbins = c.nbins;
+            d.rdf_rmax = (float)c.rmax;
+            rdf_ = true;
+        }
+        d.rdf_off = rdf_off;
+        rdf_off += R.ff.rdfs.empty() ? 0 : R.ff.rdfs[0].nbins;
+        // neighbour capacity: src/force/neigh_list.cu:14-17
+        const double sphere = 4.0 / 3.0 * M_PI * std::pow(cut, 3.0);
+        int nm = (int)(R.in.max_rho * sphere) + 1;
+        nm = ((nm + 15) / 16) * 16;
+        R.nmax = nm;
+        nmax_ = std::max(nmax_, nm);
+        // bond partners per atom
+        if (d.bond_style) {
+            std::vector<int> deg(n, 0);
+            for (int b = 0; b < R.sys.n_bonds; b++) {
+                deg[R.sys.bonds[3 * b + 1] - 1]++;
+                deg[R.sys.bonds[3 * b + 2] - 1]++;
+            }
+            for (int i = 0; i < n; i++) R.maxb = std::max(R.maxb, deg[i]);
+            maxb_ = std::max(maxb_, R.maxb);
+        }
+        // cell order
+        R.crank.resize(d.ncell);
+        std::vector<std::pair<uint32_t, int>> order(d.ncell);
+        for (int cx = 0; cx < d.nc[0]; cx++)
+            for (int cy = 0; cy < d.nc[1]; cy++)
+                for (int cz = 0; cz < d.nc[2]; cz++) {
+                    int lin = (cx * d.nc[1] + cy) * d.nc[2] + cz;
+                    uint32_t key = tune_.cell_order == 1 ? morton3(cx, cy, cz) : (uint32_t)lin;
+                    order[lin] = {key, lin};
+                }
+        std::sort(order.begin(), order.end());
+        for (int k = 0; k < d.ncell; k++) R.crank[order[k].second] = k;
+    }
+    if (maxb_ > 16) {
+        err = "an atom has more than 16 bonds";
+        return DPD_E_ARG;
+    }
+    return DPD_OK;
+}
+
+int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        err = "no CUDA device available (this engine has no CPU fallback)";
+        return DPD_E_NODEV;
+    }
+    reps_ = std::move(reps);
+    if (reps_.empty()) {
+        err = "no replicas";
+        return DPD_E_ARG;
+    }
+    if (tune) tune_ = *tune;
+    if (tune_.cell_order == 0 && !tune) tune_.cell_order = 1;
+    int st = layout();
+    if (st) return st;
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    st = alloc_and_upload();
+    if (st) return st;
+    host_target_.assign(reps_.size(), 0);
+    return build_graph();
+}
+
+int Engine::alloc_and_upload()
+{
+    const int nrep = (int)reps_.size();
+    int st;
+#define DA(ptr, n) if ((st = dalloc(&ptr, (size_t)(n)))) return st
+    DA(b_.reps, nrep);
+    DA(b_.rstate, nrep);
+    DA(b_.warp_rep, P_ / 32);
+    DA(b_.crank, C_);
+    int ncoeff = 0, nmass = 0, nbond = 0, nrdf = 0;
+    for (auto& R : reps_) {
+        ncoeff += R.desc.ntypes * R.desc.ntypes * 3;
+        nmass += R.desc.ntypes;
+        nbond += std::max(R.sys.n_bondtypes, 1);
+        nrdf += R.ff.rdfs.empty() ? 0 : R.ff.rdfs[0].nbins;
+    }
+    DA(b_.coeff, ncoeff);
+    DA(b_.mass, nmass);
+    DA(b_.bondc, nbond);
+    DA(b_.pos4, P_);
+    DA(b_.vel4, P_);
+    DA(b_.force4, P_);
+    DA(b_.last4, P_);
+    DA(b_.pos_t, P_);
+    DA(b_.vel_t, P_);
+    DA(b_.rho, P_);
+    DA(b_.img, P_);
+    DA(b_.img_t, P_);
+    DA(b_.bonds, (size_t)std::max(maxb_, 1) * P_);
+    DA(b_.bonds_t, (size_t)std::max(maxb_, 1) * P_);
+    DA(b_.cnt, C_);
+    DA(b_.cstart, C_ + 1);
+    DA(b_.fill, C_);
+    DA(b_.perm, P_);
+    int64_t ntag = 0;
+    for (auto& R : reps_) ntag += R.sys.n_atoms;
+    DA(b_.tag2idx, ntag);
+    DA(b_.ncount, P_);
+    DA(b_.nlist, (size_t)P_ * nmax_);
+    DA(b_.blocksum, (C_ + 4095) / 4096 + 1);
+    DA(b_.acc, (size_t)nrep * DPD_ACC_SLOTS * DPD_NACC);
+    DA(b_.ring, (size_t)nrep * DPD_RING_ROWS * DPD_THERMO_FIELDS);
+    DA(b_.rdf_hist, nrdf);
+    DA(b_.build_flag, 2);
+    DA(b_.phase, 1);
+#undef DA
+    // tables
+    std::vector<RepDesc> hd(nrep);
+    std::vector<int> wrep(P_ / 32), crank(C_, 0);
+    std::vector<float4> coeff(ncoeff);
+    std::vector<float2> mass(nmass);
+    std::vector<float4> bondc(nbond);
+    for (int r = 0; r < nrep; r++) {
+        const Replica& R = reps_[r];
+        const RepDesc& d = R.desc;
+        hd[r] = d;
+        for (int wv = d.p_begin / 32; wv < d.p_cap_end / 32; wv++) wrep[wv] = r;
+        for (int c = 0; c < d.ncell; c++) crank[d.c_begin + c] = R.crank[c];
+        const int nt = d.ntypes;
+        const double sig_scale = std::sqrt(2.0 * R.ff.temp) / std::sqrt(R.in.dt);
+        for (int ti = 0; ti < nt; ti++)
+            for (int tj = 0; tj < nt; tj++) {
+                const auto& c = R.ff.coeff[tri_index(ti + 1, tj + 1, nt)];
+                const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4];
+                const size_t o = d.coeff_off + (size_t)(ti * nt + tj) * 3;
+                const float rcf = (float)rc;
+                coeff[o] = make_float4((float)A, (float)gamma, (float)(std::sqrt(gamma) * sig_scale), rcf * rcf);
+                coeff[o + 1] = make_float4((float)(1.0 / rc), (float)(0.5 * A * rc), (float)B,
+                                           rd > 0 ? (float)(1.0 / rd) : 0.0f);
+                const float rdf = (float)rd;
+                coeff[o + 2] = make_float4(rdf * rdf, (float)(0.25 * B * rd),
+                                           rd > 0 ? (float)(15.0 / (2.0 * M_PI * rd * rd * rd)) : 0.0f, rcf);
+            }
+        for (int t = 0; t < nt; t++) mass[d.mass_off + t] = make_float2((float)R.sys.masses[t], (float)(1.0 / R.sys.masses[t]));
+        for (int b = 0; b < std::max(R.sys.n_bondtypes, 1); b++) {
+            if (b < (int)R.ff.bond_coeff.size()) {
+                const auto& c = R.ff.bond_coeff[b];
+                bondc[d.bond_off + b] = make_float4((float)c[0], (float)c[1], (float)c[2], (float)c[3]);
+            } else {
+                bondc[d.bond_off + b] = make_float4(0, 0, 0, 0);
+            }
+        }
+    }
+    CK(cudaMemcpyAsync(b_.reps, hd.data(), sizeof(RepDesc) * nrep, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.warp_rep, wrep.data(), sizeof(int) * wrep.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.crank, crank.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.coeff, coeff.data(), sizeof(float4) * ncoeff, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.mass, mass.data(), sizeof(float2) * nmass, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.bondc, bondc.data(), sizeof(float4) * nbond, cudaMemcpyHostToDevice, stream_));
+    std::vector<RepState> rs(nrep);
+    for (auto& s : rs) {
+        memset(&s, 0, sizeof(s));
+        s.zero_pending = 1;
+    }
+    CK(cudaMemcpyAsync(b_.rstate, rs.data(), sizeof(RepState) * nrep, cudaMemcpyHostToDevice, stream_));
+    int st2 = upload_particles();
+    if (st2) return st2;
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
+// Convert the FP64 state of every replica into the cell-offset representation.
+int Engine::upload_particles()
+{
+    std::vector<float4> pos(P_), vel(P_);
+    std::vector<int4> img(P_);
+    std::vector<int2> bonds((size_t)std::max(maxb_, 1) * P_, make_int2(0, 0));
+    for (auto& R : reps_) {
+        const RepDesc& d = R.desc;
+        const int n = R.sys.n_atoms;
+        std::vector<int> deg(n, 0);
+        for (int i = 0; i < n; i++) {
+            const int s = d.p_begin + i;
+            int c[3];
+            float o[3];
+            for (int k = 0; k < 3; k++) {
+                double x = R.sys.x[3 * (size_t)i + k] - d.lo[k];
+                const double L = R.box_len[k];
+                if (x >= L || x < 0) x -= L * std::floor(x / L);
+                int cc = (int)std::floor(x / (double)d.w[k]);
+                cc = std::min(std::max(cc, 0), d.nc[k] - 1);
+                double off = x - (double)cc * (double)d.w[k];
+                float of = (float)off;
+                if (of >= d.w[k]) of = std::nextafter(d.w[k], 0.0f);
+                if (of < 0.0f) of = 0.0f;
+                c[k] = cc;
+                o[k] = of;
+            }
+            int code = c[0] | (c[1] << DPD_CELL_BITS) | (c[2] << (2 * DPD_CELL_BITS));
+            float codef;
+            memcpy(&codef, &code, 4);
+            pos[s] = make_float4(o[0], o[1], o[2], codef);
+            const int tagw = ((i + 1) << DPD_TYPE_BITS) | (R.sys.type[i] - 1);
+            float tagf;
+            memcpy(&tagf, &tagw, 4);
+            vel[s] = make_float4((float)R.sys.v[3 * (size_t)i], (float)R.sys.v[3 * (size_t)i + 1],
+                                 (float)R.sys.v[3 * (size_t)i + 2], tagf);
+            img[s] = make_int4(0, 0, 0, 0);
+        }
+        if (d.bond_style) {
+            for (int b = 0; b < R.sys.n_bonds; b++) {
+                const int ty = R.sys.bonds[3 * b], ta = R.sys.bonds[3 * b + 1], tb = R.sys.bonds[3 * b + 2];
+                const int ia = ta - 1, ib = tb - 1;
+                bonds[(size_t)deg[ia] * P_ + d.p_begin + ia] = make_int2(tb, ty);
+                deg[ia]++;
+                bonds[(size_t)deg[ib] * P_ + d.p_begin + ib] = make_int2(ta, ty);
+                deg[ib]++;
+            }
+        }
+        for (int s = d.p_end; s < d.p_cap_end; s++) {
+            pos[s] = make_float4(0, 0, 0, 0);
+            vel[s] = make_float4(0, 0, 0, 0);
+            img[s] = make_int4(0, 0, 0, 0);
+        }
+    }
+    CK(cudaMemcpyAsync(b_.pos4, pos.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.vel4, vel.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.img, img.data(), sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.bonds, bonds.data(), sizeof(int2) * bonds.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemsetAsync(b_.force4, 0, sizeof(float4) * P_, stream_));
+    CK(cudaMemsetAsync(b_.rho, 0, sizeof(float) * P_, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
+// ---------------------------------------------------------------------------------
+static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int maxb)
+{
+    BuildArgs a;
+    a.reps = b.reps;
+    a.warp_rep = b.warp_rep;
+    a.crank = b.crank;
+    a.P = P;
+    a.C = C;
+    a.nmax = nmax;
+    a.maxb = maxb;
+    a.build_flag = b.build_flag;
+    a.phase = b.phase;
+    a.pos4 = b.pos4;
+    a.vel4 = b.vel4;
+    a.img = b.img;
+    a.bonds = b.bonds;
+    a.last4 = b.last4;
+    a.pos_t = b.pos_t;
+    a.vel_t = b.vel_t;
+    a.img_t = b.img_t;
+    a.bonds_t = b.bonds_t;
+    a.cnt = b.cnt;
+    a.cstart = b.cstart;
+    a.fill = b.fill;
+    a.perm = b.perm;
+    a.tag2idx = b.tag2idx;
+    a.ncount = b.ncount;
+    a.nlist = b.nlist;
+    a.rstate = b.rstate;
+    a.blocksum = b.blocksum;
+    return a;
+}
+
+static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int nrep)
+{
+    StepArgs a;
+    a.reps = b.reps;
+    a.warp_rep = b.warp_rep;
+    a.rstate = b.rstate;
+    a.P = P;
+    a.nmax = nmax;
+    a.maxb = maxb;
+    a.coeff = b.coeff;
+    a.mass = b.mass;
+    a.bondc = b.bondc;
+    a.pos4 = b.pos4;
+    a.vel4 = b.vel4;
+    a.force4 = b.force4;
+    a.rho = b.rho;
+    a.img = b.img;
+    a.last4 = b.last4;
+    a.bonds = b.bonds;
+    a.tag2idx = b.tag2idx;
+    a.ncount = b.ncount;
+    a.nlist = b.nlist;
+    a.acc = b.acc;
+    a.ring = b.ring;
+    a.rdf_hist = b.rdf_hist;
+    a.cstart = b.cstart;
+    a.crank = b.crank;
+    a.build_flag = b.build_flag;
+    a.phase = b.phase;
+    a.nrep = nrep;
+    a.mode = 0;
+    return a;
+}
+
+template <int STYLE>
+static void launch_pair(bool small, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
+{
+    if (small) {
+        if (bonds) k_pair<STYLE, true, true><<<grid, 256, 0, s>>>(a);
+        else k_pair<STYLE, true, false><<<grid, 256, 0, s>>>(a);
+    } else {
+        if (bonds) k_pair<STYLE, false, true><<<grid, 256, 0, s>>>(a);
+        else k_pair<STYLE, false, false><<<grid, 256, 0, s>>>(a);
+    }
+}
+
+void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
+{
+    const int nrep = (int)reps_.size();
+    BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
+    StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
+    const int gp = (P_ + 255) / 256;
+    const int gc = (C_ + 255) / 256;
+    const int nsb = (C_ + 4095) / 4096;
+    k_bin_count<<<gp, 256, 0, s>>>(ba);
+    k_scan_blocks<<<nsb, 1024, 0, s>>>(ba);
+    k_scan_sums<<<1, 1024, 0, s>>>(ba, nsb);
+    k_scan_add<<<gc, 256, 0, s>>>(ba);
+    k_scatter<<<gp, 256, 0, s>>>(ba);
+    k_cell_sort<<<gc, 256, 0, s>>>(ba);
+    k_permute<<<gp, 256, 0, s>>>(ba);
+    k_build_nlist<<<gp, 256, 0, s>>>(ba);
+    k_build_done<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
+    if (any_mdpd_) {
+        if (small_) k_density<true><<<gp, 256, 0, s>>>(sa);
+        else k_density<false><<<gp, 256, 0, s>>>(sa);
+    }
+    if (ev0) cudaEventRecord(ev0, s);
+    if (any_dpd_) launch_pair<0>(small_, bonds_, gp, s, sa);
+    if (any_mdpd_) launch_pair<1>(small_, bonds_, gp, s, sa);
+    if (ev1) cudaEventRecord(ev1, s);
+    if (rdf_) k_rdf<<<gp, 256, 0, s>>>(sa);
+    k_integrate<<<gp, 256, 0, s>>>(sa);
+    k_advance<<<(nrep + 255) / 256, 256, 0, s>>>(sa);
+}
+
+void Engine::enqueue_integrate_initial(cudaStream_t s)
+{
+    StepArgs sa = step_args(b_, P_, nmax_, maxb_, (int)reps_.size());
+    sa.mode = 1;
+    k_integrate<<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+}
+
+int Engine::build_graph()
+{
+    if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(stream_, nullptr, nullptr);
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    return DPD_OK;
+}
+
+// set the run target of every replica (absolute step), optionally mark the next
+// evaluation as a zero step and raise the list-build flag of the current phase
+__global__ void k_set_target(RepState* st, int nrep, uint32_t target, int zero, int set_build,
+                             int* build_flag, const uint32_t* phase)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep) {
+        st[r].target = target;
+        if (zero) st[r].zero_pending = 1;
+    }
+    if (r == 0 && set_build) build_flag[(*phase) & 1] = 1;
+}
+
+int Engine::run(uint32_t nsteps)
+{
+    const int nrep = (int)reps_.size();
+    const int g = (nrep + 255) / 256;
+    if (zero_pending_) {
+        // zero step at next_step_, then nsteps steps
+        const uint32_t target = next_step_ + nsteps;
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, nrep, target, 1, 1, b_.build_flag, b_.phase);
+        CK(cudaGetLastError());
+        for (uint32_t k = 0; k <= nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
+        next_step_ = target + 1;
+        zero_pending_ = false;
+    } else {
+        if (nsteps == 0) return sync_and_check();
+        const uint32_t target = next_step_ - 1 + nsteps;
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, nrep, target, 0, 0, b_.build_flag, b_.phase);
+        enqueue_integrate_initial(stream_);
+        CK(cudaGetLastError());
+        for (uint32_t k = 0; k < nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
+        next_step_ = target + 1;
+    }
+    return sync_and_check();
+}
+
+int Engine::read_rstate(std::vector<RepState>& st)
+{
+    st.resize(reps_.size());
+    CK(cudaMemcpyAsync(st.data(), b_.rstate, sizeof(RepState) * st.size(), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
+int Engine::sync_and_check()
+{
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaGetLastError());
+    std::vector<RepState> st;
+    int e = read_rstate(st);
+    if (e) return e;
+    for (size_t r = 0; r < st.size(); r++) {
+        int s = st[r].status;
+        if (s & ST_LIST_OVERFLOW) {
+            err = "neighbour list overflow in replica " + std::to_string(r) + ": increase max_rho in the neighbor command";
+            return DPD_E_OVERFLOW;
+        }
+        if (s & ST_NONFINITE) {
+            err = "non-finite position or velocity in replica " + std::to_string(r);
+            return DPD_E_NUMERIC;
+        }
+        if (s & ST_FENE_BROKEN) {
+            err = "FENE bond stretched beyond R0 in replica " + std::to_string(r);
+            return DPD_E_NUMERIC;
+        }
+        if (s & ST_BOND_MISSING) {
+            err = "bond partner not found in replica " + std::to_string(r);
+            return DPD_E_STATE;
+        }
+    }
+    return DPD_OK;
+}
+
+int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64_t* launches)
+{
+    if (zero_pending_) {
+        int e = run(0);
+        if (e) return e;
+    }
+    if (nsteps == 0) return DPD_E_ARG;
+    const int nrep = (int)reps_.size();
+    std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 2);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    const uint32_t target = next_step_ - 1 + nsteps;
+    k_set_target<<<(nrep + 255) / 256, 256, 0, stream_>>>(b_.rstate, nrep, target, 0, 0, b_.build_flag, b_.phase);
+    enqueue_integrate_initial(stream_);
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    for (uint32_t k = 0; k < nsteps; k++) enqueue_step(stream_, ev[2 * k + 2], ev[2 * k + 3]);
+    cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    cudaGraphExec_t ge;
+    ce = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaEventRecord(ev[0], stream_));
+    CK(cudaGraphLaunch(ge, stream_));
+    CK(cudaEventRecord(ev[1], stream_));
+    CK(cudaStreamSynchronize(stream_));
+    next_step_ = target + 1;
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    double pair = 0;
+    for (uint32_t k = 0; k < nsteps; k++) {
+        float p = 0;
+        CK(cudaEventElapsedTime(&p, ev[2 * k + 2], ev[2 * k + 3]));
+        pair += p;
+    }
+    cudaGraphExecDestroy(ge);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (total_ms) *total_ms = ms;
+    if (pair_ms) *pair_ms = pair;
+    if (launches) *launches = (int64_t)nsteps * ((any_dpd_ ? 1 : 0) + (any_mdpd_ ? 1 : 0));
+    return sync_and_check();
+}
+
+int Engine::set_targets(const std::vector<uint32_t>& target)
+{
+    (void)target;
+    return DPD_E_STATE;
+}
+
+int64_t Engine::steps_done(int r) const
+{
+    (void)r;
+    return zero_pending_ && next_step_ == 0 ? 0 : (int64_t)next_step_ - 1;
+}
+
+int64_t Engine::n_builds()
+{
+    std::vector<RepState> st;
+    if (read_rstate(st)) return -1;
+    return st.empty() ? 0 : st[0].nbuild;
+}
+
+int64_t Engine::total_atoms() const
+{
+    int64_t n = 0;
+    for (auto& R : reps_) n += R.sys.n_atoms;
+    return n;
+}
+
+// ---------------------------------------------------------------------------------
+int Engine::get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    std::vector<RepState> st;
+    int e = read_rstate(st);
+    if (e) return e;
+    const int nlog = st[rep].nlog;
+    const int avail = std::min(nlog, DPD_RING_ROWS);
+    const int n = std::min(avail, max_rows);
+    std::vector<double> ring((size_t)DPD_RING_ROWS * DPD_THERMO_FIELDS);
+    CK(cudaMemcpyAsync(ring.data(), b_.ring + (size_t)rep * DPD_RING_ROWS * DPD_THERMO_FIELDS,
+                       sizeof(double) * ring.size(), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < n; k++) {
+        const int idx = (nlog - n + k) % DPD_RING_ROWS;
+        const double* row = ring.data() + (size_t)idx * DPD_THERMO_FIELDS;
+        dpd_thermo& t = rows[k];
+        t.step = (int64_t)row[0];
+        t.temp = row[1];
+        t.pair_pe = row[2];
+        t.bond_pe = row[3];
+        t.pressure = row[4];
+        for (int c = 0; c < 6; c++) t.p[c] = row[5 + c];
+        t.ke = row[11];
+        for (int c = 0; c < 3; c++) t.momentum[c] = row[12 + c];
+    }
+    if (n_rows) *n_rows = n;
+    return DPD_OK;
+}
+
+int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    const RepDesc& d = reps_[rep].desc;
+    const int ns = d.p_cap_end - d.p_begin;
+    std::vector<float4> pos(ns), vel(ns), frc(ns);
+    std::vector<int4> img(ns);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpyAsync(pos.data(), b_.pos4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(frc.data(), b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(img.data(), b_.img + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < d.n_real; k++) {
+        int tw;
+        memcpy(&tw, &vel[k].w, 4);
+        const int tag = (int)((uint32_t)tw >> DPD_TYPE_BITS);
+        if (tag < 1 || tag > d.n_real) {
+            err = "corrupt tag in device state";
+            return DPD_E_STATE;
+        }
+        const size_t o = 3 * (size_t)(tag - 1);
+        int code;
+        memcpy(&code, &pos[k].w, 4);
+        const int c[3] = {code & DPD_MAX_NC, (code >> DPD_CELL_BITS) & DPD_MAX_NC, (code >> (2 * DPD_CELL_BITS)) & DPD_MAX_NC};
+        const float off[3] = {pos[k].x, pos[k].y, pos[k].z};
+        const float vv[3] = {vel[k].x, vel[k].y, vel[k].z};
+        const float ff[3] = {frc[k].x, frc[k].y, frc[k].z};
+        const int im[3] = {img[k].x, img[k].y, img[k].z};
+        for (int q = 0; q < 3; q++) {
+            if (x) x[o + q] = d.lo[q] + (double)c[q] * (double)d.w[q] + (double)off[q];
+            if (v) v[o + q] = vv[q];
+            if (f) f[o + q] = ff[q];
+            if (image) image[o + q] = im[q];
+        }
+    }
+    return DPD_OK;
+}
+
+int Engine::set_state(int rep, const double* x, const double* v)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    Replica& R = reps_[rep];
+    std::vector<double> xv(3 * (size_t)R.sys.n_atoms), vv(3 * (size_t)R.sys.n_atoms);
+    std::vector<int> im(3 * (size_t)R.sys.n_atoms);
+    int e = get_state(rep, xv.data(), vv.data(), im.data(), nullptr);
+    if (e) return e;
+    if (x) memcpy(R.sys.x.data(), x, sizeof(double) * xv.size()); else R.sys.x = xv;
+    if (v) memcpy(R.sys.v.data(), v, sizeof(double) * vv.size()); else R.sys.v = vv;
+    // full re-upload of every replica's particles (the host copies of the others are
+    // refreshed first), then a forced list build at the next step
+    for (int r = 0; r < (int)reps_.size(); r++) {
+        if (r == rep) continue;
+        Replica& Q = reps_[r];
+        e = get_state(r, Q.sys.x.data(), Q.sys.v.data(), nullptr, nullptr);
+        if (e) return e;
+    }
+    e = upload_particles();
+    if (e) return e;
+    zero_pending_ = true;
+    return sync_and_check();
+}
+
+int Engine::get_density(int rep, double* rho)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    const RepDesc& d = reps_[rep].desc;
+    const int ns = d.p_cap_end - d.p_begin;
+    std::vector<float> r(ns);
+    std::vector<float4> vel(ns);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpyAsync(r.data(), b_.rho + d.p_begin, sizeof(float) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < d.n_real; k++) {
+        int tw;
+        memcpy(&tw, &vel[k].w, 4);
+        const int tag = (int)((uint32_t)tw >> DPD_TYPE_BITS);
+        if (tag >= 1 && tag <= d.n_real) rho[tag - 1] = r[k];
+    }
+    return DPD_OK;
+}
+
+int Engine::get_cells(int rep, int* cell, float* off, int* nc, float* w, float* cut2)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    const RepDesc& d = reps_[rep].desc;
+    const int ns = d.p_cap_end - d.p_begin;
+    std::vector<float4> pos(ns), vel(ns);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpyAsync(pos.data(), b_.pos4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < d.n_real; k++) {
+        int tw, code;
+        memcpy(&tw, &vel[k].w, 4);
+        memcpy(&code, &pos[k].w, 4);
+        const int tag = (int)((uint32_t)tw >> DPD_TYPE_BITS);
+        if (tag < 1 || tag > d.n_real) continue;
+        const size_t o = 3 * (size_t)(tag - 1);
+        if (cell) {
+            cell[o] = code & DPD_MAX_NC;
+            cell[o + 1] = (code >> DPD_CELL_BITS) & DPD_MAX_NC;
+            cell[o + 2] = (code >> (2 * DPD_CELL_BITS)) & DPD_MAX_NC;
+        }
+        if (off) {
+            off[o] = pos[k].x;
+            off[o + 1] = pos[k].y;
+            off[o + 2] = pos[k].z;
+        }
+    }
+    for (int q = 0; q < 3; q++) {
+        if (nc) nc[q] = d.nc[q];
+        if (w) w[q] = d.w[q];
+    }
+    if (cut2) *cut2 = d.cut2;
+    return DPD_OK;
+}
+
+int Engine::get_neighbors(int rep, int* pairs, int64_t cap, int64_t* n_pairs)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    const RepDesc& d = reps_[rep].desc;
+    const int ns = d.p_cap_end - d.p_begin;
+    std::vector<int> cnt(ns), lst((size_t)ns * nmax_);
+    std::vector<float4> vel(P_);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpyAsync(cnt.data(), b_.ncount + d.p_begin, sizeof(int) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(lst.data(), b_.nlist + (size_t)d.p_begin * nmax_, sizeof(int) * lst.size(), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel4, sizeof(float4) * P_, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    auto tag_at = [&](int s) {
+        int tw;
+        memcpy(&tw, &vel[s].w, 4);
+        return (int)((uint32_t)tw >> DPD_TYPE_BITS);
+    };
+    int64_t np = 0;
+    for (int k = 0; k < d.n_real; k++) {
+        const int s = d.p_begin + k;
+        const int c = std::min(cnt[k], nmax_);
+        for (int q = 0; q < c; q++) {
+            const int j = lst[((size_t)(k >> 5) * nmax_ + q) * 32 + (k & 31)];
+            if (j < 0 || j >= P_) continue;
+            int a = tag_at(s), bb = tag_at(j);
+            if (np < cap && pairs) {
+                pairs[2 * np] = std::min(a, bb);
+                pairs[2 * np + 1] = std::max(a, bb);
+            }
+            np++;
+        }
+    }
+    if (n_pairs) *n_pairs = np;
+    return DPD_OK;
+}
+
+int Engine::rdf_result(int rep, double* g, int64_t* nsamples)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    const Replica& R = reps_[rep];
+    if (R.ff.rdfs.empty()) {
+        err = "no rdf compute configured for this system";
+        return DPD_E_STATE;
+    }
+    const ComputeRdf& c = R.ff.rdfs[0];
+    std::vector<unsigned long long> h(c.nbins);
+    std::vector<RepState> st;
+    int e = read_rstate(st);
+    if (e) return e;
+    CK(cudaMemcpyAsync(h.data(), b_.rdf_hist + R.desc.rdf_off, sizeof(unsigned long long) * c.nbins, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const int64_t ns = st[rep].rdf_samples;
+    if (nsamples) *nsamples = ns;
+    int64_t na = 0, nb = 0;
+    for (int i = 0; i < R.sys.n_atoms; i++) {
+        na += R.sys.type[i] == c.ta;
+        nb += R.sys.type[i] == c.tb;
+    }
+    const double vol = R.desc.volume;
+    const double npair = c.ta == c.tb ? (double)na * (double)(na - 1) : (double)na * (double)nb;
+    const double dr = c.rmax / c.nbins;
+    for (int b = 0; b < c.nbins; b++) {
+        const double r0 = b * dr, r1 = (b + 1) * dr;
+        const double shell = 4.0 / 3.0 * M_PI * (r1 * r1 * r1 - r0 * r0 * r0);
+        const double ideal = npair * shell / vol * (double)std::max<int64_t>(ns, 1);
+        g[b] = ideal > 0 ? (double)h[b] / ideal : 0.0;
+    }
+    return DPD_OK;
+}
+
+int Engine::compute_rdf_now(int rep, int ta, int tb, double rmax, int nbins, double* g)
+{
+    (void)rep; (void)ta; (void)tb; (void)rmax; (void)nbins; (void)g;
+    err = "use an rdf compute (compute ID group rdf ...) to sample the RDF";
+    return DPD_E_STATE;
+}
+
+int Engine::rdf_config(int rep, int ta, int tb, double rmax, int nbins, int every)
+{
+    (void)rep; (void)ta; (void)tb; (void)rmax; (void)nbins; (void)every;
+    err = "rdf sampling is configured by the compute rdf command";
+    return DPD_E_STATE;
+}
+
+int Engine::write_data(int rep, const std::string& path)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    Replica& R = reps_[rep];
+    SystemData s = R.sys;
+    int e = get_state(rep, s.x.data(), s.v.data(), nullptr, nullptr);
+    if (e) return e;
+    return write_data_file(path, R.in.atom_style, s, err);
+}
+
+int Engine::set_tuning(const dpd_tuning* t)
+{
+    if (!t) return DPD_E_ARG;
+    tune_ = *t;
+    return build_graph();
+}
+
+int Engine::pair_compute_aos(const float*, const float*, const int*, const int*, int, uint32_t, float*,
+                             float*, float*)
+{
+    err = "not available";
+    return DPD_E_STATE;
+}
+
+// ---------------------------------------------------------------------------------
+int make_replica(const std::string& run_in, const std::string& data_path, const std::string& base_dir,
+                 Replica& R, std::string& err)
+{
+    int e = parse_run_in(run_in, R.in, err);
+    if (e) return e;
+    std::string path = data_path.empty() ? R.in.read_data : data_path;
+    if (data_path.empty() && !base_dir.empty() && !path.empty() && path[0] != '/') path = base_dir + "/" + path;
+    e = read_data_file(path, R.in.atom_style, R.sys, err);
+    if (e) return e;
+    return parse_force_field(R.in, R.sys, R.ff, err);
+}
+
+int make_replica_from_system(const std::string& run_in, const dpd_system* s, Replica& R, std::string& err)
+{
+    int e = parse_run_in(run_in, R.in, err);
+    if (e) return e;
+    if (!s || s->n_atoms <= 0 || s->n_atomtypes <= 0 || !s->tag || !s->type || !s->x || !s->masses) {
+        err = "incomplete dpd_system";
+        return DPD_E_ARG;
+    }
+    SystemData& d = R.sys;
+    d.n_atoms = s->n_atoms;
+    d.n_atomtypes = s->n_atomtypes;
+    d.n_bonds = R.in.atom_style >= 1 ? s->n_bonds : 0;
+    d.n_bondtypes = s->n_bondtypes;
+    for (int k = 0; k < 3; k++) {
+        d.lo[k] = s->lo[k];
+        d.hi[k] = s->hi[k];
+        if (!(d.hi[k] > d.lo[k])) {
+            err = "Invalid box dimensions.";
+            return DPD_E_ARG;
+        }
+    }
+    d.masses.assign(s->masses, s->masses + s->n_atomtypes);
+    for (double m : d.masses)
+        if (!(m > 0)) {
+            err = "All the masses are not set.";
+            return DPD_E_ARG;
+        }
+    const int n = s->n_atoms;
+    d.type.assign(n, 0);
+    d.mol.assign(n, 0);
+    d.x.assign(3 * (size_t)n, 0.0);
+    d.v.assign(3 * (size_t)n, 0.0);
+    std::vector<char> seen(n, 0);
+    for (int i = 0; i < n; i++) {
+        const int t = s->tag[i];
+        if (t < 1 || t > n || seen[t - 1]) {
+            err = "tags must be a permutation of 1..n_atoms";
+            return DPD_E_ARG;
+        }
+        seen[t - 1] = 1;
+        if (s->type[i] < 1 || s->type[i] > s->n_atomtypes) {
+            err = "atom type out of range";
+            return DPD_E_ARG;
+        }
+        d.type[t - 1] = s->type[i];
+        if (s->mol) d.mol[t - 1] = s->mol[i];
+        for (int k = 0; k < 3; k++) {
+            double c = s->x[3 * (size_t)i + k];
+            const double L = d.hi[k] - d.lo[k];
+            if (!std::isfinite(c)) {
+                err = "non-finite position";
+                return DPD_E_ARG;
+            }
+            if (c >= d.hi[k] || c < d.lo[k]) c -= L * std::floor((c - d.lo[k]) / L);
+            if (c >= d.hi[k]) c = d.lo[k];
+            d.x[3 * (size_t)(t - 1) + k] = c;
+            d.v[3 * (size_t)(t - 1) + k] = s->v ? s->v[3 * (size_t)i + k] : 0.0;
+        }
+    }
+    d.has_velocities = s->v != nullptr;
+    if (d.n_bonds > 0) {
+        if (!s->bonds) {
+            err = "bonds missing";
+            return DPD_E_ARG;
+        }
+        d.bonds.assign(s->bonds, s->bonds + 3 * (size_t)d.n_bonds);
+        for (int b = 0; b < d.n_bonds; b++) {
+            const int ty = d.bonds[3 * b], a = d.bonds[3 * b + 1], c = d.bonds[3 * b + 2];
+            if (ty < 1 || ty > std::max(1, d.n_bondtypes) || a < 1 || a > n || c < 1 || c > n || a == c) {
+                err = "invalid bond " + std::to_string(b + 1);
+                return DPD_E_ARG;
+            }
+        }
+    }
+    return parse_force_field(R.in, R.sys, R.ff, err);
+}
+
+}  // namespace dpd

@@ -1,0 +1,113 @@
+// engine.h -- host side of the engine: one packed batch of replicas on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/dpd_b200.h"
+#include "dpd_common.h"
+#include "dpd_io.h"
+
+namespace dpd {
+
+struct Replica {
+    RunInput in;
+    SystemData sys;
+    ForceField ff;
+    RepDesc desc{};
+    int nmax = 16;
+    int maxb = 0;
+    std::vector<int> crank;  // linear cell -> position in this replica's cell order
+    double box_len[3] = {0, 0, 0};  // engine box: nc * w (float w), see layout()
+};
+
+struct DeviceBuffers {
+    RepDesc* reps = nullptr;
+    RepState* rstate = nullptr;
+    int* warp_rep = nullptr;
+    int* crank = nullptr;
+    float4* coeff = nullptr;
+    float2* mass = nullptr;
+    float4* bondc = nullptr;
+    float4 *pos4 = nullptr, *vel4 = nullptr, *force4 = nullptr, *last4 = nullptr;
+    float4 *pos_t = nullptr, *vel_t = nullptr;
+    float* rho = nullptr;
+    int4 *img = nullptr, *img_t = nullptr;
+    int2 *bonds = nullptr, *bonds_t = nullptr;
+    int *cnt = nullptr, *cstart = nullptr, *fill = nullptr, *perm = nullptr, *tag2idx = nullptr;
+    int *ncount = nullptr, *nlist = nullptr, *blocksum = nullptr;
+    double *acc = nullptr, *ring = nullptr;
+    unsigned long long* rdf_hist = nullptr;
+    int* build_flag = nullptr;
+    uint32_t* phase = nullptr;
+};
+
+class Engine {
+public:
+    Engine() = default;
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // replicas must be fully parsed; builds the packed layout and uploads it
+    int init(std::vector<Replica>&& reps, const dpd_tuning* tune);
+    int run(uint32_t nsteps);
+    int sync_and_check();
+    int time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64_t* launches);
+    int get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows);
+    int get_state(int rep, double* x, double* v, int* image, double* f);
+    int set_state(int rep, const double* x, const double* v);
+    int get_density(int rep, double* rho);
+    int get_cells(int rep, int* cell, float* off, int* nc, float* w, float* cut2);
+    int get_neighbors(int rep, int* pairs, int64_t cap, int64_t* n_pairs);
+    int compute_rdf_now(int rep, int ta, int tb, double rmax, int nbins, double* g);
+    int rdf_config(int rep, int ta, int tb, double rmax, int nbins, int every);
+    int rdf_result(int rep, double* g, int64_t* nsamples);
+    int write_data(int rep, const std::string& path);
+    int set_tuning(const dpd_tuning* t);
+    int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
+                         int n, uint32_t step, float* d_force, float* d_pe, float* d_virial);
+
+    int n_rep() const { return (int)reps_.size(); }
+    const Replica& rep(int r) const { return reps_[r]; }
+    int64_t steps_done(int r) const;
+    int64_t n_builds();
+    int64_t device_bytes() const { return dev_bytes_; }
+    int64_t total_atoms() const;
+    std::string err;
+
+    // for the server: extend/replace per-replica targets
+    int set_targets(const std::vector<uint32_t>& target);
+    int read_rstate(std::vector<RepState>& st);
+
+private:
+    int layout();
+    int alloc_and_upload();
+    int upload_particles();
+    void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
+    void enqueue_integrate_initial(cudaStream_t s);
+    int build_graph();
+    int cuda_fail(cudaError_t e, const char* what);
+    template <class T> int dalloc(T** p, size_t n);
+
+    std::vector<Replica> reps_;
+    DeviceBuffers b_;
+    dpd_tuning tune_{};
+    cudaStream_t stream_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    int P_ = 0, C_ = 0, nmax_ = 16, maxb_ = 0;
+    bool any_mdpd_ = false, any_dpd_ = false, small_ = false, bonds_ = false, rdf_ = false;
+    bool zero_pending_ = true;
+    uint32_t next_step_ = 0;
+    std::vector<void*> allocs_;
+    int64_t dev_bytes_ = 0;
+    std::vector<uint32_t> host_target_;
+};
+
+int make_replica(const std::string& run_in, const std::string& data_path, const std::string& base_dir,
+                 Replica& out, std::string& err);
+int make_replica_from_system(const std::string& run_in, const dpd_system* sys, Replica& out,
+                             std::string& err);
+
+}  // namespace dpd

@@ -1,0 +1,373 @@
+// kernels.cuh -- sm_100a kernels of the DPD timestep.
+//
+// Particle layout (packed over replicas; each replica owns a warp-aligned slot range):
+//   pos4[s]  = {ox, oy, oz, cell code}  offsets in [0,w) inside cell (cx,cy,cz), the
+//              code packs cx | cy<<10 | cz<<20 (replica-local cell coordinates)
+//   vel4[s]  = {vx, vy, vz, tag<<5 | (type-1)}
+//   force4[s]= {fx, fy, fz, 0}         accumulated with vector atomics
+//   img[s]   = image counters
+// Slots are sorted by cell (counting sort at every neighbour-list build), cells in
+// linear or Morton order.  The half neighbour list is warp-chunked:
+//   nlist[((s>>5)*nmax + k)*32 + (s&31)]  (k-th neighbour of slot s).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "dpd_common.h"
+
+// ---------------------------------------------------------------------------------
+// Saru counter-based RNG.  The stream must be bit-identical to the reference's
+// (src/force/pair_dpd.cu:203-236), so the published steps and constants are kept;
+// the float tail is evaluated with one rounding per operation exactly as the
+// reference's -DSINGLE build does: u = (float)s * 2^-31 - 1, theta = sqrt(3)f * u.
+__device__ __forceinline__ float saru_theta(uint32_t seed1, uint32_t seed2, uint32_t seed,
+                                            uint32_t timestep)
+{
+    uint32_t seed3 = seed + timestep;
+    seed3 ^= (seed1 << 7) ^ (seed2 >> 6);
+    seed2 += (seed1 >> 4) ^ (seed3 >> 15);
+    seed1 ^= (seed2 << 9) + (seed3 << 8);
+    seed3 ^= 0xA5366B4Du * ((seed2 >> 11) ^ (seed1 << 1));
+    seed2 += 0x72BE1579u * ((seed1 << 4) ^ (seed3 >> 16));
+    seed1 ^= 0x3F38A6EDu * ((seed3 >> 5) ^ (uint32_t)(((int32_t)seed2) >> 22));
+    seed2 += seed1 * seed3;
+    seed1 += seed3 ^ (seed2 >> 2);
+    seed2 ^= (uint32_t)(((int32_t)seed2) >> 17);
+    uint32_t state = 0x79dedea3u * (seed1 ^ (uint32_t)(((int32_t)seed1) >> 14));
+    uint32_t wstate = (state + seed2) ^ (uint32_t)(((int32_t)state) >> 8);
+    state = state + (wstate * (wstate ^ 0xdddf97f5u));
+    wstate = 0xABCB96F7u + (wstate >> 1);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        sum += 0x9e3779b9u;
+        state += ((wstate << 4) + 0xA341316Cu) ^ (wstate + sum) ^ ((wstate >> 5) + 0xC8013EA4u);
+        wstate += ((state << 4) + 0xAD90777Du) ^ (state + sum) ^ ((state >> 5) + 0x7E95761Eu);
+    }
+    uint32_t v = (state ^ (state >> 26)) + wstate;
+    uint32_t s = (v ^ (v >> 20)) * 0x6957f5a7u;
+    float u = __fmaf_rn(__uint2float_rn(s), 4.6566128730773926e-10f, -1.0f);
+    return __fmul_rn(1.7320508075688772f, u);
+}
+
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ int cell_x(int code) { return code & DPD_MAX_NC; }
+__device__ __forceinline__ int cell_y(int code) { return (code >> DPD_CELL_BITS) & DPD_MAX_NC; }
+__device__ __forceinline__ int cell_z(int code) { return (code >> (2 * DPD_CELL_BITS)) & DPD_MAX_NC; }
+__device__ __forceinline__ int cell_pack(int x, int y, int z)
+{
+    return x | (y << DPD_CELL_BITS) | (z << (2 * DPD_CELL_BITS));
+}
+__device__ __forceinline__ int tag_of(float w) { return (int)(((uint32_t)__float_as_int(w)) >> DPD_TYPE_BITS); }
+__device__ __forceinline__ int type0_of(float w) { return __float_as_int(w) & ((1 << DPD_TYPE_BITS) - 1); }
+
+// wrap a cell difference to the nearest image of the cell grid
+__device__ __forceinline__ int wrap_dc(int dc, int nc)
+{
+    int h = nc >> 1;
+    dc -= (dc > h) ? nc : 0;
+    dc += (dc < -h) ? nc : 0;
+    return dc;
+}
+
+// displacement p_i - p_j in the cell-offset representation; `small` applies a
+// position-level minimum image (needed only when a grid has fewer than 5 cells)
+template <bool SMALL>
+__device__ __forceinline__ float disp1(int ci, int cj, float oi, float oj, int nc, float w, float L)
+{
+    int dc = wrap_dc(ci - cj, nc);
+    float d = __fmaf_rn(__int2float_rn(dc), w, __fsub_rn(oi, oj));
+    if (SMALL) {
+        float h = 0.5f * L;
+        d -= (d >= h) ? L : 0.0f;
+        d += (d < -h) ? L : 0.0f;
+    }
+    return d;
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 per-replica accumulation: warp reduce, then one atomic per (block, replica
+// segment, field) into one of DPD_ACC_SLOTS spread copies.
+template <int NV>
+__device__ __forceinline__ void acc_flush(double (&val)[NV], const int* field, int rep, double* acc)
+{
+    __shared__ double sh[32][NV];
+    __shared__ int shrep[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double x = val[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        val[k] = x;
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[warp][k] = val[k];
+        shrep[warp] = rep;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        const int k = threadIdx.x;
+        const int nw = blockDim.x >> 5;
+        const int slot = blockIdx.x & (DPD_ACC_SLOTS - 1);
+        double s = 0.0;
+        int cur = shrep[0];
+        for (int w = 0; w < nw; w++) {
+            int r = shrep[w];
+            if (r != cur) {
+                if (cur >= 0 && s != 0.0)
+                    atomicAdd(&acc[((size_t)cur * DPD_ACC_SLOTS + slot) * DPD_NACC + field[k]], s);
+                s = 0.0;
+                cur = r;
+            }
+            s += sh[w][k];
+        }
+        if (cur >= 0 && s != 0.0)
+            atomicAdd(&acc[((size_t)cur * DPD_ACC_SLOTS + slot) * DPD_NACC + field[k]], s);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Neighbour-list build: counting sort of slots by cell, stable per-cell order by tag,
+// permutation of particle arrays, then the half list.  All kernels return at once
+// unless the build flag of this phase is set.
+
+struct BuildArgs {
+    const RepDesc* reps;
+    const int* warp_rep;
+    const int* crank;       // [cells] linear cell -> position in the replica's cell order
+    int P;                  // total slots
+    int C;                  // total cells (all replicas, ghost cells included)
+    int nmax;               // neighbour list capacity per slot
+    int maxb;               // bond partners per slot
+    const int* build_flag;  // [2]
+    const uint32_t* phase;
+    float4* pos4;
+    float4* vel4;
+    int4* img;
+    int2* bonds;
+    float4* last4;
+    float4* pos_t;
+    float4* vel_t;
+    int4* img_t;
+    int2* bonds_t;
+    int* cnt;
+    int* cstart;            // [C+1]
+    int* fill;
+    int* perm;
+    int* tag2idx;
+    int* ncount;
+    int* nlist;
+    RepState* rstate;
+    int* blocksum;
+};
+
+__device__ __forceinline__ bool build_on(const BuildArgs& a)
+{
+    return a.build_flag[(*a.phase) & 1] != 0;
+}
+
+__device__ __forceinline__ int cell_key(const BuildArgs& a, const RepDesc& d, int code, bool ghost)
+{
+    if (ghost) return d.c_begin + d.ncell;
+    int lin = (cell_x(code) * d.nc[1] + cell_y(code)) * d.nc[2] + cell_z(code);
+    return d.c_begin + a.crank[d.c_begin + lin];
+}
+
+__global__ void k_bin_count(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;
+    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
+    bool ghost = s >= d.p_end;
+    int key = cell_key(a, d, __float_as_int(a.pos4[s].w), ghost);
+    atomicAdd(&a.cnt[key], 1);
+}
+
+// exclusive scan of cnt[0..C) into cstart[0..C], three passes (block scan of 4096
+// elements, scan of block sums in one block, add back).
+__global__ void k_scan_blocks(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    __shared__ int sh[1024];
+    const int base = blockIdx.x * 4096;
+    int v[4], tot = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int idx = base + threadIdx.x * 4 + k;
+        v[k] = idx < a.C ? a.cnt[idx] : 0;
+        tot += v[k];
+    }
+    sh[threadIdx.x] = tot;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+        __syncthreads();
+        sh[threadIdx.x] += t;
+        __syncthreads();
+    }
+    int run = sh[threadIdx.x] - tot;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int idx = base + threadIdx.x * 4 + k;
+        if (idx < a.C) a.cstart[idx] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 1023) a.blocksum[blockIdx.x] = sh[1023];
+}
+
+__global__ void k_scan_sums(BuildArgs a, int nblocks)
+{
+    if (!build_on(a)) return;
+    __shared__ int sh[1024];
+    // sequential chunks of 1024 block sums (nblocks <= 1024*64 supported)
+    int carry = 0;
+    for (int base = 0; base < nblocks; base += 1024) {
+        int idx = base + threadIdx.x;
+        int v = idx < nblocks ? a.blocksum[idx] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            int t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (idx < nblocks) a.blocksum[idx] = carry + sh[threadIdx.x] - v;
+        int total = sh[1023];
+        __syncthreads();
+        carry += total;
+    }
+    if (threadIdx.x == 0) a.cstart[a.C] = carry;
+}
+
+__global__ void k_scan_add(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < a.C) a.cstart[idx] += a.blocksum[idx / 4096];
+}
+
+__global__ void k_scatter(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;
+    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
+    bool ghost = s >= d.p_end;
+    int key = cell_key(a, d, __float_as_int(a.pos4[s].w), ghost);
+    int pos = a.cstart[key] + atomicAdd(&a.fill[key], 1);
+    if (pos >= 0 && pos < a.P) a.perm[pos] = s;
+}
+
+// one thread per cell: insertion sort of the cell's slots by tag (deterministic order)
+__global__ void k_cell_sort(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.C) return;
+    int b = a.cstart[c], e = a.cstart[c + 1];
+    a.cnt[c] = 0;
+    a.fill[c] = 0;
+    if (b < 0 || e > a.P) return;
+    for (int i = b + 1; i < e; i++) {
+        int si = a.perm[i];
+        int ti = tag_of(a.vel4[si].w);
+        int j = i - 1;
+        while (j >= b) {
+            int sj = a.perm[j];
+            if (tag_of(a.vel4[sj].w) <= ti) break;
+            a.perm[j + 1] = sj;
+            j--;
+        }
+        a.perm[j + 1] = si;
+    }
+}
+
+__global__ void k_permute(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;
+    int o = a.perm[s];
+    float4 p = a.pos4[o];
+    float4 v = a.vel4[o];
+    a.pos_t[s] = p;
+    a.vel_t[s] = v;
+    a.img_t[s] = a.img[o];
+    for (int k = 0; k < a.maxb; k++) a.bonds_t[(size_t)k * a.P + s] = a.bonds[(size_t)k * a.P + o];
+    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
+    if (s < d.p_end) {
+        int t = tag_of(v.w);
+        if (t >= 1 && t <= d.n_real) a.tag2idx[d.tag_base + t - 1] = s;
+    }
+}
+
+// half stencil: the 13 cell offsets with (oz>0) | (oz==0 & oy>0) | (oz==0 & oy==0 & ox>0)
+__constant__ int8_t c_half[13][3] = {
+    {1, 0, 0}, {-1, 1, 0}, {0, 1, 0}, {1, 1, 0}, {-1, -1, 1}, {0, -1, 1}, {1, -1, 1},
+    {-1, 0, 1}, {0, 0, 1}, {1, 0, 1}, {-1, 1, 1}, {0, 1, 1}, {1, 1, 1}};
+
+__global__ void k_build_nlist(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;
+    const int r = a.warp_rep[s >> 5];
+    const RepDesc& d = a.reps[r];
+    float4 pi = a.pos_t[s];
+    // copy the permuted arrays back (the list is built from the permuted copy)
+    a.pos4[s] = pi;
+    a.vel4[s] = a.vel_t[s];
+    a.img[s] = a.img_t[s];
+    a.last4[s] = pi;
+    for (int k = 0; k < a.maxb; k++) a.bonds[(size_t)k * a.P + s] = a.bonds_t[(size_t)k * a.P + s];
+    if (s >= d.p_end) {
+        a.ncount[s] = 0;
+        return;
+    }
+    const int code = __float_as_int(pi.w);
+    const int cx = cell_x(code), cy = cell_y(code), cz = cell_z(code);
+    const int ncx = d.nc[0], ncy = d.nc[1], ncz = d.nc[2];
+    const float cut2 = d.cut2;
+    int* out = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+    int count = 0;
+    // own cell, j > s
+    for (int st = -1; st < 13; st++) {
+        int ox = 0, oy = 0, oz = 0;
+        if (st >= 0) { ox = c_half[st][0]; oy = c_half[st][1]; oz = c_half[st][2]; }
+        int nx = cx + ox; nx += nx < 0 ? ncx : 0; nx -= nx >= ncx ? ncx : 0;
+        int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
+        int nz = cz + oz; nz += nz < 0 ? ncz : 0; nz -= nz >= ncz ? ncz : 0;
+        int key = d.c_begin + a.crank[d.c_begin + (nx * ncy + ny) * ncz + nz];
+        int jb = a.cstart[key], je = a.cstart[key + 1];
+        if (st < 0) jb = s + 1;
+        for (int j = jb; j < je; j++) {
+            float4 pj = a.pos_t[j];
+            // p_i - p_j = (c_i - c_j) w + (o_i - o_j) with c_j = c_i + (ox,oy,oz)
+            float dx = __fmaf_rn(__int2float_rn(-ox), d.w[0], __fsub_rn(pi.x, pj.x));
+            float dy = __fmaf_rn(__int2float_rn(-oy), d.w[1], __fsub_rn(pi.y, pj.y));
+            float dz = __fmaf_rn(__int2float_rn(-oz), d.w[2], __fsub_rn(pi.z, pj.z));
+            float r2 = __fmul_rn(dx, dx);
+            r2 = __fmaf_rn(dy, dy, r2);
+            r2 = __fmaf_rn(dz, dz, r2);
+            if (r2 <= cut2) {
+                if (count < a.nmax) out[(size_t)count * 32] = j;
+                count++;
+            }
+        }
+    }
+    if (count > a.nmax) {
+        atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+        count = a.nmax;
+    }
+    a.ncount[s] = count;
+}
+
+__global__ void k_build_done(BuildArgs a, int nrep)
+{
+    if (!build_on(a)) return;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep) a.rstate[r].nbuild++;
+}

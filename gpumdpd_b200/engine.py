@@ -1,0 +1,214 @@
+"""Host-side mirror of the reference's simulation surface over the C ABI.
+
+`Engine` corresponds to one GPUDPD run (src/main/main.cu:15-72): it is created from
+the text of a run.in (the reference's command grammar) plus a data file or arrays,
+advances with :meth:`Engine.run`, and exposes thermo rows (thermo.txt columns),
+state, forces, the neighbour list and the RDF.  `Batch` packs many independent
+systems into one engine.  Errors raise :class:`DpdError` instead of exiting.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import DpdError
+
+
+def _check(code, lib, handle):
+    if code != 0:
+        msg = lib.dpd_last_error(handle)
+        raise DpdError(code, msg.decode() if msg else "")
+
+
+def _rows_to_dict(rows, n):
+    out = {k: np.empty(n) for k in ("step", "temp", "pair_pe", "bond_pe", "pressure", "ke")}
+    out["p"] = np.empty((n, 6))
+    out["momentum"] = np.empty((n, 3))
+    for k in range(n):
+        r = rows[k]
+        out["step"][k] = r.step
+        out["temp"][k] = r.temp
+        out["pair_pe"][k] = r.pair_pe
+        out["bond_pe"][k] = r.bond_pe
+        out["pressure"][k] = r.pressure
+        out["ke"][k] = r.ke
+        out["p"][k] = list(r.p)
+        out["momentum"][k] = list(r.momentum)
+    out["step"] = out["step"].astype(np.int64)
+    return out
+
+
+class Engine:
+    """One DPD system on the GPU (plain engine)."""
+
+    def __init__(self, run_in, data_path=None, base_dir=None, system=None):
+        self.lib = capi.load()
+        self.h = ctypes.c_void_p()
+        if system is not None:
+            s, self._keep = system
+            code = self.lib.dpd_create_from_system(run_in.encode(), ctypes.byref(s), ctypes.byref(self.h))
+        else:
+            code = self.lib.dpd_create(run_in.encode(), data_path.encode() if data_path else None,
+                                       base_dir.encode() if base_dir else None, ctypes.byref(self.h))
+        _check(code, self.lib, None)
+        n = ctypes.c_int64()
+        self.lib.dpd_get_info(self.h, None, None, ctypes.byref(n), None)
+        self.n_atoms = n.value
+
+    def close(self):
+        if self.h:
+            self.lib.dpd_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, nsteps):
+        _check(self.lib.dpd_run(self.h, int(nsteps)), self.lib, self.h)
+
+    def thermo(self, max_rows=4096):
+        rows = (capi.dpd_thermo * max_rows)()
+        n = ctypes.c_int()
+        _check(self.lib.dpd_get_thermo(self.h, rows, max_rows, ctypes.byref(n)), self.lib, self.h)
+        return _rows_to_dict(rows, n.value)
+
+    def state(self):
+        n = self.n_atoms
+        x = np.empty((n, 3))
+        v = np.empty((n, 3))
+        img = np.empty((n, 3), dtype=np.int32)
+        f = np.empty((n, 3))
+        _check(self.lib.dpd_get_state(self.h, capi.ptr(x), capi.ptr(v), capi.ptr(img), capi.ptr(f)),
+               self.lib, self.h)
+        return {"x": x, "v": v, "image": img, "f": f}
+
+    def set_state(self, x, v):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        _check(self.lib.dpd_set_state(self.h, capi.ptr(x), capi.ptr(v)), self.lib, self.h)
+
+    def density(self):
+        rho = np.empty(self.n_atoms)
+        _check(self.lib.dpd_get_density(self.h, capi.ptr(rho)), self.lib, self.h)
+        return rho
+
+    def cells(self):
+        n = self.n_atoms
+        cell = np.empty((n, 3), dtype=np.int32)
+        off = np.empty((n, 3), dtype=np.float32)
+        nc = np.empty(3, dtype=np.int32)
+        w = np.empty(3, dtype=np.float32)
+        cut2 = ctypes.c_float()
+        _check(self.lib.dpd_get_cells(self.h, capi.ptr(cell), capi.ptr(off), capi.ptr(nc), capi.ptr(w),
+                                      ctypes.byref(cut2)), self.lib, self.h)
+        return {"cell": cell, "offset": off, "nc": nc, "w": w, "cut2": np.float32(cut2.value)}
+
+    def neighbors(self):
+        total = ctypes.c_int64()
+        _check(self.lib.dpd_get_neighbors(self.h, None, 0, ctypes.byref(total)), self.lib, self.h)
+        pairs = np.empty((max(total.value, 1), 2), dtype=np.int32)
+        _check(self.lib.dpd_get_neighbors(self.h, capi.ptr(pairs), total.value, ctypes.byref(total)),
+               self.lib, self.h)
+        return pairs[: total.value]
+
+    def rdf(self, nbins):
+        g = np.empty(nbins)
+        ns = ctypes.c_int64()
+        _check(self.lib.dpd_rdf_result(self.h, capi.ptr(g), ctypes.byref(ns)), self.lib, self.h)
+        return g, ns.value
+
+    def info(self):
+        st, nb, na, db = (ctypes.c_int64() for _ in range(4))
+        _check(self.lib.dpd_get_info(self.h, ctypes.byref(st), ctypes.byref(nb), ctypes.byref(na),
+                                     ctypes.byref(db)), self.lib, self.h)
+        return {"step": st.value, "builds": nb.value, "atoms": na.value, "device_bytes": db.value}
+
+    def time_steps(self, nsteps):
+        tot, pair, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _check(self.lib.dpd_time_steps(self.h, int(nsteps), ctypes.byref(tot), ctypes.byref(pair),
+                                       ctypes.byref(nl)), self.lib, self.h)
+        return {"total_ms": tot.value, "pair_ms": pair.value, "pair_launches": nl.value}
+
+    def write_data(self, path):
+        _check(self.lib.dpd_write_data(self.h, path.encode()), self.lib, self.h)
+
+    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0):
+        t = capi.dpd_tuning()
+        t.pair_block, t.pair_variant, t.cell_order = pair_block, pair_variant, cell_order
+        _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
+
+
+class Batch:
+    """Many independent systems advanced together in one packed engine."""
+
+    def __init__(self, run_ins, systems, tuning=None):
+        self.lib = capi.load()
+        self.h = ctypes.c_void_p()
+        n = len(run_ins)
+        texts = (ctypes.c_char_p * n)(*[t.encode() for t in run_ins])
+        structs = (capi.dpd_system * n)()
+        self._keep = [texts]
+        self.n_atoms = []
+        for r, (s, keep) in enumerate(systems):
+            structs[r] = s
+            self._keep.append(keep)
+            self.n_atoms.append(s.n_atoms)
+        self._keep.append(structs)
+        tune = None
+        if tuning is not None:
+            tune = capi.dpd_tuning()
+            for k, v in tuning.items():
+                setattr(tune, k, v)
+            tune = ctypes.byref(tune)
+        code = self.lib.dpd_batch_create(n, texts, structs, tune, ctypes.byref(self.h))
+        _check(code, self.lib, None)
+        self.n = n
+
+    def close(self):
+        if self.h:
+            self.lib.dpd_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, nsteps):
+        _check(self.lib.dpd_run(self.h, int(nsteps)), self.lib, self.h)
+
+    def thermo(self, rep, max_rows=4096):
+        rows = (capi.dpd_thermo * max_rows)()
+        n = ctypes.c_int()
+        _check(self.lib.dpd_batch_get_thermo(self.h, rep, rows, max_rows, ctypes.byref(n)), self.lib, self.h)
+        return _rows_to_dict(rows, n.value)
+
+    def state(self, rep):
+        n = self.n_atoms[rep]
+        x, v, f = np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
+        img = np.empty((n, 3), dtype=np.int32)
+        _check(self.lib.dpd_batch_get_state(self.h, rep, capi.ptr(x), capi.ptr(v), capi.ptr(img), capi.ptr(f)),
+               self.lib, self.h)
+        return {"x": x, "v": v, "image": img, "f": f}
+
+    def rdf(self, rep, nbins):
+        g = np.empty(nbins)
+        ns = ctypes.c_int64()
+        _check(self.lib.dpd_batch_rdf_result(self.h, rep, capi.ptr(g), ctypes.byref(ns)), self.lib, self.h)
+        return g, ns.value
+
+    def time_steps(self, nsteps):
+        tot, pair, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        _check(self.lib.dpd_time_steps(self.h, int(nsteps), ctypes.byref(tot), ctypes.byref(pair),
+                                       ctypes.byref(nl)), self.lib, self.h)
+        return {"total_ms": tot.value, "pair_ms": pair.value, "pair_launches": nl.value}

@@ -1,0 +1,224 @@
+/*
+ * dpd_b200.h -- C ABI of libdpd_b200.so, a B200-native DPD timestep engine.
+ *
+ * The reference (xxin125/gpumdpd, "GPUDPD") is a monolithic CUDA executable whose
+ * plugin boundary is a set of C++ classes registered at static-init time
+ * (Pair, Bond, Fix, Compute; src/force/pair.cuh:8-15, src/force/bond.cuh:8-15,
+ * src/fix/fix.cuh:7-26, src/compute/compute.cuh:7-22) sharing a `System&` of raw
+ * device pointers, driven by src/main/utils.cuh:166-314.  It has no FFI of its own,
+ * so every entry point below names the reference interface whose job it takes over.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 on success, a negative DPD_E_* code on
+ *    failure (the reference calls exit(1) instead: src/main/common.cuh:46-60,175-200).
+ *    dpd_last_error() gives the message of the most recent failure on that handle
+ *    (or of a failed create when the handle is NULL).
+ *  - A dpd_engine owns all of its device memory and its CUDA stream; one engine is
+ *    used from one host thread at a time.  Nothing here exits the process.
+ *  - Particles are identified by their 1-based tag (the data file's atom id); arrays
+ *    returned "by tag" have tag-1 as their row index.  Types are 1-based.
+ *  - Host arrays are plain C arrays; no torch or CUDA types cross the boundary.
+ */
+#ifndef DPD_B200_H
+#define DPD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPD_OK 0
+#define DPD_E_ARG -1       /* invalid argument or command (run.in grammar error) */
+#define DPD_E_IO -2        /* file cannot be read or written                       */
+#define DPD_E_CUDA -3      /* a CUDA call failed                                    */
+#define DPD_E_NOMEM -4     /* device memory could not be allocated / over budget    */
+#define DPD_E_OVERFLOW -5  /* neighbour list or cell capacity exceeded (max_rho)    */
+#define DPD_E_STATE -6     /* call not valid in the engine's current state          */
+#define DPD_E_NUMERIC -7   /* non-finite position/velocity, or a FENE bond broke    */
+#define DPD_E_NODEV -8     /* no CUDA device: there is no CPU fallback               */
+
+typedef struct dpd_engine dpd_engine;
+
+/* One system given as arrays instead of a data file (same content as the data file
+ * read by src/system/read_data.cu:201-343).  x and v are double[3*n_atoms] rows in
+ * `tag` order of the arrays given (any order; tags must be 1..n_atoms).  v may be
+ * NULL (zero velocities, as a data file without a Velocities section).            */
+typedef struct dpd_system {
+    int n_atoms;
+    int n_atomtypes;
+    int n_bonds;       /* 0 for atom_style atomic */
+    int n_bondtypes;
+    double lo[3];
+    double hi[3];
+    const double* masses; /* [n_atomtypes] */
+    const int* tag;       /* [n_atoms], 1-based, a permutation of 1..n_atoms */
+    const int* type;      /* [n_atoms], 1-based */
+    const int* mol;       /* [n_atoms] or NULL */
+    const double* x;      /* [3*n_atoms] */
+    const double* v;      /* [3*n_atoms] or NULL */
+    const int* bonds;     /* [3*n_bonds]: type, tag_i, tag_j */
+} dpd_system;
+
+/* Thermo row, the columns of thermo.txt (src/compute/thermo.cu:39-62,122-214) in
+ * FP64, plus total momentum and kinetic energy. */
+typedef struct dpd_thermo {
+    int64_t step;
+    double temp;
+    double pair_pe;
+    double bond_pe;
+    double pressure;
+    double p[6];        /* pxx pxy pxz pyy pyz pzz */
+    double ke;
+    double momentum[3];
+} dpd_thermo;
+
+/* Launch/tuning knobs chosen by the autotuner (gpumdpd_b200/tune.py); zero fields
+ * mean "engine default". */
+typedef struct dpd_tuning {
+    int pair_block;        /* threads per block of the pair kernel               */
+    int pair_variant;      /* 0 = thread per particle, 1 = warp pair-queue         */
+    int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
+    int reserved[5];
+} dpd_tuning;
+
+/* ---- plain engine: replaces main()/read_info/preprocess/zero_step/simulation
+ *      (src/main/main.cu:15-72, src/main/utils.cuh:117-314) ---------------------- */
+
+/* Create an engine from the text of a run.in file (the reference's command grammar,
+ * src/main/read_in.cu:40-290 plus each plugin's isEnabled/validateParams) and either
+ * the data file it names (data_path == NULL: use the read_data line, resolved
+ * relative to base_dir when base_dir is not NULL) or an explicit data_path. */
+int dpd_create(const char* run_in_text, const char* data_path, const char* base_dir,
+               dpd_engine** out);
+
+/* Same, with the system given as arrays (the read_data line is then ignored). */
+int dpd_create_from_system(const char* run_in_text, const dpd_system* sys, dpd_engine** out);
+
+/* Advance nsteps timesteps (the first call also performs the reference's zero step:
+ * neighbour build, force evaluation and thermo at step 0).  Asynchronous on the
+ * engine's stream except for error checking at the end. */
+int dpd_run(dpd_engine* eng, uint32_t nsteps);
+
+/* Wait for outstanding work and report any device-side error status. */
+int dpd_sync(dpd_engine* eng);
+
+/* Thermo rows logged so far (every `thermo` steps, as src/compute/thermo.cu:96-220).
+ * Copies up to max_rows of the most recent rows; *n_rows receives the number copied. */
+int dpd_get_thermo(dpd_engine* eng, dpd_thermo* rows, int max_rows, int* n_rows);
+
+/* Current state by tag: x wrapped into the box, v, image counters, forces of the
+ * last evaluated step (any pointer may be NULL). Replaces Dump/write_data reads of
+ * d_pos/d_vel/d_force (src/system/dump.cu:23-201). */
+int dpd_get_state(dpd_engine* eng, double* x, double* v, int* image, double* f);
+
+/* Overwrite positions/velocities by tag (x wrapped into the box on load). */
+int dpd_set_state(dpd_engine* eng, const double* x, const double* v);
+
+/* Local density of the last mDPD evaluation by tag (src/force/pair_mdpd.cu:219-300). */
+int dpd_get_density(dpd_engine* eng, double* rho);
+
+/* Engine's internal FP32 representation by tag: cell coordinates (3 ints) and
+ * offsets within the cell (3 floats); plus the grid (nc[3], w[3]).  For parity
+ * tests of the neighbour predicate. */
+int dpd_get_cells(dpd_engine* eng, int* cell, float* offset, int* nc, float* w, float* cut2);
+
+/* Current half neighbour list as unordered tag pairs (lo, hi), at most cap pairs;
+ * *n_pairs receives the total (Neigh_list::build, src/force/neigh_list.cu:397-479). */
+int dpd_get_neighbors(dpd_engine* eng, int* pairs, int64_t cap, int64_t* n_pairs);
+
+/* Radial distribution function g(r) between types ta and tb, nbins bins on [0,rmax),
+ * evaluated on the current state (new: the reference has no RDF). */
+int dpd_compute_rdf(dpd_engine* eng, int ta, int tb, double rmax, int nbins, double* g);
+
+/* Accumulated RDF over sampling steps configured with dpd_rdf_config. */
+int dpd_rdf_config(dpd_engine* eng, int ta, int tb, double rmax, int nbins, int every);
+int dpd_rdf_result(dpd_engine* eng, double* g, int64_t* nsamples);
+
+/* Counters: steps done, neighbour-list builds, particles, bytes of device memory. */
+int dpd_get_info(dpd_engine* eng, int64_t* step, int64_t* n_builds, int64_t* n_atoms,
+                 int64_t* device_bytes);
+
+/* Apply tuning knobs (takes effect at the next run). */
+int dpd_set_tuning(dpd_engine* eng, const dpd_tuning* t);
+
+/* Write a data file in the reference's write_data format (src/system/read_data.cu:473-637). */
+int dpd_write_data(dpd_engine* eng, const char* path);
+
+/* Time `nsteps` steps on the device with CUDA events: total milliseconds of the
+ * timed region and of the pair kernel alone (sum over launches). */
+int dpd_time_steps(dpd_engine* eng, uint32_t nsteps, double* total_ms, double* pair_ms,
+                   int64_t* pair_launches);
+
+const char* dpd_last_error(dpd_engine* eng);
+int dpd_destroy(dpd_engine* eng);
+
+/* ---- in-loop drop-in for Pair::compute_force on the reference's own buffers ---
+ * Computes the pair force of the enabled style into the reference's AoS device
+ * arrays, from its AoS positions/velocities (d_pos/d_vel numtyp[3N] with numtyp =
+ * float, d_id/d_type int[N]); same memset-then-accumulate contract as
+ * Pair_dpd::compute_force (src/force/pair_dpd.cu:564-633) and Pair_mdpd's
+ * (src/force/pair_mdpd.cu:689-779): d_force is overwritten; when d_pe/d_virial are
+ * not NULL they are overwritten with per-atom PE and the 6-component per-atom virial
+ * ((1/2) r (x) F per pair to each atom).  The engine keeps its own cell list and
+ * rebuilds it when any particle moved more than skin/2 since the last build.  All
+ * pointers are device pointers; runs on the engine's stream and synchronises.   */
+int dpd_pair_compute_aos(dpd_engine* eng, const float* d_pos, const float* d_vel,
+                         const int* d_id, const int* d_type, int n, uint32_t step,
+                         float* d_force, float* d_pe, float* d_virial);
+
+/* ---- batched replicas (one engine, many independent systems) --------------------
+ * Replicas are packed into one offset-indexed particle array and advanced together
+ * by the same kernels, one launch per stage; the timestep is captured in a CUDA
+ * graph.  run_in_texts[r] / systems[r] describe replica r as for the plain engine. */
+int dpd_batch_create(int n_rep, const char* const* run_in_texts, const dpd_system* systems,
+                     const dpd_tuning* tune, dpd_engine** out);
+int dpd_batch_n(dpd_engine* eng, int* n_rep);
+int dpd_batch_get_thermo(dpd_engine* eng, int rep, dpd_thermo* rows, int max_rows,
+                         int* n_rows);
+int dpd_batch_get_state(dpd_engine* eng, int rep, double* x, double* v, int* image,
+                        double* f);
+int dpd_batch_rdf_result(dpd_engine* eng, int rep, double* g, int64_t* nsamples);
+
+/* ---- serving: continuous batching of DPD jobs -----------------------------------
+ * A server owns a device-memory budget.  Jobs are submitted at any time; at each
+ * scheduling point (every `chunk` steps) finished jobs are retired, their memory is
+ * released, and queued jobs are admitted while they fit the budget; all admitted
+ * jobs advance together in one packed batch.  Each job keeps its own tags, seed and
+ * step counter, so its trajectory does not depend on which other jobs share the
+ * batch. */
+typedef struct dpd_server dpd_server;
+
+typedef struct dpd_job_result {
+    int64_t job_id;
+    int status;            /* 0 done, >0 still queued/running, <0 error code      */
+    int64_t steps;
+    double mean_temp;      /* mean over logged rows after the first               */
+    double mean_pressure;
+    double submit_s, start_s, finish_s; /* host clock seconds since server creation */
+    dpd_thermo last;
+} dpd_job_result;
+
+int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning* tune,
+                      dpd_server** out);
+/* Submit a job (copies the inputs); *job_id receives its id. */
+int dpd_server_submit(dpd_server* srv, const char* run_in_text, const dpd_system* sys,
+                      int64_t* job_id);
+/* Advance the server by one scheduling chunk (admit, step, retire).  *n_active and
+ * *n_queued receive the counts after the chunk. */
+int dpd_server_step(dpd_server* srv, int* n_active, int* n_queued);
+int dpd_server_result(dpd_server* srv, int64_t job_id, dpd_job_result* res);
+int dpd_server_job_state(dpd_server* srv, int64_t job_id, double* x, double* v);
+int dpd_server_job_rdf(dpd_server* srv, int64_t job_id, double* g, int64_t* nsamples);
+int dpd_server_stats(dpd_server* srv, int64_t* particle_steps, double* busy_s,
+                     int64_t* device_bytes);
+const char* dpd_server_last_error(dpd_server* srv);
+int dpd_server_destroy(dpd_server* srv);
+
+/* Library version string. */
+const char* dpd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DPD_B200_H */

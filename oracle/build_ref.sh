@@ -1,0 +1,49 @@
+#!/usr/bin/env bash
+# Build the reference GPUDPD executable (xxin125/gpumdpd) from its own sources, untouched,
+# into oracle/_ref/.  This is test and baseline infrastructure only: the binary is the
+# reference's own CUDA build, used to generate golden fixtures on a GPU host and as the
+# "reference" arm of bench.py.  Nothing in the product links or calls it.
+#
+# The stock Makefile targets sm_60 and fails on CUDA 12.9 because two sources use
+# thrust::max_element/min_element without including <thrust/extrema.h>; the header is
+# force-included on the command line instead of editing any source.
+#
+# Usage: oracle/build_ref.sh [SINGLE|DOUBLE]   (default SINGLE, the reference's default)
+set -euo pipefail
+PREC="${1:-SINGLE}"
+REF_SRC="${REF_SRC:-/root/reference/src}"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+OBJ="$OUT/obj_${PREC}"
+if [ ! -d "$REF_SRC" ]; then
+    echo "reference sources not found at $REF_SRC" >&2
+    exit 1
+fi
+mkdir -p "$OBJ"
+FLAGS=(-O3 -std=c++14 -gencode arch=compute_100a,code=sm_100a -I"$REF_SRC" "-D$PREC" -include thrust/extrema.h)
+objs=()
+pids=()
+for src in "$REF_SRC"/*/*.cu; do
+    rel="${src#$REF_SRC/}"
+    o="$OBJ/${rel//\//_}.o"
+    objs+=("$o")
+    if [ ! -f "$o" ] || [ "$src" -nt "$o" ]; then
+        nvcc "${FLAGS[@]}" -dc "$src" -o "$o" &
+        pids+=($!)
+        # keep at most 8 compilers in flight
+        if [ "${#pids[@]}" -ge 8 ]; then
+            for p in "${pids[@]}"; do wait "$p"; done
+            pids=()
+        fi
+    fi
+done
+for p in "${pids[@]}"; do wait "$p"; done
+lower="$(echo "$PREC" | tr 'A-Z' 'a-z')"
+nvcc "${FLAGS[@]}" "${objs[@]}" -o "$OUT/gpudpd_${lower}"
+echo "built $OUT/gpudpd_${lower}"
+if [ "$PREC" = "SINGLE" ]; then
+    # Saru known-answer harness: the reference's pair_dpd.cu compiled inside
+    # oracle/ref_saru_harness.cu, linked with the reference's pair registry object.
+    nvcc "${FLAGS[@]}" -rdc=true "$HERE/ref_saru_harness.cu" "$OBJ/force_pair.cu.o" -o "$OUT/ref_saru"
+    echo "built $OUT/ref_saru"
+fi

@@ -1,0 +1,712 @@
+/*
+ * dpd_oracle.c -- FP64 single-threaded CPU restatement of the GPUDPD timestep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine in
+ * gpumdpd_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * reference legs of bench.py load it.  The product never links or calls it.
+ *
+ * Every function states the reference lines (xxin125/gpumdpd, paths relative to
+ * the project root) whose arithmetic it restates.  State is double precision
+ * throughout except two places that deliberately reproduce single precision:
+ *   - oracle_saru(): the integer mixing is bit-exact uint32 and the float tail
+ *     is evaluated in float exactly as src/force/pair_dpd.cu:233-235 does, so the
+ *     random numbers are identical to the reference's and to the CUDA engine's;
+ *   - oracle_pairs_f32(): the neighbour predicate evaluated in the engine's own
+ *     FP32 cell-offset representation with a fixed operation order, which is the
+ *     definition of the "bit-exact" neighbour set the engine is tested against.
+ * Compile with -ffp-contract=off so that no FMA is formed implicitly.
+ *
+ * Parity is pinned by golden vectors produced by the reference's own CUDA build
+ * (oracle/build_ref.sh + tests/golden/gen_ref_fixtures.py), see tests/test_oracle.py.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+#define ORACLE_MAXT 32
+#define M_PI 3.14159265358979323846 /* src/force/pair_mdpd.cu:3 */
+
+/* ------------------------------------------------------------------------- */
+/* Saru counter-based RNG: src/force/pair_dpd.cu:203-236 (same constants; the
+ * stream must be identical, so the steps are kept as published).              */
+
+float oracle_saru(uint32_t seed1, uint32_t seed2, uint32_t seed, int32_t timestep)
+{
+    uint32_t seed3 = seed + (uint32_t)timestep;
+    seed3 ^= (seed1 << 7) ^ (seed2 >> 6);
+    seed2 += (seed1 >> 4) ^ (seed3 >> 15);
+    seed1 ^= (seed2 << 9) + (seed3 << 8);
+    seed3 ^= 0xA5366B4Du * ((seed2 >> 11) ^ (seed1 << 1));
+    seed2 += 0x72BE1579u * ((seed1 << 4) ^ (seed3 >> 16));
+    seed1 ^= 0x3F38A6EDu * ((seed3 >> 5) ^ (uint32_t)(((int32_t)seed2) >> 22));
+    seed2 += seed1 * seed3;
+    seed1 += seed3 ^ (seed2 >> 2);
+    seed2 ^= (uint32_t)(((int32_t)seed2) >> 17);
+    uint32_t state = 0x79dedea3u * (seed1 ^ (uint32_t)(((int32_t)seed1) >> 14));
+    uint32_t wstate = (state + seed2) ^ (uint32_t)(((int32_t)state) >> 8);
+    state = state + (wstate * (wstate ^ 0xdddf97f5u));
+    wstate = 0xABCB96F7u + (wstate >> 1);
+    uint32_t sum = 0;
+    for (int r = 0; r < 8; r++) {
+        sum += 0x9e3779b9u;
+        state += ((wstate << 4) + 0xA341316Cu) ^ (wstate + sum) ^ ((wstate >> 5) + 0xC8013EA4u);
+        wstate += ((state << 4) + 0xAD90777Du) ^ (state + sum) ^ ((state >> 5) + 0x7E95761Eu);
+    }
+    uint32_t v = (state ^ (state >> 26)) + wstate;
+    uint32_t s = (v ^ (v >> 20)) * 0x6957f5a7u;
+    /* float tail, one rounding per operation as in the reference's -DSINGLE build:
+       (float)s * 2^-32 * 2 is exact scaling, then -1 rounds, then *sqrt(3)f rounds */
+    volatile float a = (float)s;
+    volatile float u = a * 4.6566128730773926e-10f - 1.0f; /* 2^-31 */
+    volatile float th = 1.7320508075688772f * u;
+    return th;
+}
+
+void oracle_saru_batch(int n, const uint32_t* t1, const uint32_t* t2, uint32_t seed,
+                       const int32_t* step, float* out)
+{
+    for (int k = 0; k < n; k++) out[k] = oracle_saru(t1[k], t2[k], seed, step[k]);
+}
+
+/* ------------------------------------------------------------------------- */
+/* minimum image: src/force/neigh_list.cu:377-379 (d -= L*((d>=L/2)-(d<-L/2)))  */
+
+static inline double min_image(double d, double L)
+{
+    double h = 0.5 * L;
+    return d - L * (double)((d >= h) - (d < -h));
+}
+
+/* triangular type-pair index: src/force/pair_dpd.cu:134 (0-based result) */
+static inline int tri_index(int ti, int tj, int nt)
+{
+    int a = ti < tj ? ti : tj, b = ti < tj ? tj : ti;
+    return ((a - 1) * nt - (a - 1) * (a - 2) / 2 + b - a + 1) - 1;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Half pair enumeration over a cell grid (cells >= cutoff, >= 3 per dim) or
+ * all pairs when the box is too small.  The callback receives every unordered
+ * pair {i,j} whose minimum-image distance squared is <= cut2.                 */
+
+typedef void (*pair_cb)(int i, int j, double dx, double dy, double dz, double r2, void* ctx);
+
+static void for_each_pair(int n, const double* x, const double* lo, const double* L,
+                          double cut, pair_cb cb, void* ctx)
+{
+    double cut2 = cut * cut;
+    int nc[3];
+    for (int d = 0; d < 3; d++) nc[d] = (int)floor(L[d] / cut);
+    if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) {
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) {
+                double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+                double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+                double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+                double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 <= cut2) cb(i, j, dx, dy, dz, r2, ctx);
+            }
+        return;
+    }
+    long ncell = (long)nc[0] * nc[1] * nc[2];
+    int* head = (int*)malloc(sizeof(int) * ncell);
+    int* next = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
+    int* cidx = (int*)malloc(sizeof(int) * 3 * (n > 0 ? n : 1));
+    for (long c = 0; c < ncell; c++) head[c] = -1;
+    for (int i = n - 1; i >= 0; i--) {
+        int c3[3];
+        for (int d = 0; d < 3; d++) {
+            int k = (int)floor((x[3 * i + d] - lo[d]) / (L[d] / nc[d]));
+            if (k < 0) k = 0;
+            if (k >= nc[d]) k = nc[d] - 1;
+            c3[d] = k;
+            cidx[3 * i + d] = k;
+        }
+        long c = ((long)c3[0] * nc[1] + c3[1]) * nc[2] + c3[2];
+        next[i] = head[c];
+        head[c] = i;
+    }
+    for (int i = 0; i < n; i++) {
+        for (int ox = -1; ox <= 1; ox++)
+            for (int oy = -1; oy <= 1; oy++)
+                for (int oz = -1; oz <= 1; oz++) {
+                    int cx = (cidx[3 * i] + ox + nc[0]) % nc[0];
+                    int cy = (cidx[3 * i + 1] + oy + nc[1]) % nc[1];
+                    int cz = (cidx[3 * i + 2] + oz + nc[2]) % nc[2];
+                    long c = ((long)cx * nc[1] + cy) * nc[2] + cz;
+                    for (int j = head[c]; j >= 0; j = next[j]) {
+                        if (j <= i) continue;
+                        double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+                        double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+                        double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+                        double r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 <= cut2) cb(i, j, dx, dy, dz, r2, ctx);
+                    }
+                }
+    }
+    free(head);
+    free(next);
+    free(cidx);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Neighbour pairs (tag pairs, tag_lo < tag_hi) within `cut`, FP64 predicate.  */
+
+typedef struct {
+    const int* tag;
+    int* out;
+    long cap, cnt;
+} pairs_ctx;
+
+static void pairs_collect(int i, int j, double dx, double dy, double dz, double r2, void* c)
+{
+    (void)dx; (void)dy; (void)dz; (void)r2;
+    pairs_ctx* p = (pairs_ctx*)c;
+    if (p->cnt < p->cap) {
+        int a = p->tag[i], b = p->tag[j];
+        p->out[2 * p->cnt] = a < b ? a : b;
+        p->out[2 * p->cnt + 1] = a < b ? b : a;
+    }
+    p->cnt++;
+}
+
+long oracle_pairs_f64(int n, const int* tag, const double* x, const double* lo, const double* L,
+                      double cut, int* out, long cap)
+{
+    pairs_ctx p = {tag, out, cap, 0};
+    for_each_pair(n, x, lo, L, cut, pairs_collect, &p);
+    return p.cnt;
+}
+
+/* The engine's neighbour predicate in its own FP32 representation: particle i is
+ * in cell (cx,cy,cz) of an nc-grid of widths w (float) at float offset o within
+ * the cell.  Displacement d = dc*w + (o_i - o_j) with dc the cell difference
+ * wrapped to the nearest image; r2 = fma(dz,dz,fma(dy,dy,dx*dx)); kept when
+ * r2 <= cut2 (float).  Same predicate as the engine's list builder; it restates
+ * the reference's r2 <= (global_cut+skin)^2 test (src/force/neigh_list.cu:373-382)
+ * on the cell-offset representation.  Returns unordered tag pairs.            */
+long oracle_pairs_f32(int n, const int* tag, const int* cell /*3n*/, const float* off /*3n*/,
+                      const int* nc, const float* w, float cut2, int* out, long cap)
+{
+    long cnt = 0;
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++) {
+            float d[3];
+            int near = 1;
+            for (int k = 0; k < 3; k++) {
+                int dc = cell[3 * i + k] - cell[3 * j + k];
+                if (dc > nc[k] / 2) dc -= nc[k];
+                if (dc < -(nc[k] / 2)) dc += nc[k];
+                if (dc > 1 || dc < -1) { near = 0; break; }
+                volatile float diff = off[3 * i + k] - off[3 * j + k];
+                d[k] = fmaf((float)dc, w[k], diff);
+            }
+            if (!near) continue;
+            volatile float r2 = d[0] * d[0];
+            r2 = fmaf(d[1], d[1], r2);
+            r2 = fmaf(d[2], d[2], r2);
+            if (r2 <= cut2) {
+                if (cnt < cap) {
+                    int a = tag[i], b = tag[j];
+                    out[2 * cnt] = a < b ? a : b;
+                    out[2 * cnt + 1] = a < b ? b : a;
+                }
+                cnt++;
+            }
+        }
+    return cnt;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Force field description passed from Python.                               */
+
+typedef struct {
+    int style;           /* 0 = dpd (src/force/pair_dpd.cu), 1 = mdpd (src/force/pair_mdpd.cu) */
+    int ntypes;
+    double kT;           /* pair_style temp */
+    double dt;
+    uint32_t seed;
+    double coeff[ORACLE_MAXT * ORACLE_MAXT][5]; /* [type pair (triangular)] A, B, gamma, rc, rd */
+    double mass[ORACLE_MAXT];
+    int bond_style;      /* 0 none, 1 harmonic (src/force/bond_harmonic.cu), 2 fene (new) */
+    int nbondtypes;
+    double bond_coeff[ORACLE_MAXT][4]; /* harmonic: k, r0 ; fene: K, R0, eps, sigma */
+} oracle_ff;
+
+typedef struct {
+    const oracle_ff* ff;
+    const int* tag;
+    const int* type;
+    const double* v;
+    const double* rho;
+    uint32_t step;
+    double* f;
+    double* rho_out;
+    double pe;
+    double vir[6];
+    double sig_scale; /* sqrt(2 kT) / sqrt(dt), src/force/pair_dpd.cu:577-578 */
+} force_ctx;
+
+/* mDPD local density: src/force/pair_mdpd.cu:253-297.  rho_i = sum over j != i of
+ * 15/(2 pi rd^3) (1 - r/rd)^2 for r < rd, no self term.                        */
+static void density_cb(int i, int j, double dx, double dy, double dz, double r2, void* c)
+{
+    (void)dx; (void)dy; (void)dz;
+    force_ctx* k = (force_ctx*)c;
+    int idx = tri_index(k->type[i], k->type[j], k->ff->ntypes);
+    double rd = k->ff->coeff[idx][4];
+    double r = sqrt(r2);
+    double wd = 1.0 - r / rd;
+    if (wd < 0.0) wd = 0.0;
+    double factor = 15.0 / 2.0 / M_PI / (rd * rd * rd);
+    double add = factor * wd * wd;
+    k->rho_out[i] += add;
+    k->rho_out[j] += add;
+}
+
+/* DPD pair force: src/force/pair_dpd.cu:292-403 (log variant: PE 0.5*A*rc*wc^2
+ * per pair, virial r (x) F per pair).  mDPD: src/force/pair_mdpd.cu:399-521.   */
+static void force_cb(int i, int j, double dx, double dy, double dz, double r2, void* c)
+{
+    force_ctx* k = (force_ctx*)c;
+    const oracle_ff* ff = k->ff;
+    int idx = tri_index(k->type[i], k->type[j], ff->ntypes);
+    double A = ff->coeff[idx][0], B = ff->coeff[idx][1], gamma = ff->coeff[idx][2];
+    double rc = ff->coeff[idx][3], rd = ff->coeff[idx][4];
+    if (!(r2 <= rc * rc)) return;
+    double r = sqrt(r2);
+    if (r < 1.0e-10) return;
+    double rinv = 1.0 / r;
+    double dvx = k->v[3 * i] - k->v[3 * j];
+    double dvy = k->v[3 * i + 1] - k->v[3 * j + 1];
+    double dvz = k->v[3 * i + 2] - k->v[3 * j + 2];
+    double dot = dx * dvx + dy * dvy + dz * dvz;
+    double wc = 1.0 - r / rc;
+    double wr = wc;
+    int a = k->tag[i], b = k->tag[j];
+    uint32_t t1 = (uint32_t)(a < b ? a : b), t2 = (uint32_t)(a < b ? b : a);
+    double theta = (double)oracle_saru(t1, t2, ff->seed, (int32_t)k->step);
+    double sigma = sqrt(gamma) * k->sig_scale;
+    double fpair;
+    double pe;
+    if (ff->style == 0) {
+        fpair = A * wc - gamma * wr * wr * dot * rinv + sigma * wr * theta;
+        pe = 0.5 * A * rc * wc * wc;
+    } else {
+        double wd = 1.0 - r / rd;
+        if (wd < 0.0) wd = 0.0;
+        double rhoi = k->rho[i], rhoj = k->rho[j];
+        fpair = A * wc + B * (rhoi + rhoj) * wd - gamma * wr * wr * dot * rinv + sigma * wr * theta;
+        pe = 0.5 * A * rc * wc * wc + 0.25 * B * rd * (rhoi + rhoj) * wd * wd;
+    }
+    fpair *= rinv;
+    double fx = dx * fpair, fy = dy * fpair, fz = dz * fpair;
+    k->f[3 * i] += fx;
+    k->f[3 * i + 1] += fy;
+    k->f[3 * i + 2] += fz;
+    k->f[3 * j] -= fx;
+    k->f[3 * j + 1] -= fy;
+    k->f[3 * j + 2] -= fz;
+    k->pe += pe;
+    k->vir[0] += dx * fx;
+    k->vir[1] += dx * fy;
+    k->vir[2] += dx * fz;
+    k->vir[3] += dy * fy;
+    k->vir[4] += dy * fz;
+    k->vir[5] += dz * fz;
+}
+
+static double max_rc(const oracle_ff* ff)
+{
+    double m = 0.0;
+    int np = ff->ntypes * (ff->ntypes + 1) / 2;
+    for (int p = 0; p < np; p++)
+        if (ff->coeff[p][3] > m) m = ff->coeff[p][3];
+    return m;
+}
+
+/* Bonds.  Harmonic: src/force/bond_harmonic.cu:208-268: E = k (r-r0)^2,
+ * F_i = -2 k (r-r0)/r * d, d = x_i - x_j, virial d (x) F_i.
+ * FENE (not in the reference): E = -0.5 K R0^2 ln(1-(r/R0)^2) plus the WCA
+ * repulsion 4 eps[(s/r)^12-(s/r)^6]+eps for r < 2^(1/6) s.                    */
+static int bond_forces(int n, const int* tag_to_idx, int ntag, const double* x, const double* lo,
+                       const double* L, const oracle_ff* ff, int nbonds, const int* bonds,
+                       double* f, double* pe_out, double* vir)
+{
+    (void)n; (void)lo;
+    int status = 0;
+    for (int b = 0; b < nbonds; b++) {
+        int bt = bonds[3 * b], ta = bonds[3 * b + 1], tb = bonds[3 * b + 2];
+        if (ta < 1 || ta > ntag || tb < 1 || tb > ntag) { status = -1; continue; }
+        int i = tag_to_idx[ta - 1], j = tag_to_idx[tb - 1];
+        double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+        double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+        double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+        double r2 = dx * dx + dy * dy + dz * dz;
+        double r = sqrt(r2);
+        double fbond = 0.0, e = 0.0;
+        const double* bc = ff->bond_coeff[bt - 1];
+        if (ff->bond_style == 1) {
+            fbond = r > 0.0 ? -2.0 * bc[0] * (r - bc[1]) / r : 0.0;
+            e = bc[0] * (r - bc[1]) * (r - bc[1]);
+        } else if (ff->bond_style == 2) {
+            double K = bc[0], R0 = bc[1], eps = bc[2], sg = bc[3];
+            double rr = r2 / (R0 * R0);
+            if (rr >= 1.0) { status = -2; rr = 0.999; }
+            fbond = -K / (1.0 - rr);
+            e = -0.5 * K * R0 * R0 * log(1.0 - rr);
+            if (eps > 0.0 && r2 < pow(2.0, 1.0 / 3.0) * sg * sg) {
+                double sr2 = sg * sg / r2, sr6 = sr2 * sr2 * sr2;
+                fbond += 48.0 * eps * sr6 * (sr6 - 0.5) / r2;
+                e += 4.0 * eps * sr6 * (sr6 - 1.0) + eps;
+            }
+        }
+        double fx = dx * fbond, fy = dy * fbond, fz = dz * fbond;
+        f[3 * i] += fx; f[3 * i + 1] += fy; f[3 * i + 2] += fz;
+        f[3 * j] -= fx; f[3 * j + 1] -= fy; f[3 * j + 2] -= fz;
+        *pe_out += e;
+        vir[0] += dx * fx; vir[1] += dx * fy; vir[2] += dx * fz;
+        vir[3] += dy * fy; vir[4] += dy * fz; vir[5] += dz * fz;
+    }
+    return status;
+}
+
+/* Forces at one state.  out: f[3n], rho[n] (mdpd, may be NULL), energy[2] = pair,
+ * bond; virial[6] = xx xy xz yy yz zz (pair + bond).                            */
+int oracle_forces(int n, const int* tag, const int* type, const double* x, const double* v,
+                  const double* lo, const double* L, const oracle_ff* ff, uint32_t step,
+                  int nbonds, const int* bonds, double* f, double* rho, double* energy,
+                  double* virial)
+{
+    memset(f, 0, sizeof(double) * 3 * n);
+    double* rho_buf = rho ? rho : (double*)calloc(n > 0 ? n : 1, sizeof(double));
+    force_ctx k;
+    memset(&k, 0, sizeof(k));
+    k.ff = ff; k.tag = tag; k.type = type; k.v = v; k.step = step; k.f = f;
+    k.sig_scale = sqrt(2.0 * ff->kT) / sqrt(ff->dt);
+    double cut = max_rc(ff);
+    if (ff->style == 1) {
+        memset(rho_buf, 0, sizeof(double) * n);
+        k.rho_out = rho_buf;
+        for_each_pair(n, x, lo, L, cut, density_cb, &k);
+    }
+    k.rho = rho_buf;
+    for_each_pair(n, x, lo, L, cut, force_cb, &k);
+    double bpe = 0.0, bvir[6] = {0, 0, 0, 0, 0, 0};
+    int status = 0;
+    if (ff->bond_style != 0 && nbonds > 0) {
+        int ntag = 0;
+        for (int i = 0; i < n; i++) if (tag[i] > ntag) ntag = tag[i];
+        int* t2i = (int*)malloc(sizeof(int) * (ntag > 0 ? ntag : 1));
+        for (int t = 0; t < ntag; t++) t2i[t] = -1;
+        for (int i = 0; i < n; i++) t2i[tag[i] - 1] = i;
+        status = bond_forces(n, t2i, ntag, x, lo, L, ff, nbonds, bonds, f, &bpe, bvir);
+        free(t2i);
+    }
+    if (energy) { energy[0] = k.pe; energy[1] = bpe; }
+    if (virial) for (int c = 0; c < 6; c++) virial[c] = k.vir[c] + bvir[c];
+    if (!rho) free(rho_buf);
+    return status;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Thermo: src/compute/thermo.cu:240-246 (KE), 301-303 (T = 2KE/(3N-3)),
+ * 422-434 + 506-517 (P_ab = (sum m v_a v_b + W_ab)/V, P = trace/3).
+ * out[12]: T, pair_pe, bond_pe, P, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz, KE, spare     */
+static void thermo(int n, const int* type, const double* v, const double* L, const oracle_ff* ff,
+                   const double* energy, const double* virial, double* out)
+{
+    double ke = 0.0, kin[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < n; i++) {
+        double m = ff->mass[type[i] - 1];
+        const double* vi = v + 3 * i;
+        ke += 0.5 * m * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
+        kin[0] += m * vi[0] * vi[0]; kin[1] += m * vi[0] * vi[1]; kin[2] += m * vi[0] * vi[2];
+        kin[3] += m * vi[1] * vi[1]; kin[4] += m * vi[1] * vi[2]; kin[5] += m * vi[2] * vi[2];
+    }
+    double vol = L[0] * L[1] * L[2];
+    out[0] = 2.0 * ke / (3.0 * n - 3.0);
+    out[1] = energy[0];
+    out[2] = energy[1];
+    for (int c = 0; c < 6; c++) out[4 + c] = (kin[c] + virial[c]) / vol;
+    out[3] = (out[4] + out[7] + out[9]) / 3.0;
+    out[10] = ke;
+    out[11] = 0.0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Velocity-Verlet run with the reference's step order (src/main/utils.cuh:166-213
+ * for step 0, :254-303 per step; src/fix/fix_nve.cu:42-86 and :131-149).
+ * State in/out: x (wrapped into [lo, lo+L)), v, img (image counters, 3n ints).
+ * Steps first_step .. first_step+nsteps-1 are run after an optional zero step
+ * (do_zero_step != 0 computes forces and thermo at step first_step-1 first).
+ * thermo_out receives 12 doubles per logged step (step % log_f == 0), the step
+ * numbers go to log_steps; returns the number of logged rows (or <0 on error).
+ * f_out holds the last computed forces.                                       */
+int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int* img,
+               const double* lo, const double* L, const oracle_ff* ff, int nbonds,
+               const int* bonds, uint32_t first_step, int nsteps, int do_zero_step,
+               uint32_t log_f, double* thermo_out, int* log_steps, int max_log, double* f_out,
+               double* rho_out)
+{
+    double* f = f_out;
+    double energy[2], virial[6];
+    int nlog = 0;
+    int status = 0;
+    double dt = ff->dt;
+    if (do_zero_step) {
+        uint32_t s0 = first_step - 1;
+        status |= oracle_forces(n, tag, type, x, v, lo, L, ff, s0, nbonds, bonds, f, rho_out,
+                                energy, virial);
+        if (log_f && s0 % log_f == 0 && nlog < max_log) {
+            thermo(n, type, v, L, ff, energy, virial, thermo_out + 12 * nlog);
+            log_steps[nlog++] = (int)s0;
+        }
+    }
+    for (int s = 0; s < nsteps; s++) {
+        uint32_t step = first_step + (uint32_t)s;
+        for (int i = 0; i < n; i++) {
+            double dtm = 0.5 * dt / ff->mass[type[i] - 1];
+            for (int d = 0; d < 3; d++) {
+                v[3 * i + d] += dtm * f[3 * i + d];
+                double p = x[3 * i + d] + dt * v[3 * i + d];
+                double hi = lo[d] + L[d];
+                while (p >= hi || p < lo[d]) {
+                    int k = (p >= hi) - (p < lo[d]);
+                    p -= L[d] * k;
+                    img[3 * i + d] += k;
+                }
+                x[3 * i + d] = p;
+            }
+        }
+        status |= oracle_forces(n, tag, type, x, v, lo, L, ff, step, nbonds, bonds, f, rho_out,
+                                energy, virial);
+        for (int i = 0; i < n; i++) {
+            double dtm = 0.5 * dt / ff->mass[type[i] - 1];
+            for (int d = 0; d < 3; d++) v[3 * i + d] += dtm * f[3 * i + d];
+        }
+        if (log_f && step % log_f == 0 && nlog < max_log) {
+            thermo(n, type, v, L, ff, energy, virial, thermo_out + 12 * nlog);
+            log_steps[nlog++] = (int)step;
+        }
+    }
+    return status < 0 ? status : nlog;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Radial distribution function between type sets (new: the reference has none).
+ * g(r) for pairs (a in type ta, b in type tb), bins of width dr up to rmax:
+ * g_k = count_k / (N_a N_b' 4/3 pi (r_{k+1}^3 - r_k^3) / V), where N_b' = N_b
+ * (or N_a - 1 when ta == tb and pairs are counted both ways).                 */
+typedef struct {
+    const int* type;
+    int ta, tb;
+    double dr;
+    int nbins;
+    double* hist;
+} rdf_ctx;
+
+static void rdf_cb(int i, int j, double dx, double dy, double dz, double r2, void* c)
+{
+    (void)dx; (void)dy; (void)dz;
+    rdf_ctx* k = (rdf_ctx*)c;
+    int a = k->type[i], b = k->type[j];
+    int match = (a == k->ta && b == k->tb) || (a == k->tb && b == k->ta);
+    if (!match) return;
+    int bin = (int)(sqrt(r2) / k->dr);
+    if (bin < k->nbins) {
+        double w = (k->ta == k->tb) ? 2.0 : 1.0;
+        k->hist[bin] += w;
+    }
+}
+
+int oracle_rdf(int n, const int* type, const double* x, const double* lo, const double* L,
+               int ta, int tb, double rmax, int nbins, double* g_out)
+{
+    rdf_ctx k = {type, ta, tb, rmax / nbins, nbins, g_out};
+    memset(g_out, 0, sizeof(double) * nbins);
+    for_each_pair(n, x, lo, L, rmax, rdf_cb, &k);
+    long na = 0, nb = 0;
+    for (int i = 0; i < n; i++) {
+        if (type[i] == ta) na++;
+        if (type[i] == tb) nb++;
+    }
+    double vol = L[0] * L[1] * L[2];
+    double npair = (ta == tb) ? (double)na * (double)(na - 1) : (double)na * (double)nb;
+    for (int b = 0; b < nbins; b++) {
+        double r0 = b * k.dr, r1 = (b + 1) * k.dr;
+        double shell = 4.0 / 3.0 * M_PI * (r1 * r1 * r1 - r0 * r0 * r0);
+        double ideal = npair * shell / vol;
+        g_out[b] = ideal > 0 ? g_out[b] / ideal : 0.0;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
+/* CPU baseline timing path: the reference's algorithm (half Verlet list with
+ * skin, rebuilt on the reference's displacement criterion, src/force/neigh_list.cu
+ * :322-393 and :483-514) over a DPD system, in FP64, split over nthreads POSIX
+ * threads with thread-private force buffers.  Advances nsteps after a step-0
+ * force evaluation and returns the number of list builds.                     */
+typedef struct {
+    int i0, i1, n, nmax;
+    const int *tag, *type, *nl, *nn;
+    const double *x, *v, *L;
+    const oracle_ff* ff;
+    double* fl;
+    uint32_t step;
+    double sig_scale;
+} bench_task;
+
+static void* bench_force_range(void* arg)
+{
+    bench_task* t = (bench_task*)arg;
+    const oracle_ff* ff = t->ff;
+    const double *x = t->x, *v = t->v, *L = t->L;
+    double* fl = t->fl;
+    memset(fl, 0, sizeof(double) * 3 * (size_t)t->n);
+    for (int i = t->i0; i < t->i1; i++) {
+        for (int k = 0; k < t->nn[i]; k++) {
+            int j = t->nl[(size_t)i * t->nmax + k];
+            double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+            double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+            double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+            double r2 = dx * dx + dy * dy + dz * dz;
+            int idx = tri_index(t->type[i], t->type[j], ff->ntypes);
+            double A = ff->coeff[idx][0], gamma = ff->coeff[idx][2], rc = ff->coeff[idx][3];
+            if (!(r2 <= rc * rc)) continue;
+            double r = sqrt(r2);
+            if (r < 1e-10) continue;
+            double dvx = v[3 * i] - v[3 * j], dvy = v[3 * i + 1] - v[3 * j + 1],
+                   dvz = v[3 * i + 2] - v[3 * j + 2];
+            double dot = dx * dvx + dy * dvy + dz * dvz;
+            double wc = 1.0 - r / rc;
+            int a = t->tag[i], b = t->tag[j];
+            double th = oracle_saru((uint32_t)(a < b ? a : b), (uint32_t)(a < b ? b : a),
+                                    ff->seed, (int32_t)t->step);
+            double fp = (A * wc - gamma * wc * wc * dot / r + sqrt(gamma) * t->sig_scale * wc * th) / r;
+            fl[3 * i] += dx * fp; fl[3 * i + 1] += dy * fp; fl[3 * i + 2] += dz * fp;
+            fl[3 * j] -= dx * fp; fl[3 * j + 1] -= dy * fp; fl[3 * j + 2] -= dz * fp;
+        }
+    }
+    return NULL;
+}
+
+int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double* v,
+                       const double* lo, const double* L, const oracle_ff* ff, int nbonds,
+                       const int* bonds, uint32_t first_step, int nsteps, double skin,
+                       int nthreads)
+{
+    (void)nbonds; (void)bonds;
+    double cut = max_rc(ff) + skin;
+    double cut2 = cut * cut;
+    int nc[3];
+    for (int d = 0; d < 3; d++) nc[d] = (int)floor(L[d] / cut);
+    if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) return -1;
+    int nt = nthreads > 0 ? nthreads : 1;
+    if (nt > 256) nt = 256;
+    long ncell = (long)nc[0] * nc[1] * nc[2];
+    int nmax = 256;
+    int* nl = (int*)malloc(sizeof(int) * (size_t)n * nmax);
+    int* nn = (int*)malloc(sizeof(int) * n);
+    double* xlast = (double*)malloc(sizeof(double) * 3 * n);
+    double* f = (double*)calloc((size_t)3 * n, sizeof(double));
+    int* head = (int*)malloc(sizeof(int) * ncell);
+    int* next = (int*)malloc(sizeof(int) * n);
+    int* cid = (int*)malloc(sizeof(int) * 3 * n);
+    double* fpriv = (double*)malloc(sizeof(double) * 3 * (size_t)n * nt);
+    pthread_t th[256];
+    bench_task task[256];
+    double sig_scale = sqrt(2.0 * ff->kT) / sqrt(ff->dt);
+    int builds = 0;
+    int need = 1;
+    for (int s = -1; s < nsteps; s++) {
+        uint32_t step = first_step + (uint32_t)s;
+        if (s >= 0) {
+            for (int i = 0; i < n; i++) {
+                double dtm = 0.5 * ff->dt / ff->mass[type[i] - 1];
+                for (int d = 0; d < 3; d++) {
+                    v[3 * i + d] += dtm * f[3 * i + d];
+                    double p = x[3 * i + d] + ff->dt * v[3 * i + d];
+                    double hi = lo[d] + L[d];
+                    while (p >= hi || p < lo[d]) p -= L[d] * ((p >= hi) - (p < lo[d]));
+                    x[3 * i + d] = p;
+                }
+            }
+            double h2 = 0.25 * skin * skin;
+            need = 0;
+            for (int i = 0; i < n && !need; i++) {
+                double dx = min_image(x[3 * i] - xlast[3 * i], L[0]);
+                double dy = min_image(x[3 * i + 1] - xlast[3 * i + 1], L[1]);
+                double dz = min_image(x[3 * i + 2] - xlast[3 * i + 2], L[2]);
+                if (dx * dx + dy * dy + dz * dz >= h2) need = 1;
+            }
+        }
+        if (need) {
+            builds++;
+            for (long c = 0; c < ncell; c++) head[c] = -1;
+            for (int i = n - 1; i >= 0; i--) {
+                for (int d = 0; d < 3; d++) {
+                    int k = (int)floor((x[3 * i + d] - lo[d]) / (L[d] / nc[d]));
+                    if (k < 0) k = 0;
+                    if (k >= nc[d]) k = nc[d] - 1;
+                    cid[3 * i + d] = k;
+                }
+                long c = ((long)cid[3 * i] * nc[1] + cid[3 * i + 1]) * nc[2] + cid[3 * i + 2];
+                next[i] = head[c];
+                head[c] = i;
+            }
+            for (int i = 0; i < n; i++) {
+                int cnt = 0;
+                for (int ox = -1; ox <= 1; ox++)
+                    for (int oy = -1; oy <= 1; oy++)
+                        for (int oz = -1; oz <= 1; oz++) {
+                            int cx = (cid[3 * i] + ox + nc[0]) % nc[0];
+                            int cy = (cid[3 * i + 1] + oy + nc[1]) % nc[1];
+                            int cz = (cid[3 * i + 2] + oz + nc[2]) % nc[2];
+                            long c = ((long)cx * nc[1] + cy) * nc[2] + cz;
+                            for (int j = head[c]; j >= 0; j = next[j]) {
+                                if (j <= i) continue;
+                                double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+                                double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+                                double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+                                if (dx * dx + dy * dy + dz * dz <= cut2 && cnt < nmax)
+                                    nl[(size_t)i * nmax + cnt++] = j;
+                            }
+                        }
+                nn[i] = cnt;
+            }
+            memcpy(xlast, x, sizeof(double) * 3 * n);
+        }
+        for (int t = 0; t < nt; t++) {
+            task[t].i0 = (int)((long)n * t / nt);
+            task[t].i1 = (int)((long)n * (t + 1) / nt);
+            task[t].n = n; task[t].nmax = nmax;
+            task[t].tag = tag; task[t].type = type; task[t].nl = nl; task[t].nn = nn;
+            task[t].x = x; task[t].v = v; task[t].L = L; task[t].ff = ff;
+            task[t].fl = fpriv + (size_t)3 * n * t;
+            task[t].step = step; task[t].sig_scale = sig_scale;
+        }
+        for (int t = 1; t < nt; t++) pthread_create(&th[t], NULL, bench_force_range, &task[t]);
+        bench_force_range(&task[0]);
+        for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
+        for (int i = 0; i < 3 * n; i++) {
+            double acc = 0.0;
+            for (int t = 0; t < nt; t++) acc += fpriv[(size_t)3 * n * t + i];
+            f[i] = acc;
+        }
+        if (s >= 0) {
+            for (int i = 0; i < n; i++) {
+                double dtm = 0.5 * ff->dt / ff->mass[type[i] - 1];
+                for (int d = 0; d < 3; d++) v[3 * i + d] += dtm * f[3 * i + d];
+            }
+        }
+    }
+    free(nl); free(nn); free(xlast); free(f); free(head); free(next); free(cid); free(fpriv);
+    return builds;
+}
+
+int oracle_max_types(void) { return ORACLE_MAXT; }
+int oracle_ff_size(void) { return (int)sizeof(oracle_ff); }

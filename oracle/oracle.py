@@ -1,0 +1,238 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/dpd_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+cpu_baseline / reference legs as the checker; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "liboracle.so")
+MAXT = 32
+
+
+class OracleFF(ctypes.Structure):
+    _fields_ = [
+        ("style", ctypes.c_int), ("ntypes", ctypes.c_int), ("kT", ctypes.c_double),
+        ("dt", ctypes.c_double), ("seed", ctypes.c_uint32),
+        ("coeff", (ctypes.c_double * 5) * (MAXT * MAXT)), ("mass", ctypes.c_double * MAXT),
+        ("bond_style", ctypes.c_int), ("nbondtypes", ctypes.c_int),
+        ("bond_coeff", (ctypes.c_double * 4) * MAXT),
+    ]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        build()
+    lib = ctypes.CDLL(LIB)
+    vp, i, u32, d, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_double, ctypes.c_long
+    lib.oracle_saru.restype = ctypes.c_float
+    lib.oracle_saru.argtypes = [u32, u32, u32, ctypes.c_int32]
+    lib.oracle_saru_batch.restype = None
+    lib.oracle_saru_batch.argtypes = [i, vp, vp, u32, vp, vp]
+    lib.oracle_pairs_f64.restype = i64
+    lib.oracle_pairs_f64.argtypes = [i, vp, vp, vp, vp, d, vp, i64]
+    lib.oracle_pairs_f32.restype = i64
+    lib.oracle_pairs_f32.argtypes = [i, vp, vp, vp, vp, vp, ctypes.c_float, vp, i64]
+    lib.oracle_forces.restype = i
+    lib.oracle_forces.argtypes = [i, vp, vp, vp, vp, vp, vp, ctypes.POINTER(OracleFF), u32, i, vp, vp,
+                                  vp, vp, vp]
+    lib.oracle_run.restype = i
+    lib.oracle_run.argtypes = [i, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(OracleFF), i, vp, u32, i,
+                               i, u32, vp, vp, i, vp, vp]
+    lib.oracle_rdf.restype = i
+    lib.oracle_rdf.argtypes = [i, vp, vp, vp, vp, i, i, d, i, vp]
+    lib.oracle_bench_steps.restype = i
+    lib.oracle_bench_steps.argtypes = [i, vp, vp, vp, vp, vp, vp, ctypes.POINTER(OracleFF), i, vp,
+                                       u32, i, d, i]
+    assert lib.oracle_ff_size() == ctypes.sizeof(OracleFF)
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def tri_index(ti, tj, nt):
+    a, b = min(ti, tj), max(ti, tj)
+    return ((a - 1) * nt - (a - 1) * (a - 2) // 2 + b - a + 1) - 1
+
+
+def make_ff(style, ntypes, coeffs, kT, dt, seed, masses, bond_style=0, bond_coeffs=()):
+    """coeffs: {(ti,tj): (A, B, gamma, rc, rd)}; bond_coeffs: list of 4-tuples."""
+    ff = OracleFF()
+    ff.style = style
+    ff.ntypes = ntypes
+    ff.kT = kT
+    ff.dt = dt
+    ff.seed = seed
+    for (ti, tj), c in coeffs.items():
+        idx = tri_index(ti, tj, ntypes)
+        for k in range(5):
+            ff.coeff[idx][k] = c[k]
+    for t, m in enumerate(masses):
+        ff.mass[t] = m
+    ff.bond_style = bond_style
+    ff.nbondtypes = len(bond_coeffs)
+    for b, c in enumerate(bond_coeffs):
+        for k in range(len(c)):
+            ff.bond_coeff[b][k] = c[k]
+    return ff
+
+
+def ff_from_run_in(text, masses):
+    """Force field of a run.in text (pair_style/pair_coeff/bond_style/bond_coeff/timestep)."""
+    style, kT, rc, rd, seed, dt = 0, 1.0, 1.0, 0.0, 0, 0.01
+    coeffs, bonds, bstyle = {}, {}, 0
+    raw = []
+    for line in text.splitlines():
+        t = line.split("#")[0].split()
+        if t:
+            raw.append(t)
+    for t in raw:
+        if t[0] == "timestep":
+            dt = float(t[1])
+        if t[0] == "pair_style":
+            if t[1] == "dpd":
+                style, kT, rc, seed = 0, float(t[2]), float(t[3]), int(t[4])
+            else:
+                style, kT, rc, rd, seed = 1, float(t[2]), float(t[3]), float(t[4]), int(t[5])
+        if t[0] == "bond_style":
+            bstyle = {"harmonic": 1, "fene": 2}[t[1]]
+    for t in raw:
+        if t[0] == "pair_coeff":
+            ti, tj = int(t[1]), int(t[2])
+            if style == 0:
+                A, g = float(t[3]), float(t[4])
+                r = float(t[5]) if len(t) > 5 else rc
+                coeffs[(ti, tj)] = (A, 0.0, g, r, 0.0)
+            else:
+                A, B, g = float(t[3]), float(t[4]), float(t[5])
+                r, d = (float(t[6]), float(t[7])) if len(t) > 6 else (rc, rd)
+                coeffs[(ti, tj)] = (A, B, g, r, d)
+        if t[0] == "bond_coeff":
+            bonds[int(t[1])] = tuple(float(v) for v in t[2:])
+    bc = [bonds[k] for k in sorted(bonds)]
+    return make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc)
+
+
+def saru(t1, t2, seed, step):
+    lib = load()
+    t1 = np.ascontiguousarray(t1, dtype=np.uint32)
+    t2 = np.ascontiguousarray(t2, dtype=np.uint32)
+    st = np.ascontiguousarray(np.broadcast_to(step, t1.shape), dtype=np.int32)
+    out = np.empty(t1.shape, dtype=np.float32)
+    lib.oracle_saru_batch(len(t1), _p(t1), _p(t2), seed, _p(st), _p(out))
+    return out
+
+
+def forces(ff, tags, types, x, v, lo, L, step, bonds=None):
+    lib = load()
+    n = len(types)
+    tags = np.ascontiguousarray(tags, dtype=np.int32)
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    lo = np.ascontiguousarray(lo, dtype=np.float64)
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    f = np.empty((n, 3))
+    rho = np.empty(n)
+    en = np.empty(2)
+    vir = np.empty(6)
+    nb = 0 if bonds is None else len(bonds)
+    b = None if bonds is None else np.ascontiguousarray(bonds, dtype=np.int32)
+    st = lib.oracle_forces(n, _p(tags), _p(types), _p(x), _p(v), _p(lo), _p(L), ctypes.byref(ff), step,
+                           nb, _p(b), _p(f), _p(rho), _p(en), _p(vir))
+    return {"f": f, "rho": rho, "pair_pe": en[0], "bond_pe": en[1], "virial": vir, "status": st}
+
+
+def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zero_step=True):
+    """Velocity-Verlet in FP64; returns final state and logged thermo rows."""
+    lib = load()
+    n = len(types)
+    tags = np.ascontiguousarray(tags, dtype=np.int32)
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    x = np.array(x, dtype=np.float64, order="C")
+    v = np.array(v, dtype=np.float64, order="C")
+    img = np.zeros((n, 3), dtype=np.int32)
+    lo = np.ascontiguousarray(lo, dtype=np.float64)
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    maxlog = nsteps + 2
+    th = np.zeros((maxlog, 12))
+    ls = np.zeros(maxlog, dtype=np.int32)
+    f = np.zeros((n, 3))
+    rho = np.zeros(n)
+    nb = 0 if bonds is None else len(bonds)
+    b = None if bonds is None else np.ascontiguousarray(bonds, dtype=np.int32)
+    nlog = lib.oracle_run(n, _p(tags), _p(types), _p(x), _p(v), _p(img), _p(lo), _p(L), ctypes.byref(ff),
+                          nb, _p(b), first_step, nsteps, 1 if zero_step else 0, log_f, _p(th), _p(ls),
+                          maxlog, _p(f), _p(rho))
+    if nlog < 0:
+        raise RuntimeError(f"oracle_run failed: {nlog}")
+    cols = ["temp", "pair_pe", "bond_pe", "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "ke"]
+    thermo = {c: th[:nlog, k] for k, c in enumerate(cols)}
+    thermo["step"] = ls[:nlog]
+    return {"x": x, "v": v, "image": img, "f": f, "rho": rho, "thermo": thermo}
+
+
+def pairs_f64(tags, x, lo, L, cut):
+    lib = load()
+    n = len(tags)
+    tags = np.ascontiguousarray(tags, dtype=np.int32)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    lo = np.ascontiguousarray(lo, dtype=np.float64)
+    L = np.ascontiguousarray(L, dtype=np.float64)
+    cnt = lib.oracle_pairs_f64(n, _p(tags), _p(x), _p(lo), _p(L), cut, None, 0)
+    out = np.empty((max(cnt, 1), 2), dtype=np.int32)
+    lib.oracle_pairs_f64(n, _p(tags), _p(x), _p(lo), _p(L), cut, _p(out), cnt)
+    return out[:cnt]
+
+
+def pairs_f32(tags, cell, off, nc, w, cut2):
+    lib = load()
+    n = len(tags)
+    tags = np.ascontiguousarray(tags, dtype=np.int32)
+    cell = np.ascontiguousarray(cell, dtype=np.int32)
+    off = np.ascontiguousarray(off, dtype=np.float32)
+    nc = np.ascontiguousarray(nc, dtype=np.int32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    cnt = lib.oracle_pairs_f32(n, _p(tags), _p(cell), _p(off), _p(nc), _p(w), float(cut2), None, 0)
+    out = np.empty((max(cnt, 1), 2), dtype=np.int32)
+    lib.oracle_pairs_f32(n, _p(tags), _p(cell), _p(off), _p(nc), _p(w), float(cut2), _p(out), cnt)
+    return out[:cnt]
+
+
+def rdf(types, x, lo, L, ta, tb, rmax, nbins):
+    lib = load()
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    g = np.empty(nbins)
+    lib.oracle_rdf(len(types), _p(types), _p(x), _p(np.asarray(lo, dtype=np.float64)),
+                   _p(np.asarray(L, dtype=np.float64)), ta, tb, rmax, nbins, _p(g))
+    return g
+
+
+def bench_steps(ff, tags, types, x, v, lo, L, first_step, nsteps, skin, nthreads):
+    """The reference algorithm (half Verlet list + skin) in FP64 on nthreads host threads."""
+    lib = load()
+    tags = np.ascontiguousarray(tags, dtype=np.int32)
+    types = np.ascontiguousarray(types, dtype=np.int32)
+    x = np.array(x, dtype=np.float64, order="C")
+    v = np.array(v, dtype=np.float64, order="C")
+    return lib.oracle_bench_steps(len(types), _p(tags), _p(types), _p(x), _p(v),
+                                  _p(np.asarray(lo, dtype=np.float64)), _p(np.asarray(L, dtype=np.float64)),
+                                  ctypes.byref(ff), 0, None, first_step, nsteps, skin, nthreads)
