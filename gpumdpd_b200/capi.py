@@ -21,7 +21,7 @@ EXPORTED = [
     "dpd_create", "dpd_create_from_system", "dpd_run", "dpd_sync", "dpd_get_thermo",
     "dpd_get_state", "dpd_set_state", "dpd_get_density", "dpd_get_cells", "dpd_get_neighbors",
     "dpd_compute_rdf", "dpd_rdf_config", "dpd_rdf_result", "dpd_get_info", "dpd_set_tuning",
-    "dpd_write_data", "dpd_time_steps", "dpd_last_error", "dpd_destroy", "dpd_pair_compute_aos",
+    "dpd_write_data", "dpd_time_steps", "dpd_get_list_stats", "dpd_last_error", "dpd_destroy", "dpd_pair_compute_aos",
     "dpd_batch_create", "dpd_batch_n", "dpd_batch_get_thermo", "dpd_batch_get_state",
     "dpd_batch_rdf_result", "dpd_server_create", "dpd_server_submit", "dpd_server_step",
     "dpd_server_result", "dpd_server_job_state", "dpd_server_job_rdf", "dpd_server_stats",
@@ -101,6 +101,7 @@ def load():
         "dpd_rdf_result": (i, [vp, vp, P(i64)]),
         "dpd_get_info": (i, [vp, P(i64), P(i64), P(i64), P(i64)]),
         "dpd_set_tuning": (i, [vp, P(dpd_tuning)]),
+        "dpd_get_list_stats": (i, [vp, P(i64), P(i64), P(i64)]),
         "dpd_write_data": (i, [vp, cp]),
         "dpd_time_steps": (i, [vp, u32, P(d), P(d), P(i64)]),
         "dpd_last_error": (cp, [vp]),

@@ -171,6 +171,12 @@ int dpd_get_info(dpd_engine* h, int64_t* step, int64_t* n_builds, int64_t* n_ato
     return DPD_OK;
 }
 
+int dpd_get_list_stats(dpd_engine* h, int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
+{
+    ENG_CHECK(h);
+    return h->eng.list_stats(n_pairs, n_atoms, n_builds);
+}
+
 int dpd_set_tuning(dpd_engine* h, const dpd_tuning* t)
 {
     ENG_CHECK(h);

@@ -890,6 +890,21 @@ int Engine::write_data(int rep, const std::string& path)
     return write_data_file(path, R.in.atom_style, s, err);
 }
 
+int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
+{
+    const RepDesc& d = reps_[0].desc;
+    const int ns = d.p_cap_end - d.p_begin;
+    std::vector<int> cnt(ns);
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(cnt.data(), b_.ncount + d.p_begin, sizeof(int) * ns, cudaMemcpyDeviceToHost));
+    int64_t tot = 0;
+    for (int k = 0; k < d.n_real; k++) tot += std::min(cnt[k], nmax_);
+    if (n_pairs) *n_pairs = tot;
+    if (n_atoms) *n_atoms = d.n_real;
+    if (n_builds) *n_builds = this->n_builds();
+    return DPD_OK;
+}
+
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;

@@ -66,6 +66,7 @@ public:
     int rdf_result(int rep, double* g, int64_t* nsamples);
     int write_data(int rep, const std::string& path);
     int set_tuning(const dpd_tuning* t);
+    int list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds);
     int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
                          int n, uint32_t step, float* d_force, float* d_pe, float* d_virial);
 

@@ -138,6 +138,13 @@ class Engine:
                                        ctypes.byref(nl)), self.lib, self.h)
         return {"total_ms": tot.value, "pair_ms": pair.value, "pair_launches": nl.value}
 
+    def list_stats(self):
+        p, n, b = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(self.lib.dpd_get_list_stats(self.h, ctypes.byref(p), ctypes.byref(n), ctypes.byref(b)),
+               self.lib, self.h)
+        return {"pairs": p.value, "atoms": n.value, "builds": b.value,
+                "mean_half_list": p.value / max(n.value, 1)}
+
     def write_data(self, path):
         _check(self.lib.dpd_write_data(self.h, path.encode()), self.lib, self.h)
 

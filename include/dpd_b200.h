@@ -139,6 +139,10 @@ int dpd_rdf_result(dpd_engine* eng, double* g, int64_t* nsamples);
 int dpd_get_info(dpd_engine* eng, int64_t* step, int64_t* n_builds, int64_t* n_atoms,
                  int64_t* device_bytes);
 
+/* Neighbour-list statistics of replica 0: pairs in the current half list, particles,
+ * list builds so far (the mean half-list length is pairs/particles). */
+int dpd_get_list_stats(dpd_engine* eng, int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds);
+
 /* Apply tuning knobs (takes effect at the next run). */
 int dpd_set_tuning(dpd_engine* eng, const dpd_tuning* t);
 

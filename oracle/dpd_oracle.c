@@ -32,7 +32,24 @@
 /* Saru counter-based RNG: src/force/pair_dpd.cu:203-236 (same constants; the
  * stream must be identical, so the steps are kept as published).              */
 
+/* 0: float tail of the -DSINGLE build (the engine's); 1: tail of the -DDOUBLE build,
+ * where (float)s * 2^-32f is float and the rest is double (pair_dpd.cu:235 with
+ * numtyp = double).  Only the golden-vector tests against the DOUBLE build set 1. */
+static int g_saru_double_tail = 0;
+void oracle_set_saru_double_tail(int on) { g_saru_double_tail = on; }
+
+static double saru_value(uint32_t seed1, uint32_t seed2, uint32_t seed, int32_t timestep);
+
 float oracle_saru(uint32_t seed1, uint32_t seed2, uint32_t seed, int32_t timestep)
+{
+    int keep = g_saru_double_tail;
+    g_saru_double_tail = 0;
+    float r = (float)saru_value(seed1, seed2, seed, timestep);
+    g_saru_double_tail = keep;
+    return r;
+}
+
+static double saru_value(uint32_t seed1, uint32_t seed2, uint32_t seed, int32_t timestep)
 {
     uint32_t seed3 = seed + (uint32_t)timestep;
     seed3 ^= (seed1 << 7) ^ (seed2 >> 6);
@@ -59,9 +76,13 @@ float oracle_saru(uint32_t seed1, uint32_t seed2, uint32_t seed, int32_t timeste
     /* float tail, one rounding per operation as in the reference's -DSINGLE build:
        (float)s * 2^-32 * 2 is exact scaling, then -1 rounds, then *sqrt(3)f rounds */
     volatile float a = (float)s;
+    if (g_saru_double_tail) {
+        volatile float a32 = a * 2.3283064365386963e-10f; /* 2^-32, exact */
+        return 1.7320508075688772935274463 * ((double)a32 * 2.0 - 1.0);
+    }
     volatile float u = a * 4.6566128730773926e-10f - 1.0f; /* 2^-31 */
     volatile float th = 1.7320508075688772f * u;
-    return th;
+    return (double)th;
 }
 
 void oracle_saru_batch(int n, const uint32_t* t1, const uint32_t* t2, uint32_t seed,
@@ -287,7 +308,7 @@ static void force_cb(int i, int j, double dx, double dy, double dz, double r2, v
     double wr = wc;
     int a = k->tag[i], b = k->tag[j];
     uint32_t t1 = (uint32_t)(a < b ? a : b), t2 = (uint32_t)(a < b ? b : a);
-    double theta = (double)oracle_saru(t1, t2, ff->seed, (int32_t)k->step);
+    double theta = saru_value(t1, t2, ff->seed, (int32_t)k->step);
     double sigma = sqrt(gamma) * k->sig_scale;
     double fpair;
     double pe;
@@ -594,6 +615,57 @@ static void* bench_force_range(void* arg)
     return NULL;
 }
 
+typedef struct {
+    int i0, i1, n, nmax;
+    const int *head, *next, *cid, *nc;
+    const double *x, *L;
+    double cut2;
+    int* nl;
+    int* nn;
+    double* f;
+    const double* fpriv;
+    int nt;
+} build_task;
+
+static void* bench_build_range(void* arg)
+{
+    build_task* t = (build_task*)arg;
+    const double *x = t->x, *L = t->L;
+    const int* nc = t->nc;
+    for (int i = t->i0; i < t->i1; i++) {
+        int cnt = 0;
+        for (int ox = -1; ox <= 1; ox++)
+            for (int oy = -1; oy <= 1; oy++)
+                for (int oz = -1; oz <= 1; oz++) {
+                    int cx = (t->cid[3 * i] + ox + nc[0]) % nc[0];
+                    int cy = (t->cid[3 * i + 1] + oy + nc[1]) % nc[1];
+                    int cz = (t->cid[3 * i + 2] + oz + nc[2]) % nc[2];
+                    long c = ((long)cx * nc[1] + cy) * nc[2] + cz;
+                    for (int j = t->head[c]; j >= 0; j = t->next[j]) {
+                        if (j <= i) continue;
+                        double dx = min_image(x[3 * i] - x[3 * j], L[0]);
+                        double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
+                        double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
+                        if (dx * dx + dy * dy + dz * dz <= t->cut2 && cnt < t->nmax)
+                            t->nl[(size_t)i * t->nmax + cnt++] = j;
+                    }
+                }
+        t->nn[i] = cnt;
+    }
+    return NULL;
+}
+
+static void* bench_reduce_range(void* arg)
+{
+    build_task* t = (build_task*)arg;
+    for (long k = 3L * t->i0; k < 3L * t->i1; k++) {
+        double acc = 0.0;
+        for (int q = 0; q < t->nt; q++) acc += t->fpriv[(size_t)3 * t->n * q + k];
+        t->f[k] = acc;
+    }
+    return NULL;
+}
+
 int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double* v,
                        const double* lo, const double* L, const oracle_ff* ff, int nbonds,
                        const int* bonds, uint32_t first_step, int nsteps, double skin,
@@ -658,26 +730,17 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
                 next[i] = head[c];
                 head[c] = i;
             }
-            for (int i = 0; i < n; i++) {
-                int cnt = 0;
-                for (int ox = -1; ox <= 1; ox++)
-                    for (int oy = -1; oy <= 1; oy++)
-                        for (int oz = -1; oz <= 1; oz++) {
-                            int cx = (cid[3 * i] + ox + nc[0]) % nc[0];
-                            int cy = (cid[3 * i + 1] + oy + nc[1]) % nc[1];
-                            int cz = (cid[3 * i + 2] + oz + nc[2]) % nc[2];
-                            long c = ((long)cx * nc[1] + cy) * nc[2] + cz;
-                            for (int j = head[c]; j >= 0; j = next[j]) {
-                                if (j <= i) continue;
-                                double dx = min_image(x[3 * i] - x[3 * j], L[0]);
-                                double dy = min_image(x[3 * i + 1] - x[3 * j + 1], L[1]);
-                                double dz = min_image(x[3 * i + 2] - x[3 * j + 2], L[2]);
-                                if (dx * dx + dy * dy + dz * dz <= cut2 && cnt < nmax)
-                                    nl[(size_t)i * nmax + cnt++] = j;
-                            }
-                        }
-                nn[i] = cnt;
+            build_task bt[256];
+            for (int t = 0; t < nt; t++) {
+                bt[t].i0 = (int)((long)n * t / nt);
+                bt[t].i1 = (int)((long)n * (t + 1) / nt);
+                bt[t].n = n; bt[t].nmax = nmax; bt[t].head = head; bt[t].next = next;
+                bt[t].cid = cid; bt[t].nc = nc; bt[t].x = x; bt[t].L = L; bt[t].cut2 = cut2;
+                bt[t].nl = nl; bt[t].nn = nn;
             }
+            for (int t = 1; t < nt; t++) pthread_create(&th[t], NULL, bench_build_range, &bt[t]);
+            bench_build_range(&bt[0]);
+            for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
             memcpy(xlast, x, sizeof(double) * 3 * n);
         }
         for (int t = 0; t < nt; t++) {
@@ -692,10 +755,16 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
         for (int t = 1; t < nt; t++) pthread_create(&th[t], NULL, bench_force_range, &task[t]);
         bench_force_range(&task[0]);
         for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
-        for (int i = 0; i < 3 * n; i++) {
-            double acc = 0.0;
-            for (int t = 0; t < nt; t++) acc += fpriv[(size_t)3 * n * t + i];
-            f[i] = acc;
+        {
+            build_task rt[256];
+            for (int t = 0; t < nt; t++) {
+                rt[t].i0 = (int)((long)n * t / nt);
+                rt[t].i1 = (int)((long)n * (t + 1) / nt);
+                rt[t].n = n; rt[t].nt = nt; rt[t].f = f; rt[t].fpriv = fpriv;
+            }
+            for (int t = 1; t < nt; t++) pthread_create(&th[t], NULL, bench_reduce_range, &rt[t]);
+            bench_reduce_range(&rt[0]);
+            for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
         }
         if (s >= 0) {
             for (int i = 0; i < n; i++) {

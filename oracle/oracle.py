@@ -41,6 +41,8 @@ def load():
     vp, i, u32, d, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_double, ctypes.c_long
     lib.oracle_saru.restype = ctypes.c_float
     lib.oracle_saru.argtypes = [u32, u32, u32, ctypes.c_int32]
+    lib.oracle_set_saru_double_tail.restype = None
+    lib.oracle_set_saru_double_tail.argtypes = [i]
     lib.oracle_saru_batch.restype = None
     lib.oracle_saru_batch.argtypes = [i, vp, vp, u32, vp, vp]
     lib.oracle_pairs_f64.restype = i64
@@ -128,6 +130,11 @@ def ff_from_run_in(text, masses):
             bonds[int(t[1])] = tuple(float(v) for v in t[2:])
     bc = [bonds[k] for k in sorted(bonds)]
     return make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc)
+
+
+def set_saru_double_tail(on):
+    """Evaluate Saru's tail as the reference's -DDOUBLE build does (golden tests only)."""
+    load().oracle_set_saru_double_tail(1 if on else 0)
 
 
 def saru(t1, t2, seed, step):

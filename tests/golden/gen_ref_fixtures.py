@@ -90,10 +90,12 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
         frames = parse_trj(os.path.join(td, "all.trj"))
         thermo = parse_thermo(os.path.join(td, "thermo.txt"))
     save = {"run_in": np.array("\n".join(lines)), "masses": system.masses, "lo": system.lo,
-            "hi": system.hi, "types_in": system.types, "x_in": system.x, "v_in": system.v}
+            "hi": system.hi}
     if system.bonds is not None:
         save["bonds"] = system.bonds
     for step in sorted(frames):
+        if step not in (0, 1, nsteps):
+            continue
         fr = frames[step]
         order = np.argsort(fr["id"])
         for c in ("x", "y", "z", "fx", "fy", "fz", "vx", "vy", "vz"):

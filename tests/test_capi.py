@@ -1,0 +1,157 @@
+"""The C-ABI boundary on a host without a GPU: the library loads, exports every symbol
+declared in include/dpd_b200.h, applies the reference's run.in grammar and data-file
+checks (src/main/read_in.cu:40-371, plugin isEnabled/validateParams) before touching
+a device, and refuses to run without one (no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def _header_symbols():
+    text = open(os.path.join(ROOT, "include", "dpd_b200.h")).read()
+    return sorted(set(re.findall(r"\b(dpd_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from gpumdpd_b200 import capi
+    lib = capi.load()
+    syms = _header_symbols()
+    assert len(syms) >= 30
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) == set(capi.EXPORTED)
+
+
+def _create(run_in, system):
+    from gpumdpd_b200 import capi
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    s, keep = system.c_system()
+    code = lib.dpd_create_from_system(run_in.encode(), ctypes.byref(s), ctypes.byref(h))
+    msg = lib.dpd_last_error(None).decode()
+    if code == 0:
+        lib.dpd_destroy(h)
+    return code, msg
+
+
+@pytest.fixture(scope="module")
+def base():
+    from gpumdpd_b200 import inputs
+    return inputs.plain_dpd(L=6.0, seed=1)
+
+
+def _no_gpu():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="checks the no-device refusal")
+def test_valid_input_refuses_without_gpu(base):
+    code, msg = _create(base.run_in, base)
+    assert code == -8 and "no CPU fallback" in msg
+
+
+BAD = [
+    ("unknown", lambda t: t + "foo 1 2\n", "unknown command foo"),
+    ("no_run", lambda t: t.replace("run 1000\n", ""), "run command is missing"),
+    ("no_thermo", lambda t: t.replace("thermo 100\n", ""), "thermo command is missing"),
+    ("no_atom_style", lambda t: t.replace("atom_style atomic\n", ""), "atom_style command is missing"),
+    ("neighbor_args", lambda t: t.replace("neighbor 1.0 0.3 10.0 1", "neighbor 1.0 0.3 10.0"), "illegal neighbor command"),
+    ("nl_f_float", lambda t: t.replace("neighbor 1.0 0.3 10.0 1", "neighbor 1.0 0.3 10.0 1.5"), "illegal neighbor command"),
+    ("pair_args", lambda t: t.replace("pair_style dpd 1.0 1.0 1", "pair_style dpd 1.0 1.0"), "illegal pair_style dpd"),
+    ("rc_too_big", lambda t: t.replace("pair_style dpd 1.0 1.0 1", "pair_style dpd 1.0 1.5 1"), "global rc should not be bigger"),
+    ("coeff_missing", lambda t: t.replace("pair_coeff 1 1 25.0 4.5\n", ""), "all pair_coeff are not set"),
+    ("coeff_order", lambda t: t.replace("pair_coeff 1 1 25.0 4.5", "pair_coeff 2 1 25.0 4.5"), "typei <= typej"),
+    ("no_pair_style", lambda t: t.replace("pair_style dpd 1.0 1.0 1\n", ""), "pair_style command is missing"),
+    ("two_pair_styles", lambda t: t + "pair_style mdpd 1.0 1.0 0.75 3\n", "more than one enabled pair_style"),
+    ("group_type", lambda t: t.replace("group all type 1", "group all type 2"), "Type in group is not included"),
+    ("group_dup", lambda t: t + "group all type 1\n", "already exists"),
+    ("fix_group", lambda t: t.replace("fix md all nve", "fix md none nve"), "Group 'none' not found"),
+    ("fix_style", lambda t: t.replace("fix md all nve", "fix md all langevin"), "Fix type 'langevin' not found"),
+    ("fix_params", lambda t: t.replace("fix md all nve", "fix md all nve 1"), "illegal fix_nve command"),
+    ("fix_dup_id", lambda t: t + "fix md all nve\n", "already registered"),
+    ("dump_args", lambda t: t + "dump 0 10 wrapped force_no\n", "illegal dump command"),
+    ("compute_bad", lambda t: t + "compute c all msd 1 x.txt\n", "Compute type 'msd' not found"),
+    ("angle", lambda t: t.replace("atom_style atomic", "atom_style angle") + "bond_style harmonic\nangle_style harmonic\n", "not supported"),
+]
+
+
+@pytest.mark.parametrize("name,edit,msg", BAD, ids=[b[0] for b in BAD])
+def test_run_in_grammar_errors(base, name, edit, msg):
+    text = base.run_in.replace("pair_style dpd 1.0 1.0 2", "pair_style dpd 1.0 1.0 1")
+    text = re.sub(r"pair_style dpd 1\.0 1\.0 \d+", "pair_style dpd 1.0 1.0 1", text)
+    code, err = _create(edit(text), base)
+    assert code == -1, err
+    assert msg in err
+
+
+def test_mdpd_rd_checks(base):
+    from gpumdpd_b200 import inputs
+    s = inputs.mdpd_slab(Lx=6, Ly=6, Lz=12, z0=3, z1=9)
+    code, err = _create(s.run_in.replace("mdpd 1.0 1.0 0.75", "mdpd 1.0 1.0 1.25"), s)
+    assert code == -1 and "rd should not be bigger than rc" in err
+    code, err = _create(s.run_in.replace("pair_coeff 1 1 -40.0 25.0 4.5", "pair_coeff 1 1 -40.0 25.0"), s)
+    assert code == -1 and "illegal pair_coeff command for pair mdpd" in err
+
+
+def test_bond_style_checks():
+    from gpumdpd_b200 import inputs
+    s = inputs.diblock_melt(L=6.0, seed=1)
+    code, err = _create(s.run_in.replace("bond_coeff 1 4.0 0.0\n", ""), s)
+    assert code == -1 and "all bond_coeff are not set" in err
+    code, err = _create(s.run_in.replace("bond_style harmonic\n", ""), s)
+    assert code == -1 and "bond_style command is missing" in err
+    code, err = _create(s.run_in.replace("bond_coeff 1 4.0 0.0", "bond_coeff 1 4.0"), s)
+    assert code == -1 and "bond_style harmonic" in err
+
+
+def test_data_file_reader(tmp_path, base):
+    """Files in the reference's write_data layout are read (and bad ones rejected)."""
+    from gpumdpd_b200 import capi, inputs
+    lib = capi.load()
+    for s in (base, inputs.diblock_melt(L=6.0, seed=2)):
+        p = tmp_path / "in.data"
+        s.write_data(str(p))
+        h = ctypes.c_void_p()
+        code = lib.dpd_create(s.run_in.encode(), str(p).encode(), None, ctypes.byref(h))
+        err = lib.dpd_last_error(None).decode()
+        assert code in (0, -8), err
+        if code == 0:
+            lib.dpd_destroy(h)
+    # duplicate atom id
+    p = tmp_path / "bad.data"
+    base.write_data(str(p))
+    lines = open(p).read().splitlines()
+    k = next(i for i, l in enumerate(lines) if l.startswith("Atoms")) + 3
+    lines[k] = "1 " + " ".join(lines[k].split()[1:])
+    open(p, "w").write("\n".join(lines) + "\n")
+    h = ctypes.c_void_p()
+    code = lib.dpd_create(base.run_in.encode(), str(p).encode(), None, ctypes.byref(h))
+    assert code == -1 and "Atoms section" in lib.dpd_last_error(None).decode()
+    code = lib.dpd_create(base.run_in.encode(), b"/nonexistent/file.data", None, ctypes.byref(h))
+    assert code == -2
+
+
+def test_inputs_generators():
+    from gpumdpd_b200 import inputs
+    s = inputs.plain_dpd()
+    assert s.n == 3000 and np.all((s.x >= 0) & (s.x < 10))
+    assert np.abs((s.v).sum(axis=0)).max() < 1e-9
+    m = inputs.diblock_melt(L=10.0)
+    assert m.n == 3000 and len(m.bonds) == 2700
+    assert list(m.types[:10]) == [1] * 5 + [2] * 5
+    b = np.linalg.norm(((m.x[m.bonds[:, 1] - 1] - m.x[m.bonds[:, 2] - 1]) + 5) % 10 - 5, axis=1)
+    assert np.allclose(b, 0.9)
+    sl = inputs.mdpd_slab()
+    assert sl.n == 384000 and sl.x[:, 2].min() >= 40 and sl.x[:, 2].max() <= 80
+    reps = inputs.replica_sweep(n_rep=8, nsteps=10)
+    ns = [r.n for r in reps]
+    assert min(ns) >= 3 * 8 ** 3 * 0.99 and max(ns) <= 3 * 24 ** 3 * 1.01

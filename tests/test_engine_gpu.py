@@ -1,0 +1,220 @@
+"""Parity of the CUDA engine (through the C ABI) with the pinned FP64 oracle.
+
+Tolerances (stated by the spec of this engine): neighbour sets bit-exact as tag-pair
+sets; forces within 1e-5 of the RMS particle force at step 0 and over 10 steps;
+thermo rows within the FP32 state's precision; long-run T and P within statistical
+error."""
+import numpy as np
+import pytest
+
+from conftest import force_err, load_golden
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5
+
+
+def _engine_from(system):
+    from gpumdpd_b200 import Engine
+    return Engine(system.run_in, system=system.c_system())
+
+
+def _box(e):
+    c = e.cells()
+    return c["nc"].astype(np.float64) * c["w"].astype(np.float64)
+
+
+def _golden_system(name):
+    from gpumdpd_b200.inputs import System
+    g = load_golden(name)
+    x = np.column_stack([g[f"s0_{c}"] for c in "xyz"])
+    v = np.column_stack([g[f"s0_v{c}"] for c in "xyz"])
+    run_in = str(g["run_in"])
+    style = "bond" if "bonds" in g else "atomic"
+    lines = [ln for ln in run_in.splitlines() if not ln.startswith("dump")]
+    s = System(g["lo"], g["hi"], g["masses"], g["s0_type"], x, v, bonds=g.get("bonds"),
+               n_bondtypes=1 if "bonds" in g else 0, run_in="\n".join(lines) + "\n", atom_style=style)
+    return s, g
+
+
+def _systems():
+    from gpumdpd_b200 import inputs
+    return {
+        "dpd": inputs.plain_dpd(L=10.0, seed=2024),
+        "mdpd": inputs.mdpd_slab(Lx=8.0, Ly=8.0, Lz=24.0, z0=8.0, z1=16.0, seed=11, nsteps=10),
+        "diblock": inputs.diblock_melt(L=10.0, seed=5, nsteps=10),
+        "small_box": inputs.binary_mixture(4.5, 35.0, seed=3),  # 3 cells per dimension
+    }
+
+
+@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "small_box"])
+def test_neighbor_set_bit_exact(oracle_mod, name):
+    s = _systems()[name]
+    e = _engine_from(s)
+    e.run(0)
+    c = e.cells()
+    tags = np.arange(1, s.n + 1)
+    got = e.neighbors()
+    ref = oracle_mod.pairs_f32(tags, c["cell"], c["offset"], c["nc"], c["w"], c["cut2"])
+    assert len(got) == len(set(map(tuple, got.tolist())))  # no duplicates
+    assert set(map(tuple, got.tolist())) == set(map(tuple, ref.tolist()))
+    # and it contains every pair within rc in exact arithmetic
+    st = e.state()
+    inner = oracle_mod.pairs_f64(tags, st["x"], s.lo, _box(e), 1.0)
+    assert set(map(tuple, inner.tolist())) <= set(map(tuple, got.tolist()))
+
+
+@pytest.mark.parametrize("name", ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc"])
+def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
+    s, g = _golden_system(name)
+    e = _engine_from(s)
+    e.run(0)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, st["x"], st["v"], s.lo, _box(e), 0,
+                          bonds=s.bonds)
+    assert force_err(st["f"], o["f"]) < FORCE_TOL
+    f_ref = np.column_stack([g[f"s0_f{c}"] for c in "xyz"])
+    assert force_err(st["f"], f_ref) < FORCE_TOL
+    th = e.thermo()
+    assert th["step"][0] == 0
+    assert th["pair_pe"][0] == pytest.approx(o["pair_pe"], rel=1e-6)
+    assert th["bond_pe"][0] == pytest.approx(o["bond_pe"], rel=1e-6, abs=1e-9)
+    assert th["temp"][0] == pytest.approx(g["thermo_temp"][0], rel=1e-6)
+    assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
+
+
+@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock"])
+def test_trajectory_10_steps(oracle_mod, name):
+    """After equilibrating 100 steps on the GPU, 10 steps of engine and oracle from the
+    same state: forces within 1e-5 of RMS at every step, thermo rows agree."""
+    s = _systems()[name]
+    run_in = s.run_in.replace("thermo 100", "thermo 1").replace("thermo 1000", "thermo 1")
+    s.run_in = run_in
+    e = _engine_from(s)
+    e.run(100)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    tags = np.arange(1, s.n + 1)
+    L = _box(e)
+    for k in range(1, 11):
+        e.run(1)
+        got = e.state()
+        o = oracle_mod.run(ff, tags, s.types, st["x"], st["v"], s.lo, L, 101, k, 1, bonds=s.bonds,
+                           zero_step=True)
+        assert force_err(got["f"], o["f"]) < FORCE_TOL, k
+        dx = got["x"] - o["x"]
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < 1e-4
+    th = e.thermo()
+    ot = o["thermo"]
+    n = len(ot["temp"])
+    np.testing.assert_allclose(th["temp"][-n:], ot["temp"], rtol=1e-5)
+    np.testing.assert_allclose(th["pair_pe"][-n:], ot["pair_pe"], rtol=1e-5)
+    np.testing.assert_allclose(th["pressure"][-n:], ot["pressure"], rtol=1e-4)
+    # momentum is conserved (FP64 drift check): initial net momentum ~ 0
+    assert np.abs(th["momentum"]).max() < 1e-3 * np.sqrt(s.n)
+
+
+def test_mdpd_density_vs_oracle(oracle_mod):
+    s = _systems()["mdpd"]
+    e = _engine_from(s)
+    e.run(0)
+    st = e.state()
+    rho = e.density()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, st["x"], st["v"], s.lo, _box(e), 0)
+    assert np.abs(rho - o["rho"]).max() < 1e-5 * max(1.0, np.abs(o["rho"]).max())
+
+
+def test_fene_bonds_vs_oracle(oracle_mod):
+    from gpumdpd_b200 import inputs
+    s = inputs.diblock_melt(L=10.0, seed=9, nsteps=10, bond_step=0.7)
+    s.run_in = s.run_in.replace("bond_style harmonic", "bond_style fene").replace(
+        "bond_coeff 1 4.0 0.0", "bond_coeff 1 30.0 1.5 1.0 0.8")
+    e = _engine_from(s)
+    e.run(0)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, st["x"], st["v"], s.lo, _box(e), 0,
+                          bonds=s.bonds)
+    assert force_err(st["f"], o["f"]) < FORCE_TOL
+    assert e.thermo()["bond_pe"][0] == pytest.approx(o["bond_pe"], rel=1e-5)
+
+
+def test_batch_equals_single(oracle_mod):
+    """Uneven replicas packed in one engine give the same results as each alone."""
+    from gpumdpd_b200 import Batch, inputs
+    systems = [inputs.binary_mixture(L, a, seed=10 + k, nsteps=20) for k, (L, a) in
+               enumerate([(5.0, 25.0), (7.3, 30.0), (6.1, 45.0), (9.0, 35.0)])]
+    b = Batch([s.run_in for s in systems], [s.c_system() for s in systems])
+    b.run(20)
+    for r, s in enumerate(systems):
+        e = _engine_from(s)
+        e.run(20)
+        a, c = e.state(), b.state(r)
+        assert force_err(c["f"], a["f"]) < 1e-4
+        dx = c["x"] - a["x"]
+        L = _box(e)
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < 1e-4
+        ta, tb = e.thermo(), b.thermo(r)
+        np.testing.assert_allclose(tb["temp"], ta["temp"], rtol=1e-4)
+        np.testing.assert_allclose(tb["pressure"], ta["pressure"], rtol=1e-4)
+
+
+def test_rdf_vs_oracle(oracle_mod):
+    from gpumdpd_b200 import inputs
+    s = inputs.binary_mixture(8.0, 30.0, seed=21, nsteps=0, rdf=(3.0, 60, 1))
+    e = _engine_from(s)
+    e.run(0)
+    g, ns = e.rdf(60)
+    assert ns == 1
+    st = e.state()
+    go = oracle_mod.rdf(s.types, st["x"], s.lo, _box(e), 1, 2, 3.0, 60)
+    np.testing.assert_allclose(g, go, rtol=1e-6, atol=1e-9)
+
+
+def test_long_run_statistics_vs_oracle(oracle_mod):
+    """Mean T and P over 600 steps after 200 of equilibration agree with the oracle's
+    own trajectory within statistical error (block averages)."""
+    from gpumdpd_b200 import inputs
+    s = inputs.plain_dpd(L=8.0, seed=31, nsteps=800, thermo=10)
+    e = _engine_from(s)
+    e.run(800)
+    th = e.thermo()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.run(ff, np.arange(1, s.n + 1), s.types, s.x, s.v, s.lo, _box(e), 1, 800, 10)
+    sel = th["step"] >= 200
+    osel = o["thermo"]["step"] >= 200
+    for key in ("temp", "pressure"):
+        a, b = th[key][sel], o["thermo"][key][osel]
+        err = np.sqrt(a.var() / (len(a) / 5) + b.var() / (len(b) / 5)) + 1e-12
+        assert abs(a.mean() - b.mean()) < 4 * err, key
+
+
+def test_overflow_is_reported_not_silent():
+    """A neighbour capacity below need is an error status, never a silent truncation."""
+    from gpumdpd_b200 import DpdError, inputs
+    s = inputs.plain_dpd(L=8.0, seed=3, max_rho=0.2)
+    e = _engine_from(s)
+    with pytest.raises(DpdError) as ex:
+        e.run(0)
+    assert ex.value.code == -5
+
+
+def test_restart_continues_step_counter():
+    """Two run() calls equal one run() of the same total length (Saru keyed on the step)."""
+    from gpumdpd_b200 import inputs
+    s = inputs.plain_dpd(L=8.0, seed=41, nsteps=20, thermo=1)
+    a = _engine_from(s)
+    a.run(20)
+    b = _engine_from(s)
+    b.run(7)
+    b.run(13)
+    xa, xb = a.state()["x"], b.state()["x"]
+    L = _box(a)
+    d = xa - xb
+    d -= L * np.round(d / L)
+    assert np.abs(d).max() < 1e-4
+    assert list(b.thermo()["step"]) == list(range(21))
