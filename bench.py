@@ -33,6 +33,8 @@ def make_system(args):
     from gpumdpd_b200 import inputs
     if args.workload == "melt":
         return inputs.diblock_melt(L=100.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
+    if args.workload == "melt_mid":
+        return inputs.diblock_melt(L=60.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
     if args.workload == "melt_small":
         return inputs.diblock_melt(L=30.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
     if args.workload == "plain":
@@ -283,7 +285,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="melt", choices=["melt", "melt_small", "plain", "slab"])
+    ap.add_argument("--workload", default="melt", choices=["melt", "melt_mid", "melt_small", "plain", "slab"])
     ap.add_argument("--skin", type=float, default=0.3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

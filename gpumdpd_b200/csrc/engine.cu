@@ -68,7 +68,7 @@ int Engine::layout()
     nmax_ = 16;
     maxb_ = 0;
     int tag_base = 0, coeff_off = 0, mass_off = 0, bond_off = 0, rdf_off = 0;
-    any_mdpd_ = any_dpd_ = small_ = bonds_ = rdf_ = false;
+    any_mdpd_ = any_dpd_ = bonds_ = rdf_ = false;
     for (size_t r = 0; r < reps_.size(); r++) {
         Replica& R = reps_[r];
         RepDesc& d = R.desc;
@@ -91,7 +91,6 @@ int Engine::layout()
             R.box_len[k] = (double)nc * (double)d.w[k];
             d.L[k] = (float)R.box_len[k];
             d.lo[k] = R.sys.lo[k];
-            if (nc < 5) small_ = true;
         }
         const int n = R.sys.n_atoms;
         if (n > DPD_MAX_TAG) {
@@ -177,6 +176,10 @@ int Engine::layout()
         err = "an atom has more than 16 bonds";
         return DPD_E_ARG;
     }
+    if (P_ > DPD_J_MASK) {
+        err = "too many particles in one engine (the list entry holds 27 bits of slot index)";
+        return DPD_E_ARG;
+    }
     return DPD_OK;
 }
 
@@ -193,7 +196,10 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
         return DPD_E_ARG;
     }
     if (tune) tune_ = *tune;
-    if (tune_.cell_order == 0 && !tune) tune_.cell_order = 1;
+    if (!tune) {
+        tune_.cell_order = 1;
+        tune_.pair_variant = 1;
+    }
     int st = layout();
     if (st) return st;
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -222,17 +228,18 @@ int Engine::alloc_and_upload()
     DA(b_.coeff, ncoeff);
     DA(b_.mass, nmass);
     DA(b_.bondc, nbond);
-    DA(b_.pos4, P_);
-    DA(b_.vel4, P_);
+    for (int q = 0; q < 2; q++) {
+        DA(b_.pos[q], P_);
+        DA(b_.vel[q], P_);
+        DA(b_.img[q], P_);
+        DA(b_.bonds[q], (size_t)std::max(maxb_, 1) * P_);
+    }
+    DA(b_.parity, 1);
     DA(b_.force4, P_);
     DA(b_.last4, P_);
-    DA(b_.pos_t, P_);
-    DA(b_.vel_t, P_);
     DA(b_.rho, P_);
-    DA(b_.img, P_);
-    DA(b_.img_t, P_);
-    DA(b_.bonds, (size_t)std::max(maxb_, 1) * P_);
-    DA(b_.bonds_t, (size_t)std::max(maxb_, 1) * P_);
+    DA(b_.cell_rep, C_);
+    DA(b_.cell_lin, C_);
     DA(b_.cnt, C_);
     DA(b_.cstart, C_ + 1);
     DA(b_.fill, C_);
@@ -251,7 +258,7 @@ int Engine::alloc_and_upload()
 #undef DA
     // tables
     std::vector<RepDesc> hd(nrep);
-    std::vector<int> wrep(P_ / 32), crank(C_, 0);
+    std::vector<int> wrep(P_ / 32), crank(C_, 0), cell_rep(C_, 0), cell_lin(C_, -1);
     std::vector<float4> coeff(ncoeff);
     std::vector<float2> mass(nmass);
     std::vector<float4> bondc(nbond);
@@ -260,7 +267,11 @@ int Engine::alloc_and_upload()
         const RepDesc& d = R.desc;
         hd[r] = d;
         for (int wv = d.p_begin / 32; wv < d.p_cap_end / 32; wv++) wrep[wv] = r;
-        for (int c = 0; c < d.ncell; c++) crank[d.c_begin + c] = R.crank[c];
+        for (int c = 0; c < d.ncell; c++) {
+            crank[d.c_begin + c] = R.crank[c];
+            cell_lin[d.c_begin + R.crank[c]] = c;
+        }
+        for (int c = 0; c <= d.ncell; c++) cell_rep[d.c_begin + c] = r;
         const int nt = d.ntypes;
         const double sig_scale = std::sqrt(2.0 * R.ff.temp) / std::sqrt(R.in.dt);
         for (int ti = 0; ti < nt; ti++)
@@ -289,6 +300,8 @@ int Engine::alloc_and_upload()
     CK(cudaMemcpyAsync(b_.reps, hd.data(), sizeof(RepDesc) * nrep, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.warp_rep, wrep.data(), sizeof(int) * wrep.size(), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.crank, crank.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.cell_rep, cell_rep.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.cell_lin, cell_lin.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.coeff, coeff.data(), sizeof(float4) * ncoeff, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.mass, mass.data(), sizeof(float2) * nmass, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.bondc, bondc.data(), sizeof(float4) * nbond, cudaMemcpyHostToDevice, stream_));
@@ -358,10 +371,12 @@ int Engine::upload_particles()
             img[s] = make_int4(0, 0, 0, 0);
         }
     }
-    CK(cudaMemcpyAsync(b_.pos4, pos.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.vel4, vel.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.img, img.data(), sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.bonds, bonds.data(), sizeof(int2) * bonds.size(), cudaMemcpyHostToDevice, stream_));
+    // the state goes into buffer 0, which becomes the current one
+    CK(cudaMemcpyAsync(b_.pos[0], pos.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.vel[0], vel.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.img[0], img.data(), sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.bonds[0], bonds.data(), sizeof(int2) * bonds.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemsetAsync(b_.parity, 0, sizeof(int), stream_));
     CK(cudaMemsetAsync(b_.force4, 0, sizeof(float4) * P_, stream_));
     CK(cudaMemsetAsync(b_.rho, 0, sizeof(float) * P_, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -381,15 +396,16 @@ static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int 
     a.maxb = maxb;
     a.build_flag = b.build_flag;
     a.phase = b.phase;
-    a.pos4 = b.pos4;
-    a.vel4 = b.vel4;
-    a.img = b.img;
-    a.bonds = b.bonds;
+    a.parity = b.parity;
+    a.cell_rep = b.cell_rep;
+    a.cell_lin = b.cell_lin;
+    for (int q = 0; q < 2; q++) {
+        a.buf.pos[q] = b.pos[q];
+        a.buf.vel[q] = b.vel[q];
+        a.buf.img[q] = b.img[q];
+        a.buf.bonds[q] = b.bonds[q];
+    }
     a.last4 = b.last4;
-    a.pos_t = b.pos_t;
-    a.vel_t = b.vel_t;
-    a.img_t = b.img_t;
-    a.bonds_t = b.bonds_t;
     a.cnt = b.cnt;
     a.cstart = b.cstart;
     a.fill = b.fill;
@@ -414,13 +430,16 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     a.coeff = b.coeff;
     a.mass = b.mass;
     a.bondc = b.bondc;
-    a.pos4 = b.pos4;
-    a.vel4 = b.vel4;
+    for (int q = 0; q < 2; q++) {
+        a.buf.pos[q] = b.pos[q];
+        a.buf.vel[q] = b.vel[q];
+        a.buf.img[q] = b.img[q];
+        a.buf.bonds[q] = b.bonds[q];
+    }
+    a.parity = b.parity;
     a.force4 = b.force4;
     a.rho = b.rho;
-    a.img = b.img;
     a.last4 = b.last4;
-    a.bonds = b.bonds;
     a.tag2idx = b.tag2idx;
     a.ncount = b.ncount;
     a.nlist = b.nlist;
@@ -436,16 +455,21 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     return a;
 }
 
-template <int STYLE>
-static void launch_pair(bool small, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
+template <int STYLE, bool BONDS>
+static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& a)
 {
-    if (small) {
-        if (bonds) k_pair<STYLE, true, true><<<grid, 256, 0, s>>>(a);
-        else k_pair<STYLE, true, false><<<grid, 256, 0, s>>>(a);
-    } else {
-        if (bonds) k_pair<STYLE, false, true><<<grid, 256, 0, s>>>(a);
-        else k_pair<STYLE, false, false><<<grid, 256, 0, s>>>(a);
-    }
+    if (variant == 0) k_pair<STYLE, BONDS><<<grid, 256, 0, s>>>(a);
+    else if (variant == 2) k_pair_q<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
+    else k_pair_q<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
+}
+
+// pair_variant 0: thread per particle; 1 (default): warp pair-queue, 4 blocks/SM;
+// 2: warp pair-queue, 3 blocks/SM (more registers)
+template <int STYLE>
+static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
+{
+    if (bonds) launch_pair2<STYLE, true>(variant, grid, s, a);
+    else launch_pair2<STYLE, false>(variant, grid, s, a);
 }
 
 void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
@@ -463,16 +487,14 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     k_scatter<<<gp, 256, 0, s>>>(ba);
     k_cell_sort<<<gc, 256, 0, s>>>(ba);
     k_permute<<<gp, 256, 0, s>>>(ba);
+    k_flip<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
     k_build_nlist<<<gp, 256, 0, s>>>(ba);
-    k_build_done<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
-    if (any_mdpd_) {
-        if (small_) k_density<true><<<gp, 256, 0, s>>>(sa);
-        else k_density<false><<<gp, 256, 0, s>>>(sa);
-    }
-    if (ev0) cudaEventRecord(ev0, s);
-    if (any_dpd_) launch_pair<0>(small_, bonds_, gp, s, sa);
-    if (any_mdpd_) launch_pair<1>(small_, bonds_, gp, s, sa);
-    if (ev1) cudaEventRecord(ev1, s);
+    if (any_mdpd_) k_density<<<gp, 256, 0, s>>>(sa);
+    if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
+    const int variant = tune_.pair_variant;
+    if (any_dpd_) launch_pair<0>(variant, bonds_, gp, s, sa);
+    if (any_mdpd_) launch_pair<1>(variant, bonds_, gp, s, sa);
+    if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
     if (rdf_) k_rdf<<<gp, 256, 0, s>>>(sa);
     k_integrate<<<gp, 256, 0, s>>>(sa);
     k_advance<<<(nrep + 255) / 256, 256, 0, s>>>(sa);
@@ -677,18 +699,28 @@ int Engine::get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows)
     return DPD_OK;
 }
 
+int Engine::cur_parity()
+{
+    int par = 0;
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) return -1;
+    if (cudaMemcpy(&par, b_.parity, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return par & 1;
+}
+
 int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
 {
     if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
     const RepDesc& d = reps_[rep].desc;
+    const Replica& R = reps_[rep];
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<float4> pos(ns), vel(ns), frc(ns);
     std::vector<int4> img(ns);
-    CK(cudaStreamSynchronize(stream_));
-    CK(cudaMemcpyAsync(pos.data(), b_.pos4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    const int par = cur_parity();
+    if (par < 0) return cuda_fail(cudaGetLastError(), "cudaMemcpy(parity)");
+    CK(cudaMemcpyAsync(pos.data(), b_.pos[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(frc.data(), b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(img.data(), b_.img + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(img.data(), b_.img[par] + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     for (int k = 0; k < d.n_real; k++) {
         int tw;
@@ -707,10 +739,17 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
         const float ff[3] = {frc[k].x, frc[k].y, frc[k].z};
         const int im[3] = {img[k].x, img[k].y, img[k].z};
         for (int q = 0; q < 3; q++) {
-            if (x) x[o + q] = d.lo[q] + (double)c[q] * (double)d.w[q] + (double)off[q];
+            // exact position of the FP32 state; offsets may have drifted past the cell
+            // (and the box) since the last build, so wrap into [lo, lo + L)
+            double xa = (double)c[q] * (double)d.w[q] + (double)off[q];
+            const double L = R.box_len[q];
+            const double wrap = std::floor(xa / L);
+            xa -= wrap * L;
+            if (xa >= L) xa -= L;
+            if (x) x[o + q] = d.lo[q] + xa;
             if (v) v[o + q] = vv[q];
             if (f) f[o + q] = ff[q];
-            if (image) image[o + q] = im[q];
+            if (image) image[o + q] = im[q] + (int)wrap;
         }
     }
     return DPD_OK;
@@ -727,7 +766,7 @@ int Engine::set_state(int rep, const double* x, const double* v)
     if (x) memcpy(R.sys.x.data(), x, sizeof(double) * xv.size()); else R.sys.x = xv;
     if (v) memcpy(R.sys.v.data(), v, sizeof(double) * vv.size()); else R.sys.v = vv;
     // full re-upload of every replica's particles (the host copies of the others are
-    // refreshed first), then a forced list build at the next step
+    // refreshed first); the next run starts with a zero step and a list build
     for (int r = 0; r < (int)reps_.size(); r++) {
         if (r == rep) continue;
         Replica& Q = reps_[r];
@@ -747,9 +786,10 @@ int Engine::get_density(int rep, double* rho)
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<float> r(ns);
     std::vector<float4> vel(ns);
-    CK(cudaStreamSynchronize(stream_));
+    const int par = cur_parity();
+    if (par < 0) return cuda_fail(cudaGetLastError(), "cudaMemcpy(parity)");
     CK(cudaMemcpyAsync(r.data(), b_.rho + d.p_begin, sizeof(float) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     for (int k = 0; k < d.n_real; k++) {
         int tw;
@@ -766,9 +806,10 @@ int Engine::get_cells(int rep, int* cell, float* off, int* nc, float* w, float* 
     const RepDesc& d = reps_[rep].desc;
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<float4> pos(ns), vel(ns);
-    CK(cudaStreamSynchronize(stream_));
-    CK(cudaMemcpyAsync(pos.data(), b_.pos4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(vel.data(), b_.vel4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    const int par = cur_parity();
+    if (par < 0) return cuda_fail(cudaGetLastError(), "cudaMemcpy(parity)");
+    CK(cudaMemcpyAsync(pos.data(), b_.pos[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     for (int k = 0; k < d.n_real; k++) {
         int tw, code;
@@ -803,10 +844,11 @@ int Engine::get_neighbors(int rep, int* pairs, int64_t cap, int64_t* n_pairs)
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<int> cnt(ns), lst((size_t)ns * nmax_);
     std::vector<float4> vel(P_);
-    CK(cudaStreamSynchronize(stream_));
+    const int par = cur_parity();
+    if (par < 0) return cuda_fail(cudaGetLastError(), "cudaMemcpy(parity)");
     CK(cudaMemcpyAsync(cnt.data(), b_.ncount + d.p_begin, sizeof(int) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(lst.data(), b_.nlist + (size_t)d.p_begin * nmax_, sizeof(int) * lst.size(), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(vel.data(), b_.vel4, sizeof(float4) * P_, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel.data(), b_.vel[par], sizeof(float4) * P_, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     auto tag_at = [&](int s) {
         int tw;
@@ -818,7 +860,7 @@ int Engine::get_neighbors(int rep, int* pairs, int64_t cap, int64_t* n_pairs)
         const int s = d.p_begin + k;
         const int c = std::min(cnt[k], nmax_);
         for (int q = 0; q < c; q++) {
-            const int j = lst[((size_t)(k >> 5) * nmax_ + q) * 32 + (k & 31)];
+            const int j = lst[((size_t)(k >> 5) * nmax_ + q) * 32 + (k & 31)] & DPD_J_MASK;
             if (j < 0 || j >= P_) continue;
             int a = tag_at(s), bb = tag_at(j);
             if (np < cap && pairs) {

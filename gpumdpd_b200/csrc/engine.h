@@ -30,11 +30,14 @@ struct DeviceBuffers {
     float4* coeff = nullptr;
     float2* mass = nullptr;
     float4* bondc = nullptr;
-    float4 *pos4 = nullptr, *vel4 = nullptr, *force4 = nullptr, *last4 = nullptr;
-    float4 *pos_t = nullptr, *vel_t = nullptr;
+    float4* pos[2] = {nullptr, nullptr};  // double-buffered by *parity
+    float4* vel[2] = {nullptr, nullptr};
+    int4* img[2] = {nullptr, nullptr};
+    int2* bonds[2] = {nullptr, nullptr};
+    int* parity = nullptr;
+    float4 *force4 = nullptr, *last4 = nullptr;
     float* rho = nullptr;
-    int4 *img = nullptr, *img_t = nullptr;
-    int2 *bonds = nullptr, *bonds_t = nullptr;
+    int *cell_rep = nullptr, *cell_lin = nullptr;
     int *cnt = nullptr, *cstart = nullptr, *fill = nullptr, *perm = nullptr, *tag2idx = nullptr;
     int *ncount = nullptr, *nlist = nullptr, *blocksum = nullptr;
     double *acc = nullptr, *ring = nullptr;
@@ -89,6 +92,7 @@ private:
     void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
+    int cur_parity();
     int cuda_fail(cudaError_t e, const char* what);
     template <class T> int dalloc(T** p, size_t n);
 
@@ -98,7 +102,7 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     int P_ = 0, C_ = 0, nmax_ = 16, maxb_ = 0;
-    bool any_mdpd_ = false, any_dpd_ = false, small_ = false, bonds_ = false, rdf_ = false;
+    bool any_mdpd_ = false, any_dpd_ = false, bonds_ = false, rdf_ = false;
     bool zero_pending_ = true;
     uint32_t next_step_ = 0;
     std::vector<void*> allocs_;

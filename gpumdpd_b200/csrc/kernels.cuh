@@ -1,18 +1,27 @@
-// kernels.cuh -- sm_100a kernels of the DPD timestep.
+// kernels.cuh -- sm_100a kernels of the neighbour-list build, plus shared helpers.
 //
-// Particle layout (packed over replicas; each replica owns a warp-aligned slot range):
-//   pos4[s]  = {ox, oy, oz, cell code}  offsets in [0,w) inside cell (cx,cy,cz), the
-//              code packs cx | cy<<10 | cz<<20 (replica-local cell coordinates)
-//   vel4[s]  = {vx, vy, vz, tag<<5 | (type-1)}
-//   force4[s]= {fx, fy, fz, 0}         accumulated with vector atomics
-//   img[s]   = image counters
-// Slots are sorted by cell (counting sort at every neighbour-list build), cells in
-// linear or Morton order.  The half neighbour list is warp-chunked:
-//   nlist[((s>>5)*nmax + k)*32 + (s&31)]  (k-th neighbour of slot s).
+// Particle layout (packed over replicas; each replica owns a warp-aligned slot range),
+// double-buffered by a device-side parity bit (the list build permutes into the other
+// buffer and flips it):
+//   pos[s]   = {ox, oy, oz, cell code}  offsets relative to cell (cx,cy,cz); the code
+//              packs cx | cy<<10 | cz<<20 (replica-local).  Cells are assigned at a list
+//              build and kept until the next one, so offsets may drift slightly outside
+//              [0,w) in between; a build re-bins every particle.
+//   vel[s]   = {vx, vy, vz, tag<<5 | (type-1)}
+//   force4[s]= {fx, fy, fz, 0}           accumulated with vector atomics
+//   img[s]   = image counters (updated when a build re-bins across the box)
+// Slots are sorted by cell (counting sort at every build; cells in linear or Morton
+// order; within a cell by tag).  The half neighbour list is warp-chunked,
+//   nlist[((s>>5)*nmax + k)*32 + (s&31)] = j | code<<27,
+// where code = 9(dcx+1)+3(dcy+1)+(dcz+1) encodes the cell difference c_i - c_j in
+// {-1,0,1}^3 of the pair at build time; the displacement is (o_i - o_j) + code*w.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "dpd_common.h"
+
+#define DPD_J_MASK 0x07FFFFFF
+#define DPD_CODE_SHIFT 27
 
 // ---------------------------------------------------------------------------------
 // Saru counter-based RNG.  The stream must be bit-identical to the reference's
@@ -69,18 +78,15 @@ __device__ __forceinline__ int wrap_dc(int dc, int nc)
     return dc;
 }
 
-// displacement p_i - p_j in the cell-offset representation; `small` applies a
-// position-level minimum image (needed only when a grid has fewer than 5 cells)
-template <bool SMALL>
+// General displacement p_i - p_j between any two particles (bonds, RDF, skin check):
+// cell difference wrapped to the grid, then a position-level minimum image.
 __device__ __forceinline__ float disp1(int ci, int cj, float oi, float oj, int nc, float w, float L)
 {
     int dc = wrap_dc(ci - cj, nc);
     float d = __fmaf_rn(__int2float_rn(dc), w, __fsub_rn(oi, oj));
-    if (SMALL) {
-        float h = 0.5f * L;
-        d -= (d >= h) ? L : 0.0f;
-        d += (d < -h) ? L : 0.0f;
-    }
+    float h = 0.5f * L;
+    d -= (d >= h) ? L : 0.0f;
+    d += (d < -h) ? L : 0.0f;
     return d;
 }
 
@@ -128,29 +134,32 @@ __device__ __forceinline__ void acc_flush(double (&val)[NV], const int* field, i
 }
 
 // ---------------------------------------------------------------------------------
-// Neighbour-list build: counting sort of slots by cell, stable per-cell order by tag,
-// permutation of particle arrays, then the half list.  All kernels return at once
-// unless the build flag of this phase is set.
+// Double-buffered particle arrays; `par` selects the current buffer.
+struct PBuf {
+    float4* pos[2];
+    float4* vel[2];
+    int4* img[2];
+    int2* bonds[2];
+};
 
+// Neighbour-list build: counting sort of slots by (re-binned) cell, per-cell order by
+// tag, permutation into the other buffer, parity flip, then the half list.  All
+// kernels return at once unless the build flag of this phase is set.
 struct BuildArgs {
     const RepDesc* reps;
     const int* warp_rep;
     const int* crank;       // [cells] linear cell -> position in the replica's cell order
+    const int* cell_rep;    // [cells] replica of a cell key
+    const int* cell_lin;    // [cells] linear index of a cell key (-1: ghost cell)
     int P;                  // total slots
     int C;                  // total cells (all replicas, ghost cells included)
     int nmax;               // neighbour list capacity per slot
     int maxb;               // bond partners per slot
     const int* build_flag;  // [2]
     const uint32_t* phase;
-    float4* pos4;
-    float4* vel4;
-    int4* img;
-    int2* bonds;
+    int* parity;
+    PBuf buf;
     float4* last4;
-    float4* pos_t;
-    float4* vel_t;
-    int4* img_t;
-    int2* bonds_t;
     int* cnt;
     int* cstart;            // [C+1]
     int* fill;
@@ -167,6 +176,42 @@ __device__ __forceinline__ bool build_on(const BuildArgs& a)
     return a.build_flag[(*a.phase) & 1] != 0;
 }
 
+// Re-bin a particle: move whole cell widths from the offset into the cell index,
+// wrapping the cell grid and counting images.  Returns false for a non-finite offset.
+__device__ __forceinline__ bool rebin(const RepDesc& d, float4& p, int dimg[3])
+{
+    int code = __float_as_int(p.w);
+    int c[3] = {cell_x(code), cell_y(code), cell_z(code)};
+    float o[3] = {p.x, p.y, p.z};
+    bool ok = true, moved = false;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        dimg[k] = 0;
+        if (!(o[k] >= 0.0f && o[k] < d.w[k])) {
+            if (!isfinite(o[k])) {
+                ok = false;
+                o[k] = 0.0f;
+                continue;
+            }
+            float q = floorf(o[k] * d.inv_w[k]);
+            q = fminf(fmaxf(q, -1.0e6f), 1.0e6f);
+            o[k] = __fmaf_rn(-q, d.w[k], o[k]);
+            int cc = c[k] + (int)q;
+            const int nc = d.nc[k];
+            const int wrap = cc >= 0 ? cc / nc : -((-cc + nc - 1) / nc);
+            cc -= wrap * nc;
+            dimg[k] = wrap;
+            c[k] = cc;
+            if (o[k] >= d.w[k]) o[k] = __int_as_float(__float_as_int(d.w[k]) - 1);
+            if (o[k] < 0.0f) o[k] = 0.0f;
+            moved = true;
+        }
+    }
+    if (moved) code = cell_pack(c[0], c[1], c[2]);
+    p = make_float4(o[0], o[1], o[2], __int_as_float(code));
+    return ok;
+}
+
 __device__ __forceinline__ int cell_key(const BuildArgs& a, const RepDesc& d, int code, bool ghost)
 {
     if (ghost) return d.c_begin + d.ncell;
@@ -174,15 +219,22 @@ __device__ __forceinline__ int cell_key(const BuildArgs& a, const RepDesc& d, in
     return d.c_begin + a.crank[d.c_begin + lin];
 }
 
+__device__ __forceinline__ int slot_key(const BuildArgs& a, int s, int par)
+{
+    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
+    if (s >= d.p_end) return d.c_begin + d.ncell;
+    float4 p = a.buf.pos[par][s];
+    int dimg[3];
+    rebin(d, p, dimg);
+    return cell_key(a, d, __float_as_int(p.w), false);
+}
+
 __global__ void k_bin_count(BuildArgs a)
 {
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
-    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
-    bool ghost = s >= d.p_end;
-    int key = cell_key(a, d, __float_as_int(a.pos4[s].w), ghost);
-    atomicAdd(&a.cnt[key], 1);
+    atomicAdd(&a.cnt[slot_key(a, s, *a.parity)], 1);
 }
 
 // exclusive scan of cnt[0..C) into cstart[0..C], three passes (block scan of 4096
@@ -221,7 +273,6 @@ __global__ void k_scan_sums(BuildArgs a, int nblocks)
 {
     if (!build_on(a)) return;
     __shared__ int sh[1024];
-    // sequential chunks of 1024 block sums (nblocks <= 1024*64 supported)
     int carry = 0;
     for (int base = 0; base < nblocks; base += 1024) {
         int idx = base + threadIdx.x;
@@ -254,9 +305,7 @@ __global__ void k_scatter(BuildArgs a)
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
-    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
-    bool ghost = s >= d.p_end;
-    int key = cell_key(a, d, __float_as_int(a.pos4[s].w), ghost);
+    const int key = slot_key(a, s, *a.parity);
     int pos = a.cstart[key] + atomicAdd(&a.fill[key], 1);
     if (pos >= 0 && pos < a.P) a.perm[pos] = s;
 }
@@ -271,13 +320,14 @@ __global__ void k_cell_sort(BuildArgs a)
     a.cnt[c] = 0;
     a.fill[c] = 0;
     if (b < 0 || e > a.P) return;
+    const float4* vel = a.buf.vel[*a.parity];
     for (int i = b + 1; i < e; i++) {
         int si = a.perm[i];
-        int ti = tag_of(a.vel4[si].w);
+        int ti = tag_of(vel[si].w);
         int j = i - 1;
         while (j >= b) {
             int sj = a.perm[j];
-            if (tag_of(a.vel4[sj].w) <= ti) break;
+            if (tag_of(vel[sj].w) <= ti) break;
             a.perm[j + 1] = sj;
             j--;
         }
@@ -285,23 +335,42 @@ __global__ void k_cell_sort(BuildArgs a)
     }
 }
 
+// gather into the other buffer, re-binning positions; the new positions are also the
+// reference positions of the displacement check (last4)
 __global__ void k_permute(BuildArgs a)
 {
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
+    const int par = *a.parity, nxt = par ^ 1;
+    const int r = a.warp_rep[s >> 5];
+    const RepDesc& d = a.reps[r];
     int o = a.perm[s];
-    float4 p = a.pos4[o];
-    float4 v = a.vel4[o];
-    a.pos_t[s] = p;
-    a.vel_t[s] = v;
-    a.img_t[s] = a.img[o];
-    for (int k = 0; k < a.maxb; k++) a.bonds_t[(size_t)k * a.P + s] = a.bonds[(size_t)k * a.P + o];
-    const RepDesc& d = a.reps[a.warp_rep[s >> 5]];
+    float4 p = a.buf.pos[par][o];
+    float4 v = a.buf.vel[par][o];
+    int4 im = a.buf.img[par][o];
     if (s < d.p_end) {
+        int dimg[3];
+        if (!rebin(d, p, dimg)) atomicOr(&a.rstate[r].status, ST_NONFINITE);
+        im.x += dimg[0];
+        im.y += dimg[1];
+        im.z += dimg[2];
         int t = tag_of(v.w);
         if (t >= 1 && t <= d.n_real) a.tag2idx[d.tag_base + t - 1] = s;
     }
+    a.buf.pos[nxt][s] = p;
+    a.buf.vel[nxt][s] = v;
+    a.buf.img[nxt][s] = im;
+    a.last4[s] = p;
+    for (int k = 0; k < a.maxb; k++) a.buf.bonds[nxt][(size_t)k * a.P + s] = a.buf.bonds[par][(size_t)k * a.P + o];
+}
+
+__global__ void k_flip(BuildArgs a, int nrep)
+{
+    if (!build_on(a)) return;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep) a.rstate[r].nbuild++;
+    if (r == 0) *a.parity ^= 1;
 }
 
 // half stencil: the 13 cell offsets with (oz>0) | (oz==0 & oy>0) | (oz==0 & oy==0 & ox>0)
@@ -309,52 +378,75 @@ __constant__ int8_t c_half[13][3] = {
     {1, 0, 0}, {-1, 1, 0}, {0, 1, 0}, {1, 1, 0}, {-1, -1, 1}, {0, -1, 1}, {1, -1, 1},
     {-1, 0, 1}, {0, 0, 1}, {1, 0, 1}, {-1, 1, 1}, {0, 1, 1}, {1, 1, 1}};
 
-__global__ void k_build_nlist(BuildArgs a)
+// Half list, one thread per particle (slots in cell order, so a warp's lanes share
+// most stencil cells through L1).  Candidates are the own cell's later slots (j > i)
+// and the 13 forward cells; all 14 cell ranges are loaded first and each cell's slots
+// are read 4 at a time so several loads are in flight per thread.  The predicate is
+// r2 = fma(dz,dz,fma(dy,dy,dx*dx)) <= (global_cut+skin)^2 in float with
+// d = (o_i - o_j) + (c_i - c_j) w, the reference's test (src/force/neigh_list.cu:373-382)
+// on the cell-offset representation.  Entries store j and the shift code of the pair.
+__global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
 {
     if (!build_on(a)) return;
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
-    float4 pi = a.pos_t[s];
-    // copy the permuted arrays back (the list is built from the permuted copy)
-    a.pos4[s] = pi;
-    a.vel4[s] = a.vel_t[s];
-    a.img[s] = a.img_t[s];
-    a.last4[s] = pi;
-    for (int k = 0; k < a.maxb; k++) a.bonds[(size_t)k * a.P + s] = a.bonds_t[(size_t)k * a.P + s];
     if (s >= d.p_end) {
         a.ncount[s] = 0;
         return;
     }
+    const float4* pos = a.buf.pos[*a.parity];
+    const float4 pi = pos[s];
     const int code = __float_as_int(pi.w);
     const int cx = cell_x(code), cy = cell_y(code), cz = cell_z(code);
     const int ncx = d.nc[0], ncy = d.nc[1], ncz = d.nc[2];
     const float cut2 = d.cut2;
+    const float wx = d.w[0], wy = d.w[1], wz = d.w[2];
     int* out = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
     int count = 0;
-    // own cell, j > s
-    for (int st = -1; st < 13; st++) {
-        int ox = 0, oy = 0, oz = 0;
-        if (st >= 0) { ox = c_half[st][0]; oy = c_half[st][1]; oz = c_half[st][2]; }
+    int jb[14], je[14];
+#pragma unroll
+    for (int st = 0; st < 14; st++) {
+        const int ox = st ? c_half[st - 1][0] : 0, oy = st ? c_half[st - 1][1] : 0, oz = st ? c_half[st - 1][2] : 0;
         int nx = cx + ox; nx += nx < 0 ? ncx : 0; nx -= nx >= ncx ? ncx : 0;
         int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
         int nz = cz + oz; nz += nz < 0 ? ncz : 0; nz -= nz >= ncz ? ncz : 0;
-        int key = d.c_begin + a.crank[d.c_begin + (nx * ncy + ny) * ncz + nz];
-        int jb = a.cstart[key], je = a.cstart[key + 1];
-        if (st < 0) jb = s + 1;
-        for (int j = jb; j < je; j++) {
-            float4 pj = a.pos_t[j];
-            // p_i - p_j = (c_i - c_j) w + (o_i - o_j) with c_j = c_i + (ox,oy,oz)
-            float dx = __fmaf_rn(__int2float_rn(-ox), d.w[0], __fsub_rn(pi.x, pj.x));
-            float dy = __fmaf_rn(__int2float_rn(-oy), d.w[1], __fsub_rn(pi.y, pj.y));
-            float dz = __fmaf_rn(__int2float_rn(-oz), d.w[2], __fsub_rn(pi.z, pj.z));
-            float r2 = __fmul_rn(dx, dx);
-            r2 = __fmaf_rn(dy, dy, r2);
-            r2 = __fmaf_rn(dz, dz, r2);
-            if (r2 <= cut2) {
-                if (count < a.nmax) out[(size_t)count * 32] = j;
-                count++;
+        jb[st] = d.c_begin + __ldg(a.crank + d.c_begin + (nx * ncy + ny) * ncz + nz);
+    }
+#pragma unroll
+    for (int st = 0; st < 14; st++) {
+        const int key = jb[st];
+        jb[st] = __ldg(a.cstart + key);
+        je[st] = __ldg(a.cstart + key + 1);
+    }
+    jb[0] = s + 1;
+#pragma unroll
+    for (int st = 0; st < 14; st++) {
+        const int ox = st ? c_half[st - 1][0] : 0, oy = st ? c_half[st - 1][1] : 0, oz = st ? c_half[st - 1][2] : 0;
+        // (c_i - c_j) w with c_j = c_i + (ox,oy,oz): exact multiples of w
+        const float sx = __int2float_rn(-ox) * wx, sy = __int2float_rn(-oy) * wy, sz = __int2float_rn(-oz) * wz;
+        const int tagbits = ((1 - ox) * 9 + (1 - oy) * 3 + (1 - oz)) << DPD_CODE_SHIFT;
+        const int e = je[st];
+        for (int j0 = jb[st]; j0 < e; j0 += 4) {
+            float4 pj[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (j0 + u < e) pj[u] = pos[j0 + u];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (j0 + u < e) {
+                    const float dx = __fadd_rn(__fsub_rn(pi.x, pj[u].x), sx);
+                    const float dy = __fadd_rn(__fsub_rn(pi.y, pj[u].y), sy);
+                    const float dz = __fadd_rn(__fsub_rn(pi.z, pj[u].z), sz);
+                    float r2 = __fmul_rn(dx, dx);
+                    r2 = __fmaf_rn(dy, dy, r2);
+                    r2 = __fmaf_rn(dz, dz, r2);
+                    if (r2 <= cut2) {
+                        if (count < a.nmax) out[(size_t)count * 32] = (j0 + u) | tagbits;
+                        count++;
+                    }
+                }
             }
         }
     }
@@ -363,11 +455,4 @@ __global__ void k_build_nlist(BuildArgs a)
         count = a.nmax;
     }
     a.ncount[s] = count;
-}
-
-__global__ void k_build_done(BuildArgs a, int nrep)
-{
-    if (!build_on(a)) return;
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < nrep) a.rstate[r].nbuild++;
 }

@@ -13,13 +13,11 @@ struct StepArgs {
     const float4* coeff;   // 3 float4 per ordered type pair, per replica
     const float2* mass;    // (m, 1/m) per type, per replica
     const float4* bondc;   // per bond type, per replica: harmonic {k, r0}; fene {K, R0, eps, sigma}
-    float4* pos4;
-    float4* vel4;
+    PBuf buf;
+    const int* parity;
     float4* force4;
     float* rho;
-    int4* img;
     const float4* last4;
-    const int2* bonds;
     const int* tag2idx;
     const int* ncount;
     const int* nlist;
@@ -36,46 +34,72 @@ struct StepArgs {
 
 __device__ __forceinline__ bool rep_active(const RepState& st) { return st.step <= st.target; }
 
-// ---------------------------------------------------------------------------------
-// displacement between two slots (cell-offset representation)
-template <bool SMALL>
+// displacement between two arbitrary particles (bonds, RDF)
 __device__ __forceinline__ void disp3(const RepDesc& d, int ci, float4 pi, float4 pj, float& dx,
                                       float& dy, float& dz)
 {
     const int cj = __float_as_int(pj.w);
-    dx = disp1<SMALL>(cell_x(ci), cell_x(cj), pi.x, pj.x, d.nc[0], d.w[0], d.L[0]);
-    dy = disp1<SMALL>(cell_y(ci), cell_y(cj), pi.y, pj.y, d.nc[1], d.w[1], d.L[1]);
-    dz = disp1<SMALL>(cell_z(ci), cell_z(cj), pi.z, pj.z, d.nc[2], d.w[2], d.L[2]);
+    dx = disp1(cell_x(ci), cell_x(cj), pi.x, pj.x, d.nc[0], d.w[0], d.L[0]);
+    dy = disp1(cell_y(ci), cell_y(cj), pi.y, pj.y, d.nc[1], d.w[1], d.L[1]);
+    dz = disp1(cell_z(ci), cell_z(cj), pi.z, pj.z, d.nc[2], d.w[2], d.L[2]);
+}
+
+// per-warp table of the 27 cell shifts (c_i - c_j) * w of a replica
+__device__ __forceinline__ void fill_shift(float4* tab, const RepDesc& d, int lane)
+{
+    if (lane < 27) {
+        const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+        tab[lane] = make_float4(__int2float_rn(dx) * d.w[0], __int2float_rn(dy) * d.w[1],
+                                __int2float_rn(dz) * d.w[2], 0.0f);
+    }
+}
+
+// displacement of a listed pair: (o_i - o_j) + (c_i - c_j) w, bit-identical to the
+// list predicate
+__device__ __forceinline__ void pair_disp(const float4* tab, int ent, float4 pi, float4 pj, float& dx,
+                                          float& dy, float& dz)
+{
+    const float4 sh = tab[(uint32_t)ent >> DPD_CODE_SHIFT];
+    dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sh.x);
+    dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sh.y);
+    dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sh.z);
 }
 
 // ---------------------------------------------------------------------------------
 // mDPD local density, src/force/pair_mdpd.cu:219-300: rho_i = sum_j 15/(2 pi rd^3)
 // max(0, 1-r/rd)^2 over the half list, both sides.
-template <bool SMALL>
 __global__ void __launch_bounds__(256) k_density(StepArgs a)
 {
+    __shared__ float4 tab[8][27];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
-    if (!rep_active(a.rstate[r]) || s >= d.p_end) return;
-    const float4 pi = a.pos4[s];
-    const int ci = __float_as_int(pi.w);
-    const int ti = type0_of(a.vel4[s].w);
+    if (!rep_active(a.rstate[r]) || d.style != 1) return;  // warp-uniform
+    fill_shift(tab[warp], d, lane);
+    __syncwarp();
+    if (s >= d.p_end) return;
+    const int par = *a.parity;
+    const float4* pos = a.buf.pos[par];
+    const float4* vel = a.buf.vel[par];
+    const float4 pi = pos[s];
+    const int ti = type0_of(vel[s].w);
     const float4* crow = a.coeff + d.coeff_off + ti * d.ntypes * 3;
     const int n = min(a.ncount[s], a.nmax);
-    const int* lst = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+    const int* lst = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + lane;
     float rho_i = 0.0f;
     for (int k = 0; k < n; k++) {
-        const int j = __ldg(lst + (size_t)k * 32);
-        const float4 pj = __ldg(a.pos4 + j);
+        const int ent = __ldg(lst + (size_t)k * 32);
+        const int j = ent & DPD_J_MASK;
+        const float4 pj = __ldg(pos + j);
         float dx, dy, dz;
-        disp3<SMALL>(d, ci, pi, pj, dx, dy, dz);
+        pair_disp(tab[warp], ent, pi, pj, dx, dy, dz);
         const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-        const int tj = type0_of(__ldg(&a.vel4[j].w));
-        const float4 c1 = __ldg(crow + tj * 3 + 1);
+        const int tj = type0_of(__ldg(&vel[j].w));
         const float4 c2 = __ldg(crow + tj * 3 + 2);
         if (r2 < c2.x) {
+            const float4 c1 = __ldg(crow + tj * 3 + 1);
             const float rr = r2 * rsqrtf(fmaxf(r2, 1e-30f));
             const float wd = fmaxf(1.0f - rr * c1.w, 0.0f);
             const float add = c2.z * wd * wd;
@@ -86,85 +110,18 @@ __global__ void __launch_bounds__(256) k_density(StepArgs a)
     atomicAdd(&a.rho[s], rho_i);
 }
 
-// ---------------------------------------------------------------------------------
-// Pair force over the half list with the Saru random force; j-side by vector atomics.
-// DPD: src/force/pair_dpd.cu:468-558; mDPD: src/force/pair_mdpd.cu:587-682.
-// LOG adds PE and the pair virial (src/force/pair_dpd.cu:366-383) in FP64.
-template <bool LOG, int STYLE, bool SMALL>
-__device__ __forceinline__ void pair_loop(const StepArgs& a, const RepDesc& d, const int s,
-                                          const float4 pi, const float4 vi, const float rho_i,
-                                          const uint32_t step, float& fx, float& fy, float& fz,
-                                          double (&accv)[8])
-{
-    const int ci = __float_as_int(pi.w);
-    const int tagi = tag_of(vi.w);
-    const int ti = type0_of(vi.w);
-    const float4* crow = a.coeff + d.coeff_off + ti * d.ntypes * 3;
-    const int n = min(a.ncount[s], a.nmax);
-    const int* lst = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
-    const float rcmax2 = d.rcmax2;
-    for (int k = 0; k < n; k++) {
-        const int j = __ldg(lst + (size_t)k * 32);
-        const float4 pj = __ldg(a.pos4 + j);
-        float dx, dy, dz;
-        disp3<SMALL>(d, ci, pi, pj, dx, dy, dz);
-        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-        if (r2 > rcmax2) continue;
-        const float4 vj = __ldg(a.vel4 + j);
-        const int tj = type0_of(vj.w);
-        const float4 c0 = __ldg(crow + tj * 3 + 0);
-        if (!(r2 <= c0.w)) continue;
-        const float rinv = rsqrtf(r2);
-        const float r = r2 * rinv;
-        if (r < 1.0e-10f) continue;
-        const float4 c1 = __ldg(crow + tj * 3 + 1);
-        const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
-        const float dot = dx * dvx + dy * dvy + dz * dvz;
-        const float wc = 1.0f - r * c1.x;
-        const int tagj = tag_of(vj.w);
-        const float th = saru_theta((uint32_t)min(tagi, tagj), (uint32_t)max(tagi, tagj), d.seed, step);
-        float fpair = c0.x * wc;
-        float wd = 0.0f, rho_j = 0.0f;
-        float4 c2;
-        if (STYLE == 1) {
-            c2 = __ldg(crow + tj * 3 + 2);
-            wd = fmaxf(1.0f - r * c1.w, 0.0f);
-            rho_j = __ldg(a.rho + j);
-            fpair += c1.z * (rho_i + rho_j) * wd;
-        }
-        fpair -= c0.y * wc * wc * dot * rinv;
-        fpair += c0.z * wc * th;
-        fpair *= rinv;
-        const float ffx = dx * fpair, ffy = dy * fpair, ffz = dz * fpair;
-        fx += ffx;
-        fy += ffy;
-        fz += ffz;
-        atomicAdd(&a.force4[j], make_float4(-ffx, -ffy, -ffz, 0.0f));
-        if (LOG) {
-            double pe = (double)(c1.y * wc * wc);
-            if (STYLE == 1) pe += (double)(c2.y * (rho_i + rho_j) * wd * wd);
-            accv[0] += pe;
-            accv[2] += (double)dx * ffx;
-            accv[3] += (double)dx * ffy;
-            accv[4] += (double)dx * ffz;
-            accv[5] += (double)dy * ffy;
-            accv[6] += (double)dy * ffz;
-            accv[7] += (double)dz * ffz;
-        }
-    }
-}
-
 // Bond forces computed by both partners (each takes its own side; energy and virial
 // halved), so bonds need no atomics.  Harmonic: src/force/bond_harmonic.cu:208-268
 // (E = k (r-r0)^2, F_i = -2k(r-r0)/r d).  FENE: -0.5 K R0^2 ln(1-(r/R0)^2) + WCA.
-template <bool LOG, bool SMALL>
-__device__ __forceinline__ void bond_loop(const StepArgs& a, const RepDesc& d, const int r_idx,
-                                          const int s, const float4 pi, float& fx, float& fy,
-                                          float& fz, double (&accv)[8])
+template <bool LOG>
+__device__ __forceinline__ void bond_loop(const StepArgs& a, const RepDesc& d, const float4* pos,
+                                          const int2* bonds, const int r_idx, const int s,
+                                          const float4 pi, float& fx, float& fy, float& fz,
+                                          double (&accv)[8])
 {
     const int ci = __float_as_int(pi.w);
     for (int b = 0; b < a.maxb; b++) {
-        const int2 bp = a.bonds[(size_t)b * a.P + s];
+        const int2 bp = bonds[(size_t)b * a.P + s];
         if (bp.x <= 0) break;
         if (bp.x > d.n_real) {
             atomicOr(&a.rstate[r_idx].status, ST_BOND_MISSING);
@@ -175,9 +132,9 @@ __device__ __forceinline__ void bond_loop(const StepArgs& a, const RepDesc& d, c
             atomicOr(&a.rstate[r_idx].status, ST_BOND_MISSING);
             continue;
         }
-        const float4 pj = a.pos4[j];
+        const float4 pj = pos[j];
         float dx, dy, dz;
-        disp3<true>(d, ci, pi, pj, dx, dy, dz);
+        disp3(d, ci, pi, pj, dx, dy, dz);
         const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
         const float4 bc = __ldg(a.bondc + d.bond_off + bp.y - 1);
         float fbond = 0.0f, e = 0.0f;
@@ -217,34 +174,112 @@ __device__ __forceinline__ void bond_loop(const StepArgs& a, const RepDesc& d, c
     }
 }
 
-template <int STYLE, bool SMALL, bool BONDS>
+// One DPD / mDPD pair (src/force/pair_dpd.cu:495-547, src/force/pair_mdpd.cu:616-672):
+// F = [A w + B (rho_i+rho_j) w_d - gamma w^2 (r.v)/r + sigma w theta] r/r with
+// w = 1 - r/rc, theta = Saru(min tag, max tag, seed + step).  Returns false when the
+// pair is outside its cutoff.
+template <int STYLE, bool LOG>
+__device__ __forceinline__ bool pair_force(const float4* crow, float r2, float dx, float dy, float dz,
+                                           float4 vi, float4 vj, float rho_i, float rho_j, uint32_t seed,
+                                           uint32_t step, float& fx, float& fy, float& fz,
+                                           double (&accv)[8])
+{
+    const int tj = type0_of(vj.w);
+    const float4 c0 = __ldg(crow + tj * 3 + 0);
+    if (!(r2 <= c0.w)) return false;
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    if (r < 1.0e-10f) return false;
+    const float4 c1 = __ldg(crow + tj * 3 + 1);
+    const float dot = dx * (vi.x - vj.x) + dy * (vi.y - vj.y) + dz * (vi.z - vj.z);
+    const float wc = 1.0f - r * c1.x;
+    const int tagi = tag_of(vi.w), tagj = tag_of(vj.w);
+    const float th = saru_theta((uint32_t)min(tagi, tagj), (uint32_t)max(tagi, tagj), seed, step);
+    float fpair = c0.x * wc;
+    float wd = 0.0f;
+    float4 c2;
+    if (STYLE == 1) {
+        c2 = __ldg(crow + tj * 3 + 2);
+        wd = fmaxf(1.0f - r * c1.w, 0.0f);
+        fpair += c1.z * (rho_i + rho_j) * wd;
+    }
+    fpair -= c0.y * wc * wc * dot * rinv;
+    fpair += c0.z * wc * th;
+    fpair *= rinv;
+    fx = dx * fpair;
+    fy = dy * fpair;
+    fz = dz * fpair;
+    if (LOG) {
+        double pe = (double)(c1.y * wc * wc);
+        if (STYLE == 1) pe += (double)(c2.y * (rho_i + rho_j) * wd * wd);
+        accv[0] += pe;
+        accv[2] += (double)dx * fx;
+        accv[3] += (double)dx * fy;
+        accv[4] += (double)dx * fz;
+        accv[5] += (double)dy * fy;
+        accv[6] += (double)dy * fz;
+        accv[7] += (double)dz * fz;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------------
+// Pair force, thread-per-particle schedule (kept for comparison by the tuner).
+template <int STYLE, bool BONDS>
 __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 {
+    __shared__ float4 tab[8][27];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
-    bool work = false, log = false;
+    bool work = false, log = false, wactive = false;
     uint32_t step = 0;
     if (s < a.P) {
         r = a.warp_rep[s >> 5];
         const RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
-        work = rep_active(st) && s < d.p_end;
+        wactive = rep_active(st) && d.style == STYLE;
+        work = wactive && s < d.p_end;
         step = st.step;
-        log = rep_active(st) && (step % (uint32_t)d.log_f) == 0u;
+        log = wactive && (step % (uint32_t)d.log_f) == 0u;
+        if (wactive) fill_shift(tab[warp], d, lane);
     }
+    __syncwarp();
     double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (work) {
         const RepDesc& d = a.reps[r];
-        const float4 pi = a.pos4[s];
-        const float4 vi = a.vel4[s];
+        const int par = *a.parity;
+        const float4* pos = a.buf.pos[par];
+        const float4* vel = a.buf.vel[par];
+        const float4 pi = pos[s];
+        const float4 vi = vel[s];
         const float rho_i = STYLE == 1 ? a.rho[s] : 0.0f;
+        const float4* crow = a.coeff + d.coeff_off + type0_of(vi.w) * d.ntypes * 3;
+        const int n = min(a.ncount[s], a.nmax);
+        const int* lst = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + lane;
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        if (log) {
-            pair_loop<true, STYLE, SMALL>(a, d, s, pi, vi, rho_i, step, fx, fy, fz, accv);
-            if (BONDS) bond_loop<true, SMALL>(a, d, r, s, pi, fx, fy, fz, accv);
-        } else {
-            pair_loop<false, STYLE, SMALL>(a, d, s, pi, vi, rho_i, step, fx, fy, fz, accv);
-            if (BONDS) bond_loop<false, SMALL>(a, d, r, s, pi, fx, fy, fz, accv);
+        for (int k = 0; k < n; k++) {
+            const int ent = __ldg(lst + (size_t)k * 32);
+            const int j = ent & DPD_J_MASK;
+            const float4 pj = __ldg(pos + j);
+            float dx, dy, dz;
+            pair_disp(tab[warp], ent, pi, pj, dx, dy, dz);
+            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+            if (r2 > d.rcmax2) continue;
+            const float4 vj = __ldg(vel + j);
+            const float rho_j = STYLE == 1 ? __ldg(a.rho + j) : 0.0f;
+            float gx, gy, gz;
+            bool ok = log ? pair_force<STYLE, true>(crow, r2, dx, dy, dz, vi, vj, rho_i, rho_j, d.seed, step, gx, gy, gz, accv)
+                          : pair_force<STYLE, false>(crow, r2, dx, dy, dz, vi, vj, rho_i, rho_j, d.seed, step, gx, gy, gz, accv);
+            if (!ok) continue;
+            fx += gx;
+            fy += gy;
+            fz += gz;
+            atomicAdd(&a.force4[j], make_float4(-gx, -gy, -gz, 0.0f));
+        }
+        if (BONDS) {
+            if (log) bond_loop<true>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+            else bond_loop<false>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
         }
         atomicAdd(&a.force4[s], make_float4(fx, fy, fz, 0.0f));
     }
@@ -256,35 +291,199 @@ __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 }
 
 // ---------------------------------------------------------------------------------
+// Pair force, warp pair-queue schedule.  Thread-per-particle loops diverge on the
+// ~130-instruction Saru evaluation (only the pairs inside rc need it), so each warp
+// first filters its 32 particles' list candidates (DPD_U per lane per iteration, loads
+// issued before use), compacts the pairs inside the cutoff into a shared-memory queue
+// with a ballot, and evaluates 32 queued pairs at a time with every lane busy.  The
+// i-side force is reduced through shared-memory atomics, the j-side with one float4
+// atomic per pair.
+#define DPD_U 4                 // candidates per lane per filter iteration
+#define DPD_Q (32 + 32 * DPD_U)  // queue capacity per warp
+template <int STYLE, bool BONDS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
+{
+    __shared__ int sq_j[8][DPD_Q];
+    __shared__ int sq_i[8][DPD_Q];
+    __shared__ float4 sq_d[8][DPD_Q];
+    __shared__ float4 s_vi[8][32];
+    __shared__ float s_rho[8][32];
+    __shared__ float s_f[8][32][3];
+    __shared__ float4 tab[8][27];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = -1;
+    bool work = false, log = false, wactive = false;
+    uint32_t step = 0;
+    if (s < a.P) {
+        r = a.warp_rep[s >> 5];
+        const RepState st = a.rstate[r];
+        const RepDesc& d = a.reps[r];
+        wactive = rep_active(st) && d.style == STYLE;
+        work = wactive && s < d.p_end;
+        step = st.step;
+        log = wactive && (step % (uint32_t)d.log_f) == 0u;
+    }
+    double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (wactive) {  // warp-uniform
+        const RepDesc& d = a.reps[r];
+        const int par = *a.parity;
+        const float4* pos = a.buf.pos[par];
+        const float4* vel = a.buf.vel[par];
+        fill_shift(tab[warp], d, lane);
+        float4 pi = make_float4(0, 0, 0, 0), vi = make_float4(0, 0, 0, 0);
+        float rho_i = 0.0f;
+        int n = 0;
+        if (work) {
+            pi = pos[s];
+            vi = vel[s];
+            if (STYLE == 1) rho_i = a.rho[s];
+            n = min(a.ncount[s], a.nmax);
+        }
+        s_vi[warp][lane] = vi;
+        s_rho[warp][lane] = rho_i;
+        s_f[warp][lane][0] = 0.0f;
+        s_f[warp][lane][1] = 0.0f;
+        s_f[warp][lane][2] = 0.0f;
+        const int nw = __reduce_max_sync(0xffffffffu, n);
+        const int* lst = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + lane;
+        const float rcmax2 = d.rcmax2;
+        const unsigned lt = (1u << lane) - 1u;
+        const float4* cbase = a.coeff + d.coeff_off;
+        const int nt = d.ntypes;
+        const uint32_t seed = d.seed;
+        // Queue invariant: entries [base, qn) are pending.  The filter runs only when
+        // fewer than 32 are pending (they are first moved to the front), so before it
+        // qn <= 31 and after it qn <= 31 + 32*DPD_U < DPD_Q.
+        int k = 0, qn = 0, base = 0;
+        __syncwarp();
+        while (true) {
+            if (k < nw && qn - base < 32) {
+                if (base > 0) {
+                    // source starts at base >= 32, destination ends below 32: no overlap
+                    const int left = qn - base;
+                    if (lane < left) {
+                        sq_j[warp][lane] = sq_j[warp][base + lane];
+                        sq_i[warp][lane] = sq_i[warp][base + lane];
+                        sq_d[warp][lane] = sq_d[warp][base + lane];
+                    }
+                    qn = left;
+                    base = 0;
+                    __syncwarp();
+                }
+                // list entries carry the shift code in bits 27-31, so they may be negative
+                // as ints: validity is k + u < n, not the sign
+                int ee[DPD_U];
+                float4 pp[DPD_U];
+#pragma unroll
+                for (int u = 0; u < DPD_U; u++) ee[u] = (k + u < n) ? __ldg(lst + (size_t)(k + u) * 32) : 0;
+#pragma unroll
+                for (int u = 0; u < DPD_U; u++)
+                    if (k + u < n) pp[u] = __ldg(pos + (ee[u] & DPD_J_MASK));
+#pragma unroll
+                for (int u = 0; u < DPD_U; u++) {
+                    bool hit = false;
+                    float dx = 0, dy = 0, dz = 0, r2 = 0;
+                    if (k + u < n) {
+                        pair_disp(tab[warp], ee[u], pi, pp[u], dx, dy, dz);
+                        r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+                        hit = r2 <= rcmax2;
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        const int pos_q = qn + __popc(m & lt);
+                        sq_j[warp][pos_q] = ee[u] & DPD_J_MASK;
+                        sq_i[warp][pos_q] = lane;
+                        sq_d[warp][pos_q] = make_float4(dx, dy, dz, r2);
+                    }
+                    qn += __popc(m);
+                }
+                k += DPD_U;
+            }
+            const bool tail = k >= nw;
+            const int avail = qn - base;
+            if (avail < 32 && !(tail && avail > 0)) {
+                if (tail) break;  // nothing pending and no candidates left
+                continue;         // partial chunk: filter more candidates first
+            }
+            __syncwarp();
+            const int cnt = min(avail, 32);
+            if (lane < cnt) {
+                const int j = sq_j[warp][base + lane];
+                const int il = sq_i[warp][base + lane];
+                const float4 dd = sq_d[warp][base + lane];
+                const float4 vv = s_vi[warp][il];
+                const float4 vj = __ldg(vel + j);
+                const float4* crow = cbase + type0_of(vv.w) * nt * 3;
+                const float rho_j = STYLE == 1 ? __ldg(a.rho + j) : 0.0f;
+                float fx, fy, fz;
+                bool ok = log ? pair_force<STYLE, true>(crow, dd.w, dd.x, dd.y, dd.z, vv, vj, s_rho[warp][il], rho_j, seed, step, fx, fy, fz, accv)
+                              : pair_force<STYLE, false>(crow, dd.w, dd.x, dd.y, dd.z, vv, vj, s_rho[warp][il], rho_j, seed, step, fx, fy, fz, accv);
+                if (ok) {
+                    atomicAdd(&s_f[warp][il][0], fx);
+                    atomicAdd(&s_f[warp][il][1], fy);
+                    atomicAdd(&s_f[warp][il][2], fz);
+                    atomicAdd(&a.force4[j], make_float4(-fx, -fy, -fz, 0.0f));
+                }
+            }
+            __syncwarp();  // chunk entries are read before any compaction overwrites them
+            base += cnt;
+            if (base == qn) {
+                qn = 0;
+                base = 0;
+            }
+        }
+        __syncwarp();
+        float fx = s_f[warp][lane][0], fy = s_f[warp][lane][1], fz = s_f[warp][lane][2];
+        if (work) {
+            if (BONDS) {
+                if (log) bond_loop<true>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+                else bond_loop<false>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+            }
+            atomicAdd(&a.force4[s], make_float4(fx, fy, fz, 0.0f));
+        }
+    }
+    if (__syncthreads_or(log)) {
+        const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
+                               ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+        acc_flush<8>(accv, fields, log ? r : -1, a.acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Velocity Verlet, src/fix/fix_nve.cu:30-152, fused: final half kick of step n (and
-// the thermo sums of step n), then initial half kick + drift of step n+1, cell
-// re-wrap with image counters, displacement check for the next list build
-// (src/force/neigh_list.cu:483-514), and zeroing of the force accumulators.
+// the thermo sums of step n), then initial half kick + drift of step n+1, the
+// displacement check for the next list build (src/force/neigh_list.cu:483-514), and
+// zeroing of the force accumulators.  Cells stay fixed between builds, so the drift
+// only moves the offsets.
 __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
-    bool work = false, log = false;
+    bool log = false;
     double accv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (s < a.P) {
         r = a.warp_rep[s >> 5];
         const RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
-        const bool active = a.mode == 1 ? st.step <= st.target : rep_active(st);
-        work = active && s < d.p_end;
-        bool fin = a.mode == 0 && !st.zero_pending;
+        const bool active = rep_active(st);
+        const bool work = active && s < d.p_end;
+        const bool fin = a.mode == 0 && !st.zero_pending;
         log = a.mode == 0 && active && (st.step % (uint32_t)d.log_f) == 0u;
-        bool init = a.mode == 1 ? true : st.step < st.target;
-        uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
-        bool check = init && (next % (uint32_t)d.nl_f) == 0u;
+        const bool init = a.mode == 1 ? true : st.step < st.target;
+        const uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
+        const bool check = init && (next % (uint32_t)d.nl_f) == 0u;
         if (work) {
-            float4 v = a.vel4[s];
-            float4 f = a.force4[s];
-            float4 p = a.pos4[s];
+            const int par = *a.parity;
+            float4* posp = a.buf.pos[par];
+            float4* velp = a.buf.vel[par];
+            float4 v = velp[s];
+            const float4 f = a.force4[s];
             const int t0 = type0_of(v.w);
             const float2 m = __ldg(a.mass + d.mass_off + t0);
             const bool integ = (d.integ_mask >> t0) & 1u;
-            const float dtm = (0.5f * d.dt) * m.y;
+            const float dt = d.dt;
+            const float dtm = (0.5f * dt) * m.y;
             if (fin && integ) {
                 v.x = __fmaf_rn(dtm, f.x, v.x);
                 v.y = __fmaf_rn(dtm, f.y, v.y);
@@ -304,69 +503,37 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
                 accv[9] = mm * vz;
             }
             if (init) {
-                int code = __float_as_int(p.w);
+                float4 p = posp[s];
                 if (integ) {
                     v.x = __fmaf_rn(dtm, f.x, v.x);
                     v.y = __fmaf_rn(dtm, f.y, v.y);
                     v.z = __fmaf_rn(dtm, f.z, v.z);
-                    float o[3] = {__fmaf_rn(d.dt, v.x, p.x), __fmaf_rn(d.dt, v.y, p.y),
-                                  __fmaf_rn(d.dt, v.z, p.z)};
-                    int c[3] = {cell_x(code), cell_y(code), cell_z(code)};
-                    int dimg[3] = {0, 0, 0};
-                    bool moved = false;
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        if (!(o[k] >= 0.0f && o[k] < d.w[k])) {
-                            if (!isfinite(o[k])) {
-                                atomicOr(&a.rstate[r].status, ST_NONFINITE);
-                                o[k] = 0.0f;
-                                continue;
-                            }
-                            float q = floorf(o[k] * d.inv_w[k]);
-                            q = fminf(fmaxf(q, -1.0e6f), 1.0e6f);
-                            o[k] = __fmaf_rn(-q, d.w[k], o[k]);
-                            int cc = c[k] + (int)q;
-                            int nc = d.nc[k];
-                            int wrap = cc >= 0 ? cc / nc : -((-cc + nc - 1) / nc);
-                            cc -= wrap * nc;
-                            dimg[k] = wrap;
-                            c[k] = cc;
-                            if (o[k] >= d.w[k]) o[k] = __int_as_float(__float_as_int(d.w[k]) - 1);
-                            if (o[k] < 0.0f) o[k] = 0.0f;
-                            moved = true;
-                        }
-                    }
-                    if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z))
+                    p.x = __fmaf_rn(dt, v.x, p.x);
+                    p.y = __fmaf_rn(dt, v.y, p.y);
+                    p.z = __fmaf_rn(dt, v.z, p.z);
+                    if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) ||
+                        !isfinite(v.y) || !isfinite(v.z))
                         atomicOr(&a.rstate[r].status, ST_NONFINITE);
-                    if (moved) code = cell_pack(c[0], c[1], c[2]);
-                    if (dimg[0] | dimg[1] | dimg[2]) {
-                        int4 im = a.img[s];
-                        im.x += dimg[0];
-                        im.y += dimg[1];
-                        im.z += dimg[2];
-                        a.img[s] = im;
-                    }
-                    p = make_float4(o[0], o[1], o[2], __int_as_float(code));
-                    a.pos4[s] = p;
+                    posp[s] = p;
                 }
                 if (check) {
                     bool need = d.skin_zero != 0;
                     if (!need) {
+                        // same cell as at the last build: the displacement is the offset change
                         const float4 q = a.last4[s];
-                        float dx, dy, dz;
-                        disp3<true>(d, code, p, q, dx, dy, dz);
+                        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
                         const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-                        need = r2 >= d.hskin2;
+                        need = !(r2 < d.hskin2);
                     }
                     if (need) {
-                        uint32_t ph = *a.phase + (a.mode == 1 ? 0u : 1u);
+                        const uint32_t ph = *a.phase + (a.mode == 1 ? 0u : 1u);
                         a.build_flag[ph & 1] = 1;
                     }
                 }
                 a.force4[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 if (d.style == 1) a.rho[s] = 0.0f;
             }
-            a.vel4[s] = v;
+            velp[s] = v;
         }
     }
     if (a.mode == 0 && __syncthreads_or(log)) {
@@ -447,13 +614,16 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
     // every warp is single-replica, so `on` is warp-uniform
     if (!on) return;
     const RepDesc& d = a.reps[r];
+    const int par = *a.parity;
+    const float4* pos = a.buf.pos[par];
+    const float4* vel = a.buf.vel[par];
     const int nb = min(d.rdf_nbins, DPD_RDF_MAXBINS);
     for (int b = lane; b < nb; b += 32) hs[warp][b] = 0u;
     __syncwarp();
     if (s == d.p_begin) atomicAdd((unsigned long long*)&a.rstate[r].rdf_samples, 1ull);
     if (s < d.p_end) {
-        const float4 pi = a.pos4[s];
-        const int ti = type0_of(a.vel4[s].w) + 1;
+        const float4 pi = pos[s];
+        const int ti = type0_of(vel[s].w) + 1;
         if (ti == d.rdf_ta) {
             const int ci = __float_as_int(pi.w);
             const int cx = cell_x(ci), cy = cell_y(ci), cz = cell_z(ci);
@@ -480,11 +650,11 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
                         const int jb = a.cstart[key], je = a.cstart[key + 1];
                         for (int j = jb; j < je; j++) {
                             if (j == s) continue;
-                            const float4 vj = __ldg(a.vel4 + j);
+                            const float4 vj = __ldg(vel + j);
                             if (type0_of(vj.w) + 1 != d.rdf_tb) continue;
-                            const float4 pj = __ldg(a.pos4 + j);
+                            const float4 pj = __ldg(pos + j);
                             float dx, dy, dz;
-                            disp3<true>(d, ci, pi, pj, dx, dy, dz);
+                            disp3(d, ci, pi, pj, dx, dy, dz);
                             const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
                             if (r2 < rmax2) {
                                 int bin = (int)(sqrtf(r2) * inv_dr);

@@ -167,8 +167,9 @@ def forces(ff, tags, types, x, v, lo, L, step, bonds=None):
     return {"f": f, "rho": rho, "pair_pe": en[0], "bond_pe": en[1], "virial": vir, "status": st}
 
 
-def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zero_step=True):
-    """Velocity-Verlet in FP64; returns final state and logged thermo rows."""
+def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zero_step=True, f0=None):
+    """Velocity-Verlet in FP64; returns final state and logged thermo rows.  Without a zero
+    step, f0 are the forces of step first_step-1 (used by the first half kick)."""
     lib = load()
     n = len(types)
     tags = np.ascontiguousarray(tags, dtype=np.int32)
@@ -181,7 +182,7 @@ def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zer
     maxlog = nsteps + 2
     th = np.zeros((maxlog, 12))
     ls = np.zeros(maxlog, dtype=np.int32)
-    f = np.zeros((n, 3))
+    f = np.zeros((n, 3)) if f0 is None else np.array(f0, dtype=np.float64, order="C")
     rho = np.zeros(n)
     nb = 0 if bonds is None else len(bonds)
     b = None if bonds is None else np.ascontiguousarray(bonds, dtype=np.int32)
