@@ -164,21 +164,23 @@ def run_ours(args, world, rank, local):
     pair_ms = res["pair_ms"]
     n = system.n
     value = world * n * args.steps / (total_ms / 1000.0)
-    # end to end through the C ABI: host state -> device, K steps, device -> host
-    chunk = max(args.steps // 2, 10)
-    st = eng.state()
+    # end to end through the C ABI with host buffers: the state (x, v in FP64) goes host
+    # -> device, K steps run (a zero-step force evaluation and list build first), the
+    # final x, v come back device -> host with the thermo rows
+    chunk = args.steps
+    st = eng.state(forces=False, images=False)
     x = np.ascontiguousarray(st["x"])
     v = np.ascontiguousarray(st["v"])
     barrier(world)
     t0 = time.perf_counter()
     eng.set_state(x, v)
     eng.run(chunk)
-    st2 = eng.state()
+    st2 = eng.state(forces=False, images=False)
     th = eng.thermo(max_rows=4)
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
     e2e = world * n * chunk / e2e_s
     h2d = n * 6 * 8 / chunk
-    d2h = (n * (3 * 8 * 3 + 3 * 4) + 4 * 8 * 16) / chunk
+    d2h = (n * 6 * 8 + 4 * 8 * 16) / chunk
     maxb = 2 if system.bonds is not None else 0
     bpp = algorithmic_bytes_per_particle(ls["mean_half_list"], maxb)
     per_launch_ms = pair_ms / max(res["pair_launches"], 1)

@@ -30,6 +30,7 @@ enum {
     ST_BOND_MISSING = 4,
     ST_FENE_BROKEN = 8,
     ST_BOND_OVERFLOW = 16,
+    ST_BAD_INPUT = 32,  // an AoS input carried an id or type outside the system
 };
 
 // Per-replica constant description (device copy, read through the L1 cache).

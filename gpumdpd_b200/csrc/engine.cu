@@ -7,9 +7,12 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <atomic>
+#include <thread>
 
 #include "engine.h"
 #include "kernels.cuh"
+#include "kernels_aos.cuh"
 #include "kernels_step.cuh"
 
 namespace dpd {
@@ -44,6 +47,8 @@ Engine::~Engine()
     if (graph_) cudaGraphExecDestroy(graph_);
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : allocs_) cudaFree(p);
+    for (void* p : {(void*)h_pos_, (void*)h_vel_, (void*)h_frc_, (void*)h_img_})
+        if (p) cudaFreeHost(p);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -317,17 +322,47 @@ int Engine::alloc_and_upload()
     return DPD_OK;
 }
 
-// Convert the FP64 state of every replica into the cell-offset representation.
+// Host loop over [0, n) split across hardware threads (state conversion of millions of
+// particles on every upload/download).
+template <class F>
+static void parallel_for(int64_t n, F fn)
+{
+    int nt = (int)std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    if (n < 65536) nt = 1;
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back([=] { fn(n * t / nt, n * (t + 1) / nt); });
+    fn(0, n / nt);
+    for (auto& x : th) x.join();
+}
+
+int Engine::staging()
+{
+    if (h_pos_) return DPD_OK;
+    CK(cudaMallocHost((void**)&h_pos_, sizeof(float4) * P_));
+    CK(cudaMallocHost((void**)&h_vel_, sizeof(float4) * P_));
+    CK(cudaMallocHost((void**)&h_frc_, sizeof(float4) * P_));
+    CK(cudaMallocHost((void**)&h_img_, sizeof(int4) * P_));
+    return DPD_OK;
+}
+
+// Convert the FP64 state of every replica into the cell-offset representation and
+// upload it (tag order) into buffer 0.  The bond partner table is built once, kept on
+// the device in tag order, and copied on later uploads.
 int Engine::upload_particles()
 {
-    std::vector<float4> pos(P_), vel(P_);
-    std::vector<int4> img(P_);
-    std::vector<int2> bonds((size_t)std::max(maxb_, 1) * P_, make_int2(0, 0));
+    int st = staging();
+    if (st) return st;
+    float4* pos = h_pos_;
+    float4* vel = h_vel_;
+    int4* img = h_img_;
+    const bool first = !bonds_tag_;
+    std::vector<int2> bonds;
+    if (first) bonds.assign((size_t)std::max(maxb_, 1) * P_, make_int2(0, 0));
     for (auto& R : reps_) {
         const RepDesc& d = R.desc;
         const int n = R.sys.n_atoms;
-        std::vector<int> deg(n, 0);
-        for (int i = 0; i < n; i++) {
+        parallel_for(n, [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; i++) {
             const int s = d.p_begin + i;
             int c[3];
             float o[3];
@@ -355,7 +390,9 @@ int Engine::upload_particles()
                                  (float)R.sys.v[3 * (size_t)i + 2], tagf);
             img[s] = make_int4(0, 0, 0, 0);
         }
-        if (d.bond_style) {
+        });
+        if (first && d.bond_style) {
+            std::vector<int> deg(n, 0);
             for (int b = 0; b < R.sys.n_bonds; b++) {
                 const int ty = R.sys.bonds[3 * b], ta = R.sys.bonds[3 * b + 1], tb = R.sys.bonds[3 * b + 2];
                 const int ia = ta - 1, ib = tb - 1;
@@ -372,11 +409,25 @@ int Engine::upload_particles()
         }
     }
     // the state goes into buffer 0, which becomes the current one
-    CK(cudaMemcpyAsync(b_.pos[0], pos.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.vel[0], vel.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.img[0], img.data(), sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.bonds[0], bonds.data(), sizeof(int2) * bonds.size(), cudaMemcpyHostToDevice, stream_));
+    const size_t nb = (size_t)std::max(maxb_, 1) * P_;
+    if (first) {
+        if ((st = dalloc(&bonds_tag_, nb))) return st;
+        CK(cudaMemcpyAsync(bonds_tag_, bonds.data(), sizeof(int2) * nb, cudaMemcpyHostToDevice, stream_));
+    }
+    CK(cudaMemcpyAsync(b_.pos[0], pos, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.vel[0], vel, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.img[0], img, sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.bonds[0], bonds_tag_, sizeof(int2) * nb, cudaMemcpyDeviceToDevice, stream_));
     CK(cudaMemsetAsync(b_.parity, 0, sizeof(int), stream_));
+    // slots are in tag order until the first build
+    {
+        std::vector<int> t2i;
+        for (auto& R : reps_)
+            for (int t = 0; t < R.sys.n_atoms; t++) t2i.push_back(R.desc.p_begin + t);
+        CK(cudaMemcpyAsync(b_.tag2idx, t2i.data(), sizeof(int) * t2i.size(), cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+    }
+    aos_built_ = false;
     CK(cudaMemsetAsync(b_.force4, 0, sizeof(float4) * P_, stream_));
     CK(cudaMemsetAsync(b_.rho, 0, sizeof(float) * P_, stream_));
     CK(cudaStreamSynchronize(stream_));
@@ -459,12 +510,14 @@ template <int STYLE, bool BONDS>
 static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& a)
 {
     if (variant == 0) k_pair<STYLE, BONDS><<<grid, 256, 0, s>>>(a);
-    else if (variant == 2) k_pair_q<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
-    else k_pair_q<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
+    else if (variant == 2) k_pair_q<STYLE, BONDS, 4, true><<<grid, 256, 0, s>>>(a);
+    else if (variant == 3) k_pair_q<STYLE, BONDS, 3, false><<<grid, 256, 0, s>>>(a);
+    else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
 }
 
-// pair_variant 0: thread per particle; 1 (default): warp pair-queue, 4 blocks/SM;
-// 2: warp pair-queue, 3 blocks/SM (more registers)
+// pair_variant 0: thread per particle; 1 (default): warp pair-queue, i-side and
+// j-side forces by float4 reductions in L2, 4 blocks/SM; 2: warp pair-queue with the
+// i-side reduced through shared-memory atomics; 3: as 1 with 3 blocks/SM
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -472,11 +525,11 @@ static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const
     else launch_pair2<STYLE, false>(variant, grid, s, a);
 }
 
-void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
+// The list-build chain; every kernel returns at once unless this phase's flag is set.
+void Engine::enqueue_build(cudaStream_t s)
 {
     const int nrep = (int)reps_.size();
     BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
-    StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
     const int gp = (P_ + 255) / 256;
     const int gc = (C_ + 255) / 256;
     const int nsb = (C_ + 4095) / 4096;
@@ -489,6 +542,14 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     k_permute<<<gp, 256, 0, s>>>(ba);
     k_flip<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
     k_build_nlist<<<gp, 256, 0, s>>>(ba);
+}
+
+void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
+{
+    const int nrep = (int)reps_.size();
+    StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
+    const int gp = (P_ + 255) / 256;
+    enqueue_build(s);
     if (any_mdpd_) k_density<<<gp, 256, 0, s>>>(sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
     const int variant = tune_.pair_variant;
@@ -593,6 +654,10 @@ int Engine::sync_and_check()
         if (s & ST_BOND_MISSING) {
             err = "bond partner not found in replica " + std::to_string(r);
             return DPD_E_STATE;
+        }
+        if (s & ST_BAD_INPUT) {
+            err = "an atom id or type in the AoS input is outside the engine's system";
+            return DPD_E_ARG;
         }
     }
     return DPD_OK;
@@ -713,22 +778,30 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
     const RepDesc& d = reps_[rep].desc;
     const Replica& R = reps_[rep];
     const int ns = d.p_cap_end - d.p_begin;
-    std::vector<float4> pos(ns), vel(ns), frc(ns);
-    std::vector<int4> img(ns);
+    int st = staging();
+    if (st) return st;
+    float4* pos = h_pos_;
+    float4* vel = h_vel_;
+    float4* frc = h_frc_;
+    int4* img = h_img_;
     const int par = cur_parity();
     if (par < 0) return cuda_fail(cudaGetLastError(), "cudaMemcpy(parity)");
-    CK(cudaMemcpyAsync(pos.data(), b_.pos[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(vel.data(), b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(frc.data(), b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(img.data(), b_.img[par] + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(vel, b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    if (x || image) {
+        CK(cudaMemcpyAsync(pos, b_.pos[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(img, b_.img[par] + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
+    }
+    if (f) CK(cudaMemcpyAsync(frc, b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
-    for (int k = 0; k < d.n_real; k++) {
+    std::atomic<int> bad{0};
+    parallel_for(d.n_real, [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; k++) {
         int tw;
         memcpy(&tw, &vel[k].w, 4);
         const int tag = (int)((uint32_t)tw >> DPD_TYPE_BITS);
         if (tag < 1 || tag > d.n_real) {
-            err = "corrupt tag in device state";
-            return DPD_E_STATE;
+            bad = 1;
+            continue;
         }
         const size_t o = 3 * (size_t)(tag - 1);
         int code;
@@ -752,6 +825,11 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
             if (image) image[o + q] = im[q] + (int)wrap;
         }
     }
+    });
+    if (bad) {
+        err = "corrupt tag in device state";
+        return DPD_E_STATE;
+    }
     return DPD_OK;
 }
 
@@ -759,12 +837,17 @@ int Engine::set_state(int rep, const double* x, const double* v)
 {
     if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
     Replica& R = reps_[rep];
-    std::vector<double> xv(3 * (size_t)R.sys.n_atoms), vv(3 * (size_t)R.sys.n_atoms);
-    std::vector<int> im(3 * (size_t)R.sys.n_atoms);
-    int e = get_state(rep, xv.data(), vv.data(), im.data(), nullptr);
-    if (e) return e;
-    if (x) memcpy(R.sys.x.data(), x, sizeof(double) * xv.size()); else R.sys.x = xv;
-    if (v) memcpy(R.sys.v.data(), v, sizeof(double) * vv.size()); else R.sys.v = vv;
+    const size_t n3 = 3 * (size_t)R.sys.n_atoms;
+    int e = DPD_OK;
+    if (!x || !v) {
+        std::vector<double> xv(n3), vv(n3);
+        e = get_state(rep, xv.data(), vv.data(), nullptr, nullptr);
+        if (e) return e;
+        R.sys.x = xv;
+        R.sys.v = vv;
+    }
+    if (x) memcpy(R.sys.x.data(), x, sizeof(double) * n3);
+    if (v) memcpy(R.sys.v.data(), v, sizeof(double) * n3);
     // full re-upload of every replica's particles (the host copies of the others are
     // refreshed first); the next run starts with a zero step and a list build
     for (int r = 0; r < (int)reps_.size(); r++) {
@@ -954,11 +1037,47 @@ int Engine::set_tuning(const dpd_tuning* t)
     return build_graph();
 }
 
-int Engine::pair_compute_aos(const float*, const float*, const int*, const int*, int, uint32_t, float*,
-                             float*, float*)
+// Pair::compute_force on the reference's AoS device buffers (see kernels_aos.cuh).  Bonds
+// are left to the caller's own bond style, as the reference computes them separately.
+int Engine::pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
+                             int n, uint32_t step, float* d_force, float* d_pe, float* d_virial)
 {
-    err = "not available";
-    return DPD_E_STATE;
+    if (reps_.size() != 1) {
+        err = "the AoS pair entry point works on a single-system engine";
+        return DPD_E_STATE;
+    }
+    const RepDesc& d = reps_[0].desc;
+    if (!d_pos || !d_vel || !d_id || !d_type || !d_force) {
+        err = "null device pointer";
+        return DPD_E_ARG;
+    }
+    if (n != d.n_real) {
+        err = "n does not match the number of atoms of the engine's system";
+        return DPD_E_ARG;
+    }
+    int st;
+    if ((d_pe || d_virial) && !pe_slot_) {
+        if ((st = dalloc(&pe_slot_, P_))) return st;
+        if ((st = dalloc(&vir_slot_, 6 * (size_t)P_))) return st;
+    }
+    StepArgs sa = step_args(b_, P_, nmax_, maxb_, 1);
+    const int gp = (P_ + 255) / 256;
+    k_aos_in<<<(n + 255) / 256, 256, 0, stream_>>>(sa, d_pos, d_vel, d_id, d_type, n, step, aos_built_ ? 0 : 1);
+    enqueue_build(stream_);
+    if (any_mdpd_) k_density<<<gp, 256, 0, stream_>>>(sa);
+    const bool peratom = d_pe || d_virial;
+    if (d.style == 0) {
+        if (peratom) k_pair_peratom<0><<<gp, 256, 0, stream_>>>(sa, pe_slot_, vir_slot_);
+        else launch_pair<0>(tune_.pair_variant, false, gp, stream_, sa);
+    } else {
+        if (peratom) k_pair_peratom<1><<<gp, 256, 0, stream_>>>(sa, pe_slot_, vir_slot_);
+        else launch_pair<1>(tune_.pair_variant, false, gp, stream_, sa);
+    }
+    k_aos_out<<<gp, 256, 0, stream_>>>(sa, d_force, d_pe, d_virial, pe_slot_, vir_slot_);
+    k_aos_done<<<1, 1, 0, stream_>>>(b_.build_flag, b_.phase);
+    CK(cudaGetLastError());
+    aos_built_ = true;
+    return sync_and_check();
 }
 
 // ---------------------------------------------------------------------------------

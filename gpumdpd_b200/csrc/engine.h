@@ -90,9 +90,11 @@ private:
     int alloc_and_upload();
     int upload_particles();
     void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
+    void enqueue_build(cudaStream_t s);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
     int cur_parity();
+    int staging();
     int cuda_fail(cudaError_t e, const char* what);
     template <class T> int dalloc(T** p, size_t n);
 
@@ -106,6 +108,11 @@ private:
     bool zero_pending_ = true;
     uint32_t next_step_ = 0;
     std::vector<void*> allocs_;
+    float4 *h_pos_ = nullptr, *h_vel_ = nullptr, *h_frc_ = nullptr;  // pinned staging
+    int4* h_img_ = nullptr;
+    int2* bonds_tag_ = nullptr;  // bond partner table in tag order (device)
+    float *pe_slot_ = nullptr, *vir_slot_ = nullptr;  // per-atom PE/virial of the AoS entry
+    bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
 };

@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 // atomic per pair.
 #define DPD_U 4                 // candidates per lane per filter iteration
 #define DPD_Q (32 + 32 * DPD_U)  // queue capacity per warp
-template <int STYLE, bool BONDS, int MINB>
+template <int STYLE, bool BONDS, int MINB, bool ISMEM>
 __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 {
     __shared__ int sq_j[8][DPD_Q];
@@ -420,9 +420,13 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
                 bool ok = log ? pair_force<STYLE, true>(crow, dd.w, dd.x, dd.y, dd.z, vv, vj, s_rho[warp][il], rho_j, seed, step, fx, fy, fz, accv)
                               : pair_force<STYLE, false>(crow, dd.w, dd.x, dd.y, dd.z, vv, vj, s_rho[warp][il], rho_j, seed, step, fx, fy, fz, accv);
                 if (ok) {
-                    atomicAdd(&s_f[warp][il][0], fx);
-                    atomicAdd(&s_f[warp][il][1], fy);
-                    atomicAdd(&s_f[warp][il][2], fz);
+                    if (ISMEM) {
+                        atomicAdd(&s_f[warp][il][0], fx);
+                        atomicAdd(&s_f[warp][il][1], fy);
+                        atomicAdd(&s_f[warp][il][2], fz);
+                    } else {
+                        atomicAdd(&a.force4[(s & ~31) + il], make_float4(fx, fy, fz, 0.0f));
+                    }
                     atomicAdd(&a.force4[j], make_float4(-fx, -fy, -fz, 0.0f));
                 }
             }

@@ -81,12 +81,12 @@ class Engine:
         _check(self.lib.dpd_get_thermo(self.h, rows, max_rows, ctypes.byref(n)), self.lib, self.h)
         return _rows_to_dict(rows, n.value)
 
-    def state(self):
+    def state(self, forces=True, images=True):
         n = self.n_atoms
         x = np.empty((n, 3))
         v = np.empty((n, 3))
-        img = np.empty((n, 3), dtype=np.int32)
-        f = np.empty((n, 3))
+        img = np.empty((n, 3), dtype=np.int32) if images else None
+        f = np.empty((n, 3)) if forces else None
         _check(self.lib.dpd_get_state(self.h, capi.ptr(x), capi.ptr(v), capi.ptr(img), capi.ptr(f)),
                self.lib, self.h)
         return {"x": x, "v": v, "image": img, "f": f}
@@ -147,6 +147,11 @@ class Engine:
 
     def write_data(self, path):
         _check(self.lib.dpd_write_data(self.h, path.encode()), self.lib, self.h)
+
+    def pair_compute_aos(self, d_pos, d_vel, d_id, d_type, n, step, d_force, d_pe=None, d_virial=None):
+        """Pair::compute_force on AoS device buffers (integer device addresses)."""
+        _check(self.lib.dpd_pair_compute_aos(self.h, d_pos, d_vel, d_id, d_type, int(n), int(step), d_force,
+                                             d_pe, d_virial), self.lib, self.h)
 
     def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0):
         t = capi.dpd_tuning()
