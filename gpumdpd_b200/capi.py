@@ -25,8 +25,12 @@ EXPORTED = [
     "dpd_batch_create", "dpd_batch_n", "dpd_batch_get_thermo", "dpd_batch_get_state",
     "dpd_batch_rdf_result", "dpd_server_create", "dpd_server_submit", "dpd_server_step",
     "dpd_server_result", "dpd_server_job_state", "dpd_server_job_rdf", "dpd_server_stats",
-    "dpd_server_last_error", "dpd_server_destroy", "dpd_version",
+    "dpd_server_last_error", "dpd_server_destroy", "dpd_pair_forces_noalloc", "dpd_version",
 ]
+
+NOALLOC_MAX_ATOMS = 262144
+NOALLOC_MAX_CELLS = 262144
+NOALLOC_MAX_TYPES = 8
 
 
 class DpdError(RuntimeError):
@@ -67,6 +71,14 @@ class dpd_job_result(ctypes.Structure):
         ("mean_temp", ctypes.c_double), ("mean_pressure", ctypes.c_double),
         ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double),
         ("last", dpd_thermo),
+    ]
+
+
+class dpd_pair_params(ctypes.Structure):
+    _fields_ = [
+        ("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3), ("ntypes", ctypes.c_int),
+        ("coeff", ((ctypes.c_double * 3) * NOALLOC_MAX_TYPES) * NOALLOC_MAX_TYPES),
+        ("kT", ctypes.c_double), ("dt", ctypes.c_double), ("seed", ctypes.c_uint32),
     ]
 
 
@@ -121,6 +133,7 @@ def load():
         "dpd_server_stats": (i, [vp, P(i64), P(d), P(i64)]),
         "dpd_server_last_error": (cp, [vp]),
         "dpd_server_destroy": (i, [vp]),
+        "dpd_pair_forces_noalloc": (i, [P(dpd_pair_params), vp, vp, vp, vp, i, u32, vp, vp]),
         "dpd_version": (cp, []),
     }
     for name, (res, args) in sig.items():

@@ -219,6 +219,44 @@ int dpd_server_stats(dpd_server* srv, int64_t* particle_steps, double* busy_s,
 const char* dpd_server_last_error(dpd_server* srv);
 int dpd_server_destroy(dpd_server* srv);
 
+/* ---- pair force without device allocation ---------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate device memory:
+ * a force plugin inside a host MD code or framework that owns all device memory
+ * (its caching allocator or a fixed arena set up at start-up), and fixed-latency
+ * loops, where cudaMalloc/cudaFree can synchronize the whole device and stall other
+ * streams, or fail when the device is nearly full in the middle of a run.  Computes the
+ * pair_style dpd force (Saru random force keyed on min/max id, seed + step) on AoS
+ * device buffers, like dpd_pair_compute_aos, but needs no engine and calls no
+ * cudaMalloc, cudaFree or allocating library routine: the cell binning lives in a
+ * file-scope static device array of about 5 MB, which every device that loads the
+ * library holds until exit.  Limits: n <= DPD_NOALLOC_MAX_ATOMS, at most
+ * DPD_NOALLOC_MAX_CELLS cells of edge >= max rc with at least 3 per dimension,
+ * ntypes <= DPD_NOALLOC_MAX_TYPES; larger inputs return DPD_E_ARG before any launch.
+ * Positions must lie in [lo, hi).  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture.  All calls share the array and it keeps the last
+ * call's contents (each call clears what must start at zero), so calls that overlap on
+ * the GPU -- other streams, other threads -- race and must be serialized by the caller.
+ * Work goes on `stream` (a cudaStream_t, NULL = legacy default stream) and the call
+ * returns after the forces are written; d_force is overwritten. */
+#define DPD_NOALLOC_MAX_ATOMS 262144
+#define DPD_NOALLOC_MAX_CELLS 262144
+#define DPD_NOALLOC_MAX_TYPES 8
+
+typedef struct dpd_pair_params {
+    double lo[3];
+    double hi[3];
+    int ntypes;
+    double coeff[DPD_NOALLOC_MAX_TYPES][DPD_NOALLOC_MAX_TYPES][3]; /* A, gamma, rc; symmetric */
+    double kT;      /* pair_style dpd temp */
+    double dt;      /* timestep */
+    uint32_t seed;  /* pair_style dpd seed */
+} dpd_pair_params;
+
+int dpd_pair_forces_noalloc(const dpd_pair_params* params, const float* d_pos, const float* d_vel,
+                            const int* d_id, const int* d_type, int n, uint32_t step, float* d_force,
+                            void* stream);
+
 /* Library version string. */
 const char* dpd_version(void);
 
