@@ -151,6 +151,8 @@ def run_ours(args, world, rank, local):
     from gpumdpd_b200 import Engine
     system = make_system(args)
     eng = Engine(system.run_in, system=system.c_system())
+    if args.pair_variant is not None:
+        eng.set_tuning(pair_variant=args.pair_variant, cell_order=1)
     eng.run(0)
     eng.run(args.warmup)
     ls = eng.list_stats()
@@ -289,6 +291,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="melt", choices=["melt", "melt_mid", "melt_small", "plain", "slab"])
     ap.add_argument("--skin", type=float, default=0.3)
+    ap.add_argument("--pair-variant", type=int, default=None,
+                    help="pair-kernel schedule (default: the engine's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -203,7 +203,7 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
     if (tune) tune_ = *tune;
     if (!tune) {
         tune_.cell_order = 1;
-        tune_.pair_variant = 1;
+        tune_.pair_variant = 4;
     }
     int st = layout();
     if (st) return st;
@@ -260,7 +260,13 @@ int Engine::alloc_and_upload()
     DA(b_.rdf_hist, nrdf);
     DA(b_.build_flag, 2);
     DA(b_.phase, 1);
+    DA(b_.limit, nrep);
 #undef DA
+    {
+        std::vector<uint32_t> lim(nrep, 0xFFFFFFFFu);
+        CK(cudaMemcpyAsync(b_.limit, lim.data(), sizeof(uint32_t) * nrep, cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+    }
     // tables
     std::vector<RepDesc> hd(nrep);
     std::vector<int> wrep(P_ / 32), crank(C_, 0), cell_rep(C_, 0), cell_lin(C_, -1);
@@ -512,12 +518,15 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
     if (variant == 0) k_pair<STYLE, BONDS><<<grid, 256, 0, s>>>(a);
     else if (variant == 2) k_pair_q<STYLE, BONDS, 4, true><<<grid, 256, 0, s>>>(a);
     else if (variant == 3) k_pair_q<STYLE, BONDS, 3, false><<<grid, 256, 0, s>>>(a);
+    else if (variant == 4) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
+    else if (variant == 5) k_pair_flat<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
     else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
 }
 
-// pair_variant 0: thread per particle; 1 (default): warp pair-queue, i-side and
+// pair_variant 0: thread per particle; 1: warp pair-queue, i-side and
 // j-side forces by float4 reductions in L2, 4 blocks/SM; 2: warp pair-queue with the
-// i-side reduced through shared-memory atomics; 3: as 1 with 3 blocks/SM
+// i-side reduced through shared-memory atomics; 3: as 1 with 3 blocks/SM; 4: flattened
+// warp schedule, 4 blocks/SM (the default); 5: flattened, 3 blocks/SM
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -587,38 +596,45 @@ int Engine::build_graph()
 
 // set the run target of every replica (absolute step), optionally mark the next
 // evaluation as a zero step and raise the list-build flag of the current phase
-__global__ void k_set_target(RepState* st, int nrep, uint32_t target, int zero, int set_build,
-                             int* build_flag, const uint32_t* phase)
+__global__ void k_set_target(RepState* st, const uint32_t* limit, int nrep, uint32_t target, int zero,
+                             int set_build, int* build_flag, const uint32_t* phase)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nrep) {
-        st[r].target = target;
+        st[r].target = min(target, limit[r]);
         if (zero) st[r].zero_pending = 1;
     }
     if (r == 0 && set_build) build_flag[(*phase) & 1] = 1;
 }
 
-int Engine::run(uint32_t nsteps)
+int Engine::run_async(uint32_t nsteps)
 {
     const int nrep = (int)reps_.size();
     const int g = (nrep + 255) / 256;
     if (zero_pending_) {
         // zero step at next_step_, then nsteps steps
         const uint32_t target = next_step_ + nsteps;
-        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, nrep, target, 1, 1, b_.build_flag, b_.phase);
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 1, 1, b_.build_flag, b_.phase);
         CK(cudaGetLastError());
         for (uint32_t k = 0; k <= nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
         next_step_ = target + 1;
         zero_pending_ = false;
     } else {
-        if (nsteps == 0) return sync_and_check();
+        if (nsteps == 0) return DPD_OK;
         const uint32_t target = next_step_ - 1 + nsteps;
-        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, nrep, target, 0, 0, b_.build_flag, b_.phase);
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 0, 0, b_.build_flag, b_.phase);
         enqueue_integrate_initial(stream_);
         CK(cudaGetLastError());
         for (uint32_t k = 0; k < nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
         next_step_ = target + 1;
     }
+    return DPD_OK;
+}
+
+int Engine::run(uint32_t nsteps)
+{
+    int e = run_async(nsteps);
+    if (e) return e;
     return sync_and_check();
 }
 
@@ -674,7 +690,7 @@ int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64
     std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 2);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     const uint32_t target = next_step_ - 1 + nsteps;
-    k_set_target<<<(nrep + 255) / 256, 256, 0, stream_>>>(b_.rstate, nrep, target, 0, 0, b_.build_flag, b_.phase);
+    k_set_target<<<(nrep + 255) / 256, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 0, 0, b_.build_flag, b_.phase);
     enqueue_integrate_initial(stream_);
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -707,10 +723,54 @@ int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64
     return sync_and_check();
 }
 
-int Engine::set_targets(const std::vector<uint32_t>& target)
+int Engine::set_limits(const std::vector<uint32_t>& limit)
 {
-    (void)target;
-    return DPD_E_STATE;
+    if (limit.size() != reps_.size()) return DPD_E_ARG;
+    CK(cudaMemcpyAsync(b_.limit, limit.data(), sizeof(uint32_t) * limit.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
+// Device bytes that init() allocates for these replicas, from the same sizes as
+// layout() and alloc_and_upload() (the server admits jobs against its budget with it).
+int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
+{
+    int64_t P = 0, C = 0, ntag = 0, ncoeff = 0, nmass = 0, nbond = 0, nrdf = 0;
+    int64_t nmax = 16, maxb = 0;
+    const int64_t nrep = (int64_t)reps.size();
+    for (const Replica* R : reps) {
+        const double cut = R->in.global_cut + R->in.skin;
+        int64_t ncell = 1;
+        for (int k = 0; k < 3; k++)
+            ncell *= std::max(1, (int)std::floor((R->sys.hi[k] - R->sys.lo[k]) / cut));
+        const int64_t n = R->sys.n_atoms;
+        P += ((n + 31) / 32) * 32;
+        C += ncell + 1;
+        ntag += n;
+        const int64_t nt = R->sys.n_atomtypes;
+        ncoeff += nt * nt * 3;
+        nmass += nt;
+        nbond += std::max(R->sys.n_bondtypes, 1);
+        nrdf += R->ff.rdfs.empty() ? 0 : R->ff.rdfs[0].nbins;
+        const double sphere = 4.0 / 3.0 * M_PI * std::pow(cut, 3.0);
+        const int64_t nm = (int64_t)(R->in.max_rho * sphere) + 1;
+        nmax = std::max(nmax, ((nm + 15) / 16) * 16);
+        if (R->sys.n_bonds > 0) {
+            std::vector<int> deg(n, 0);
+            for (int b = 0; b < R->sys.n_bonds; b++) {
+                deg[R->sys.bonds[3 * b + 1] - 1]++;
+                deg[R->sys.bonds[3 * b + 2] - 1]++;
+            }
+            for (int d : deg) maxb = std::max<int64_t>(maxb, d);
+        }
+    }
+    const int64_t mb = std::max<int64_t>(maxb, 1);
+    int64_t bytes = nrep * ((int64_t)sizeof(RepDesc) + (int64_t)sizeof(RepState) + 4);
+    bytes += (P / 32) * 4 + ncoeff * 16 + nmass * 8 + nbond * 16 + nrdf * 8;
+    bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 4 + 4 * nmax + mb * 8);
+    bytes += C * (4 * 6) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
+    bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
+    return bytes;
 }
 
 int64_t Engine::steps_done(int r) const
@@ -1033,6 +1093,11 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
+    if (t->pair_variant < 0 || t->pair_variant > 5 || t->cell_order < 0 || t->cell_order > 1 ||
+        t->pair_block < 0) {
+        err = "dpd_set_tuning: pair_variant must be 0..5, cell_order 0 or 1";
+        return DPD_E_ARG;
+    }
     tune_ = *t;
     return build_graph();
 }

@@ -44,6 +44,7 @@ struct DeviceBuffers {
     unsigned long long* rdf_hist = nullptr;
     int* build_flag = nullptr;
     uint32_t* phase = nullptr;
+    uint32_t* limit = nullptr;  // per replica: last step it may evaluate (job length)
 };
 
 class Engine {
@@ -56,6 +57,8 @@ public:
     // replicas must be fully parsed; builds the packed layout and uploads it
     int init(std::vector<Replica>&& reps, const dpd_tuning* tune);
     int run(uint32_t nsteps);
+    // enqueue nsteps steps on the engine's stream and return without waiting
+    int run_async(uint32_t nsteps);
     int sync_and_check();
     int time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64_t* launches);
     int get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows);
@@ -81,9 +84,12 @@ public:
     int64_t total_atoms() const;
     std::string err;
 
-    // for the server: extend/replace per-replica targets
-    int set_targets(const std::vector<uint32_t>& target);
+    // per-replica step limits: replica r evaluates no step beyond limit[r]
+    int set_limits(const std::vector<uint32_t>& limit);
     int read_rstate(std::vector<RepState>& st);
+    cudaStream_t stream() const { return stream_; }
+    // device bytes init() would allocate for these replicas (no CUDA calls)
+    static int64_t estimate_bytes(const std::vector<const Replica*>& reps);
 
 private:
     int layout();

@@ -99,6 +99,25 @@ __device__ __forceinline__ void acc_flush(double (&val)[NV], const int* field, i
     }
 }
 
+// The same per warp: warp reduce, then lane k adds field k into the spread slot of this
+// warp.  Needs no block barrier; call it from warp-uniform code only.
+template <int NV>
+__device__ __forceinline__ void acc_flush_warp(double (&val)[NV], const int* field, int rep, double* acc)
+{
+    const int lane = threadIdx.x & 31;
+    const int slot = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & (DPD_ACC_SLOTS - 1);
+    double mine = 0.0;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double x = val[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == k) mine = x;
+    }
+    if (lane < NV && mine != 0.0)
+        atomicAdd(&acc[((size_t)rep * DPD_ACC_SLOTS + slot) * DPD_NACC + field[lane]], mine);
+}
+
 // ---------------------------------------------------------------------------------
 // Double-buffered particle arrays; `par` selects the current buffer.
 struct PBuf {

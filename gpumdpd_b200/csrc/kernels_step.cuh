@@ -455,6 +455,123 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 }
 
 // ---------------------------------------------------------------------------------
+// Pair force, flattened warp schedule.  The list entries of a warp's 32 particles are
+// taken as one sequence, particle by particle (lane-major); an exclusive scan of the
+// counts gives each particle's start.  Every iteration evaluates 32 consecutive entries,
+// one per lane, so all lanes are busy whatever the per-particle counts, with no
+// compaction queue; the owner of entry t is found by a 5-step binary search over the
+// starts.  The next chunk's entries are fetched while the current chunk is evaluated, and
+// the pos/vel gathers of a chunk are issued together, so each chunk waits for one L2
+// round trip.  Entries outside rc idle their lane for the Saru part, so this schedule
+// suits small skins (at skin 0 every listed pair is inside rc).  Both the i-side and
+// j-side forces go to L2 as float4 reductions.  FP64 log sums are flushed per warp, so
+// no block barrier is needed on non-log steps.
+template <int STYLE, bool BONDS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
+{
+    __shared__ int s_start[8][33];
+    __shared__ float4 s_pi[8][32];
+    __shared__ float4 s_vi[8][32];
+    __shared__ float s_rho[8][32];
+    __shared__ float4 tab[8][27];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((s & ~31) >= a.P) return;  // whole warp beyond the slots
+    const int r = a.warp_rep[s >> 5];
+    const RepState st = a.rstate[r];
+    const RepDesc& d = a.reps[r];
+    if (!rep_active(st) || d.style != STYLE) return;  // warp-uniform
+    const bool work = s < d.p_end;
+    const uint32_t step = st.step;
+    const bool log = (step % (uint32_t)d.log_f) == 0u;
+    double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int par = *a.parity;
+    const float4* pos = a.buf.pos[par];
+    const float4* vel = a.buf.vel[par];
+    fill_shift(tab[warp], d, lane);
+    float4 pi = make_float4(0, 0, 0, 0), vi = make_float4(0, 0, 0, 0);
+    float rho_i = 0.0f;
+    int n = 0;
+    if (work) {
+        pi = pos[s];
+        vi = vel[s];
+        if (STYLE == 1) rho_i = a.rho[s];
+        n = min(a.ncount[s], a.nmax);
+    }
+    s_pi[warp][lane] = pi;
+    s_vi[warp][lane] = vi;
+    s_rho[warp][lane] = rho_i;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    s_start[warp][lane] = incl - n;
+    if (lane == 31) s_start[warp][32] = total;
+    __syncwarp();
+    const int* wl = a.nlist + (size_t)(s >> 5) * a.nmax * 32;
+    const float rcmax2 = d.rcmax2;
+    const float4* cbase = a.coeff + d.coeff_off;
+    const int nt = d.ntypes;
+    const uint32_t seed = d.seed;
+    const int wbase = s & ~31;
+    // owner lane and list entry of flat entry t (t < total)
+    auto locate = [&](int t, int& l, int& ent) {
+        int lo = 0;  // largest l with start[l] <= t (empty particles share a start)
+#pragma unroll
+        for (int stp = 16; stp >= 1; stp >>= 1)
+            if (s_start[warp][lo + stp] <= t) lo += stp;
+        l = lo;
+        ent = __ldg(wl + (size_t)(t - s_start[warp][lo]) * 32 + lo);
+    };
+    int l_nx = 0, ent_nx = 0;
+    if (lane < total) locate(lane, l_nx, ent_nx);
+    for (int t0 = 0; t0 < total; t0 += 32) {
+        const bool valid = t0 + lane < total;
+        const int l = l_nx, ent = ent_nx;
+        float4 pj = make_float4(0, 0, 0, 0), vj = make_float4(0, 0, 0, 0);
+        float rho_j = 0.0f;
+        const int j = ent & DPD_J_MASK;
+        if (valid) {
+            pj = __ldg(pos + j);
+            vj = __ldg(vel + j);
+            if (STYLE == 1) rho_j = __ldg(a.rho + j);
+        }
+        if (t0 + 32 + lane < total) locate(t0 + 32 + lane, l_nx, ent_nx);
+        if (valid) {
+            const float4 pil = s_pi[warp][l];
+            float dx, dy, dz;
+            pair_disp(tab[warp], ent, pil, pj, dx, dy, dz);
+            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+            if (r2 <= rcmax2) {
+                const float4 vv = s_vi[warp][l];
+                const float4* crow = cbase + type0_of(vv.w) * nt * 3;
+                float fx, fy, fz;
+                const bool ok = log ? pair_force<STYLE, true>(crow, r2, dx, dy, dz, vv, vj, s_rho[warp][l], rho_j, seed, step, fx, fy, fz, accv)
+                                    : pair_force<STYLE, false>(crow, r2, dx, dy, dz, vv, vj, s_rho[warp][l], rho_j, seed, step, fx, fy, fz, accv);
+                if (ok) {
+                    atomicAdd(&a.force4[j], make_float4(-fx, -fy, -fz, 0.0f));
+                    atomicAdd(&a.force4[wbase + l], make_float4(fx, fy, fz, 0.0f));
+                }
+            }
+        }
+    }
+    if (BONDS && work) {
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        if (log) bond_loop<true>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+        else bond_loop<false>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+        atomicAdd(&a.force4[s], make_float4(fx, fy, fz, 0.0f));
+    }
+    if (log) {
+        const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
+                               ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+        acc_flush_warp<8>(accv, fields, r, a.acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Velocity Verlet, src/fix/fix_nve.cu:30-152, fused: final half kick of step n (and
 // the thermo sums of step n), then initial half kick + drift of step n+1, the
 // displacement check for the next list build (src/force/neigh_list.cu:483-514), and

@@ -77,7 +77,8 @@ typedef struct dpd_thermo {
  * mean "engine default". */
 typedef struct dpd_tuning {
     int pair_block;        /* threads per block of the pair kernel               */
-    int pair_variant;      /* 0 = thread per particle, 1 = warp pair-queue         */
+    int pair_variant;      /* 0 = thread per particle, 1-3 = warp pair-queue,
+                              4-5 = flattened warp schedule (small skins)         */
     int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
     int reserved[5];
 } dpd_tuning;

@@ -86,6 +86,36 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("name", ["mdpd_slab", "diblock", "mix_rc"])
+def test_pair_schedules_agree_with_oracle(oracle_mod, name, variant):
+    """Every pair-kernel schedule the tuner may pick gives the oracle's step-0 forces and
+    thermo (log step: PE and virial accumulated by the same kernel)."""
+    s, g = _golden_system(name)
+    e = _engine_from(s)
+    e.set_tuning(pair_variant=variant, cell_order=1)
+    e.run(0)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, st["x"], st["v"], s.lo, _box(e), 0,
+                          bonds=s.bonds)
+    assert force_err(st["f"], o["f"]) < FORCE_TOL
+    th = e.thermo()
+    assert th["pair_pe"][0] == pytest.approx(o["pair_pe"], rel=1e-6)
+    assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
+    # five non-log steps (with list reuse) agree with the default schedule up to FP32
+    # summation order
+    e.run(5)
+    base = _engine_from(s)
+    base.run(0)
+    base.run(5)
+    a, b = e.state(), base.state()
+    dx = a["x"] - b["x"]
+    dx -= _box(e) * np.round(dx / _box(e))
+    assert np.abs(dx).max() < 1e-4
+    assert force_err(a["f"], b["f"]) < 1e-4
+
+
 @pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock"])
 def test_trajectory_10_steps(oracle_mod, name):
     """After equilibrating 100 steps on the GPU, 10 steps of engine and oracle from the
