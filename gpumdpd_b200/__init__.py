@@ -7,5 +7,6 @@ synthetic inputs (`inputs`).
 """
 from .capi import DpdError, load  # noqa: F401
 from .engine import Batch, Engine  # noqa: F401
+from .server import Server  # noqa: F401
 
-__all__ = ["Engine", "Batch", "DpdError", "load"]
+__all__ = ["Engine", "Batch", "Server", "DpdError", "load"]

@@ -770,7 +770,7 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 4 + 4 * nmax + mb * 8);
     bytes += C * (4 * 6) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
-    return bytes;
+    return bytes + 64 * 1024 + nrep * 1024;  // arrays of size 0 still take one element
 }
 
 int64_t Engine::steps_done(int r) const
