@@ -1,11 +1,16 @@
 """bench.py -- timestep throughput of the B200 DPD engine (one JSON line on rank 0).
 
-Workload (default): the binary A5B5 diblock melt -- periodic 100^3 box at density 3,
+Headline workload: the binary A5B5 diblock melt -- periodic 100^3 box at density 3,
 N = 3.0M beads in 300k linear 10-bead chains, harmonic bonds k=4 r0=0, a_AA=a_BB=25,
-a_AB=40, gamma=4.5, kT=1, dt=0.04, skin 0.3 -- seeded synthetic input (chains grown as
-random walks with step 0.9; no dataset).  A step is one velocity-Verlet timestep of the
-whole system (list build when due, pair+bond forces with the Saru random force, fused
-integration).  Metric: particle-steps/s.
+a_AB=40, gamma=4.5, kT=1, dt=0.04 -- seeded synthetic input (chains grown as random walks
+with step 0.9; no dataset), skin 0 (the tuner's choice: this system rebuilds its list
+every step at any skin up to 0.3).  A step is one velocity-Verlet timestep of the whole
+system (list build when due, pair+bond forces with the Saru random force, fused
+integration).  Value: particle-steps/s.
+
+Beside it (N=1 only): "batched" -- 256 uneven A/B mixtures in one packed engine against
+the plain engine one replica at a time; "served" -- a Poisson stream of jobs through the
+continuous-batching server (p50/p99 latency) against the plain engine one job at a time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -26,7 +31,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "a5b5_diblock_melt_L100_N3M_skin0.3"
+METRIC = "particle-steps/s: batched/served vs plain at matched P,T error; p50/p99 latency"
+
+
+def workload_name(args):
+    if args.workload == "melt":
+        return f"a5b5_diblock_melt_L100_N3M_skin{args.skin}"
+    return f"{args.workload}_skin{args.skin}"
 
 
 def make_system(args):
@@ -149,19 +160,28 @@ def cpu_baseline(system, nthreads, nsteps=2):
 def run_ours(args, world, rank, local):
     import torch
     from gpumdpd_b200 import Engine
+    tuned = "defaults (skin and schedule chosen by gpumdpd_b200/tune.py on this workload)"
+    if args.tune:
+        from gpumdpd_b200 import tune
+        best, table = tune.tune_system(make_system(args))
+        args.skin = best["skin"]
+        args.pair_variant = best["pair_variant"]
+        tuned = {"best": best, "table": table}
     system = make_system(args)
     eng = Engine(system.run_in, system=system.c_system())
-    if args.pair_variant is not None:
-        eng.set_tuning(pair_variant=args.pair_variant, cell_order=1)
+    pair_variant = 4 if args.pair_variant is None else args.pair_variant
+    eng.set_tuning(pair_variant=pair_variant, cell_order=1)
     eng.run(0)
     eng.run(args.warmup)
     ls = eng.list_stats()
+    b0 = eng.info()["builds"]
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         res = eng.time_steps(args.steps)
     torch.cuda.synchronize()
     barrier(world)
+    builds_per_step = (eng.info()["builds"] - b0) / args.steps
     total_ms = allreduce_max(res["total_ms"], world)
     pair_ms = res["pair_ms"]
     n = system.n
@@ -202,14 +222,15 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     out = {
-        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64-reductions",
         "data": "synthetic (seeded generator, gpumdpd_b200/inputs.py)",
-        "config": {"workload": WORKLOAD if args.workload == "melt" else args.workload, "n_particles": n,
+        "config": {"workload": workload_name(args), "n_particles": n,
                    "n_bonds": 0 if system.bonds is None else len(system.bonds), "box": system.box.tolist(),
                    "dt": 0.04, "skin": args.skin, "mean_half_list": ls["mean_half_list"],
-                   "list_builds": ls["builds"], "parallelism": f"replicas{world}",
+                   "list_builds_per_step": builds_per_step, "pair_variant": pair_variant,
+                   "tuned": tuned, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state+list > 1 GB)"},
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "chunk_steps": chunk, "path": "dpd_set_state + dpd_run + dpd_get_state (C ABI, host buffers)"},
@@ -221,12 +242,128 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(res["pair_launches"] * 12 + 2),
         "impl": "ours",
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(system, os.cpu_count() or 1)
-    if rank == 0:
-        print(json.dumps(out))
     del th, st2
     eng.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(system, os.cpu_count() or 1)
+    if world == 1 and not args.no_extras:
+        out["batched"] = run_batched(args)
+        out["served"] = run_served(args)
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def plain_step_ms(system, steps):
+    """The plain engine on one system alone: device ms per step over `steps` steps (after
+    the zero step and a 3-step warm-up; creation is not timed)."""
+    from gpumdpd_b200 import Engine
+    eng = Engine(system.run_in, system=system.c_system())
+    eng.run(0)
+    eng.run(3)
+    r = eng.time_steps(steps)
+    th = eng.thermo()
+    eng.close()
+    return r["total_ms"] / steps, th
+
+
+def run_batched(args):
+    """Batched sweep: uneven A/B mixtures (a_AB over 25..45, L log-uniform over 8..24) in one
+    packed engine, one launch per stage and the step captured in a CUDA graph, against the
+    plain engine running the same replicas one at a time (device time per step summed)."""
+    from gpumdpd_b200 import Batch, inputs, tune
+    systems = inputs.replica_sweep(n_rep=args.replicas, nsteps=5000)
+    for s in systems:
+        s.run_in = tune.with_skin(s.run_in, args.batch_skin)
+    n_tot = sum(s.n for s in systems)
+    b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
+              tuning={"pair_variant": 4, "cell_order": 1})
+    b.run(0)
+    b.run(args.warmup)
+    K = args.batch_steps
+    r = b.time_steps(K)
+    batched = n_tot * K / (r["total_ms"] / 1000.0)
+    rows_b = [b.thermo(k) for k in range(min(8, len(systems)))]
+    b.close()
+    plain_ms = []
+    rows_p = []
+    for k, s in enumerate(systems):
+        ms, th = plain_step_ms(s, args.plain_steps)
+        plain_ms.append(ms)
+        if k < 8:
+            rows_p.append(th)
+    plain = n_tot / (sum(plain_ms) / 1000.0)
+    # same physics: per-replica mean T and P over the rows both runs logged
+    dt_max = dp_max = 0.0
+    for tb, tp in zip(rows_b, rows_p):
+        m = min(len(tb["temp"]), len(tp["temp"]))
+        if m > 1:
+            dt_max = max(dt_max, abs(tb["temp"][1:m].mean() / tp["temp"][1:m].mean() - 1))
+            dp_max = max(dp_max, abs(tb["pressure"][1:m].mean() / tp["pressure"][1:m].mean() - 1))
+    return {"workload": f"{len(systems)}_replica_AB_sweep_L8-24_skin{args.batch_skin}", "replicas": len(systems),
+            "particles": n_tot, "value": batched, "unit": "particle-steps/s", "steps": K,
+            "plain_one_at_a_time": plain, "speedup_vs_plain": batched / plain,
+            "plain_steps_per_replica": args.plain_steps,
+            "matched_accuracy": {"same_kernels_and_precision": True,
+                                 "max_rel_diff_mean_T_first8": dt_max, "max_rel_diff_mean_P_first8": dp_max}}
+
+
+def served_run(jobs, args, rate_label):
+    """One pass of a job stream through the server; returns (summary, results, ids)."""
+    from gpumdpd_b200.server import Server, latency_percentiles
+    srv = Server(120e9, chunk_steps=args.chunk)
+    srv.set_policy(args.max_wait, args.min_jobs)
+    pending = list(jobs)
+    ids = []
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while pending and pending[0][0] <= now:
+            _, s, _ = pending.pop(0)
+            ids.append((srv.submit(s), s))
+        a, q = srv.step()
+        if a == 0 and q == 0:
+            if not pending:
+                break
+            time.sleep(max(0.0, pending[0][0] - (time.perf_counter() - t0)))
+    makespan = time.perf_counter() - t0
+    res = [srv.result(j) for j, _ in ids]
+    assert all(r["status"] == "done" for r in res), [r["status"] for r in res]
+    work = sum(s.n * r["steps"] for (_, s), r in zip(ids, res))
+    st = srv.stats()
+    srv.close()
+    pct = latency_percentiles(res)
+    return {"rate_jobs_per_s": rate_label, "value": work / makespan, "makespan_s": makespan,
+            "busy_s": st["busy_s"], "p50_latency_s": pct.get("p50"), "p99_latency_s": pct.get("p99"),
+            "particle_steps": work}, res, ids
+
+
+def run_served(args):
+    """Served stream: Poisson arrivals of DPD jobs (1-3 species, a_ij ~ U[25,50], N
+    log-uniform 1k-200k, A5B5 chains in 0-50% of beads, steps U[1k,20k], T/P/RDF
+    requested) through the continuous-batching server under a 120 GB budget; aggregate
+    particle-steps/s over the makespan and p50/p99 job latency, against the plain engine
+    running the same jobs one at a time (device time per step x steps, per job)."""
+    from gpumdpd_b200 import inputs
+    rates = [float(x) for x in args.rates.split(",")]
+    sweep = []
+    for rate in rates:
+        jobs = inputs.job_stream(n_jobs=args.jobs, seed=11, rate=rate, skin=args.batch_skin)
+        summary, res, ids = served_run(jobs, args, rate)
+        sweep.append(summary)
+    # the same jobs one at a time on the plain engine (job contents do not depend on the rate)
+    plain_s = 0.0
+    for (_, s), r in zip(ids, res):
+        ms, _ = plain_step_ms(s, min(args.plain_steps, r["steps"]))
+        plain_s += ms / 1000.0 * r["steps"]
+    plain = sweep[-1]["particle_steps"] / plain_s
+    head = max(sweep, key=lambda x: x["value"])
+    return {"workload": f"{len(ids)}_job_poisson_stream", "jobs": len(ids), "value": head["value"],
+            "unit": "particle-steps/s", "rate_jobs_per_s": head["rate_jobs_per_s"],
+            "p50_latency_s": head["p50_latency_s"], "p99_latency_s": head["p99_latency_s"],
+            "plain_one_at_a_time": plain, "speedup_vs_plain": head["value"] / plain, "rate_sweep": sweep,
+            "hbm_budget_bytes": 120e9, "chunk_steps": args.chunk,
+            "admission_window": {"max_wait_s": args.max_wait, "min_jobs": args.min_jobs},
+            "plain_timing": f"device time per step over min({args.plain_steps}, steps) steps x steps, per job"}
 
 
 def run_reference(args, world, rank):
@@ -243,9 +380,9 @@ def run_reference(args, world, rank):
     if not os.path.exists(binary):
         # no reference build: time the FP64 port on the host cores instead
         cb = cpu_baseline(system, os.cpu_count() or 1)
-        print(json.dumps({"metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s",
+        print(json.dumps({"metric": METRIC, "value": cb["value"], "unit": "particle-steps/s",
                           "n_gpus": world, "steps": 2, "warmup": 0, "higher_is_better": True, "impl": "reference",
-                          "config": {"workload": WORKLOAD}, "cpu_baseline": cb,
+                          "config": {"workload": workload_name(args)}, "cpu_baseline": cb,
                           "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
@@ -270,10 +407,10 @@ def run_reference(args, world, rank):
         return
     dt = stamps[2 * K] - stamps[K]
     value = system.n * K / dt
-    out = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+    out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
            "steps": K, "warmup": K, "ms_per_step": dt * 1000 / K, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator and seed)",
-           "config": {"workload": WORKLOAD, "n_particles": system.n, "skin": args.skin,
+           "config": {"workload": workload_name(args), "n_particles": system.n, "skin": args.skin,
                       "parallelism": "single GPU, rank 0 only"},
            "impl": "reference",
            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
@@ -290,10 +427,22 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="melt", choices=["melt", "melt_mid", "melt_small", "plain", "slab"])
-    ap.add_argument("--skin", type=float, default=0.3)
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="neighbour skin (0.0: the tuner's choice for the 3M melt, which rebuilds every step)")
+    ap.add_argument("--tune", action="store_true", help="run the autotuner first (skin and pair schedule)")
     ap.add_argument("--pair-variant", type=int, default=None,
                     help="pair-kernel schedule (default: the engine's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and served lines")
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--batch-skin", type=float, default=0.0)
+    ap.add_argument("--plain-steps", type=int, default=200)
+    ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--rates", default="4,64", help="served arrival rates (jobs/s) to sweep")
+    ap.add_argument("--max-wait", type=float, default=0.0, help="server admission window (s)")
+    ap.add_argument("--min-jobs", type=int, default=1, help="server admission batch size")
+    ap.add_argument("--chunk", type=int, default=200, help="server scheduling chunk (steps)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -23,7 +23,7 @@ EXPORTED = [
     "dpd_compute_rdf", "dpd_rdf_config", "dpd_rdf_result", "dpd_get_info", "dpd_set_tuning",
     "dpd_write_data", "dpd_time_steps", "dpd_get_list_stats", "dpd_last_error", "dpd_destroy", "dpd_pair_compute_aos",
     "dpd_batch_create", "dpd_batch_n", "dpd_batch_get_thermo", "dpd_batch_get_state",
-    "dpd_batch_rdf_result", "dpd_server_create", "dpd_server_submit", "dpd_server_step",
+    "dpd_batch_rdf_result", "dpd_server_create", "dpd_server_submit", "dpd_server_set_policy", "dpd_server_step",
     "dpd_server_result", "dpd_server_job_state", "dpd_server_job_rdf", "dpd_server_stats",
     "dpd_server_last_error", "dpd_server_destroy", "dpd_pair_forces_noalloc", "dpd_version",
 ]
@@ -126,6 +126,7 @@ def load():
         "dpd_batch_rdf_result": (i, [vp, i, vp, P(i64)]),
         "dpd_server_create": (i, [d, i, P(dpd_tuning), P(vp)]),
         "dpd_server_submit": (i, [vp, cp, P(dpd_system), P(i64)]),
+        "dpd_server_set_policy": (i, [vp, d, i]),
         "dpd_server_step": (i, [vp, P(i), P(i)]),
         "dpd_server_result": (i, [vp, i64, P(dpd_job_result)]),
         "dpd_server_job_state": (i, [vp, i64, vp, vp]),

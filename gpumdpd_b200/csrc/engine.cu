@@ -33,8 +33,10 @@ template <class T>
 int Engine::dalloc(T** p, size_t n)
 {
     size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc((void**)p, bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    // stream-ordered: neither allocation nor release synchronizes the device, so engines
+    // of the job server can come and go while other engines' kernels run
+    cudaError_t e = cudaMallocAsync((void**)p, bytes, stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     allocs_.push_back((void*)*p);
     dev_bytes_ += (int64_t)bytes;
     e = cudaMemsetAsync(*p, 0, bytes, stream_);
@@ -46,7 +48,8 @@ Engine::~Engine()
 {
     if (graph_) cudaGraphExecDestroy(graph_);
     if (stream_) cudaStreamSynchronize(stream_);
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) cudaFreeAsync(p, stream_);
+    if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : {(void*)h_pos_, (void*)h_vel_, (void*)h_frc_, (void*)h_img_})
         if (p) cudaFreeHost(p);
     if (stream_) cudaStreamDestroy(stream_);

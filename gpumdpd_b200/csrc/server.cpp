@@ -6,8 +6,9 @@
 //      memory of the admitted set fits the budget; the jobs admitted together become
 //      one cohort: one packed engine (one launch per stage for all of them, the step
 //      captured in a CUDA graph) on its own CUDA stream;
-//   2. advances every cohort by one chunk of steps, all cohorts enqueued before any is
-//      waited on, so the cohorts' kernels overlap on the device;
+//   2. keeps every cohort's stream fed with chunks of steps: a cohort whose chunk has
+//      completed gets its next one at once, without waiting for the others, so the
+//      cohorts' kernels overlap on the device;
 //   3. retires the jobs that reached their `run N`: their thermo rows, final state and
 //      RDF are copied out, and a cohort's device memory returns to the budget when its
 //      last job has finished.
@@ -23,6 +24,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dpd_b200.h"
@@ -58,6 +60,7 @@ struct Cohort {
     uint32_t max_steps = 0;     // longest job in the cohort
     uint32_t issued = 0;        // steps issued after the zero step
     bool started = false;
+    bool inflight = false;      // a chunk is enqueued and not yet checked
     int64_t bytes = 0;
 };
 
@@ -91,6 +94,8 @@ struct dpd_server {
     std::vector<std::unique_ptr<Cohort>> cohorts;
     int64_t next_id = 1;
     int64_t used_bytes = 0;
+    double max_wait_s = 0.0;  // admission window (see dpd_server_set_policy)
+    int min_jobs = 1;
     int64_t particle_steps = 0;
     double busy_s = 0;
     Clock::time_point t0 = Clock::now();
@@ -113,6 +118,12 @@ struct dpd_server {
 int dpd_server::admit()
 {
     if (queue.empty()) return DPD_OK;
+    // admission window: while cohorts are running, queued jobs are gathered until there
+    // are min_jobs of them or the oldest has waited max_wait_s, so that jobs arriving
+    // close together share one packed engine
+    if (!cohorts.empty() && (int)queue.size() < min_jobs &&
+        now() - jobs[queue.front()].submit_s < max_wait_s)
+        return DPD_OK;
     std::vector<int64_t> pick;
     int64_t sum = 0, slots = 0, sum_list = 0, sum_bond = 0;
     int nmax_c = 16, maxb_c = 0;
@@ -195,59 +206,72 @@ void dpd_server::retire_job(Cohort& c, int r, int64_t id)
     particle_steps += (int64_t)n * j.steps;
 }
 
-// Advance every cohort by one chunk: all are enqueued first (each on its own stream),
-// then waited on, so their kernels overlap; then finished jobs are retired.
+// One scheduling pass over the cohorts, without waiting for any of them: a cohort whose
+// chunk has completed is checked, its finished jobs are retired and its next chunk is
+// enqueued at once, so every cohort's stream stays fed while the others run and the
+// cohorts' kernels overlap on the device.  When no cohort has completed a chunk the pass
+// sleeps briefly instead of spinning.
 int dpd_server::advance()
 {
     if (cohorts.empty()) return DPD_OK;
     const double t_begin = now();
-    std::vector<int> rc(cohorts.size(), DPD_OK);
-    std::vector<uint32_t> todo(cohorts.size(), 0);
-    for (size_t k = 0; k < cohorts.size(); k++) {
-        Cohort& c = *cohorts[k];
-        const uint32_t n = std::min<uint32_t>((uint32_t)chunk, c.max_steps - c.issued);
-        todo[k] = n;
-        if (n == 0 && c.started) continue;
-        rc[k] = c.eng->run_async(n);  // the first call also runs the zero step
-    }
     int first_err = DPD_OK;
-    for (size_t k = 0; k < cohorts.size(); k++) {
-        Cohort& c = *cohorts[k];
-        if (!rc[k]) rc[k] = c.eng->sync_and_check();
-        c.started = true;
-        c.issued += todo[k];
+    bool progressed = false;
+    auto fail_cohort = [&](Cohort& c, int rc) {
         const double t = now();
-        if (rc[k]) {
-            for (size_t r = 0; r < c.jobs.size(); r++)
-                if (!c.finished[r]) {
-                    jobs[c.jobs[r]].status = rc[k];
-                    jobs[c.jobs[r]].finish_s = t;
-                    c.finished[r] = true;
-                }
-            err = "cohort failed: " + c.eng->err;
-            if (!first_err) first_err = rc[k];
-            continue;
-        }
-        std::vector<RepState> st;
-        if (c.eng->read_rstate(st)) continue;
-        for (size_t r = 0; r < c.jobs.size(); r++) {
-            if (c.finished[r]) continue;
-            if (st[r].step > jobs[c.jobs[r]].steps) {
-                retire_job(c, (int)r, c.jobs[r]);
+        for (size_t r = 0; r < c.jobs.size(); r++)
+            if (!c.finished[r]) {
+                jobs[c.jobs[r]].status = rc;
+                jobs[c.jobs[r]].finish_s = t;
                 c.finished[r] = true;
             }
+        err = "cohort failed: " + c.eng->err;
+        if (!first_err) first_err = rc;
+    };
+    for (auto& cp : cohorts) {
+        Cohort& c = *cp;
+        if (c.inflight) {
+            if (cudaStreamQuery(c.eng->stream()) == cudaErrorNotReady) continue;
+            c.inflight = false;
+            progressed = true;
+            int rc = c.eng->sync_and_check();
+            std::vector<RepState> st;
+            if (!rc) rc = c.eng->read_rstate(st);
+            if (rc) {
+                fail_cohort(c, rc);
+                continue;
+            }
+            for (size_t r = 0; r < c.jobs.size(); r++) {
+                if (c.finished[r]) continue;
+                if (st[r].step > jobs[c.jobs[r]].steps) {
+                    retire_job(c, (int)r, c.jobs[r]);
+                    c.finished[r] = true;
+                }
+            }
         }
+        if (std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; })) continue;
+        const uint32_t n = std::min<uint32_t>((uint32_t)chunk, c.max_steps - c.issued);
+        const int rc = c.eng->run_async(n);  // the first call also runs the zero step
+        if (rc) {
+            fail_cohort(c, rc);
+            continue;
+        }
+        c.started = true;
+        c.issued += n;
+        c.inflight = true;
+        progressed = true;
     }
     // release cohorts whose jobs have all finished
     for (size_t k = 0; k < cohorts.size();) {
         Cohort& c = *cohorts[k];
-        if (std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; })) {
+        if (!c.inflight && std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; })) {
             used_bytes -= c.bytes;
             cohorts.erase(cohorts.begin() + k);
         } else {
             k++;
         }
     }
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(100));
     busy_s += now() - t_begin;
     return first_err;
 }
@@ -295,6 +319,14 @@ int dpd_server_submit(dpd_server* srv, const char* run_in_text, const dpd_system
     srv->jobs.emplace(id, std::move(j));
     srv->queue.push_back(id);
     if (job_id) *job_id = id;
+    return DPD_OK;
+}
+
+int dpd_server_set_policy(dpd_server* srv, double max_wait_s, int min_jobs)
+{
+    if (!srv || !(max_wait_s >= 0) || min_jobs < 1) return DPD_E_ARG;
+    srv->max_wait_s = max_wait_s;
+    srv->min_jobs = min_jobs;
     return DPD_OK;
 }
 

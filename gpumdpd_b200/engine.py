@@ -199,6 +199,11 @@ class Batch:
     def run(self, nsteps):
         _check(self.lib.dpd_run(self.h, int(nsteps)), self.lib, self.h)
 
+    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0):
+        t = capi.dpd_tuning()
+        t.pair_block, t.pair_variant, t.cell_order = pair_block, pair_variant, cell_order
+        _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
+
     def thermo(self, rep, max_rows=4096):
         rows = (capi.dpd_thermo * max_rows)()
         n = ctypes.c_int()

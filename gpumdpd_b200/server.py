@@ -47,6 +47,11 @@ class Server:
         except Exception:
             pass
 
+    def set_policy(self, max_wait_s=0.0, min_jobs=1):
+        """Admission window: gather queued jobs into one batch until `min_jobs` wait or the
+        oldest has waited `max_wait_s` (only while other jobs are running)."""
+        self._check(self.lib.dpd_server_set_policy(self.h, float(max_wait_s), int(min_jobs)))
+
     def submit(self, system, run_in=None):
         """Queue a job; returns its id.  `run_in` defaults to the system's own text."""
         s, keep = system.c_system()

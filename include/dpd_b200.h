@@ -209,8 +209,16 @@ int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning
 /* Submit a job (copies the inputs); *job_id receives its id. */
 int dpd_server_submit(dpd_server* srv, const char* run_in_text, const dpd_system* sys,
                       int64_t* job_id);
-/* Advance the server by one scheduling chunk (admit, step, retire).  *n_active and
- * *n_queued receive the counts after the chunk. */
+/* Admission window.  While jobs are running, queued jobs are admitted together once
+ * min_jobs are waiting or the oldest has waited max_wait_s seconds (defaults 1 and 0:
+ * admit at every scheduling point).  Jobs admitted together share one packed engine,
+ * so a window trades a bounded extra wait for fewer, larger batches.  An idle server
+ * admits at once. */
+int dpd_server_set_policy(dpd_server* srv, double max_wait_s, int min_jobs);
+/* One scheduling pass (admit; for every cohort whose chunk of steps has completed,
+ * retire its finished jobs and enqueue its next chunk; never waits for a running chunk).
+ * Call it in a loop; *n_active and *n_queued receive the running and queued job counts
+ * after the pass. */
 int dpd_server_step(dpd_server* srv, int* n_active, int* n_queued);
 int dpd_server_result(dpd_server* srv, int64_t job_id, dpd_job_result* res);
 int dpd_server_job_state(dpd_server* srv, int64_t job_id, double* x, double* v);

@@ -100,7 +100,7 @@ def test_budget_admission_and_release():
     srv = Server(hbm_budget_bytes=budget, chunk_steps=32)
     ids = [srv.submit(s) for s in systems]
     saw_queue = False
-    for _ in range(10000):
+    for _ in range(10 ** 6):
         a, q = srv.step()
         assert srv.stats()["device_bytes"] <= budget
         saw_queue |= q > 0
