@@ -377,7 +377,9 @@ __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
     if (s >= a.P) return;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
-    if (s >= d.p_end) {
+    // ghosts, and replicas past their last step (a finished job of a server cohort),
+    // get no list
+    if (s >= d.p_end || a.rstate[r].step > a.rstate[r].target) {
         a.ncount[s] = 0;
         return;
     }

@@ -3,9 +3,9 @@
 // Jobs (a run.in text plus a system) are submitted at any time and queued.  At every
 // scheduling point (dpd_server_step) the server
 //   1. admits queued jobs, in submission order with backfilling, while the device
-//      memory of the admitted set fits the budget; the jobs admitted together become
-//      one cohort: one packed engine (one launch per stage for all of them, the step
-//      captured in a CUDA graph) on its own CUDA stream;
+//      memory of the admitted set fits the budget; admitted jobs of similar length
+//      (steps within a factor 2) become one cohort: one packed engine (one launch per
+//      stage for all of them, the step captured in a CUDA graph) on its own CUDA stream;
 //   2. keeps every cohort's stream fed with chunks of steps: a cohort whose chunk has
 //      completed gets its next one at once, without waiting for the others, so the
 //      cohorts' kernels overlap on the device;
@@ -108,6 +108,7 @@ struct dpd_server {
         return code;
     }
     int admit();
+    int make_cohort(const std::vector<int64_t>& ids);
     int advance();
     void retire_job(Cohort& c, int r, int64_t id);
 };
@@ -147,34 +148,53 @@ int dpd_server::admit()
         maxb_c = mb;
     }
     if (pick.empty()) return DPD_OK;
+    for (int64_t id : pick) queue.erase(std::find(queue.begin(), queue.end(), id));
+    // Jobs of similar length share a cohort (steps in [2^k, 2^(k+1))): a cohort's step
+    // costs as much as all its particles, finished jobs included, so a long job packed
+    // with many short ones would crawl after they finish.
+    std::map<int, std::vector<int64_t>> groups;
+    for (int64_t id : pick) {
+        int k = 0;
+        while ((jobs[id].steps >> (k + 1)) != 0u) k++;
+        groups[k].push_back(id);
+    }
+    int first_err = DPD_OK;
+    for (auto& g : groups) {
+        const int e = make_cohort(g.second);
+        if (e && !first_err) first_err = e;
+    }
+    return first_err;
+}
+
+int dpd_server::make_cohort(const std::vector<int64_t>& ids)
+{
     auto c = std::make_unique<Cohort>();
     std::vector<dpd::Replica> reps;
     std::vector<uint32_t> limits;
-    for (int64_t id : pick) {
+    for (int64_t id : ids) {
         Job& j = jobs[id];
         reps.push_back(std::move(j.rep));
         limits.push_back(j.steps);
         c->jobs.push_back(id);
         c->max_steps = std::max(c->max_steps, j.steps);
     }
-    c->finished.assign(pick.size(), false);
+    c->finished.assign(ids.size(), false);
     c->eng = std::make_unique<dpd::Engine>();
     int e = c->eng->init(std::move(reps), has_tune ? &tune : nullptr);
     if (!e) e = c->eng->set_limits(limits);
     const double t = now();
-    for (int64_t id : pick) queue.erase(std::find(queue.begin(), queue.end(), id));
     if (e) {
         // the jobs of a cohort that cannot be created fail with the engine's message
         const std::string msg = c->eng->err;
-        for (int64_t id : pick) {
+        for (int64_t id : ids) {
             jobs[id].status = e;
             jobs[id].finish_s = t;
         }
-        return fail(e, "admitting " + std::to_string(pick.size()) + " job(s): " + msg);
+        return fail(e, "admitting " + std::to_string(ids.size()) + " job(s): " + msg);
     }
     c->bytes = c->eng->device_bytes();
     used_bytes += c->bytes;
-    for (int64_t id : pick) {
+    for (int64_t id : ids) {
         jobs[id].status = JOB_RUNNING;
         jobs[id].start_s = t;
     }
