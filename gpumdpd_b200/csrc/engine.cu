@@ -523,13 +523,15 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
     else if (variant == 3) k_pair_q<STYLE, BONDS, 3, false><<<grid, 256, 0, s>>>(a);
     else if (variant == 4) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
     else if (variant == 5) k_pair_flat<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
+    else if (variant == 6) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
     else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
 }
 
 // pair_variant 0: thread per particle; 1: warp pair-queue, i-side and
 // j-side forces by float4 reductions in L2, 4 blocks/SM; 2: warp pair-queue with the
 // i-side reduced through shared-memory atomics; 3: as 1 with 3 blocks/SM; 4: flattened
-// warp schedule, 4 blocks/SM (the default); 5: flattened, 3 blocks/SM
+// warp schedule, 4 blocks/SM (the default); 5: flattened, 3 blocks/SM; 6: the flattened
+// schedule with the list build fused into it (DPD; mDPD falls back to 4)
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -538,7 +540,7 @@ static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const
 }
 
 // The list-build chain; every kernel returns at once unless this phase's flag is set.
-void Engine::enqueue_build(cudaStream_t s)
+void Engine::enqueue_build(cudaStream_t s, bool list)
 {
     const int nrep = (int)reps_.size();
     BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
@@ -553,7 +555,7 @@ void Engine::enqueue_build(cudaStream_t s)
     k_cell_sort<<<gc, 256, 0, s>>>(ba);
     k_permute<<<gp, 256, 0, s>>>(ba);
     k_flip<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
-    k_build_nlist<<<gp, 256, 0, s>>>(ba);
+    if (list) k_build_nlist<<<gp, 256, 0, s>>>(ba);
 }
 
 void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
@@ -561,11 +563,19 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     const int nrep = (int)reps_.size();
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
     const int gp = (P_ + 255) / 256;
-    enqueue_build(s);
+    const int variant = tune_.pair_variant;
+    // schedule 6: the DPD list build runs inside the pair kernel
+    const bool fused = variant == 6 && !any_mdpd_;
+    enqueue_build(s, !fused);
     if (any_mdpd_) k_density<<<gp, 256, 0, s>>>(sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
-    const int variant = tune_.pair_variant;
-    if (any_dpd_) launch_pair<0>(variant, bonds_, gp, s, sa);
+    if (fused) {
+        const BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
+        if (bonds_) k_build_pair<true, 4><<<gp, 256, 0, s>>>(sa, ba);
+        else k_build_pair<false, 4><<<gp, 256, 0, s>>>(sa, ba);
+    } else if (any_dpd_) {
+        launch_pair<0>(variant, bonds_, gp, s, sa);
+    }
     if (any_mdpd_) launch_pair<1>(variant, bonds_, gp, s, sa);
     if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
     if (rdf_) k_rdf<<<gp, 256, 0, s>>>(sa);
@@ -594,6 +604,7 @@ int Engine::build_graph()
     e = cudaGraphInstantiate(&graph_, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    CK(cudaGraphUpload(graph_, stream_));
     return DPD_OK;
 }
 
@@ -704,6 +715,9 @@ int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64
     ce = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+    // upload the executable graph before the timed region (a first launch would otherwise
+    // include the upload)
+    CK(cudaGraphUpload(ge, stream_));
     CK(cudaStreamSynchronize(stream_));
     CK(cudaEventRecord(ev[0], stream_));
     CK(cudaGraphLaunch(ge, stream_));
@@ -1096,9 +1110,9 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 5 || t->cell_order < 0 || t->cell_order > 1 ||
+    if (t->pair_variant < 0 || t->pair_variant > 6 || t->cell_order < 0 || t->cell_order > 1 ||
         t->pair_block < 0) {
-        err = "dpd_set_tuning: pair_variant must be 0..5, cell_order 0 or 1";
+        err = "dpd_set_tuning: pair_variant must be 0..6, cell_order 0 or 1";
         return DPD_E_ARG;
     }
     tune_ = *t;

@@ -96,7 +96,7 @@ private:
     int alloc_and_upload();
     int upload_particles();
     void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
-    void enqueue_build(cudaStream_t s);
+    void enqueue_build(cudaStream_t s, bool list = true);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
     int cur_parity();

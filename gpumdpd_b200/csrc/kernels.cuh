@@ -370,10 +370,8 @@ __constant__ int8_t c_half[13][3] = {
 // r2 = fma(dz,dz,fma(dy,dy,dx*dx)) <= (global_cut+skin)^2 in float with
 // d = (o_i - o_j) + (c_i - c_j) w, the reference's test (src/force/neigh_list.cu:373-382)
 // on the cell-offset representation.  Entries store j and the shift code of the pair.
-__global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
+__device__ __forceinline__ void build_nlist_slot(const BuildArgs& a, const int s)
 {
-    if (!build_on(a)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
@@ -442,4 +440,10 @@ __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
         count = a.nmax;
     }
     a.ncount[s] = count;
+}
+
+__global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
+{
+    if (!build_on(a)) return;
+    build_nlist_slot(a, blockIdx.x * blockDim.x + threadIdx.x);
 }

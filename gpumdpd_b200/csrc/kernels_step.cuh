@@ -466,8 +466,8 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 // suits small skins (at skin 0 every listed pair is inside rc).  Both the i-side and
 // j-side forces go to L2 as float4 reductions.  FP64 log sums are flushed per warp, so
 // no block barrier is needed on non-log steps.
-template <int STYLE, bool BONDS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
+template <int STYLE, bool BONDS>
+__device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
 {
     __shared__ int s_start[8][33];
     __shared__ float4 s_pi[8][32];
@@ -524,7 +524,8 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
         for (int stp = 16; stp >= 1; stp >>= 1)
             if (s_start[warp][lo + stp] <= t) lo += stp;
         l = lo;
-        ent = __ldg(wl + (size_t)(t - s_start[warp][lo]) * 32 + lo);
+        // a plain load: the fused kernel reads entries its own warp has just written
+        ent = wl[(size_t)(t - s_start[warp][lo]) * 32 + lo];
     };
     int l_nx = 0, ent_nx = 0;
     if (lane < total) locate(lane, l_nx, ent_nx);
@@ -569,6 +570,27 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
                                ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
         acc_flush_warp<8>(accv, fields, r, a.acc);
     }
+}
+
+template <int STYLE, bool BONDS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
+{
+    pair_flat_warp<STYLE, BONDS>(a);
+}
+
+// List build fused with the flattened pair force (DPD only: mDPD needs every density
+// before any force).  On a build step each warp first builds its 32 particles' half list
+// (the list of the build kernel, bit for bit), then evaluates those pairs at once, while
+// the neighbours' positions are still in L1; on other steps it is the flattened pair
+// kernel.  One launch instead of two, and the list is read back from L1/L2.
+template <bool BONDS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs b)
+{
+    if (build_on(b)) {
+        build_nlist_slot(b, blockIdx.x * blockDim.x + threadIdx.x);
+        __syncwarp();
+    }
+    pair_flat_warp<0, BONDS>(a);
 }
 
 // ---------------------------------------------------------------------------------
