@@ -102,7 +102,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend="nccl"):
+    """One process per GPU (torch.distributed.run sets RANK/LOCAL_RANK/WORLD_SIZE).  The
+    only collectives are the barriers around the timed region and the max-over-ranks of
+    its time: replicas share nothing on the step path."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -111,10 +114,13 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        os.environ.setdefault("CUDA_VISIBLE_DEVICES_ORIG", "")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            os.environ["DPD_B200_DEVICE"] = str(local)  # the engine library's device
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
@@ -123,9 +129,17 @@ def allreduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_value(n_per_rank, steps, local_ms, world):
+    """Whole-job particle-steps/s: every rank advances its own replica of n particles, and
+    the job takes as long as the slowest rank."""
+    total_ms = allreduce_max(local_ms, world)
+    return world * n_per_rank * steps / (total_ms / 1000.0), total_ms
 
 
 def barrier(world):
@@ -182,10 +196,9 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     builds_per_step = (eng.info()["builds"] - b0) / args.steps
-    total_ms = allreduce_max(res["total_ms"], world)
-    pair_ms = res["pair_ms"]
     n = system.n
-    value = world * n * args.steps / (total_ms / 1000.0)
+    value, total_ms = job_value(n, args.steps, res["total_ms"], world)
+    pair_ms = res["pair_ms"]
     # end to end through the C ABI with host buffers: the state (x, v in FP64) goes host
     # -> device, K steps run (a zero-step force evaluation and list build first), the
     # final x, v come back device -> host with the thermo rows

@@ -5,6 +5,7 @@
 //   [final half kick n, thermo n, initial half kick + drift n+1, build check] [advance]
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <atomic>
@@ -197,6 +198,16 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         err = "no CUDA device available (this engine has no CPU fallback)";
         return DPD_E_NODEV;
+    }
+    // one process per GPU: DPD_B200_DEVICE picks this process's device (the library's
+    // own CUDA runtime does not see a device chosen through another runtime copy)
+    if (const char* dv = std::getenv("DPD_B200_DEVICE")) {
+        const int dev = std::atoi(dv);
+        if (dev < 0 || dev >= ndev) {
+            err = "DPD_B200_DEVICE is not a device index";
+            return DPD_E_NODEV;
+        }
+        CK(cudaSetDevice(dev));
     }
     reps_ = std::move(reps);
     if (reps_.empty()) {
