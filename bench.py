@@ -260,10 +260,44 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(system, os.cpu_count() or 1)
     if world == 1 and not args.no_extras:
+        out["slab"] = run_slab(args)
         out["batched"] = run_batched(args)
         out["served"] = run_served(args)
     if rank == 0:
         print(json.dumps(out))
+
+
+def run_slab(args):
+    """Many-body DPD liquid slab: box 40x40x120, density 6 in z in [40,80] (N = 384k), A=-40,
+    B=25, rc=1, rd=0.75, gamma=4.5, kT=1, dt=0.01, two-pass density then force, 20k steps
+    timed on the device; the z density profile (bins 0.5) of the final state and
+    gamma_s = (Lz/2)<P_zz - (P_xx+P_yy)/2> over the second half of the run."""
+    from gpumdpd_b200 import Engine, inputs, observables, tune
+    s = inputs.mdpd_slab(nsteps=args.slab_steps, thermo=100)
+    s.run_in = tune.with_skin(s.run_in, args.batch_skin)
+    eng = Engine(s.run_in, system=s.c_system())
+    eng.set_tuning(pair_variant=4, cell_order=1)
+    eng.run(0)
+    total_ms, done = 0.0, 0
+    while done < args.slab_steps:  # timed in graphs of at most 500 steps
+        k = min(500, args.slab_steps - done)
+        total_ms += eng.time_steps(k)["total_ms"]
+        done += k
+    r = {"total_ms": total_ms}
+    th = eng.thermo()
+    st = eng.state(forces=False, images=False)
+    eng.close()
+    c, rho = observables.density_profile(st["x"], s.lo, s.hi, axis=2, width=0.5)
+    liq, vap = observables.slab_densities(c, rho, 40.0, 80.0, margin=5.0)
+    half = len(th["step"]) // 2
+    g, gerr = observables.surface_tension(th["p"], s.box[2], skip=half)
+    return {"workload": f"mdpd_slab_40x40x120_N{s.n}_skin{args.batch_skin}", "particles": s.n,
+            "steps": args.slab_steps, "value": s.n * args.slab_steps / (r["total_ms"] / 1000.0),
+            "unit": "particle-steps/s", "ms_per_step": r["total_ms"] / args.slab_steps,
+            "liquid_density": liq, "vapour_density": vap,
+            "surface_tension": g, "surface_tension_stderr": gerr,
+            "mean_temp_second_half": float(np.mean(th["temp"][half:])),
+            "density_profile_z0.5": [round(float(v), 3) for v in rho]}
 
 
 def plain_step_ms(system, steps):
@@ -447,6 +481,7 @@ def main():
                     help="pair-kernel schedule (default: the engine's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served lines")
+    ap.add_argument("--slab-steps", type=int, default=20000)
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-skin", type=float, default=0.0)
