@@ -183,7 +183,7 @@ def run_ours(args, world, rank, local):
         tuned = {"best": best, "table": table}
     system = make_system(args)
     eng = Engine(system.run_in, system=system.c_system())
-    pair_variant = 4 if args.pair_variant is None else args.pair_variant
+    pair_variant = 8 if args.pair_variant is None else args.pair_variant
     eng.set_tuning(pair_variant=pair_variant, cell_order=1)
     eng.run(0)
     eng.run(args.warmup)
@@ -276,7 +276,7 @@ def run_slab(args):
     s = inputs.mdpd_slab(nsteps=args.slab_steps, thermo=100)
     s.run_in = tune.with_skin(s.run_in, args.batch_skin)
     eng = Engine(s.run_in, system=s.c_system())
-    eng.set_tuning(pair_variant=4, cell_order=1)
+    eng.set_tuning(pair_variant=8, cell_order=1)
     eng.run(0)
     total_ms, done = 0.0, 0
     while done < args.slab_steps:  # timed in graphs of at most 500 steps
@@ -323,7 +323,7 @@ def run_batched(args):
         s.run_in = tune.with_skin(s.run_in, args.batch_skin)
     n_tot = sum(s.n for s in systems)
     b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
-              tuning={"pair_variant": 4, "cell_order": 1})
+              tuning={"pair_variant": 8, "cell_order": 1})
     b.run(0)
     b.run(args.warmup)
     K = args.batch_steps

@@ -217,7 +217,7 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
     if (tune) tune_ = *tune;
     if (!tune) {
         tune_.cell_order = 1;
-        tune_.pair_variant = 4;
+        tune_.pair_variant = 8;
     }
     int st = layout();
     if (st) return st;
@@ -535,14 +535,23 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
     else if (variant == 4) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
     else if (variant == 5) k_pair_flat<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
     else if (variant == 6) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
+    else if (variant == 7) {
+        k_pair_flat_split<STYLE, BONDS, 0, 6><<<grid, 256, 0, s>>>(a);
+        k_pair_flat_split<STYLE, BONDS, 1, 4><<<grid, 256, 0, s>>>(a);
+    } else if (variant == 8) {
+        k_pair_flat_split<STYLE, BONDS, 0, 5><<<grid, 256, 0, s>>>(a);
+        k_pair_flat_split<STYLE, BONDS, 1, 4><<<grid, 256, 0, s>>>(a);
+    }
     else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
 }
 
 // pair_variant 0: thread per particle; 1: warp pair-queue, i-side and
 // j-side forces by float4 reductions in L2, 4 blocks/SM; 2: warp pair-queue with the
 // i-side reduced through shared-memory atomics; 3: as 1 with 3 blocks/SM; 4: flattened
-// warp schedule, 4 blocks/SM (the default); 5: flattened, 3 blocks/SM; 6: the flattened
-// schedule with the list build fused into it (DPD; mDPD falls back to 4)
+// warp schedule, 4 blocks/SM; 5: flattened, 3 blocks/SM; 6: the flattened schedule with
+// the list build fused into it (DPD; mDPD falls back to 4); 7 and 8 (the default): the
+// flattened schedule as two launches, non-log steps without FP64 sums at 6 (7) or 5 (8)
+// blocks/SM, log steps at 4
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -1121,7 +1130,7 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 6 || t->cell_order < 0 || t->cell_order > 1 ||
+    if (t->pair_variant < 0 || t->pair_variant > 8 || t->cell_order < 0 || t->cell_order > 1 ||
         t->pair_block < 0) {
         err = "dpd_set_tuning: pair_variant must be 0..6, cell_order 0 or 1";
         return DPD_E_ARG;

@@ -466,7 +466,10 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 // suits small skins (at skin 0 every listed pair is inside rc).  Both the i-side and
 // j-side forces go to L2 as float4 reductions.  FP64 log sums are flushed per warp, so
 // no block barrier is needed on non-log steps.
-template <int STYLE, bool BONDS>
+// LOGM: 2 = any step; 0 = non-log steps only (no FP64 sums: fewer registers, more
+// warps per SM); 1 = log steps only.  0 and 1 are launched together, each returning at
+// once on the other kind of step.
+template <int STYLE, bool BONDS, int LOGM = 2>
 __device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
 {
     __shared__ int s_start[8][33];
@@ -483,7 +486,9 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
     if (!rep_active(st) || d.style != STYLE) return;  // warp-uniform
     const bool work = s < d.p_end;
     const uint32_t step = st.step;
-    const bool log = (step % (uint32_t)d.log_f) == 0u;
+    const bool log_step = (step % (uint32_t)d.log_f) == 0u;
+    if ((LOGM == 0 && log_step) || (LOGM == 1 && !log_step)) return;  // warp-uniform
+    const bool log = LOGM == 2 ? log_step : LOGM == 1;
     double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const int par = *a.parity;
     const float4* pos = a.buf.pos[par];
@@ -576,6 +581,12 @@ template <int STYLE, bool BONDS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
 {
     pair_flat_warp<STYLE, BONDS>(a);
+}
+
+template <int STYLE, bool BONDS, int LOGM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
+{
+    pair_flat_warp<STYLE, BONDS, LOGM>(a);
 }
 
 // List build fused with the flattened pair force (DPD only: mDPD needs every density

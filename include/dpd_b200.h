@@ -79,7 +79,9 @@ typedef struct dpd_tuning {
     int pair_block;        /* threads per block of the pair kernel               */
     int pair_variant;      /* 0 = thread per particle, 1-3 = warp pair-queue,
                               4-5 = flattened warp schedule (small skins),
-                              6 = flattened with the list build fused (DPD)       */
+                              6 = flattened with the list build fused (DPD),
+                              7-8 = flattened, log and non-log steps split (8 is
+                              the default)                                        */
     int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
     int reserved[5];
 } dpd_tuning;

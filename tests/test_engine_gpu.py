@@ -86,7 +86,7 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("name", ["mdpd_slab", "diblock", "mix_rc"])
 def test_pair_schedules_agree_with_oracle(oracle_mod, name, variant):
     """Every pair-kernel schedule the tuner may pick gives the oracle's step-0 forces and
