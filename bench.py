@@ -252,7 +252,9 @@ def run_ours(args, world, rank, local):
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "clocks": clk.summary(),
-        "gpu_launches": int(res["pair_launches"] * 12 + 2),
+        # per step: 9 list-build kernels (each returns at once unless a build is flagged),
+        # the pair kernel(s), integrate, advance; plus 2 before the graph
+        "gpu_launches": int(args.steps * (11 + (2 if pair_variant in (7, 8) else 1)) + 2),
         "impl": "ours",
     }
     del th, st2
