@@ -346,7 +346,7 @@ __global__ void k_permute(BuildArgs a)
     a.buf.pos[nxt][s] = p;
     a.buf.vel[nxt][s] = v;
     a.buf.img[nxt][s] = im;
-    a.last4[s] = p;
+    if (!d.skin_zero) a.last4[s] = p;  // skin 0 rebuilds unconditionally: no skin check
     for (int k = 0; k < a.maxb; k++) a.buf.bonds[nxt][(size_t)k * a.P + s] = a.buf.bonds[par][(size_t)k * a.P + o];
 }
 

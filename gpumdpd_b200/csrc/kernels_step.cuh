@@ -617,6 +617,14 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
     bool log = false;
     double accv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (s < a.P) {
+        // the particle's three streams are requested first (every slot < P is valid
+        // memory), so their latency overlaps the replica-state reads
+        const int par = *a.parity;
+        float4* posp = a.buf.pos[par];
+        float4* velp = a.buf.vel[par];
+        float4 v = velp[s];
+        const float4 f = a.force4[s];
+        float4 p = posp[s];
         r = a.warp_rep[s >> 5];
         const RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
@@ -628,11 +636,6 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
         const uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
         const bool check = init && (next % (uint32_t)d.nl_f) == 0u;
         if (work) {
-            const int par = *a.parity;
-            float4* posp = a.buf.pos[par];
-            float4* velp = a.buf.vel[par];
-            float4 v = velp[s];
-            const float4 f = a.force4[s];
             const int t0 = type0_of(v.w);
             const float2 m = __ldg(a.mass + d.mass_off + t0);
             const bool integ = (d.integ_mask >> t0) & 1u;
@@ -657,7 +660,6 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
                 accv[9] = mm * vz;
             }
             if (init) {
-                float4 p = posp[s];
                 if (integ) {
                     v.x = __fmaf_rn(dtm, f.x, v.x);
                     v.y = __fmaf_rn(dtm, f.y, v.y);
@@ -690,10 +692,11 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
             velp[s] = v;
         }
     }
-    if (a.mode == 0 && __syncthreads_or(log)) {
+    // `log` is warp-uniform (a warp holds one replica): a warp-level flush, no barrier
+    if (a.mode == 0 && log) {
         const int fields[10] = {ACC_KE, ACC_KIN + 0, ACC_KIN + 1, ACC_KIN + 2, ACC_KIN + 3,
                                 ACC_KIN + 4, ACC_KIN + 5, ACC_MOM + 0, ACC_MOM + 1, ACC_MOM + 2};
-        acc_flush<10>(accv, fields, log ? r : -1, a.acc);
+        acc_flush_warp<10>(accv, fields, r, a.acc);
     }
 }
 
