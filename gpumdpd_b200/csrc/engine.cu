@@ -1162,6 +1162,9 @@ int Engine::pair_compute_aos(const float* d_pos, const float* d_vel, const int* 
         if ((st = dalloc(&pe_slot_, P_))) return st;
         if ((st = dalloc(&vir_slot_, 6 * (size_t)P_))) return st;
     }
+    // the caller's buffers were written on the legacy default stream (the reference's own
+    // kernels): this engine's stream runs after that work
+    CK(cudaStreamSynchronize(cudaStreamLegacy));
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, 1);
     const int gp = (P_ + 255) / 256;
     k_aos_in<<<(n + 255) / 256, 256, 0, stream_>>>(sa, d_pos, d_vel, d_id, d_type, n, step, aos_built_ ? 0 : 1);

@@ -8,9 +8,14 @@
 # thrust::max_element/min_element without including <thrust/extrema.h>; the header is
 # force-included on the command line instead of editing any source.
 #
-# Usage: oracle/build_ref.sh [SINGLE|DOUBLE]   (default SINGLE, the reference's default)
+# Usage: oracle/build_ref.sh [SINGLE|DOUBLE|SHIM]   (default SINGLE, the reference's default)
+#   SHIM: the SINGLE build plus gpumdpd_b200/shim/pair_dpd_b200.cu (pair_style dpd/b200 and
+#   mdpd/b200, which hand the reference's device buffers to libdpd_b200), linked against
+#   the in-tree libdpd_b200.so -> oracle/_ref/gpudpd_single_b200.
 set -euo pipefail
-PREC="${1:-SINGLE}"
+MODE="${1:-SINGLE}"
+PREC="$MODE"
+[ "$MODE" = "SHIM" ] && PREC=SINGLE
 REF_SRC="${REF_SRC:-/root/reference/src}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
@@ -39,6 +44,14 @@ for src in "$REF_SRC"/*/*.cu; do
 done
 for p in "${pids[@]}"; do wait "$p"; done
 lower="$(echo "$PREC" | tr 'A-Z' 'a-z')"
+if [ "$MODE" = "SHIM" ]; then
+    REPO="$(cd "$HERE/.." && pwd)"
+    nvcc "${FLAGS[@]}" -I"$REPO/include" -dc "$REPO/gpumdpd_b200/shim/pair_dpd_b200.cu" -o "$OBJ/shim_pair_dpd_b200.o"
+    nvcc "${FLAGS[@]}" "${objs[@]}" "$OBJ/shim_pair_dpd_b200.o" -L"$REPO/gpumdpd_b200" -ldpd_b200 \
+        -Xlinker -rpath -Xlinker '$ORIGIN/../../gpumdpd_b200' -o "$OUT/gpudpd_single_b200"
+    echo "built $OUT/gpudpd_single_b200"
+    exit 0
+fi
 nvcc "${FLAGS[@]}" "${objs[@]}" -o "$OUT/gpudpd_${lower}"
 echo "built $OUT/gpudpd_${lower}"
 if [ "$PREC" = "SINGLE" ]; then
