@@ -248,7 +248,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "chunk_steps": chunk, "path": "dpd_set_state + dpd_run + dpd_get_state (C ABI, host buffers)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_pair (DPD + bonds)",
+                     "traffic": traffic, "kernel": "k_pair_flat (flattened pair schedule, DPD + bonds)",
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "clocks": clk.summary(),
