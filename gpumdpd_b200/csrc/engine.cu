@@ -261,7 +261,8 @@ int Engine::alloc_and_upload()
     DA(b_.cell_lin, C_);
     DA(b_.cnt, C_);
     DA(b_.cstart, C_ + 1);
-    DA(b_.fill, C_);
+    DA(b_.skey, P_);
+    DA(b_.srank, P_);
     DA(b_.perm, P_);
     int64_t ntag = 0;
     for (auto& R : reps_) ntag += R.sys.n_atoms;
@@ -479,7 +480,8 @@ static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int 
     a.last4 = b.last4;
     a.cnt = b.cnt;
     a.cstart = b.cstart;
-    a.fill = b.fill;
+    a.skey = b.skey;
+    a.srank = b.srank;
     a.perm = b.perm;
     a.tag2idx = b.tag2idx;
     a.ncount = b.ncount;
@@ -804,8 +806,8 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     const int64_t mb = std::max<int64_t>(maxb, 1);
     int64_t bytes = nrep * ((int64_t)sizeof(RepDesc) + (int64_t)sizeof(RepState) + 4);
     bytes += (P / 32) * 4 + ncoeff * 16 + nmass * 8 + nbond * 16 + nrdf * 8;
-    bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 4 + 4 * nmax + mb * 8);
-    bytes += C * (4 * 6) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
+    bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 4 + 8 + 4 * nmax + mb * 8);
+    bytes += C * (4 * 5) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
     return bytes + 64 * 1024 + nrep * 1024;  // arrays of size 0 still take one element
 }

@@ -11,7 +11,7 @@
 //   force4[s]= {fx, fy, fz, 0}           accumulated with vector atomics
 //   img[s]   = image counters (updated when a build re-bins across the box)
 // Slots are sorted by cell (counting sort at every build; cells in linear or Morton
-// order; within a cell by tag).  The half neighbour list is warp-chunked,
+// order; within a cell by previous slot, so the sort is stable).  The half neighbour list is warp-chunked,
 //   nlist[((s>>5)*nmax + k)*32 + (s&31)] = j | code<<27,
 // where code = 9(dcx+1)+3(dcy+1)+(dcz+1) encodes the cell difference c_i - c_j in
 // {-1,0,1}^3 of the pair at build time; the displacement is (o_i - o_j) + code*w.
@@ -147,7 +147,8 @@ struct BuildArgs {
     float4* last4;
     int* cnt;
     int* cstart;            // [C+1]
-    int* fill;
+    int* skey;              // [P] cell key of each slot at this build
+    int* srank;             // [P] arrival rank of the slot in its cell
     int* perm;
     int* tag2idx;
     int* ncount;
@@ -219,7 +220,9 @@ __global__ void k_bin_count(BuildArgs a)
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
-    atomicAdd(&a.cnt[slot_key(a, s, *a.parity)], 1);
+    const int key = slot_key(a, s, *a.parity);
+    a.skey[s] = key;
+    a.srank[s] = atomicAdd(&a.cnt[key], 1);
 }
 
 // exclusive scan of cnt[0..C) into cstart[0..C], three passes (block scan of 4096
@@ -290,12 +293,13 @@ __global__ void k_scatter(BuildArgs a)
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
-    const int key = slot_key(a, s, *a.parity);
-    int pos = a.cstart[key] + atomicAdd(&a.fill[key], 1);
+    // the rank the counting pass drew gives the place in the cell: no second atomic
+    const int pos = a.cstart[a.skey[s]] + a.srank[s];
     if (pos >= 0 && pos < a.P) a.perm[pos] = s;
 }
 
-// one thread per cell: insertion sort of the cell's slots by tag (deterministic order)
+// one thread per cell: insertion sort of the cell's slots by their previous slot, so the
+// counting sort is stable and the layout deterministic (the first layout is tag order)
 __global__ void k_cell_sort(BuildArgs a)
 {
     if (!build_on(a)) return;
@@ -303,16 +307,13 @@ __global__ void k_cell_sort(BuildArgs a)
     if (c >= a.C) return;
     int b = a.cstart[c], e = a.cstart[c + 1];
     a.cnt[c] = 0;
-    a.fill[c] = 0;
     if (b < 0 || e > a.P) return;
-    const float4* vel = a.buf.vel[*a.parity];
     for (int i = b + 1; i < e; i++) {
-        int si = a.perm[i];
-        int ti = tag_of(vel[si].w);
+        const int si = a.perm[i];
         int j = i - 1;
         while (j >= b) {
-            int sj = a.perm[j];
-            if (tag_of(vel[sj].w) <= ti) break;
+            const int sj = a.perm[j];
+            if (sj <= si) break;
             a.perm[j + 1] = sj;
             j--;
         }
