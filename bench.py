@@ -327,11 +327,28 @@ def run_batched(args):
     b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
               tuning={"pair_variant": 8, "cell_order": 1})
     b.run(0)
-    b.run(args.warmup)
     K = args.batch_steps
-    r = b.time_steps(K)
-    batched = n_tot * K / (r["total_ms"] / 1000.0)
-    rows_b = [b.thermo(k) for k in range(min(8, len(systems)))]
+    total_ms, done = 0.0, 0
+    while done < K:  # the whole sweep (5000 steps), timed in graphs of at most 500 steps
+        k = min(500, K - done)
+        total_ms += b.time_steps(k)["total_ms"]
+        done += k
+    batched = n_tot * K / (total_ms / 1000.0)
+    rows_b = [b.thermo(k) for k in range(len(systems))]
+    # per replica: mean pressure after the first fifth of the run, and the A-B RDF's first
+    # peak (height, position)
+    per_rep = []
+    for k, s in enumerate(systems):
+        th = rows_b[k]
+        skip = max(1, len(th["pressure"]) // 5)
+        g, ns = b.rdf(k, 150)
+        rmax = min(3.0, 0.5 * float(s.box[0]))
+        ipk = int(np.argmax(g))
+        per_rep.append({"a_ab": round(25.0 + 20.0 * k / max(len(systems) - 1, 1), 3), "n": s.n,
+                        "mean_p": round(float(th["pressure"][skip:].mean()), 4),
+                        "rdf_peak": round(float(g[ipk]), 4), "rdf_peak_r": round((ipk + 0.5) * rmax / 150, 3),
+                        "rdf_samples": ns})
+    rows_b = rows_b[:8]
     b.close()
     plain_ms = []
     rows_p = []
@@ -353,7 +370,8 @@ def run_batched(args):
             "plain_one_at_a_time": plain, "speedup_vs_plain": batched / plain,
             "plain_steps_per_replica": args.plain_steps,
             "matched_accuracy": {"same_kernels_and_precision": True,
-                                 "max_rel_diff_mean_T_first8": dt_max, "max_rel_diff_mean_P_first8": dp_max}}
+                                 "max_rel_diff_mean_T_first8": dt_max, "max_rel_diff_mean_P_first8": dp_max},
+            "per_replica": per_rep}
 
 
 def served_run(jobs, args, rate_label):
@@ -485,7 +503,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served lines")
     ap.add_argument("--slab-steps", type=int, default=20000)
     ap.add_argument("--replicas", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--batch-steps", type=int, default=5000)
     ap.add_argument("--batch-skin", type=float, default=0.0)
     ap.add_argument("--plain-steps", type=int, default=200)
     ap.add_argument("--jobs", type=int, default=64)
