@@ -542,7 +542,7 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
         k_pair_flat_split<STYLE, BONDS, 1, 4><<<grid, 256, 0, s>>>(a);
     } else if (variant == 8) {
         k_pair_flat_split<STYLE, BONDS, 0, 5><<<grid, 256, 0, s>>>(a);
-        k_pair_flat_split<STYLE, BONDS, 1, 4><<<grid, 256, 0, s>>>(a);
+        k_pair_flat_logsteps<STYLE, BONDS><<<std::min(grid, 148 * 4), 256, 0, s>>>(a);
     }
     else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
 }

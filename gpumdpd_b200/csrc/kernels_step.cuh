@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 // warps per SM); 1 = log steps only.  0 and 1 are launched together, each returning at
 // once on the other kind of step.
 template <int STYLE, bool BONDS, int LOGM = 2>
-__device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
+__device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
 {
     __shared__ int s_start[8][33];
     __shared__ float4 s_pi[8][32];
@@ -478,7 +478,6 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
     __shared__ float s_rho[8][32];
     __shared__ float4 tab[8][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if ((s & ~31) >= a.P) return;  // whole warp beyond the slots
     const int r = a.warp_rep[s >> 5];
     const RepState st = a.rstate[r];
@@ -580,13 +579,32 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a)
 template <int STYLE, bool BONDS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
 {
-    pair_flat_warp<STYLE, BONDS>(a);
+    pair_flat_warp<STYLE, BONDS>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <int STYLE, bool BONDS, int LOGM, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 {
-    pair_flat_warp<STYLE, BONDS, LOGM>(a);
+    pair_flat_warp<STYLE, BONDS, LOGM>(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The log-step half of the split schedule as a small grid-stride launch: every block
+// first checks whether any replica logs this step (the common answer is no, and then the
+// launch costs one wave of tiny blocks instead of a full grid of early exits).
+template <int STYLE, bool BONDS>
+__global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
+{
+    int any = 0;
+    for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
+        const RepState st = a.rstate[r];
+        any |= rep_active(st) && (st.step % (uint32_t)a.reps[r].log_f) == 0u;
+    }
+    if (!__syncthreads_or(any)) return;
+    const int nvb = (a.P + 255) / 256;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        pair_flat_warp<STYLE, BONDS, 1>(a, vb * 256 + threadIdx.x);
+        __syncwarp();  // the warp's shared slots are reused by the next virtual block
+    }
 }
 
 // List build fused with the flattened pair force (DPD only: mDPD needs every density
@@ -601,7 +619,7 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
         build_nlist_slot(b, blockIdx.x * blockDim.x + threadIdx.x);
         __syncwarp();
     }
-    pair_flat_warp<0, BONDS>(a);
+    pair_flat_warp<0, BONDS>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------
