@@ -528,23 +528,42 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     return a;
 }
 
+// Launch with programmatic dependent launch allowed: in a captured graph the kernel's
+// launch overlaps the tail of its predecessor (every step kernel starts with
+// griddep_wait(), which orders it after the predecessor's memory).
+template <typename... KArgs, typename... Args>
+static void pdl_launch(void (*kern)(KArgs...), int grid, int block, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <int STYLE, bool BONDS>
 static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& a)
 {
-    if (variant == 0) k_pair<STYLE, BONDS><<<grid, 256, 0, s>>>(a);
-    else if (variant == 2) k_pair_q<STYLE, BONDS, 4, true><<<grid, 256, 0, s>>>(a);
-    else if (variant == 3) k_pair_q<STYLE, BONDS, 3, false><<<grid, 256, 0, s>>>(a);
-    else if (variant == 4) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
-    else if (variant == 5) k_pair_flat<STYLE, BONDS, 3><<<grid, 256, 0, s>>>(a);
-    else if (variant == 6) k_pair_flat<STYLE, BONDS, 4><<<grid, 256, 0, s>>>(a);
+    if (variant == 0) pdl_launch(k_pair<STYLE, BONDS>, grid, 256, s, a);
+    else if (variant == 2) pdl_launch(k_pair_q<STYLE, BONDS, 4, true>, grid, 256, s, a);
+    else if (variant == 3) pdl_launch(k_pair_q<STYLE, BONDS, 3, false>, grid, 256, s, a);
+    else if (variant == 4) pdl_launch(k_pair_flat<STYLE, BONDS, 4>, grid, 256, s, a);
+    else if (variant == 5) pdl_launch(k_pair_flat<STYLE, BONDS, 3>, grid, 256, s, a);
+    else if (variant == 6) pdl_launch(k_pair_flat<STYLE, BONDS, 4>, grid, 256, s, a);
     else if (variant == 7) {
-        k_pair_flat_split<STYLE, BONDS, 0, 6><<<grid, 256, 0, s>>>(a);
-        k_pair_flat_split<STYLE, BONDS, 1, 4><<<grid, 256, 0, s>>>(a);
+        pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 6>, grid, 256, s, a);
+        pdl_launch(k_pair_flat_split<STYLE, BONDS, 1, 4>, grid, 256, s, a);
     } else if (variant == 8) {
-        k_pair_flat_split<STYLE, BONDS, 0, 5><<<grid, 256, 0, s>>>(a);
-        k_pair_flat_logsteps<STYLE, BONDS><<<std::min(grid, 148 * 4), 256, 0, s>>>(a);
+        pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5>, grid, 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 4), 256, s, a);
     }
-    else k_pair_q<STYLE, BONDS, 4, false><<<grid, 256, 0, s>>>(a);
+    else pdl_launch(k_pair_q<STYLE, BONDS, 4, false>, grid, 256, s, a);
 }
 
 // pair_variant 0: thread per particle; 1: warp pair-queue, i-side and
@@ -569,15 +588,15 @@ void Engine::enqueue_build(cudaStream_t s, bool list)
     const int gp = (P_ + 255) / 256;
     const int gc = (C_ + 255) / 256;
     const int nsb = (C_ + 4095) / 4096;
-    k_bin_count<<<gp, 256, 0, s>>>(ba);
-    k_scan_blocks<<<nsb, 1024, 0, s>>>(ba);
-    k_scan_sums<<<1, 1024, 0, s>>>(ba, nsb);
-    k_scan_add<<<gc, 256, 0, s>>>(ba);
-    k_scatter<<<gp, 256, 0, s>>>(ba);
-    k_cell_sort<<<gc, 256, 0, s>>>(ba);
-    k_permute<<<gp, 256, 0, s>>>(ba);
-    k_flip<<<(nrep + 255) / 256, 256, 0, s>>>(ba, nrep);
-    if (list) k_build_nlist<<<gp, 256, 0, s>>>(ba);
+    pdl_launch(k_bin_count, gp, 256, s, ba);
+    pdl_launch(k_scan_blocks, nsb, 1024, s, ba);
+    pdl_launch(k_scan_sums, 1, 1024, s, ba, nsb);
+    pdl_launch(k_scan_add, gc, 256, s, ba);
+    pdl_launch(k_scatter, gp, 256, s, ba);
+    pdl_launch(k_cell_sort, gc, 256, s, ba);
+    pdl_launch(k_permute, gp, 256, s, ba);
+    pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
+    if (list) pdl_launch(k_build_nlist, gp, 256, s, ba);
 }
 
 void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
@@ -589,20 +608,20 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     // schedule 6: the DPD list build runs inside the pair kernel
     const bool fused = variant == 6 && !any_mdpd_;
     enqueue_build(s, !fused);
-    if (any_mdpd_) k_density<<<gp, 256, 0, s>>>(sa);
+    if (any_mdpd_) pdl_launch(k_density, gp, 256, s, sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
     if (fused) {
         const BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
-        if (bonds_) k_build_pair<true, 4><<<gp, 256, 0, s>>>(sa, ba);
-        else k_build_pair<false, 4><<<gp, 256, 0, s>>>(sa, ba);
+        if (bonds_) pdl_launch(k_build_pair<true, 4>, gp, 256, s, sa, ba);
+        else pdl_launch(k_build_pair<false, 4>, gp, 256, s, sa, ba);
     } else if (any_dpd_) {
         launch_pair<0>(variant, bonds_, gp, s, sa);
     }
     if (any_mdpd_) launch_pair<1>(variant, bonds_, gp, s, sa);
     if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
-    if (rdf_) k_rdf<<<gp, 256, 0, s>>>(sa);
-    k_integrate<<<gp, 256, 0, s>>>(sa);
-    k_advance<<<(nrep + 255) / 256, 256, 0, s>>>(sa);
+    if (rdf_) pdl_launch(k_rdf, gp, 256, s, sa);
+    pdl_launch(k_integrate, gp, 256, s, sa);
+    pdl_launch(k_advance, (nrep + 255) / 256, 256, s, sa);
 }
 
 void Engine::enqueue_integrate_initial(cudaStream_t s)

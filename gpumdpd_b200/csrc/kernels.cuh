@@ -24,6 +24,15 @@
 #define DPD_J_MASK 0x07FFFFFF
 #define DPD_CODE_SHIFT 27
 
+// Kernels of the step are launched with programmatic dependent launch: the next kernel's
+// launch overlaps the end of the previous one, and each kernel waits here (PTX
+// griddepcontrol.wait) until its predecessor's memory is visible.  Without a programmatic
+// predecessor the wait returns at once.
+__device__ __forceinline__ void griddep_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------------
 __device__ __forceinline__ int cell_x(int code) { return code & DPD_MAX_NC; }
 __device__ __forceinline__ int cell_y(int code) { return (code >> DPD_CELL_BITS) & DPD_MAX_NC; }
@@ -217,6 +226,7 @@ __device__ __forceinline__ int slot_key(const BuildArgs& a, int s, int par)
 
 __global__ void k_bin_count(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
@@ -229,6 +239,7 @@ __global__ void k_bin_count(BuildArgs a)
 // elements, scan of block sums in one block, add back).
 __global__ void k_scan_blocks(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     __shared__ int sh[1024];
     const int base = blockIdx.x * 4096;
@@ -259,6 +270,7 @@ __global__ void k_scan_blocks(BuildArgs a)
 
 __global__ void k_scan_sums(BuildArgs a, int nblocks)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     __shared__ int sh[1024];
     int carry = 0;
@@ -283,6 +295,7 @@ __global__ void k_scan_sums(BuildArgs a, int nblocks)
 
 __global__ void k_scan_add(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < a.C) a.cstart[idx] += a.blocksum[idx / 4096];
@@ -290,6 +303,7 @@ __global__ void k_scan_add(BuildArgs a)
 
 __global__ void k_scatter(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
@@ -302,6 +316,7 @@ __global__ void k_scatter(BuildArgs a)
 // counting sort is stable and the layout deterministic (the first layout is tag order)
 __global__ void k_cell_sort(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.C) return;
@@ -325,6 +340,7 @@ __global__ void k_cell_sort(BuildArgs a)
 // reference positions of the displacement check (last4)
 __global__ void k_permute(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
@@ -353,6 +369,7 @@ __global__ void k_permute(BuildArgs a)
 
 __global__ void k_flip(BuildArgs a, int nrep)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < nrep) a.rstate[r].nbuild++;
@@ -445,6 +462,7 @@ __device__ __forceinline__ void build_nlist_slot(const BuildArgs& a, const int s
 
 __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
 {
+    griddep_wait();
     if (!build_on(a)) return;
     build_nlist_slot(a, blockIdx.x * blockDim.x + threadIdx.x);
 }

@@ -70,6 +70,7 @@ __device__ __forceinline__ void pair_disp(const float4* tab, int ent, float4 pi,
 // max(0, 1-r/rd)^2 over the half list, both sides.
 __global__ void __launch_bounds__(256) k_density(StepArgs a)
 {
+    griddep_wait();
     __shared__ float4 tab[8][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -228,6 +229,7 @@ __device__ __forceinline__ bool pair_force(const float4* crow, float r2, float d
 template <int STYLE, bool BONDS>
 __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 {
+    griddep_wait();
     __shared__ float4 tab[8][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,6 +305,7 @@ __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 template <int STYLE, bool BONDS, int MINB, bool ISMEM>
 __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 {
+    griddep_wait();
     __shared__ int sq_j[8][DPD_Q];
     __shared__ int sq_i[8][DPD_Q];
     __shared__ float4 sq_d[8][DPD_Q];
@@ -579,12 +582,14 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
 template <int STYLE, bool BONDS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
 {
+    griddep_wait();
     pair_flat_warp<STYLE, BONDS>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <int STYLE, bool BONDS, int LOGM, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 {
+    griddep_wait();
     pair_flat_warp<STYLE, BONDS, LOGM>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -594,6 +599,7 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 template <int STYLE, bool BONDS>
 __global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
 {
+    griddep_wait();
     int any = 0;
     for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
         const RepState st = a.rstate[r];
@@ -615,6 +621,7 @@ __global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
 template <bool BONDS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs b)
 {
+    griddep_wait();
     if (build_on(b)) {
         build_nlist_slot(b, blockIdx.x * blockDim.x + threadIdx.x);
         __syncwarp();
@@ -630,6 +637,7 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
 // only moves the offsets.
 __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
 {
+    griddep_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
     bool log = false;
@@ -723,6 +731,7 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
 // (src/compute/thermo.cu:274-306, 479-520), step counter, build flag of this phase.
 __global__ void k_advance(StepArgs a)
 {
+    griddep_wait();
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < a.nrep) {
         RepState st = a.rstate[r];
@@ -775,6 +784,7 @@ __global__ void k_advance(StepArgs a)
 #define DPD_RDF_MAXBINS 512
 __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
 {
+    griddep_wait();
     __shared__ unsigned int hs[8][DPD_RDF_MAXBINS];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
