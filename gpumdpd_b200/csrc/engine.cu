@@ -263,7 +263,6 @@ int Engine::alloc_and_upload()
     DA(b_.cstart, C_ + 1);
     DA(b_.skey, P_);
     DA(b_.srank, P_);
-    DA(b_.perm, P_);
     int64_t ntag = 0;
     for (auto& R : reps_) ntag += R.sys.n_atoms;
     DA(b_.tag2idx, ntag);
@@ -482,7 +481,6 @@ static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int 
     a.cstart = b.cstart;
     a.skey = b.skey;
     a.srank = b.srank;
-    a.perm = b.perm;
     a.tag2idx = b.tag2idx;
     a.ncount = b.ncount;
     a.nlist = b.nlist;
@@ -592,8 +590,6 @@ void Engine::enqueue_build(cudaStream_t s, bool list)
     pdl_launch(k_scan_blocks, nsb, 1024, s, ba);
     pdl_launch(k_scan_sums, 1, 1024, s, ba, nsb);
     pdl_launch(k_scan_add, gc, 256, s, ba);
-    pdl_launch(k_scatter, gp, 256, s, ba);
-    pdl_launch(k_cell_sort, gc, 256, s, ba);
     pdl_launch(k_permute, gp, 256, s, ba);
     pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
     if (list) pdl_launch(k_build_nlist, gp, 256, s, ba);
@@ -825,7 +821,7 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     const int64_t mb = std::max<int64_t>(maxb, 1);
     int64_t bytes = nrep * ((int64_t)sizeof(RepDesc) + (int64_t)sizeof(RepState) + 4);
     bytes += (P / 32) * 4 + ncoeff * 16 + nmass * 8 + nbond * 16 + nrdf * 8;
-    bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 4 + 8 + 4 * nmax + mb * 8);
+    bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 8 + 4 * nmax + mb * 8);
     bytes += C * (4 * 5) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
     return bytes + 64 * 1024 + nrep * 1024;  // arrays of size 0 still take one element

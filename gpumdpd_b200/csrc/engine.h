@@ -38,8 +38,7 @@ struct DeviceBuffers {
     float4 *force4 = nullptr, *last4 = nullptr;
     float* rho = nullptr;
     int *cell_rep = nullptr, *cell_lin = nullptr;
-    int *cnt = nullptr, *cstart = nullptr, *skey = nullptr, *srank = nullptr, *perm = nullptr,
-        *tag2idx = nullptr;
+    int *cnt = nullptr, *cstart = nullptr, *skey = nullptr, *srank = nullptr, *tag2idx = nullptr;
     int *ncount = nullptr, *nlist = nullptr, *blocksum = nullptr;
     double *acc = nullptr, *ring = nullptr;
     unsigned long long* rdf_hist = nullptr;

@@ -11,7 +11,7 @@
 //   force4[s]= {fx, fy, fz, 0}           accumulated with vector atomics
 //   img[s]   = image counters (updated when a build re-bins across the box)
 // Slots are sorted by cell (counting sort at every build; cells in linear or Morton
-// order; within a cell by previous slot, so the sort is stable).  The half neighbour list is warp-chunked,
+// order; within a cell in the order the counting pass's atomics drew).  The half neighbour list is warp-chunked,
 //   nlist[((s>>5)*nmax + k)*32 + (s&31)] = j | code<<27,
 // where code = 9(dcx+1)+3(dcy+1)+(dcz+1) encodes the cell difference c_i - c_j in
 // {-1,0,1}^3 of the pair at build time; the displacement is (o_i - o_j) + code*w.
@@ -158,7 +158,6 @@ struct BuildArgs {
     int* cstart;            // [C+1]
     int* skey;              // [P] cell key of each slot at this build
     int* srank;             // [P] arrival rank of the slot in its cell
-    int* perm;
     int* tag2idx;
     int* ncount;
     int* nlist;
@@ -248,6 +247,7 @@ __global__ void k_scan_blocks(BuildArgs a)
     for (int k = 0; k < 4; k++) {
         int idx = base + threadIdx.x * 4 + k;
         v[k] = idx < a.C ? a.cnt[idx] : 0;
+        if (idx < a.C) a.cnt[idx] = 0;  // ready for the next build's counting pass
         tot += v[k];
     }
     sh[threadIdx.x] = tot;
@@ -301,56 +301,27 @@ __global__ void k_scan_add(BuildArgs a)
     if (idx < a.C) a.cstart[idx] += a.blocksum[idx / 4096];
 }
 
-__global__ void k_scatter(BuildArgs a)
-{
-    griddep_wait();
-    if (!build_on(a)) return;
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.P) return;
-    // the rank the counting pass drew gives the place in the cell: no second atomic
-    const int pos = a.cstart[a.skey[s]] + a.srank[s];
-    if (pos >= 0 && pos < a.P) a.perm[pos] = s;
-}
-
-// one thread per cell: insertion sort of the cell's slots by their previous slot, so the
-// counting sort is stable and the layout deterministic (the first layout is tag order)
-__global__ void k_cell_sort(BuildArgs a)
-{
-    griddep_wait();
-    if (!build_on(a)) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.C) return;
-    int b = a.cstart[c], e = a.cstart[c + 1];
-    a.cnt[c] = 0;
-    if (b < 0 || e > a.P) return;
-    for (int i = b + 1; i < e; i++) {
-        const int si = a.perm[i];
-        int j = i - 1;
-        while (j >= b) {
-            const int sj = a.perm[j];
-            if (sj <= si) break;
-            a.perm[j + 1] = sj;
-            j--;
-        }
-        a.perm[j + 1] = si;
-    }
-}
-
-// gather into the other buffer, re-binning positions; the new positions are also the
-// reference positions of the displacement check (last4)
+// scatter every slot to its place in the other buffer (cell start + the rank the counting
+// pass drew), re-binning positions; the new positions are also the reference positions
+// of the displacement check (last4).  Reads are coalesced; the writes of a warp land in
+// a few neighbouring cells.
 __global__ void k_permute(BuildArgs a)
 {
     griddep_wait();
     if (!build_on(a)) return;
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.P) return;
     const int par = *a.parity, nxt = par ^ 1;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
-    int o = a.perm[s];
-    float4 p = a.buf.pos[par][o];
-    float4 v = a.buf.vel[par][o];
-    int4 im = a.buf.img[par][o];
+    const int dst = a.cstart[a.skey[s]] + a.srank[s];
+    if (dst < d.p_begin || dst >= d.p_cap_end) {  // cannot happen: keys stay in the replica
+        atomicOr(&a.rstate[r].status, ST_BAD_INPUT);
+        return;
+    }
+    float4 p = a.buf.pos[par][s];
+    float4 v = a.buf.vel[par][s];
+    int4 im = a.buf.img[par][s];
     if (s < d.p_end) {
         int dimg[3];
         if (!rebin(d, p, dimg)) atomicOr(&a.rstate[r].status, ST_NONFINITE);
@@ -358,13 +329,14 @@ __global__ void k_permute(BuildArgs a)
         im.y += dimg[1];
         im.z += dimg[2];
         int t = tag_of(v.w);
-        if (t >= 1 && t <= d.n_real) a.tag2idx[d.tag_base + t - 1] = s;
+        if (t >= 1 && t <= d.n_real) a.tag2idx[d.tag_base + t - 1] = dst;
     }
-    a.buf.pos[nxt][s] = p;
-    a.buf.vel[nxt][s] = v;
-    a.buf.img[nxt][s] = im;
-    if (!d.skin_zero) a.last4[s] = p;  // skin 0 rebuilds unconditionally: no skin check
-    for (int k = 0; k < a.maxb; k++) a.buf.bonds[nxt][(size_t)k * a.P + s] = a.buf.bonds[par][(size_t)k * a.P + o];
+    a.buf.pos[nxt][dst] = p;
+    a.buf.vel[nxt][dst] = v;
+    a.buf.img[nxt][dst] = im;
+    if (!d.skin_zero) a.last4[dst] = p;  // skin 0 rebuilds unconditionally: no skin check
+    for (int k = 0; k < a.maxb; k++)
+        a.buf.bonds[nxt][(size_t)k * a.P + dst] = a.buf.bonds[par][(size_t)k * a.P + s];
 }
 
 __global__ void k_flip(BuildArgs a, int nrep)
