@@ -616,7 +616,8 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     if (any_mdpd_) launch_pair<1>(variant, bonds_, gp, s, sa);
     if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
     if (rdf_) pdl_launch(k_rdf, gp, 256, s, sa);
-    pdl_launch(k_integrate, gp, 256, s, sa);
+    pdl_launch(k_integrate_nolog, gp, 256, s, sa);
+    pdl_launch(k_integrate_logsteps, std::min(gp, 148 * 4), 256, s, sa);
     pdl_launch(k_advance, (nrep + 255) / 256, 256, s, sa);
 }
 

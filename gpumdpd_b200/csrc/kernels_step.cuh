@@ -635,10 +635,11 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
 // displacement check for the next list build (src/force/neigh_list.cu:483-514), and
 // zeroing of the force accumulators.  Cells stay fixed between builds, so the drift
 // only moves the offsets.
-__global__ void __launch_bounds__(256) k_integrate(StepArgs a)
+// LOGM: 2 = any step; 0 = every step except logged mode-0 steps (no FP64 sums: fewer
+// registers); 1 = logged mode-0 steps only.  0 and 1 together cover every slot once.
+template <int LOGM>
+__device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
 {
-    griddep_wait();
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     int r = -1;
     bool log = false;
     double accv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -658,6 +659,8 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
         const bool work = active && s < d.p_end;
         const bool fin = a.mode == 0 && !st.zero_pending;
         log = a.mode == 0 && active && (st.step % (uint32_t)d.log_f) == 0u;
+        if ((LOGM == 0 && log) || (LOGM == 1 && !log)) return;  // warp-uniform
+        if (LOGM == 0) log = false;
         const bool init = a.mode == 1 ? true : st.step < st.target;
         const uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
         const bool check = init && (next % (uint32_t)d.nl_f) == 0u;
@@ -724,6 +727,32 @@ __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
                                 ACC_KIN + 4, ACC_KIN + 5, ACC_MOM + 0, ACC_MOM + 1, ACC_MOM + 2};
         acc_flush_warp<10>(accv, fields, r, a.acc);
     }
+}
+
+__global__ void __launch_bounds__(256) k_integrate(StepArgs a)
+{
+    griddep_wait();
+    integrate_slot<2>(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_integrate_nolog(StepArgs a)
+{
+    griddep_wait();
+    integrate_slot<0>(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// logged steps: a small grid-stride launch that returns at once when no replica logs
+__global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
+{
+    griddep_wait();
+    int any = 0;
+    for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
+        const RepState st = a.rstate[r];
+        any |= rep_active(st) && (st.step % (uint32_t)a.reps[r].log_f) == 0u;
+    }
+    if (!__syncthreads_or(any)) return;
+    const int nvb = (a.P + 255) / 256;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1>(a, vb * 256 + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------
