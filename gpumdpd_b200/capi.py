@@ -47,6 +47,8 @@ class dpd_system(ctypes.Structure):
         ("type", ctypes.POINTER(ctypes.c_int)), ("mol", ctypes.POINTER(ctypes.c_int)),
         ("x", ctypes.POINTER(ctypes.c_double)), ("v", ctypes.POINTER(ctypes.c_double)),
         ("bonds", ctypes.POINTER(ctypes.c_int)),
+        ("n_angles", ctypes.c_int), ("n_angletypes", ctypes.c_int),
+        ("angles", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -154,7 +156,7 @@ def ptr(a):
 
 
 def make_system(box_lo, box_hi, masses, types, x, v=None, bonds=None, n_bondtypes=0, mol=None,
-                tags=None):
+                tags=None, angles=None, n_angletypes=0):
     """Build a dpd_system from numpy arrays; returns (struct, keepalive list)."""
     n = len(types)
     masses = np.ascontiguousarray(masses, dtype=np.float64)
@@ -188,4 +190,13 @@ def make_system(box_lo, box_hi, masses, types, x, v=None, bonds=None, n_bondtype
     else:
         s.n_bonds = 0
         s.n_bondtypes = int(n_bondtypes)
+    if angles is not None and len(angles):
+        angles = np.ascontiguousarray(angles, dtype=np.int32).reshape(-1)
+        keep.append(angles)
+        s.n_angles = len(angles) // 4
+        s.n_angletypes = max(int(n_angletypes), 1)
+        s.angles = angles.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    else:
+        s.n_angles = 0
+        s.n_angletypes = int(n_angletypes)
     return s, keep

@@ -21,7 +21,7 @@ class System:
     """Arrays of one system (rows in tag order) plus its run.in text."""
 
     def __init__(self, lo, hi, masses, types, x, v, bonds=None, n_bondtypes=0, mol=None,
-                 run_in="", atom_style="atomic"):
+                 run_in="", atom_style="atomic", angles=None, n_angletypes=0):
         self.lo = np.asarray(lo, dtype=np.float64)
         self.hi = np.asarray(hi, dtype=np.float64)
         self.masses = np.asarray(masses, dtype=np.float64)
@@ -33,6 +33,8 @@ class System:
         self.mol = None if mol is None else np.asarray(mol, dtype=np.int32)
         self.run_in = run_in
         self.atom_style = atom_style
+        self.angles = None if angles is None else np.ascontiguousarray(angles, dtype=np.int32)  # type, i, j, k
+        self.n_angletypes = n_angletypes
 
     @property
     def n(self):
@@ -44,7 +46,8 @@ class System:
 
     def c_system(self):
         return capi.make_system(self.lo, self.hi, self.masses, self.types, self.x, self.v,
-                                self.bonds, self.n_bondtypes, self.mol)
+                                self.bonds, self.n_bondtypes, self.mol, angles=self.angles,
+                                n_angletypes=self.n_angletypes)
 
     def write_data(self, path):
         """Data file in the layout written by the reference's write_data."""
@@ -54,9 +57,13 @@ class System:
             f.write(f"{self.n} atoms\n")
             if self.atom_style != "atomic":
                 f.write(f"{0 if self.bonds is None else len(self.bonds)} bonds\n")
+            if self.atom_style == "angle":
+                f.write(f"{0 if self.angles is None else len(self.angles)} angles\n")
             f.write(f"{len(self.masses)} atom types\n")
             if self.atom_style != "atomic":
                 f.write(f"{max(self.n_bondtypes, 1)} bond types\n")
+            if self.atom_style == "angle":
+                f.write(f"{max(self.n_angletypes, 1)} angle types\n")
             f.write("                           \n")
             for k, nm in enumerate(("x", "y", "z")):
                 f.write(f"{self.lo[k]:.9f} {self.hi[k]:.9f} {nm}lo {nm}hi\n")
@@ -86,6 +93,12 @@ class System:
                 f.write("                           \n")
                 nb = len(self.bonds)
                 np.savetxt(f, np.column_stack([np.arange(1, nb + 1), self.bonds]), fmt="%d")
+            if self.atom_style == "angle":
+                f.write("                           \n")
+                f.write("Angles\n")
+                f.write("                           \n")
+                na = len(self.angles)
+                np.savetxt(f, np.column_stack([np.arange(1, na + 1), self.angles]), fmt="%d")
 
 
 def _velocities(rng, n, kT, masses_of_atoms):
@@ -97,7 +110,7 @@ def _velocities(rng, n, kT, masses_of_atoms):
 def run_in_text(*, atom_style="atomic", global_cut=1.0, skin=0.3, max_rho=10.0, nl_f=1, dt=0.04,
                 thermo=100, run=1000, data="system.data", pair="dpd", temp=1.0, rc=1.0, rd=0.75,
                 seed=12345, coeffs=(), bond_style=None, bond_coeffs=(), groups=(("all", (1,)),),
-                fixes=(("md", "all", "nve"),), computes=(), extra=()):
+                fixes=(("md", "all", "nve"),), computes=(), extra=(), angle_style=None, angle_coeffs=()):
     lines = [f"atom_style {atom_style}",
              f"neighbor {global_cut} {skin} {max_rho} {nl_f}",
              f"timestep {dt}",
@@ -114,6 +127,10 @@ def run_in_text(*, atom_style="atomic", global_cut=1.0, skin=0.3, max_rho=10.0, 
         lines.append(f"bond_style {bond_style}")
         for c in bond_coeffs:
             lines.append("bond_coeff " + " ".join(str(v) for v in c))
+    if angle_style:
+        lines.append(f"angle_style {angle_style}")
+        for c in angle_coeffs:
+            lines.append("angle_coeff " + " ".join(str(v) for v in c))
     for name, types in groups:
         lines.append(f"group {name} type " + " ".join(str(t) for t in types))
     for fid, grp, style in fixes:
@@ -188,6 +205,28 @@ def mdpd_slab(Lx=40.0, Ly=40.0, Lz=120.0, z0=40.0, z1=80.0, rho=6.0, rho_vapour=
                       temp=kT, rc=1.0, rd=rd, seed=seed % 1000003, coeffs=[(1, 1, A, B, gamma)],
                       max_rho=max_rho)
     return System([0, 0, 0], [Lx, Ly, Lz], [1.0], np.ones(n, dtype=np.int32), x, v, run_in=run)
+
+
+def angle_chains(L=10.0, rho=3.0, chain=10, n_a=5, seed=17, bond_k=4.0, angle_k=2.0, theta0=180.0,
+                 bond_step=0.9, kT=1.0, dt=0.04, nsteps=1000, skin=0.3, thermo=100, a_same=25.0,
+                 a_ab=40.0, gamma=4.5, data="system.data", max_rho=10.0):
+    """A5B5 chains with harmonic bonds and harmonic angles (E = k (theta - theta0)^2) on every
+    consecutive bead triple (atom_style angle)."""
+    s = diblock_melt(L=L, rho=rho, chain=chain, n_a=n_a, seed=seed, bond_k=bond_k, bond_step=bond_step,
+                     kT=kT, dt=dt, nsteps=nsteps, skin=skin, thermo=thermo, a_same=a_same, a_ab=a_ab,
+                     gamma=gamma, data=data, max_rho=max_rho)
+    nchain = s.n // chain
+    idx = np.arange(nchain * chain).reshape(nchain, chain) + 1
+    ai, aj, ak = idx[:, :-2].reshape(-1), idx[:, 1:-1].reshape(-1), idx[:, 2:].reshape(-1)
+    angles = np.column_stack([np.ones(len(ai), dtype=np.int64), ai, aj, ak]).astype(np.int32)
+    run = run_in_text(atom_style="angle", skin=skin, dt=dt, thermo=thermo, run=nsteps, data=data,
+                      temp=kT, seed=seed % 1000003, max_rho=max_rho,
+                      coeffs=[(1, 1, a_same, gamma), (1, 2, a_ab, gamma), (2, 2, a_same, gamma)],
+                      bond_style="harmonic", bond_coeffs=[(1, bond_k, 0.0)],
+                      angle_style="harmonic", angle_coeffs=[(1, angle_k, theta0)],
+                      groups=(("all", (1, 2)),))
+    return System(s.lo, s.hi, s.masses, s.types, s.x, s.v, bonds=s.bonds, n_bondtypes=1, mol=s.mol,
+                  run_in=run, atom_style="angle", angles=angles, n_angletypes=1)
 
 
 def binary_mixture(L, a_ab, rho=3.0, seed=0, a_same=25.0, gamma=4.5, kT=1.0, dt=0.04, nsteps=5000,

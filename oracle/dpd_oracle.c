@@ -254,7 +254,20 @@ typedef struct {
     int bond_style;      /* 0 none, 1 harmonic (src/force/bond_harmonic.cu), 2 fene (new) */
     int nbondtypes;
     double bond_coeff[ORACLE_MAXT][4]; /* harmonic: k, r0 ; fene: K, R0, eps, sigma */
+    int angle_style;     /* 0 none, 1 harmonic (src/force/angle_harmonic.cu) */
+    int nangletypes;
+    double angle_coeff[ORACLE_MAXT][2]; /* k, theta0 in degrees */
 } oracle_ff;
+
+/* The angle list (type, tag_i, tag_j, tag_k per angle; j is the apex) of the next
+ * oracle_forces/oracle_run calls; set by the caller, NULL for none.                */
+static const int* g_angles = 0;
+static int g_nangles = 0;
+void oracle_set_angles(int nangles, const int* angles)
+{
+    g_nangles = angles ? nangles : 0;
+    g_angles = angles;
+}
 
 typedef struct {
     const oracle_ff* ff;
@@ -394,8 +407,63 @@ static int bond_forces(int n, const int* tag_to_idx, int ntag, const double* x, 
     return status;
 }
 
-/* Forces at one state.  out: f[3n], rho[n] (mdpd, may be NULL), energy[2] = pair,
- * bond; virial[6] = xx xy xz yy yz zz (pair + bond).                            */
+/* Harmonic angles: src/force/angle_harmonic.cu:187-270.  d1 = x_i - x_j, d2 = x_k - x_j
+ * (minimum image), c = cos(theta) clamped to [-1, 1], s = sin(theta) >= 0.001,
+ * E = k (theta - theta0)^2, a = -2 k (theta - theta0) / s, a11 = a c / |d1|^2,
+ * a12 = -a / (|d1| |d2|), a22 = a c / |d2|^2, F_i = a11 d1 + a12 d2,
+ * F_k = a22 d2 + a12 d1, F_j = -(F_i + F_k); virial d1 (x) F_i + d2 (x) F_k (the
+ * reference gives a third of it to each atom).                                  */
+static int angle_forces(const int* tag_to_idx, int ntag, const double* x, const double* L,
+                        const oracle_ff* ff, int nangles, const int* angles, double* f, double* pe_out,
+                        double* vir)
+{
+    int status = 0;
+    for (int a = 0; a < nangles; a++) {
+        const int at = angles[4 * a], ti = angles[4 * a + 1], tj = angles[4 * a + 2], tk = angles[4 * a + 3];
+        if (ti < 1 || ti > ntag || tj < 1 || tj > ntag || tk < 1 || tk > ntag || at < 1 || at > ff->nangletypes) {
+            status = -1;
+            continue;
+        }
+        const int i = tag_to_idx[ti - 1], j = tag_to_idx[tj - 1], k = tag_to_idx[tk - 1];
+        double d1[3], d2[3];
+        for (int c = 0; c < 3; c++) {
+            d1[c] = min_image(x[3 * i + c] - x[3 * j + c], L[c]);
+            d2[c] = min_image(x[3 * k + c] - x[3 * j + c], L[c]);
+        }
+        const double rsq1 = d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2];
+        const double rsq2 = d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2];
+        const double r1 = sqrt(rsq1), r2 = sqrt(rsq2);
+        double c = (d1[0] * d2[0] + d1[1] * d2[1] + d1[2] * d2[2]) / (r1 * r2);
+        if (c > 1.0) c = 1.0;
+        if (c < -1.0) c = -1.0;
+        double s = sqrt(1.0 - c * c);
+        if (s < 0.001) s = 0.001;
+        const double kk = ff->angle_coeff[at - 1][0];
+        const double theta0 = ff->angle_coeff[at - 1][1] * (M_PI / 180.0);
+        const double dtheta = acos(c) - theta0;
+        const double aa = -2.0 * kk * dtheta / s;
+        const double a11 = aa * c / rsq1, a12 = -aa / (r1 * r2), a22 = aa * c / rsq2;
+        double fi[3], fk[3];
+        for (int q = 0; q < 3; q++) {
+            fi[q] = a11 * d1[q] + a12 * d2[q];
+            fk[q] = a22 * d2[q] + a12 * d1[q];
+            f[3 * i + q] += fi[q];
+            f[3 * k + q] += fk[q];
+            f[3 * j + q] -= fi[q] + fk[q];
+        }
+        *pe_out += kk * dtheta * dtheta;
+        vir[0] += d1[0] * fi[0] + d2[0] * fk[0];
+        vir[1] += d1[0] * fi[1] + d2[0] * fk[1];
+        vir[2] += d1[0] * fi[2] + d2[0] * fk[2];
+        vir[3] += d1[1] * fi[1] + d2[1] * fk[1];
+        vir[4] += d1[1] * fi[2] + d2[1] * fk[2];
+        vir[5] += d1[2] * fi[2] + d2[2] * fk[2];
+    }
+    return status;
+}
+
+/* Forces at one state.  out: f[3n], rho[n] (mdpd, may be NULL), energy[3] = pair,
+ * bond, angle; virial[6] = xx xy xz yy yz zz (pair + bond + angle).             */
 int oracle_forces(int n, const int* tag, const int* type, const double* x, const double* v,
                   const double* lo, const double* L, const oracle_ff* ff, uint32_t step,
                   int nbonds, const int* bonds, double* f, double* rho, double* energy,
@@ -415,18 +483,21 @@ int oracle_forces(int n, const int* tag, const int* type, const double* x, const
     }
     k.rho = rho_buf;
     for_each_pair(n, x, lo, L, cut, force_cb, &k);
-    double bpe = 0.0, bvir[6] = {0, 0, 0, 0, 0, 0};
+    double bpe = 0.0, ape = 0.0, bvir[6] = {0, 0, 0, 0, 0, 0};
     int status = 0;
-    if (ff->bond_style != 0 && nbonds > 0) {
+    const int want_angles = ff->angle_style != 0 && g_nangles > 0;
+    if ((ff->bond_style != 0 && nbonds > 0) || want_angles) {
         int ntag = 0;
         for (int i = 0; i < n; i++) if (tag[i] > ntag) ntag = tag[i];
         int* t2i = (int*)malloc(sizeof(int) * (ntag > 0 ? ntag : 1));
         for (int t = 0; t < ntag; t++) t2i[t] = -1;
         for (int i = 0; i < n; i++) t2i[tag[i] - 1] = i;
-        status = bond_forces(n, t2i, ntag, x, lo, L, ff, nbonds, bonds, f, &bpe, bvir);
+        if (ff->bond_style != 0 && nbonds > 0)
+            status = bond_forces(n, t2i, ntag, x, lo, L, ff, nbonds, bonds, f, &bpe, bvir);
+        if (want_angles) status |= angle_forces(t2i, ntag, x, L, ff, g_nangles, g_angles, f, &ape, bvir);
         free(t2i);
     }
-    if (energy) { energy[0] = k.pe; energy[1] = bpe; }
+    if (energy) { energy[0] = k.pe; energy[1] = bpe; energy[2] = ape; }
     if (virial) for (int c = 0; c < 6; c++) virial[c] = k.vir[c] + bvir[c];
     if (!rho) free(rho_buf);
     return status;
@@ -435,7 +506,7 @@ int oracle_forces(int n, const int* tag, const int* type, const double* x, const
 /* ------------------------------------------------------------------------- */
 /* Thermo: src/compute/thermo.cu:240-246 (KE), 301-303 (T = 2KE/(3N-3)),
  * 422-434 + 506-517 (P_ab = (sum m v_a v_b + W_ab)/V, P = trace/3).
- * out[12]: T, pair_pe, bond_pe, P, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz, KE, spare     */
+ * out[12]: T, pair_pe, bond_pe, P, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz, KE, angle_pe  */
 static void thermo(int n, const int* type, const double* v, const double* L, const oracle_ff* ff,
                    const double* energy, const double* virial, double* out)
 {
@@ -454,7 +525,7 @@ static void thermo(int n, const int* type, const double* v, const double* L, con
     for (int c = 0; c < 6; c++) out[4 + c] = (kin[c] + virial[c]) / vol;
     out[3] = (out[4] + out[7] + out[9]) / 3.0;
     out[10] = ke;
-    out[11] = 0.0;
+    out[11] = energy[2];
 }
 
 /* ------------------------------------------------------------------------- */
@@ -473,7 +544,7 @@ int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int
                double* rho_out)
 {
     double* f = f_out;
-    double energy[2], virial[6];
+    double energy[3], virial[6];
     int nlog = 0;
     int status = 0;
     double dt = ff->dt;

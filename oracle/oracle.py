@@ -21,6 +21,8 @@ class OracleFF(ctypes.Structure):
         ("coeff", (ctypes.c_double * 5) * (MAXT * MAXT)), ("mass", ctypes.c_double * MAXT),
         ("bond_style", ctypes.c_int), ("nbondtypes", ctypes.c_int),
         ("bond_coeff", (ctypes.c_double * 4) * MAXT),
+        ("angle_style", ctypes.c_int), ("nangletypes", ctypes.c_int),
+        ("angle_coeff", (ctypes.c_double * 2) * MAXT),
     ]
 
 
@@ -43,6 +45,8 @@ def load():
     lib.oracle_saru.argtypes = [u32, u32, u32, ctypes.c_int32]
     lib.oracle_set_saru_double_tail.restype = None
     lib.oracle_set_saru_double_tail.argtypes = [i]
+    lib.oracle_set_angles.restype = None
+    lib.oracle_set_angles.argtypes = [i, vp]
     lib.oracle_saru_batch.restype = None
     lib.oracle_saru_batch.argtypes = [i, vp, vp, u32, vp, vp]
     lib.oracle_pairs_f64.restype = i64
@@ -74,7 +78,8 @@ def tri_index(ti, tj, nt):
     return ((a - 1) * nt - (a - 1) * (a - 2) // 2 + b - a + 1) - 1
 
 
-def make_ff(style, ntypes, coeffs, kT, dt, seed, masses, bond_style=0, bond_coeffs=()):
+def make_ff(style, ntypes, coeffs, kT, dt, seed, masses, bond_style=0, bond_coeffs=(), angle_style=0,
+            angle_coeffs=()):
     """coeffs: {(ti,tj): (A, B, gamma, rc, rd)}; bond_coeffs: list of 4-tuples."""
     ff = OracleFF()
     ff.style = style
@@ -93,13 +98,17 @@ def make_ff(style, ntypes, coeffs, kT, dt, seed, masses, bond_style=0, bond_coef
     for b, c in enumerate(bond_coeffs):
         for k in range(len(c)):
             ff.bond_coeff[b][k] = c[k]
+    ff.angle_style = angle_style
+    ff.nangletypes = len(angle_coeffs)
+    for a, c in enumerate(angle_coeffs):
+        ff.angle_coeff[a][0], ff.angle_coeff[a][1] = c[0], c[1]
     return ff
 
 
 def ff_from_run_in(text, masses):
     """Force field of a run.in text (pair_style/pair_coeff/bond_style/bond_coeff/timestep)."""
     style, kT, rc, rd, seed, dt = 0, 1.0, 1.0, 0.0, 0, 0.01
-    coeffs, bonds, bstyle = {}, {}, 0
+    coeffs, bonds, bstyle, angles, astyle = {}, {}, 0, {}, 0
     raw = []
     for line in text.splitlines():
         t = line.split("#")[0].split()
@@ -115,6 +124,8 @@ def ff_from_run_in(text, masses):
                 style, kT, rc, rd, seed = 1, float(t[2]), float(t[3]), float(t[4]), int(t[5])
         if t[0] == "bond_style":
             bstyle = {"harmonic": 1, "fene": 2}[t[1]]
+        if t[0] == "angle_style":
+            astyle = {"harmonic": 1}[t[1]]
     for t in raw:
         if t[0] == "pair_coeff":
             ti, tj = int(t[1]), int(t[2])
@@ -128,8 +139,11 @@ def ff_from_run_in(text, masses):
                 coeffs[(ti, tj)] = (A, B, g, r, d)
         if t[0] == "bond_coeff":
             bonds[int(t[1])] = tuple(float(v) for v in t[2:])
+        if t[0] == "angle_coeff":
+            angles[int(t[1])] = (float(t[2]), float(t[3]))
     bc = [bonds[k] for k in sorted(bonds)]
-    return make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc)
+    ac = [angles[k] for k in sorted(angles)]
+    return make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc, astyle, ac)
 
 
 def set_saru_double_tail(on):
@@ -147,8 +161,15 @@ def saru(t1, t2, seed, step):
     return out
 
 
-def forces(ff, tags, types, x, v, lo, L, step, bonds=None):
+def _set_angles(lib, angles):
+    a = None if angles is None else np.ascontiguousarray(angles, dtype=np.int32)
+    lib.oracle_set_angles(0 if a is None else len(a), _p(a))
+    return a
+
+
+def forces(ff, tags, types, x, v, lo, L, step, bonds=None, angles=None):
     lib = load()
+    keep = _set_angles(lib, angles)
     n = len(types)
     tags = np.ascontiguousarray(tags, dtype=np.int32)
     types = np.ascontiguousarray(types, dtype=np.int32)
@@ -158,19 +179,24 @@ def forces(ff, tags, types, x, v, lo, L, step, bonds=None):
     L = np.ascontiguousarray(L, dtype=np.float64)
     f = np.empty((n, 3))
     rho = np.empty(n)
-    en = np.empty(2)
+    en = np.empty(3)
     vir = np.empty(6)
     nb = 0 if bonds is None else len(bonds)
     b = None if bonds is None else np.ascontiguousarray(bonds, dtype=np.int32)
     st = lib.oracle_forces(n, _p(tags), _p(types), _p(x), _p(v), _p(lo), _p(L), ctypes.byref(ff), step,
                            nb, _p(b), _p(f), _p(rho), _p(en), _p(vir))
-    return {"f": f, "rho": rho, "pair_pe": en[0], "bond_pe": en[1], "virial": vir, "status": st}
+    lib.oracle_set_angles(0, None)
+    del keep
+    return {"f": f, "rho": rho, "pair_pe": en[0], "bond_pe": en[1], "angle_pe": en[2], "virial": vir,
+            "status": st}
 
 
-def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zero_step=True, f0=None):
+def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zero_step=True, f0=None,
+        angles=None):
     """Velocity-Verlet in FP64; returns final state and logged thermo rows.  Without a zero
     step, f0 are the forces of step first_step-1 (used by the first half kick)."""
     lib = load()
+    keep = _set_angles(lib, angles)
     n = len(types)
     tags = np.ascontiguousarray(tags, dtype=np.int32)
     types = np.ascontiguousarray(types, dtype=np.int32)
@@ -189,9 +215,12 @@ def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zer
     nlog = lib.oracle_run(n, _p(tags), _p(types), _p(x), _p(v), _p(img), _p(lo), _p(L), ctypes.byref(ff),
                           nb, _p(b), first_step, nsteps, 1 if zero_step else 0, log_f, _p(th), _p(ls),
                           maxlog, _p(f), _p(rho))
+    lib.oracle_set_angles(0, None)
+    del keep
     if nlog < 0:
         raise RuntimeError(f"oracle_run failed: {nlog}")
-    cols = ["temp", "pair_pe", "bond_pe", "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "ke"]
+    cols = ["temp", "pair_pe", "bond_pe", "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz", "ke",
+            "angle_pe"]
     thermo = {c: th[:nlog, k] for k, c in enumerate(cols)}
     thermo["step"] = ls[:nlog]
     return {"x": x, "v": v, "image": img, "f": f, "rho": rho, "thermo": thermo}

@@ -93,6 +93,8 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
             "hi": system.hi}
     if system.bonds is not None:
         save["bonds"] = system.bonds
+    if system.angles is not None:
+        save["angles"] = system.angles
     for step in sorted(frames):
         if step not in (0, 1, nsteps):
             continue
@@ -120,14 +122,21 @@ def systems():
     mix.run_in = mix.run_in.replace("pair_coeff 1 2 40.0 4.5", "pair_coeff 1 2 40.0 4.5 0.8 0")
     mix.run_in = mix.run_in.replace("pair_coeff 2 2 25.0 4.5", "pair_coeff 2 2 30.0 3.0 0.9 0")
     out["mix_rc"] = mix
+    # harmonic angles on every consecutive triple of A5B5 chains (atom_style angle)
+    out["angle_chains"] = inputs.angle_chains(L=8.0, seed=19, nsteps=10, angle_k=3.0, theta0=120.0)
     return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    ap.add_argument("--only", default=None, help="generate just this system's fixture")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    if a.only:
+        run_reference(a.only, systems()[a.only], a.out)
+        print("fixture written to", a.out)
+        return
     saru_kat(a.out)
     for name, s in systems().items():
         run_reference(name, s, a.out)

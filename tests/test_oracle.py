@@ -5,7 +5,7 @@ import pytest
 
 from conftest import force_err, load_golden
 
-SYSTEMS = ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc"]
+SYSTEMS = ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc", "angle_chains"]
 
 
 def _state(g, step):
@@ -40,7 +40,7 @@ def test_step0_forces_match_reference(oracle_mod, name):
     x, v, f_ref, ids, types = _state(g, 0)
     ff = oracle_mod.ff_from_run_in(str(g["run_in"]), g["masses"])
     L = g["hi"] - g["lo"]
-    o = oracle_mod.forces(ff, ids, types, x, v, g["lo"], L, 0, bonds=g.get("bonds"))
+    o = oracle_mod.forces(ff, ids, types, x, v, g["lo"], L, 0, bonds=g.get("bonds"), angles=g.get("angles"))
     assert force_err(o["f"], f_ref) < 1e-5
 
 
@@ -66,7 +66,7 @@ def test_step0_thermo_matches_reference(oracle_mod, name):
     x, v, _, ids, types = _state(g, 0)
     ff = oracle_mod.ff_from_run_in(str(g["run_in"]), g["masses"])
     L = g["hi"] - g["lo"]
-    o = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, 0, 1, bonds=g.get("bonds"))
+    o = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, 0, 1, bonds=g.get("bonds"), angles=g.get("angles"))
     th = o["thermo"]
     rtol = 2e-6 if name.endswith("double") else 2e-5
     assert th["temp"][0] == pytest.approx(g["thermo_temp"][0], rel=rtol, abs=2e-6)
@@ -76,9 +76,11 @@ def test_step0_thermo_matches_reference(oracle_mod, name):
         assert th[c][0] == pytest.approx(g[f"thermo_{c}"][0], rel=1e-4, abs=2e-5)
     if "thermo_bond_pe" in g:
         assert th["bond_pe"][0] == pytest.approx(g["thermo_bond_pe"][0], rel=rtol, abs=2e-6)
+    if "thermo_angle_pe" in g:
+        assert th["angle_pe"][0] == pytest.approx(g["thermo_angle_pe"][0], rel=rtol, abs=2e-6)
 
 
-@pytest.mark.parametrize("name", ["dpd_c1", "mdpd_slab", "diblock", "dpd_c1_double"])
+@pytest.mark.parametrize("name", ["dpd_c1", "mdpd_slab", "diblock", "dpd_c1_double", "angle_chains"])
 def test_trajectory_matches_reference(oracle_mod, name):
     """10 velocity-Verlet steps (src/main/utils.cuh:254-303) from the reference's step-0
     state: positions and forces at step 1 and 10 track the reference."""
@@ -90,15 +92,19 @@ def test_trajectory_matches_reference(oracle_mod, name):
     for steps in (1, 10):
         oracle_mod.set_saru_double_tail(dbl)
         try:
-            o = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, steps, 1, bonds=g.get("bonds"))
+            o = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, steps, 1, bonds=g.get("bonds"),
+                               angles=g.get("angles"))
         finally:
             oracle_mod.set_saru_double_tail(False)
         xr, vr, fr, _, _ = _state(g, steps)
         dx = o["x"] - xr
         dx -= L * np.round(dx / L)
-        tol_x = 1e-7 if dbl else (2e-6 if steps == 1 else 5e-5)
+        # the stiff angle term (float acos in the reference's build) makes its FP32
+        # trajectory drift from the FP64 one about twice as fast over 10 steps
+        slack = 4.0 if name == "angle_chains" and steps == 10 else 1.0
+        tol_x = 1e-7 if dbl else (2e-6 if steps == 1 else 5e-5 * slack)
         assert np.abs(dx).max() < tol_x
-        tol_f = 1e-7 if dbl else (2e-5 if steps == 1 else 3e-4)
+        tol_f = 1e-7 if dbl else (2e-5 if steps == 1 else 3e-4 * slack)
         assert force_err(o["f"], fr) < tol_f
         # thermo rows of every step
         for k in range(steps + 1):
