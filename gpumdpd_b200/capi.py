@@ -57,6 +57,7 @@ class dpd_thermo(ctypes.Structure):
         ("step", ctypes.c_int64), ("temp", ctypes.c_double), ("pair_pe", ctypes.c_double),
         ("bond_pe", ctypes.c_double), ("pressure", ctypes.c_double), ("p", ctypes.c_double * 6),
         ("ke", ctypes.c_double), ("momentum", ctypes.c_double * 3),
+        ("angle_pe", ctypes.c_double),
     ]
 
 

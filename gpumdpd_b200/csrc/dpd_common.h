@@ -5,7 +5,7 @@
 #define DPD_MAX_TYPES 32
 #define DPD_NACC 24          // FP64 accumulators per replica and slot
 #define DPD_ACC_SLOTS 32     // atomic spreading slots per replica
-#define DPD_THERMO_FIELDS 16 // doubles per logged thermo row
+#define DPD_THERMO_FIELDS 17 // doubles per logged thermo row
 #define DPD_RING_ROWS 2048   // thermo rows kept per replica on the device
 #define DPD_CELL_BITS 10     // bits per cell coordinate in the packed cell code
 #define DPD_MAX_NC ((1 << DPD_CELL_BITS) - 1)
@@ -21,6 +21,7 @@ enum {
     ACC_VIR = 9,     // 6: sum over pairs and bonds of r_a F_b
     ACC_MOM = 15,    // 3: sum m v
     ACC_NONFINITE = 18,
+    ACC_ANGLE_PE = 19,
 };
 
 // status bits (per replica, device)

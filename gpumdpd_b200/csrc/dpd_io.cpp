@@ -157,8 +157,6 @@ int parse_run_in(const std::string& text, RunInput& in, std::string& err)
         if (!got_bond_style) return fail(err, "", "bond_style command is missing");
         if (!got_angle_style) return fail(err, "", "angle_style command is missing");
     }
-    if (in.atom_style == 2)
-        return fail(err, "", "atom_style angle is not supported by this engine (angles are outside the timestep hot path)");
     if (!(in.dt > 0)) return fail(err, "", "timestep must be > 0");
     return DPD_OK;
 }
@@ -230,7 +228,7 @@ int read_data_file(const std::string& path, int atom_style, SystemData& s, std::
     s.v.assign(3 * (size_t)s.n_atoms, 0.0);
     s.masses.assign(s.n_atomtypes, 0.0);
     std::vector<char> seen(s.n_atoms, 0), mass_seen(s.n_atomtypes, 0);
-    bool got_atoms = false, got_masses = false, got_bonds = false;
+    bool got_atoms = false, got_masses = false, got_bonds = false, got_angles = false;
     auto next_rows = [&](size_t& k, int count, const std::function<bool(const std::vector<std::string>&)>& fn) -> bool {
         int done = 0;
         for (k++; k < lines.size() && done < count; k++) {
@@ -338,6 +336,27 @@ int read_data_file(const std::string& path, int atom_style, SystemData& s, std::
             });
             if (!ok) { err = "Error reading the Bonds section."; return DPD_E_ARG; }
             got_bonds = true;
+        } else if (starts_section(h, "Angles")) {
+            // src/system/read_data.cu:428-466: id type i j k, j the apex
+            s.angles.assign(4 * (size_t)s.n_angles, -1);
+            std::vector<char> aseen(s.n_angles, 0);
+            bool ok = next_rows(i, s.n_angles, [&](const std::vector<std::string>& t) {
+                long long id, ty, a, b, c;
+                if (t.size() < 5 || !parse_int(t[0], 1, s.n_angles, id) ||
+                    !parse_int(t[1], 1, std::max(1, s.n_angletypes), ty) ||
+                    !parse_int(t[2], 1, s.n_atoms, a) || !parse_int(t[3], 1, s.n_atoms, b) ||
+                    !parse_int(t[4], 1, s.n_atoms, c))
+                    return false;
+                if (aseen[id - 1] || a == b || b == c || a == c) return false;
+                aseen[id - 1] = 1;
+                s.angles[4 * (id - 1)] = (int)ty;
+                s.angles[4 * (id - 1) + 1] = (int)a;
+                s.angles[4 * (id - 1) + 2] = (int)b;
+                s.angles[4 * (id - 1) + 3] = (int)c;
+                return true;
+            });
+            if (!ok) { err = "Error reading the Angles section."; return DPD_E_ARG; }
+            got_angles = true;
         }
     }
     if (!got_masses) { err = "Masses section is missing."; return DPD_E_ARG; }
@@ -345,7 +364,9 @@ int read_data_file(const std::string& path, int atom_style, SystemData& s, std::
         if (!mass_seen[t] || !(s.masses[t] > 0)) { err = "All the masses are not set."; return DPD_E_ARG; }
     if (!got_atoms) { err = "Atoms section is missing."; return DPD_E_ARG; }
     if (atom_style >= 1 && s.n_bonds > 0 && !got_bonds) { err = "Bonds section is missing."; return DPD_E_ARG; }
+    if (atom_style == 2 && s.n_angles > 0 && !got_angles) { err = "Angles section is missing."; return DPD_E_ARG; }
     if (atom_style == 0) s.n_bonds = 0;
+    if (atom_style != 2) s.n_angles = 0;
     return DPD_OK;
 }
 
@@ -463,6 +484,38 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
         for (int b = 0; b < sys.n_bondtypes; b++)
             if (!bgot[b]) return fail(err, "", "all bond_coeff are not set");
     }
+    // angles, src/force/angle_harmonic.cu:19-147 (angle_style harmonic; angle_coeff type k theta0)
+    if (in.atom_style == 2) {
+        int nas = 0;
+        for (size_t k = 0; k < in.lines.size(); k++) {
+            const auto& t = in.lines[k];
+            if (t[0] != "angle_style") continue;
+            if (t.size() != 2) return fail(err, in.raw[k], "illegal angle_style harmonic command: angle_style angle_style");
+            if (t[1] != "harmonic") return fail(err, in.raw[k], "unknown angle_style " + t[1]);
+            ff.angle_style = 1;
+            nas++;
+        }
+        if (nas != 1) return fail(err, "", "exactly one angle_style is required");
+        int nat = std::max(sys.n_angletypes, 1);
+        ff.angle_coeff.assign(nat, {0, 0});
+        std::vector<char> agot(nat, 0);
+        for (size_t k = 0; k < in.lines.size(); k++) {
+            const auto& t = in.lines[k];
+            const std::string& line = in.raw[k];
+            if (t[0] != "angle_coeff") continue;
+            long long ty;
+            if (t.size() != 4) return fail(err, line, "illegal angle_coeff command for angle_style harmonic: angle_coeff type k theta0");
+            if (!parse_int(t[1], 1, std::numeric_limits<int>::max(), ty)) return fail(err, line, "illegal angle_coeff command for angle_style harmonic");
+            if (ty > nat) return fail(err, line, "type exceeds n_angle_types");
+            std::array<double, 2> c = {0, 0};
+            if (!parse_double(t[2], c[0]) || !parse_double(t[3], c[1]))
+                return fail(err, line, "illegal angle_coeff command for angle_style harmonic");
+            ff.angle_coeff[ty - 1] = c;
+            agot[ty - 1] = 1;
+        }
+        for (int a = 0; a < sys.n_angletypes; a++)
+            if (!agot[a]) return fail(err, "", "all angle_coeff are not set");
+    }
     // groups, src/system/system.cu:236-305
     for (size_t k = 0; k < in.lines.size(); k++) {
         const auto& t = in.lines[k];
@@ -557,8 +610,10 @@ int write_data_file(const std::string& path, int atom_style, const SystemData& s
     fprintf(f, "                         \n");
     fprintf(f, "%d atoms\n", s.n_atoms);
     if (atom_style >= 1) fprintf(f, "%d bonds\n", s.n_bonds);
+    if (atom_style == 2) fprintf(f, "%d angles\n", s.n_angles);
     fprintf(f, "%d atom types\n", s.n_atomtypes);
     if (atom_style >= 1) fprintf(f, "%d bond types\n", s.n_bondtypes);
+    if (atom_style == 2) fprintf(f, "%d angle types\n", s.n_angletypes);
     fprintf(f, "                           \n");
     fprintf(f, "%.9f %.9f xlo xhi\n", s.lo[0], s.hi[0]);
     fprintf(f, "%.9f %.9f ylo yhi\n", s.lo[1], s.hi[1]);
@@ -568,7 +623,7 @@ int write_data_file(const std::string& path, int atom_style, const SystemData& s
     fprintf(f, "                           \n");
     for (int t = 0; t < s.n_atomtypes; t++) fprintf(f, "%d %.9f\n", t + 1, s.masses[t]);
     fprintf(f, "                           \n");
-    fprintf(f, atom_style == 0 ? "Atoms  # atomic\n" : "Atoms  # bond\n");
+    fprintf(f, atom_style == 0 ? "Atoms  # atomic\n" : (atom_style == 1 ? "Atoms  # bond\n" : "Atoms  # angle\n"));
     fprintf(f, "                           \n");
     for (int i = 0; i < s.n_atoms; i++) {
         if (atom_style >= 1)
@@ -588,6 +643,14 @@ int write_data_file(const std::string& path, int atom_style, const SystemData& s
         fprintf(f, "                           \n");
         for (int b = 0; b < s.n_bonds; b++)
             fprintf(f, "%d %d %d %d\n", b + 1, s.bonds[3 * b], s.bonds[3 * b + 1], s.bonds[3 * b + 2]);
+    }
+    if (atom_style == 2) {
+        fprintf(f, "                           \n");
+        fprintf(f, "Angles\n");
+        fprintf(f, "                           \n");
+        for (int a = 0; a < s.n_angles; a++)
+            fprintf(f, "%d %d %d %d %d\n", a + 1, s.angles[4 * a], s.angles[4 * a + 1], s.angles[4 * a + 2],
+                    s.angles[4 * a + 3]);
     }
     fclose(f);
     return DPD_OK;

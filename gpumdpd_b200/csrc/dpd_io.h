@@ -35,6 +35,7 @@ struct SystemData {
     std::vector<int> type, mol;
     std::vector<double> x, v;
     std::vector<int> bonds;  // type, tag_i, tag_j
+    std::vector<int> angles;  // type, tag_i, tag_j (apex), tag_k
     bool has_velocities = false;
 };
 
@@ -60,6 +61,8 @@ struct ForceField {
     std::vector<std::array<double, 5>> coeff;  // triangular index: A, B, gamma, rc, rd
     int bond_style = 0;                        // 0 none, 1 harmonic, 2 fene
     std::vector<std::array<double, 4>> bond_coeff;
+    int angle_style = 0;                       // 0 none, 1 harmonic (src/force/angle_harmonic.cu)
+    std::vector<std::array<double, 2>> angle_coeff;  // k, theta0 in degrees
     std::map<std::string, std::vector<int>> groups;
     uint32_t integ_mask = 0;  // types integrated by fix nve
     std::vector<ComputeTemp> temps;

@@ -330,6 +330,36 @@ int Engine::alloc_and_upload()
     CK(cudaMemcpyAsync(b_.coeff, coeff.data(), sizeof(float4) * ncoeff, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.mass, mass.data(), sizeof(float2) * nmass, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.bondc, bondc.data(), sizeof(float4) * nbond, cudaMemcpyHostToDevice, stream_));
+    // harmonic angles (atom_style angle): a static table in global tag indices
+    {
+        std::vector<int4> tbl;
+        std::vector<float2> acoef;
+        std::vector<int> awrep;
+        for (int r = 0; r < nrep; r++) {
+            const Replica& R = reps_[r];
+            if (R.ff.angle_style != 1 || R.sys.angles.empty()) continue;
+            const int off = (int)acoef.size();
+            for (const auto& c : R.ff.angle_coeff)
+                acoef.push_back(make_float2((float)c[0], (float)(c[1] * (M_PI / 180.0))));
+            const int tb = R.desc.tag_base;
+            for (size_t q = 0; q < R.sys.angles.size() / 4; q++) {
+                const int* a = &R.sys.angles[4 * q];
+                tbl.push_back(make_int4(off + a[0] - 1, tb + a[1] - 1, tb + a[2] - 1, tb + a[3] - 1));
+            }
+            while (tbl.size() % 32) tbl.push_back(make_int4(-1, 0, 0, 0));
+            while (awrep.size() < tbl.size() / 32) awrep.push_back(r);
+        }
+        nang_ = (int)tbl.size();
+        if (nang_ > 0) {
+            if ((st = dalloc(&angle_tbl_, tbl.size()))) return st;
+            if ((st = dalloc(&angle_coef_, acoef.size()))) return st;
+            if ((st = dalloc(&angle_wrep_, awrep.size()))) return st;
+            CK(cudaMemcpyAsync(angle_tbl_, tbl.data(), sizeof(int4) * tbl.size(), cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(angle_coef_, acoef.data(), sizeof(float2) * acoef.size(), cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(angle_wrep_, awrep.data(), sizeof(int) * awrep.size(), cudaMemcpyHostToDevice, stream_));
+            CK(cudaStreamSynchronize(stream_));
+        }
+    }
     std::vector<RepState> rs(nrep);
     for (auto& s : rs) {
         memset(&s, 0, sizeof(s));
@@ -615,6 +645,7 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     }
     if (any_mdpd_) launch_pair<1>(variant, bonds_, gp, s, sa);
     if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
+    if (nang_ > 0) pdl_launch(k_angle, (nang_ + 255) / 256, 256, s, sa, angle_tbl_, angle_coef_, angle_wrep_, nang_);
     if (rdf_) pdl_launch(k_rdf, gp, 256, s, sa);
     pdl_launch(k_integrate_nolog, gp, 256, s, sa);
     pdl_launch(k_integrate_logsteps, std::min(gp, 148 * 4), 256, s, sa);
@@ -790,9 +821,10 @@ int Engine::set_limits(const std::vector<uint32_t>& limit)
 // layout() and alloc_and_upload() (the server admits jobs against its budget with it).
 int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
 {
-    int64_t P = 0, C = 0, ntag = 0, ncoeff = 0, nmass = 0, nbond = 0, nrdf = 0;
+    int64_t P = 0, C = 0, ntag = 0, ncoeff = 0, nmass = 0, nbond = 0, nrdf = 0, nang = 0;
     int64_t nmax = 16, maxb = 0;
     const int64_t nrep = (int64_t)reps.size();
+    for (const Replica* R : reps) nang += ((int64_t)(R->sys.angles.size() / 4) + 31) / 32 * 32;
     for (const Replica* R : reps) {
         const double cut = R->in.global_cut + R->in.skin;
         int64_t ncell = 1;
@@ -825,6 +857,7 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     bytes += P * (2 * (16 + 16 + 16) + 2 * mb * 8 + 16 + 16 + 4 + 4 + 8 + 4 * nmax + mb * 8);
     bytes += C * (4 * 5) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
+    bytes += nang * 16 + (nang / 32) * 4 + nrep * 32 * 8;  // angle table, warp replicas, coefficients
     return bytes + 64 * 1024 + nrep * 1024;  // arrays of size 0 still take one element
 }
 
@@ -874,6 +907,7 @@ int Engine::get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows)
         for (int c = 0; c < 6; c++) t.p[c] = row[5 + c];
         t.ke = row[11];
         for (int c = 0; c < 3; c++) t.momentum[c] = row[12 + c];
+        t.angle_pe = row[16];
     }
     if (n_rows) *n_rows = n;
     return DPD_OK;
@@ -1287,6 +1321,25 @@ int make_replica_from_system(const std::string& run_in, const dpd_system* s, Rep
             if (ty < 1 || ty > std::max(1, d.n_bondtypes) || a < 1 || a > n || c < 1 || c > n || a == c) {
                 err = "invalid bond " + std::to_string(b + 1);
                 return DPD_E_ARG;
+            }
+        }
+    }
+    if (R.in.atom_style == 2) {
+        d.n_angles = s->n_angles;
+        d.n_angletypes = s->n_angletypes;
+        if (d.n_angles > 0) {
+            if (!s->angles) {
+                err = "angles missing";
+                return DPD_E_ARG;
+            }
+            d.angles.assign(s->angles, s->angles + 4 * (size_t)d.n_angles);
+            for (int q = 0; q < d.n_angles; q++) {
+                const int* a = &d.angles[4 * q];
+                if (a[0] < 1 || a[0] > std::max(1, d.n_angletypes) || a[1] < 1 || a[1] > n || a[2] < 1 ||
+                    a[2] > n || a[3] < 1 || a[3] > n || a[1] == a[2] || a[2] == a[3] || a[1] == a[3]) {
+                    err = "invalid angle " + std::to_string(q + 1);
+                    return DPD_E_ARG;
+                }
             }
         }
     }

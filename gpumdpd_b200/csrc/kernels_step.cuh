@@ -756,6 +756,70 @@ __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
 }
 
 // ---------------------------------------------------------------------------------
+// Harmonic angles, src/force/angle_harmonic.cu:187-270, one thread per angle, after the
+// pair kernel: d1 = x_i - x_j, d2 = x_k - x_j (j the apex), c = cos(theta) clamped to
+// [-1, 1], s = sin(theta) >= 0.001, E = k (theta - theta0)^2, a = -2 k dtheta / s,
+// F_i = a c/|d1|^2 d1 - a/(|d1||d2|) d2, F_k likewise, F_j = -(F_i + F_k), added with
+// float4 reductions.  The table is in global tag indices (it never moves); each
+// replica's range is padded to whole warps (entries with coef < 0 are padding), so a
+// warp's FP64 sums belong to one replica.
+__global__ void __launch_bounds__(256) k_angle(StepArgs a, const int4* __restrict__ tbl,
+                                               const float2* __restrict__ coef, const int* awarp_rep, int nang)
+{
+    griddep_wait();
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((q & ~31) >= nang) return;  // nang is a multiple of 32
+    const int r = awarp_rep[q >> 5];
+    const RepState st = a.rstate[r];
+    if (!rep_active(st)) return;  // warp-uniform
+    const RepDesc& d = a.reps[r];
+    const bool log = (st.step % (uint32_t)d.log_f) == 0u;
+    double accv[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int4 e = tbl[q];
+    if (e.x >= 0) {
+        const int i = a.tag2idx[e.y], j = a.tag2idx[e.z], k = a.tag2idx[e.w];
+        if (i < d.p_begin || i >= d.p_end || j < d.p_begin || j >= d.p_end || k < d.p_begin || k >= d.p_end) {
+            atomicOr(&a.rstate[r].status, ST_BOND_MISSING);
+        } else {
+            const float4* pos = a.buf.pos[*a.parity];
+            const float4 pi = pos[i], pj = pos[j], pk = pos[k];
+            float d1x, d1y, d1z, d2x, d2y, d2z;
+            disp3(d, __float_as_int(pi.w), pi, pj, d1x, d1y, d1z);
+            disp3(d, __float_as_int(pk.w), pk, pj, d2x, d2y, d2z);
+            const float rsq1 = d1x * d1x + d1y * d1y + d1z * d1z;
+            const float rsq2 = d2x * d2x + d2y * d2y + d2z * d2z;
+            const float r1 = sqrtf(rsq1), r2 = sqrtf(rsq2);
+            float c = (d1x * d2x + d1y * d2y + d1z * d2z) / (r1 * r2);
+            c = fminf(fmaxf(c, -1.0f), 1.0f);
+            const float sn = fmaxf(sqrtf(1.0f - c * c), 0.001f);
+            const float2 kc = coef[e.x];  // {k, theta0 in radians}
+            const float dth = acosf(c) - kc.y;
+            const float aa = -2.0f * kc.x * dth / sn;
+            const float a11 = aa * c / rsq1, a12 = -aa / (r1 * r2), a22 = aa * c / rsq2;
+            const float fix = a11 * d1x + a12 * d2x, fiy = a11 * d1y + a12 * d2y, fiz = a11 * d1z + a12 * d2z;
+            const float fkx = a22 * d2x + a12 * d1x, fky = a22 * d2y + a12 * d1y, fkz = a22 * d2z + a12 * d1z;
+            atomicAdd(&a.force4[i], make_float4(fix, fiy, fiz, 0.0f));
+            atomicAdd(&a.force4[k], make_float4(fkx, fky, fkz, 0.0f));
+            atomicAdd(&a.force4[j], make_float4(-(fix + fkx), -(fiy + fky), -(fiz + fkz), 0.0f));
+            if (log) {
+                accv[0] = (double)kc.x * (double)dth * (double)dth;
+                accv[1] = (double)d1x * fix + (double)d2x * fkx;
+                accv[2] = (double)d1x * fiy + (double)d2x * fky;
+                accv[3] = (double)d1x * fiz + (double)d2x * fkz;
+                accv[4] = (double)d1y * fiy + (double)d2y * fky;
+                accv[5] = (double)d1y * fiz + (double)d2y * fkz;
+                accv[6] = (double)d1z * fiz + (double)d2z * fkz;
+            }
+        }
+    }
+    if (log) {
+        const int fields[7] = {ACC_ANGLE_PE, ACC_VIR + 0, ACC_VIR + 1, ACC_VIR + 2,
+                               ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+        acc_flush_warp<7>(accv, fields, r, a.acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // End of step bookkeeping, one thread per replica: thermo row of a logged step
 // (src/compute/thermo.cu:274-306, 479-520), step counter, build flag of this phase.
 __global__ void k_advance(StepArgs a)
@@ -790,6 +854,7 @@ __global__ void k_advance(StepArgs a)
                 row[13] = sum[ACC_MOM + 1];
                 row[14] = sum[ACC_MOM + 2];
                 row[15] = (double)st.status;
+                row[16] = sum[ACC_ANGLE_PE];
                 st.nlog++;
             }
             st.step++;

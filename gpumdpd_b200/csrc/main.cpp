@@ -42,7 +42,7 @@ int main(int argc, char** argv)
         std::string k, a;
         t >> k;
         if (k == "run") t >> nsteps;
-        if (k == "atom_style") { t >> a; atom_style = a == "atomic" ? 0 : 1; }
+        if (k == "atom_style") { t >> a; atom_style = a == "atomic" ? 0 : (a == "bond" ? 1 : 2); }
         if (k == "write_data") t >> out_data;
     }
     e = dpd_run(eng, nsteps);
@@ -58,18 +58,26 @@ int main(int argc, char** argv)
     if (atom_style == 0)
         fprintf(th, "%15s\t%10s\t%20s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\n", "step", "temp", "pair_pe",
                 "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz");
-    else
+    else if (atom_style == 1)
         fprintf(th, "%15s\t%10s\t%20s\t%20s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\n", "step", "temp",
                 "pair_pe", "bond_pe", "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz");
+    else  // src/compute/thermo.cu:55-62
+        fprintf(th, "%15s\t%10s\t%20s\t%20s\t%20s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\t%12s\n", "step",
+                "temp", "pair_pe", "bond_pe", "angle_pe", "pressure", "pxx", "pxy", "pxz", "pyy", "pyz", "pzz");
     for (int k = 0; k < n; k++) {
         const dpd_thermo& r = rows[k];
         if (atom_style == 0)
             fprintf(th, "%15lld\t%10.6f\t%20.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\n",
                     (long long)r.step, r.temp, r.pair_pe, r.pressure, r.p[0], r.p[1], r.p[2], r.p[3], r.p[4], r.p[5]);
-        else
+        else if (atom_style == 1)
             fprintf(th, "%15lld\t%10.6f\t%20.6f\t%20.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\n",
                     (long long)r.step, r.temp, r.pair_pe, r.bond_pe, r.pressure, r.p[0], r.p[1], r.p[2], r.p[3],
                     r.p[4], r.p[5]);
+        else
+            fprintf(th,
+                    "%15lld\t%10.6f\t%20.6f\t%20.6f\t%20.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\t%12.6f\n",
+                    (long long)r.step, r.temp, r.pair_pe, r.bond_pe, r.angle_pe, r.pressure, r.p[0], r.p[1], r.p[2],
+                    r.p[3], r.p[4], r.p[5]);
     }
     fclose(th);
     if (!out_data.empty()) dpd_write_data(eng, out_data.c_str());

@@ -21,7 +21,7 @@ def _check(code, lib, handle):
 
 
 def _rows_to_dict(rows, n):
-    out = {k: np.empty(n) for k in ("step", "temp", "pair_pe", "bond_pe", "pressure", "ke")}
+    out = {k: np.empty(n) for k in ("step", "temp", "pair_pe", "bond_pe", "angle_pe", "pressure", "ke")}
     out["p"] = np.empty((n, 6))
     out["momentum"] = np.empty((n, 3))
     for k in range(n):
@@ -30,6 +30,7 @@ def _rows_to_dict(rows, n):
         out["temp"][k] = r.temp
         out["pair_pe"][k] = r.pair_pe
         out["bond_pe"][k] = r.bond_pe
+        out["angle_pe"][k] = r.angle_pe
         out["pressure"][k] = r.pressure
         out["ke"][k] = r.ke
         out["p"][k] = list(r.p)

@@ -58,6 +58,9 @@ typedef struct dpd_system {
     const double* x;      /* [3*n_atoms] */
     const double* v;      /* [3*n_atoms] or NULL */
     const int* bonds;     /* [3*n_bonds]: type, tag_i, tag_j */
+    int n_angles;         /* atom_style angle: harmonic angles (src/force/angle_harmonic.cu) */
+    int n_angletypes;
+    const int* angles;    /* [4*n_angles]: type, tag_i, tag_j (apex), tag_k */
 } dpd_system;
 
 /* Thermo row, the columns of thermo.txt (src/compute/thermo.cu:39-62,122-214) in
@@ -71,6 +74,7 @@ typedef struct dpd_thermo {
     double p[6];        /* pxx pxy pxz pyy pyz pzz */
     double ke;
     double momentum[3];
+    double angle_pe;    /* atom_style angle: the angle_pe column */
 } dpd_thermo;
 
 /* Launch/tuning knobs chosen by the autotuner (gpumdpd_b200/tune.py); zero fields

@@ -80,7 +80,7 @@ BAD = [
     ("fix_dup_id", lambda t: t + "fix md all nve\n", "already registered"),
     ("dump_args", lambda t: t + "dump 0 10 wrapped force_no\n", "illegal dump command"),
     ("compute_bad", lambda t: t + "compute c all msd 1 x.txt\n", "Compute type 'msd' not found"),
-    ("angle", lambda t: t.replace("atom_style atomic", "atom_style angle") + "bond_style harmonic\nangle_style harmonic\n", "not supported"),
+    ("angle", lambda t: t.replace("atom_style atomic", "atom_style angle") + "bond_style harmonic\n", "angle_style command is missing"),
 ]
 
 
@@ -113,11 +113,28 @@ def test_bond_style_checks():
     assert code == -1 and "bond_style harmonic" in err
 
 
+def test_angle_style_checks():
+    """atom_style angle needs angle_style harmonic and every angle_coeff (reference messages,
+    src/main/read_in.cu:347-371, src/force/angle_harmonic.cu:19-147)."""
+    from gpumdpd_b200 import inputs
+    s = inputs.angle_chains(L=6.0, seed=2)
+    code, err = _create(s.run_in.replace("angle_style harmonic\n", ""), s)
+    assert code == -1 and "angle_style command is missing" in err
+    code, err = _create(s.run_in.replace("angle_coeff 1 2.0 180.0", "angle_coeff 1 2.0"), s)
+    assert code == -1 and "angle_coeff" in err
+    code, err = _create(s.run_in.replace("angle_coeff 1 2.0 180.0\n", ""), s)
+    assert code == -1 and "all angle_coeff are not set" in err
+    code, err = _create(s.run_in.replace("angle_style harmonic", "angle_style cosine"), s)
+    assert code == -1 and "angle_style" in err
+    code, err = _create(s.run_in, s)
+    assert code in (0, -8), err
+
+
 def test_data_file_reader(tmp_path, base):
     """Files in the reference's write_data layout are read (and bad ones rejected)."""
     from gpumdpd_b200 import capi, inputs
     lib = capi.load()
-    for s in (base, inputs.diblock_melt(L=6.0, seed=2)):
+    for s in (base, inputs.diblock_melt(L=6.0, seed=2), inputs.angle_chains(L=6.0, seed=3)):
         p = tmp_path / "in.data"
         s.write_data(str(p))
         h = ctypes.c_void_p()

@@ -32,10 +32,11 @@ def _golden_system(name):
     x = np.column_stack([g[f"s0_{c}"] for c in "xyz"])
     v = np.column_stack([g[f"s0_v{c}"] for c in "xyz"])
     run_in = str(g["run_in"])
-    style = "bond" if "bonds" in g else "atomic"
+    style = "angle" if "angles" in g else ("bond" if "bonds" in g else "atomic")
     lines = [ln for ln in run_in.splitlines() if not ln.startswith("dump")]
     s = System(g["lo"], g["hi"], g["masses"], g["s0_type"], x, v, bonds=g.get("bonds"),
-               n_bondtypes=1 if "bonds" in g else 0, run_in="\n".join(lines) + "\n", atom_style=style)
+               n_bondtypes=1 if "bonds" in g else 0, run_in="\n".join(lines) + "\n", atom_style=style,
+               angles=g.get("angles"), n_angletypes=1 if "angles" in g else 0)
     return s, g
 
 
@@ -46,6 +47,9 @@ def _systems():
         "mdpd": inputs.mdpd_slab(Lx=8.0, Ly=8.0, Lz=24.0, z0=8.0, z1=16.0, seed=11, nsteps=10),
         "diblock": inputs.diblock_melt(L=10.0, seed=5, nsteps=10),
         "small_box": inputs.binary_mixture(4.5, 35.0, seed=3),  # 3 cells per dimension
+        # theta0 = 180: the harmonic angle force stays smooth through straight triples (with
+        # theta0 != 180 it is singular there, and FP32 and FP64 trajectories part within steps)
+        "angles": inputs.angle_chains(L=8.0, seed=23, nsteps=10, angle_k=3.0, theta0=180.0),
     }
 
 
@@ -66,7 +70,7 @@ def test_neighbor_set_bit_exact(oracle_mod, name):
     assert set(map(tuple, inner.tolist())) <= set(map(tuple, got.tolist()))
 
 
-@pytest.mark.parametrize("name", ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc"])
+@pytest.mark.parametrize("name", ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc", "angle_chains"])
 def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     s, g = _golden_system(name)
     e = _engine_from(s)
@@ -74,7 +78,7 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     st = e.state()
     ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
     o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, st["x"], st["v"], s.lo, _box(e), 0,
-                          bonds=s.bonds)
+                          bonds=s.bonds, angles=s.angles)
     assert force_err(st["f"], o["f"]) < FORCE_TOL
     f_ref = np.column_stack([g[f"s0_f{c}"] for c in "xyz"])
     assert force_err(st["f"], f_ref) < FORCE_TOL
@@ -82,6 +86,9 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     assert th["step"][0] == 0
     assert th["pair_pe"][0] == pytest.approx(o["pair_pe"], rel=1e-6)
     assert th["bond_pe"][0] == pytest.approx(o["bond_pe"], rel=1e-6, abs=1e-9)
+    assert th["angle_pe"][0] == pytest.approx(o["angle_pe"], rel=1e-5, abs=1e-9)
+    if "thermo_angle_pe" in g:
+        assert th["angle_pe"][0] == pytest.approx(g["thermo_angle_pe"][0], rel=2e-5)
     assert th["temp"][0] == pytest.approx(g["thermo_temp"][0], rel=1e-6)
     assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
 
@@ -116,7 +123,7 @@ def test_pair_schedules_agree_with_oracle(oracle_mod, name, variant):
     assert force_err(a["f"], b["f"]) < 1e-4
 
 
-@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock"])
+@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "angles"])
 def test_trajectory_10_steps(oracle_mod, name):
     """After equilibrating 100 steps on the GPU, 10 steps of engine and oracle from the
     same state: forces within 1e-5 of RMS at every step, thermo rows agree."""
@@ -133,7 +140,7 @@ def test_trajectory_10_steps(oracle_mod, name):
         got = e.state()
         # continue from the engine's end-of-step-100 state and its step-100 forces
         o = oracle_mod.run(ff, tags, s.types, st["x"], st["v"], s.lo, L, 101, k, 1, bonds=s.bonds,
-                           zero_step=False, f0=st["f"])
+                           zero_step=False, f0=st["f"], angles=s.angles)
         # FP32 state vs FP64 oracle diverge chaotically; the stated trajectory tolerance:
         # 99.9th percentile of |dF_i| within 1e-5 of RMS, max within 3e-5 (close pairs
         # amplify sub-ulp position differences as 1/r)

@@ -43,6 +43,9 @@ def _case(name):
     elif name == "diblock":
         s = inputs.diblock_melt(L=10.0, seed=5, nsteps=100, thermo=5)
         style = "dpd"
+    elif name == "angles":
+        s = inputs.angle_chains(L=8.0, seed=29, nsteps=100, thermo=5, angle_k=3.0, theta0=120.0)
+        style = "dpd"
     else:
         s = inputs.mdpd_slab(Lx=8.0, Ly=8.0, Lz=24.0, z0=8.0, z1=16.0, seed=11, nsteps=100, thermo=5)
         style = "mdpd"
@@ -52,7 +55,7 @@ def _case(name):
 
 @pytest.mark.skipif(not (os.path.exists(STOCK) and os.path.exists(SHIM)),
                     reason="reference builds (oracle/build_ref.sh SINGLE and SHIM) not present")
-@pytest.mark.parametrize("name", ["dpd", "diblock", "mdpd"])
+@pytest.mark.parametrize("name", ["dpd", "diblock", "angles", "mdpd"])
 def test_reference_loop_with_b200_pair_style(name):
     s, run_in, style = _case(name)
     stock = _run(STOCK, s, run_in)
