@@ -111,6 +111,13 @@ int dpd_get_thermo(dpd_engine* h, dpd_thermo* rows, int max_rows, int* n_rows)
     return h->eng.get_thermo(0, rows, max_rows, n_rows);
 }
 
+int dpd_get_spring_records(dpd_engine* h, double* rows, int max_rows, int* n_rows)
+{
+    ENG_CHECK(h);
+    if (!rows || max_rows < 0) return DPD_E_ARG;
+    return h->eng.spring_records(0, rows, max_rows, n_rows);
+}
+
 int dpd_get_state(dpd_engine* h, double* x, double* v, int* image, double* f)
 {
     ENG_CHECK(h);

@@ -3,7 +3,8 @@
 #include <stdint.h>
 
 #define DPD_MAX_TYPES 32
-#define DPD_NACC 24          // FP64 accumulators per replica and slot
+#define DPD_NACC 32          // FP64 accumulators per replica and slot
+#define DPD_NACC_THERMO 20   // the first DPD_NACC_THERMO feed the thermo row
 #define DPD_ACC_SLOTS 32     // atomic spreading slots per replica
 #define DPD_THERMO_FIELDS 17 // doubles per logged thermo row
 #define DPD_RING_ROWS 2048   // thermo rows kept per replica on the device
@@ -22,6 +23,10 @@ enum {
     ACC_MOM = 15,    // 3: sum m v
     ACC_NONFINITE = 18,
     ACC_ANGLE_PE = 19,
+    // group-fix sums, consumed (and zeroed) by the fix reductions of the same step
+    ACC_SPRING_COM = 20,  // 3: sum over the spring group of m x_unwrapped
+    ACC_RVCM_P = 23,      // 3: sum over the rvcm group of m v
+    ACC_RECENTER_COM = 26 // 3: sum over the recenter group of m x_unwrapped
 };
 
 // status bits (per replica, device)
@@ -68,6 +73,26 @@ struct RepDesc {
     int rdf_ta, rdf_tb, rdf_nbins;
     float rdf_rmax;
     int rdf_off;    // offset into the RDF histogram array (nbins per replica)
+};
+
+// Per-replica group fixes (src/fix/fix_spring.cu, fix_rvcm.cu, fix_recenter.cu).
+// A mask holds bit (type-1) of each type of the fix's group; 0 = fix absent.
+struct FixDesc {
+    uint32_t spring_mask, rvcm_mask, recenter_mask;
+    uint32_t rvcm_freq, recenter_freq;
+    int rvcm_flag[3];
+    double spring_k, spring_c[3], spring_r0, spring_m;  // spring_m: group mass
+    double rvcm_m, recenter_m, recenter_c[3];
+    double L[3];           // box lengths of the cell grid (unwrapped = lo + c w + o + img L)
+    uint32_t spring_file_f; // spring record every this many steps (0 = none)
+};
+
+// Per-replica results of the fix reductions of the current step (device).
+struct FixOut {
+    float spring_a[3];     // spring force over group mass: member i gets m_i * spring_a
+    float vcm[3];          // flag * centre-of-mass velocity of a due rvcm
+    float shift[3];        // position shift of a due recenter
+    int nrec;              // spring records written
 };
 
 // Per-replica dynamic state (device).

@@ -535,8 +535,14 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
         }
         ff.groups[t[1]] = types;
     }
-    // fixes, src/fix/fix.cu:27-115: only nve is on the timestep hot path
+    // fixes, src/fix/fix.cu:27-115: nve, and the group fixes spring, rvcm and recenter
+    // (validateParams of src/fix/fix_spring.cu:17-52, fix_rvcm.cu:17-40, fix_recenter.cu:17-32)
     std::set<std::string> fix_ids;
+    auto group_mask = [&](const std::string& g) {
+        uint32_t m = 0;
+        for (int ty : ff.groups[g]) m |= 1u << (ty - 1);
+        return m;
+    };
     for (size_t k = 0; k < in.lines.size(); k++) {
         const auto& t = in.lines[k];
         const std::string& line = in.raw[k];
@@ -545,7 +551,67 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
         if (fix_ids.count(t[1])) return fail(err, line, "Fix ID '" + t[1] + "' is already registered!");
         fix_ids.insert(t[1]);
         if (!ff.groups.count(t[2])) return fail(err, line, "Group '" + t[2] + "' not found!");
-        if (t[3] != "nve") return fail(err, line, "Fix type '" + t[3] + "' not found! (this engine implements fix nve)");
+        const size_t np = t.size() - 4;
+        if (t[3] == "spring") {
+            const char* msg = "illegal fix_spring command: fix ID groupID spring spring_k spring_x spring_y spring_z spring_r0 file_name(optional) file_frequency(optional)";
+            if (np != 5 && np != 7) return fail(err, line, msg);
+            if (ff.spring.on) return fail(err, line, "this engine takes at most one fix spring");
+            double v[5];
+            for (int q = 0; q < 5; q++)
+                if (!parse_double(t[4 + q], v[q])) return fail(err, line, msg);
+            long long fq = 0;
+            if (np == 7 && !parse_int(t[10], 1, 4294967295ll, fq)) return fail(err, line, msg);
+            const char* axis[3] = {"x", "y", "z"};
+            for (int d = 0; d < 3; d++)
+                if (v[1 + d] < sys.lo[d] || v[1 + d] > sys.hi[d])
+                    return fail(err, line, std::string("spring position is out of the box in ") + axis[d] + " direction!");
+            ff.spring.on = true;
+            ff.spring.mask = group_mask(t[2]);
+            ff.spring.k = v[0];
+            for (int d = 0; d < 3; d++) ff.spring.c[d] = v[1 + d];
+            ff.spring.r0 = v[4];
+            if (np == 7) {
+                ff.spring.file = t[9];
+                ff.spring.file_freq = (unsigned)fq;
+            }
+            continue;
+        }
+        if (t[3] == "rvcm") {
+            const char* msg = "illegal fix_rvcm command: fix ID groupID rvcm frequency x_flag(0/1) y_flag(0/1) z_flag(0/1)";
+            if (np != 4) return fail(err, line, msg);
+            if (ff.rvcm.on) return fail(err, line, "this engine takes at most one fix rvcm");
+            long long fq, fl[3];
+            if (!parse_int(t[4], 1, 4294967295ll, fq)) return fail(err, line, msg);
+            for (int d = 0; d < 3; d++)
+                if (!parse_int(t[5 + d], 0, 1, fl[d])) return fail(err, line, msg);
+            ff.rvcm.on = true;
+            ff.rvcm.mask = group_mask(t[2]);
+            ff.rvcm.freq = (unsigned)fq;
+            for (int d = 0; d < 3; d++) ff.rvcm.flag[d] = (int)fl[d];
+            continue;
+        }
+        if (t[3] == "recenter") {
+            const char* msg = "illegal fix_recenter command: fix ID groupID recenter frequency recenter_x recenter_y recenter_z";
+            if (np != 4) return fail(err, line, msg);
+            if (ff.recenter.on) return fail(err, line, "this engine takes at most one fix recenter");
+            long long fq;
+            if (!parse_int(t[4], 1, 4294967295ll, fq)) return fail(err, line, msg);
+            double c[3];
+            for (int d = 0; d < 3; d++)
+                if (!parse_double(t[5 + d], c[d])) return fail(err, line, msg);
+            // src/fix/fix_recenter.cu:84-100 (its messages name the spring)
+            const char* axis[3] = {"x", "y", "z"};
+            for (int d = 0; d < 3; d++)
+                if (c[d] < sys.lo[d] || c[d] > sys.hi[d])
+                    return fail(err, line, std::string("spring position is out of the box in ") + axis[d] + " direction!");
+            ff.recenter.on = true;
+            ff.recenter.mask = group_mask(t[2]);
+            ff.recenter.freq = (unsigned)fq;
+            for (int d = 0; d < 3; d++) ff.recenter.c[d] = c[d];
+            continue;
+        }
+        if (t[3] != "nve")
+            return fail(err, line, "Fix type '" + t[3] + "' not found! (this engine implements nve, spring, rvcm, recenter)");
         if (t.size() != 4) return fail(err, line, "illegal fix_nve command: fix ID groupID nve");
         for (int ty : ff.groups[t[2]]) {
             uint32_t bit = 1u << (ty - 1);

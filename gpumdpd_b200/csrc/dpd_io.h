@@ -51,6 +51,28 @@ struct ComputeRdf {
     double rmax = 3.0;
 };
 
+// Group fixes on the timestep (src/fix/fix_spring.cu, fix_rvcm.cu, fix_recenter.cu); at most
+// one of each per system.  mask: the group's types (bit type-1).
+struct FixSpring {   // post_force: F = -k (|r| - r0) r/|r| on the group's centre of mass
+    bool on = false;
+    uint32_t mask = 0;
+    double k = 0, c[3] = {0, 0, 0}, r0 = 0;
+    std::string file;    // optional record file: step Fx Fy Fz +-|F| energy every file_freq steps
+    unsigned file_freq = 0;
+};
+struct FixRvcm {     // end_of_step every freq: remove the group's centre-of-mass velocity
+    bool on = false;
+    uint32_t mask = 0;
+    unsigned freq = 1;
+    int flag[3] = {0, 0, 0};
+};
+struct FixRecenter { // end_of_step every freq: move the group's centre of mass to c
+    bool on = false;
+    uint32_t mask = 0;
+    unsigned freq = 1;
+    double c[3] = {0, 0, 0};
+};
+
 // Pair/bond styles and their coefficients, groups, fixes and computes, parsed after
 // the data file is known (as the reference's isEnabled/validateParams do).
 struct ForceField {
@@ -65,6 +87,9 @@ struct ForceField {
     std::vector<std::array<double, 2>> angle_coeff;  // k, theta0 in degrees
     std::map<std::string, std::vector<int>> groups;
     uint32_t integ_mask = 0;  // types integrated by fix nve
+    FixSpring spring;
+    FixRvcm rvcm;
+    FixRecenter recenter;
     std::vector<ComputeTemp> temps;
     std::vector<ComputeRdf> rdfs;
 };

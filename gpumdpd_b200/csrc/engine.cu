@@ -360,6 +360,57 @@ int Engine::alloc_and_upload()
             CK(cudaStreamSynchronize(stream_));
         }
     }
+    // group fixes (spring, rvcm, recenter): group masses in FP64 from the type counts
+    {
+        std::vector<FixDesc> fd(nrep);
+        bool spring_file = false;
+        any_spring_ = any_eos_ = false;
+        for (int r = 0; r < nrep; r++) {
+            const Replica& R = reps_[r];
+            FixDesc& f = fd[r];
+            memset(&f, 0, sizeof(f));
+            auto gmass = [&](uint32_t mask) {
+                double m = 0.0;
+                for (int i = 0; i < R.sys.n_atoms; i++) {
+                    const int t = R.sys.type[i];
+                    if ((mask >> (t - 1)) & 1u) m += R.sys.masses[t - 1];
+                }
+                return m;
+            };
+            for (int k = 0; k < 3; k++) f.L[k] = R.box_len[k];
+            if (R.ff.spring.on && R.ff.spring.mask) {
+                f.spring_mask = R.ff.spring.mask;
+                f.spring_k = R.ff.spring.k;
+                for (int k = 0; k < 3; k++) f.spring_c[k] = R.ff.spring.c[k];
+                f.spring_r0 = R.ff.spring.r0;
+                f.spring_m = gmass(f.spring_mask);
+                f.spring_file_f = R.ff.spring.file_freq;
+                spring_file |= f.spring_file_f != 0;
+                any_spring_ = true;
+            }
+            if (R.ff.rvcm.on && R.ff.rvcm.mask) {
+                f.rvcm_mask = R.ff.rvcm.mask;
+                f.rvcm_freq = R.ff.rvcm.freq;
+                for (int k = 0; k < 3; k++) f.rvcm_flag[k] = R.ff.rvcm.flag[k];
+                f.rvcm_m = gmass(f.rvcm_mask);
+                any_eos_ = true;
+            }
+            if (R.ff.recenter.on && R.ff.recenter.mask) {
+                f.recenter_mask = R.ff.recenter.mask;
+                f.recenter_freq = R.ff.recenter.freq;
+                for (int k = 0; k < 3; k++) f.recenter_c[k] = R.ff.recenter.c[k];
+                f.recenter_m = gmass(f.recenter_mask);
+                any_eos_ = true;
+            }
+        }
+        if (any_spring_ || any_eos_) {
+            if ((st = dalloc(&b_.fix, nrep))) return st;
+            if ((st = dalloc(&b_.fixo, nrep))) return st;
+            if (spring_file && (st = dalloc(&b_.spring_ring, (size_t)nrep * DPD_RING_ROWS * 6))) return st;
+            CK(cudaMemcpyAsync(b_.fix, fd.data(), sizeof(FixDesc) * nrep, cudaMemcpyHostToDevice, stream_));
+            CK(cudaStreamSynchronize(stream_));
+        }
+    }
     std::vector<RepState> rs(nrep);
     for (auto& s : rs) {
         memset(&s, 0, sizeof(s));
@@ -553,6 +604,9 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     a.phase = b.phase;
     a.nrep = nrep;
     a.mode = 0;
+    a.fix = b.fix;
+    a.fixo = b.fixo;
+    a.spring_ring = b.spring_ring;
     return a;
 }
 
@@ -647,16 +701,33 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     if (ev1) cudaEventRecordWithFlags(ev1, s, cudaEventRecordExternal);
     if (nang_ > 0) pdl_launch(k_angle, (nang_ + 255) / 256, 256, s, sa, angle_tbl_, angle_coef_, angle_wrep_, nang_);
     if (rdf_) pdl_launch(k_rdf, gp, 256, s, sa);
-    pdl_launch(k_integrate_nolog, gp, 256, s, sa);
-    pdl_launch(k_integrate_logsteps, std::min(gp, 148 * 4), 256, s, sa);
-    pdl_launch(k_advance, (nrep + 255) / 256, 256, s, sa);
+    const int gr = (nrep + 255) / 256;
+    if (any_spring_) {
+        // post_force: the spring acts on the forces of this step
+        pdl_launch(k_fix_sums<0>, gp, 256, s, sa);
+        pdl_launch(k_fix_reduce<0>, gr, 256, s, sa);
+    }
+    if (any_eos_) {
+        // end_of_step: final half kick, group sums and the rvcm / recenter corrections
+        pdl_launch(k_fix_sums<1>, gp, 256, s, sa);
+        pdl_launch(k_fix_reduce<1>, gr, 256, s, sa);
+    }
+    if (any_spring_ || any_eos_) {
+        pdl_launch(k_integrate_nolog<true>, gp, 256, s, sa);
+        pdl_launch(k_integrate_logsteps<true>, std::min(gp, 148 * 4), 256, s, sa);
+    } else {
+        pdl_launch(k_integrate_nolog<false>, gp, 256, s, sa);
+        pdl_launch(k_integrate_logsteps<false>, std::min(gp, 148 * 4), 256, s, sa);
+    }
+    pdl_launch(k_advance, gr, 256, s, sa);
 }
 
 void Engine::enqueue_integrate_initial(cudaStream_t s)
 {
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, (int)reps_.size());
     sa.mode = 1;
-    k_integrate<<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+    if (any_spring_ || any_eos_) k_integrate<true><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+    else k_integrate<false><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
 }
 
 int Engine::build_graph()
@@ -858,6 +929,12 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     bytes += C * (4 * 5) + ntag * 4 + ((C + 4095) / 4096 + 1) * 4;
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
     bytes += nang * 16 + (nang / 32) * 4 + nrep * 32 * 8;  // angle table, warp replicas, coefficients
+    bytes += nrep * (int64_t)(sizeof(FixDesc) + sizeof(FixOut));  // group fixes (upper bound)
+    for (const Replica* R : reps)
+        if (R->ff.spring.on && R->ff.spring.file_freq) {
+            bytes += nrep * (int64_t)DPD_RING_ROWS * 6 * 8;
+            break;
+        }
     return bytes + 64 * 1024 + nrep * 1024;  // arrays of size 0 still take one element
 }
 
@@ -913,6 +990,26 @@ int Engine::get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows)
     return DPD_OK;
 }
 
+int Engine::spring_records(int rep, double* rows, int max_rows, int* n_rows)
+{
+    if (rep < 0 || rep >= (int)reps_.size() || max_rows < 0) return DPD_E_ARG;
+    if (n_rows) *n_rows = 0;
+    if (!b_.spring_ring) return DPD_OK;
+    FixOut fo;
+    CK(cudaMemcpyAsync(&fo, b_.fixo + rep, sizeof(FixOut), cudaMemcpyDeviceToHost, stream_));
+    std::vector<double> ring((size_t)DPD_RING_ROWS * 6);
+    CK(cudaMemcpyAsync(ring.data(), b_.spring_ring + (size_t)rep * DPD_RING_ROWS * 6, sizeof(double) * ring.size(),
+                       cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const int n = std::min(std::min(fo.nrec, DPD_RING_ROWS), max_rows);
+    for (int k = 0; k < n; k++) {
+        const int idx = (fo.nrec - n + k) % DPD_RING_ROWS;
+        memcpy(rows + 6 * (size_t)k, ring.data() + 6 * (size_t)idx, 6 * sizeof(double));
+    }
+    if (n_rows) *n_rows = n;
+    return DPD_OK;
+}
+
 int Engine::cur_parity()
 {
     int par = 0;
@@ -941,6 +1038,11 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
         CK(cudaMemcpyAsync(img, b_.img[par] + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
     }
     if (f) CK(cudaMemcpyAsync(frc, b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
+    // a spring's share of the force (post_force adds it to the force array the reference
+    // dumps, src/fix/fix_spring.cu:350-370); the engine adds it inside the half kicks
+    FixOut fo{};
+    const bool spring = f && b_.fixo && R.ff.spring.on && R.ff.spring.mask;
+    if (spring) CK(cudaMemcpyAsync(&fo, b_.fixo + rep, sizeof(FixOut), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
     std::atomic<int> bad{0};
     parallel_for(d.n_real, [&](int64_t k0, int64_t k1) {
@@ -971,6 +1073,8 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
             if (x) x[o + q] = d.lo[q] + xa;
             if (v) v[o + q] = vv[q];
             if (f) f[o + q] = ff[q];
+            if (spring && ((R.ff.spring.mask >> (tw & ((1 << DPD_TYPE_BITS) - 1))) & 1u))
+                f[o + q] += (double)fo.spring_a[q] * R.sys.masses[tw & ((1 << DPD_TYPE_BITS) - 1)];
             if (image) image[o + q] = im[q] + (int)wrap;
         }
     }

@@ -45,6 +45,9 @@ struct DeviceBuffers {
     int* build_flag = nullptr;
     uint32_t* phase = nullptr;
     uint32_t* limit = nullptr;  // per replica: last step it may evaluate (job length)
+    FixDesc* fix = nullptr;     // per replica group fixes (allocated when any replica has one)
+    FixOut* fixo = nullptr;
+    double* spring_ring = nullptr;  // spring records (allocated when a spring writes a file)
 };
 
 class Engine {
@@ -73,6 +76,8 @@ public:
     int write_data(int rep, const std::string& path);
     int set_tuning(const dpd_tuning* t);
     int list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds);
+    // spring records {step, Fx, Fy, Fz, +-|F|, energy} of a replica (newest DPD_RING_ROWS)
+    int spring_records(int rep, double* rows, int max_rows, int* n_rows);
     int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
                          int n, uint32_t step, float* d_force, float* d_pe, float* d_virial);
 
@@ -111,6 +116,7 @@ private:
     cudaGraphExec_t graph_ = nullptr;
     int P_ = 0, C_ = 0, nmax_ = 16, maxb_ = 0;
     bool any_mdpd_ = false, any_dpd_ = false, bonds_ = false, rdf_ = false;
+    bool any_spring_ = false, any_eos_ = false;  // some replica has a spring / an rvcm or recenter
     bool zero_pending_ = true;
     uint32_t next_step_ = 0;
     std::vector<void*> allocs_;

@@ -30,7 +30,21 @@ struct StepArgs {
     uint32_t* phase;
     int nrep;
     int mode;              // integrate kernel: 0 = per-step (final+initial), 1 = initial only
+    const FixDesc* fix;    // [nrep] group fixes (null when no replica has one)
+    FixOut* fixo;          // [nrep]
+    double* spring_ring;   // [nrep][DPD_RING_ROWS][6] spring records (null: none)
 };
+
+// end-of-step fixes due at the current step of a replica: bit 0 rvcm, bit 1 recenter
+// (src/main/utils.cuh:287: Fix_end_of_step after the final half kick of steps >= 1)
+__device__ __forceinline__ int fix_eos_due(const FixDesc& f, const RepState& st, int mode)
+{
+    if (mode != 0 || st.zero_pending || !(st.step <= st.target)) return 0;
+    int due = 0;
+    if (f.rvcm_mask && (st.step % f.rvcm_freq) == 0u) due |= 1;
+    if (f.recenter_mask && (st.step % f.recenter_freq) == 0u) due |= 2;
+    return due;
+}
 
 __device__ __forceinline__ bool rep_active(const RepState& st) { return st.step <= st.target; }
 
@@ -637,7 +651,7 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
 // only moves the offsets.
 // LOGM: 2 = any step; 0 = every step except logged mode-0 steps (no FP64 sums: fewer
 // registers); 1 = logged mode-0 steps only.  0 and 1 together cover every slot once.
-template <int LOGM>
+template <int LOGM, bool FIX>
 __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
 {
     int r = -1;
@@ -670,10 +684,40 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
             const bool integ = (d.integ_mask >> t0) & 1u;
             const float dt = d.dt;
             const float dtm = (0.5f * dt) * m.y;
-            if (fin && integ) {
-                v.x = __fmaf_rn(dtm, f.x, v.x);
-                v.y = __fmaf_rn(dtm, f.y, v.y);
-                v.z = __fmaf_rn(dtm, f.z, v.z);
+            float4 fe = f;
+            int eos = 0;
+            bool shifted = false;
+            if (FIX) {
+                // group fixes: the spring's share m_i F / M joins the force of both half
+                // kicks (post_force); a due rvcm or recenter (end_of_step) has had its
+                // final half kick in k_fix_sums<1> and acts here before the thermo sums
+                const FixDesc& fd = a.fix[r];
+                eos = fix_eos_due(fd, st, a.mode);
+                if ((fd.spring_mask >> t0) & 1u) {
+                    const FixOut& fo = a.fixo[r];
+                    fe.x = __fmaf_rn(fo.spring_a[0], m.x, fe.x);
+                    fe.y = __fmaf_rn(fo.spring_a[1], m.x, fe.y);
+                    fe.z = __fmaf_rn(fo.spring_a[2], m.x, fe.z);
+                }
+                if (eos) {
+                    const FixOut& fo = a.fixo[r];
+                    if ((eos & 1) && ((fd.rvcm_mask >> t0) & 1u)) {
+                        v.x -= fo.vcm[0];
+                        v.y -= fo.vcm[1];
+                        v.z -= fo.vcm[2];
+                    }
+                    if ((eos & 2) && ((fd.recenter_mask >> t0) & 1u)) {
+                        p.x += fo.shift[0];
+                        p.y += fo.shift[1];
+                        p.z += fo.shift[2];
+                        shifted = true;
+                    }
+                }
+            }
+            if (fin && integ && !eos) {
+                v.x = __fmaf_rn(dtm, fe.x, v.x);
+                v.y = __fmaf_rn(dtm, fe.y, v.y);
+                v.z = __fmaf_rn(dtm, fe.z, v.z);
             }
             if (log) {
                 const double vx = v.x, vy = v.y, vz = v.z, mm = m.x;
@@ -688,11 +732,12 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                 accv[8] = mm * vy;
                 accv[9] = mm * vz;
             }
+            if (FIX && shifted && !(init && integ)) posp[s] = p;
             if (init) {
                 if (integ) {
-                    v.x = __fmaf_rn(dtm, f.x, v.x);
-                    v.y = __fmaf_rn(dtm, f.y, v.y);
-                    v.z = __fmaf_rn(dtm, f.z, v.z);
+                    v.x = __fmaf_rn(dtm, fe.x, v.x);
+                    v.y = __fmaf_rn(dtm, fe.y, v.y);
+                    v.z = __fmaf_rn(dtm, fe.z, v.z);
                     p.x = __fmaf_rn(dt, v.x, p.x);
                     p.y = __fmaf_rn(dt, v.y, p.y);
                     p.z = __fmaf_rn(dt, v.z, p.z);
@@ -729,19 +774,22 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
     }
 }
 
+template <bool FIX>
 __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
 {
     griddep_wait();
-    integrate_slot<2>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    integrate_slot<2, FIX>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+template <bool FIX>
 __global__ void __launch_bounds__(256) k_integrate_nolog(StepArgs a)
 {
     griddep_wait();
-    integrate_slot<0>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    integrate_slot<0, FIX>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // logged steps: a small grid-stride launch that returns at once when no replica logs
+template <bool FIX>
 __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
 {
     griddep_wait();
@@ -752,7 +800,162 @@ __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
     }
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1>(a, vb * 256 + threadIdx.x);
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, FIX>(a, vb * 256 + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------------
+// Group fixes.  Sums over a group are warp-reduced into the spread FP64 accumulators
+// (fields ACC_SPRING_COM, ACC_RVCM_P, ACC_RECENTER_COM) and reduced per replica by
+// k_fix_reduce of the same phase, which zeroes them again.  Unwrapped positions are
+// lo + c w + o + img L (the reference keeps them as uwpos, src/system/system.cuh:14).
+//  PH 0 (every step, replicas with a spring): sum m x over the spring group, from the
+//       positions the forces of this step were evaluated at (src/fix/fix_spring.cu:281-300).
+//  PH 1 (replicas with an rvcm or recenter due this step): the final half kick (with the
+//       spring share), then sum m v over the rvcm group (src/fix/fix_rvcm.cu:233-262) and
+//       m x over the recenter group (src/fix/fix_recenter.cu:270-300).
+__device__ __forceinline__ double unwrapped(const RepDesc& d, const FixDesc& fd, int code, float o,
+                                            int img, int k)
+{
+    const int c = (code >> (k * DPD_CELL_BITS)) & DPD_MAX_NC;
+    return d.lo[k] + (double)c * (double)d.w[k] + (double)o + (double)img * fd.L[k];
+}
+
+template <int PH>
+__global__ void __launch_bounds__(256) k_fix_sums(StepArgs a)
+{
+    griddep_wait();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;  // P is a multiple of 32: warp-uniform
+    const int r = a.warp_rep[s >> 5];
+    const RepState st = a.rstate[r];
+    const FixDesc& fd = a.fix[r];
+    int eos = 0;
+    if (PH == 0) {
+        if (!rep_active(st) || !fd.spring_mask) return;
+    } else {
+        eos = fix_eos_due(fd, st, a.mode);
+        if (!eos) return;
+    }
+    const RepDesc& d = a.reps[r];
+    double accv[6] = {0, 0, 0, 0, 0, 0};
+    if (s < d.p_end) {
+        const int par = *a.parity;
+        float4 v = a.buf.vel[par][s];
+        const int t0 = type0_of(v.w);
+        const float2 m = __ldg(a.mass + d.mass_off + t0);
+        if (PH == 1) {
+            if ((d.integ_mask >> t0) & 1u) {
+                float4 f = a.force4[s];
+                if ((fd.spring_mask >> t0) & 1u) {
+                    const FixOut& fo = a.fixo[r];
+                    f.x = __fmaf_rn(fo.spring_a[0], m.x, f.x);
+                    f.y = __fmaf_rn(fo.spring_a[1], m.x, f.y);
+                    f.z = __fmaf_rn(fo.spring_a[2], m.x, f.z);
+                }
+                const float dtm = (0.5f * d.dt) * m.y;
+                v.x = __fmaf_rn(dtm, f.x, v.x);
+                v.y = __fmaf_rn(dtm, f.y, v.y);
+                v.z = __fmaf_rn(dtm, f.z, v.z);
+                a.buf.vel[par][s] = v;
+            }
+            if ((eos & 1) && ((fd.rvcm_mask >> t0) & 1u)) {
+                accv[0] = (double)m.x * v.x;
+                accv[1] = (double)m.x * v.y;
+                accv[2] = (double)m.x * v.z;
+            }
+        }
+        const uint32_t gm = PH == 0 ? fd.spring_mask : ((eos & 2) ? fd.recenter_mask : 0u);
+        if ((gm >> t0) & 1u) {
+            const float4 p = a.buf.pos[par][s];
+            const int4 im = a.buf.img[par][s];
+            const int code = __float_as_int(p.w);
+            const int base = PH == 0 ? 0 : 3;
+            accv[base + 0] = (double)m.x * unwrapped(d, fd, code, p.x, im.x, 0);
+            accv[base + 1] = (double)m.x * unwrapped(d, fd, code, p.y, im.y, 1);
+            accv[base + 2] = (double)m.x * unwrapped(d, fd, code, p.z, im.z, 2);
+        }
+    }
+    if (PH == 0) {
+        double v3[3] = {accv[0], accv[1], accv[2]};
+        const int fields[3] = {ACC_SPRING_COM + 0, ACC_SPRING_COM + 1, ACC_SPRING_COM + 2};
+        acc_flush_warp<3>(v3, fields, r, a.acc);
+    } else {
+        const int fields[6] = {ACC_RVCM_P + 0, ACC_RVCM_P + 1, ACC_RVCM_P + 2,
+                               ACC_RECENTER_COM + 0, ACC_RECENTER_COM + 1, ACC_RECENTER_COM + 2};
+        acc_flush_warp<6>(accv, fields, r, a.acc);
+    }
+}
+
+// sum and zero three fields of a replica's spread accumulators
+__device__ __forceinline__ void acc_take3(double* acc, int r, int field, double out[3])
+{
+    double* base = acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC;
+    out[0] = out[1] = out[2] = 0.0;
+    for (int sl = 0; sl < DPD_ACC_SLOTS; sl++)
+        for (int k = 0; k < 3; k++) {
+            out[k] += base[sl * DPD_NACC + field + k];
+            base[sl * DPD_NACC + field + k] = 0.0;
+        }
+}
+
+// One thread per replica.  PH 0: the spring force F = -k (r - r0) d / r, d = com - c,
+// when r > 1e-10 (src/fix/fix_spring.cu:300-340), kept as F / M, and the spring record
+// {step, Fx, Fy, Fz, +-|F|, k (r - r0)^2 / 2} of file steps.  PH 1: flag * vcm of a due
+// rvcm (src/fix/fix_rvcm.cu:262-286) and target - com of a due recenter
+// (src/fix/fix_recenter.cu:300-335).
+template <int PH>
+__global__ void k_fix_reduce(StepArgs a)
+{
+    griddep_wait();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nrep) return;
+    const RepState st = a.rstate[r];
+    const FixDesc& fd = a.fix[r];
+    FixOut& fo = a.fixo[r];
+    if (PH == 0) {
+        if (!rep_active(st) || !fd.spring_mask) return;
+        double sum[3];
+        acc_take3(a.acc, r, ACC_SPRING_COM, sum);
+        double dv[3], r2 = 0.0;
+        for (int k = 0; k < 3; k++) {
+            dv[k] = (fd.spring_m > 0.0 ? sum[k] / fd.spring_m : 0.0) - fd.spring_c[k];
+            r2 += dv[k] * dv[k];
+        }
+        const double rr = sqrt(r2), dr = rr - fd.spring_r0;
+        double F[3] = {0.0, 0.0, 0.0}, fm = 0.0, e = 0.0;
+        if (rr > 1.0e-10 && fd.spring_m > 0.0) {
+            for (int k = 0; k < 3; k++) F[k] = -fd.spring_k * dr * dv[k] / rr;
+            fm = sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+            if (dr < 0.0) fm = -fm;
+            e = 0.5 * fd.spring_k * dr * dr;
+        }
+        for (int k = 0; k < 3; k++) fo.spring_a[k] = fd.spring_m > 0.0 ? (float)(F[k] / fd.spring_m) : 0.0f;
+        if (a.spring_ring && fd.spring_file_f && (st.step % fd.spring_file_f) == 0u) {
+            double* row = a.spring_ring + ((size_t)r * DPD_RING_ROWS + (fo.nrec % DPD_RING_ROWS)) * 6;
+            row[0] = (double)st.step;
+            row[1] = F[0];
+            row[2] = F[1];
+            row[3] = F[2];
+            row[4] = fm;
+            row[5] = e;
+            fo.nrec++;
+        }
+    } else {
+        const int eos = fix_eos_due(fd, st, a.mode);
+        if (!eos) return;
+        if (eos & 1) {
+            double P[3];
+            acc_take3(a.acc, r, ACC_RVCM_P, P);
+            for (int k = 0; k < 3; k++)
+                fo.vcm[k] = fd.rvcm_flag[k] && fd.rvcm_m > 0.0 ? (float)(P[k] / fd.rvcm_m) : 0.0f;
+        }
+        if (eos & 2) {
+            double c[3];
+            acc_take3(a.acc, r, ACC_RECENTER_COM, c);
+            for (int k = 0; k < 3; k++)
+                fo.shift[k] = fd.recenter_m > 0.0 ? (float)(fd.recenter_c[k] - c[k] / fd.recenter_m) : 0.0f;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -831,11 +1034,11 @@ __global__ void k_advance(StepArgs a)
         const RepDesc& d = a.reps[r];
         if (rep_active(st)) {
             if ((st.step % (uint32_t)d.log_f) == 0u) {
-                double sum[DPD_NACC];
-                for (int k = 0; k < DPD_NACC; k++) sum[k] = 0.0;
+                double sum[DPD_NACC_THERMO];
+                for (int k = 0; k < DPD_NACC_THERMO; k++) sum[k] = 0.0;
                 double* base = a.acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC;
                 for (int sl = 0; sl < DPD_ACC_SLOTS; sl++)
-                    for (int k = 0; k < DPD_NACC; k++) {
+                    for (int k = 0; k < DPD_NACC_THERMO; k++) {
                         sum[k] += base[sl * DPD_NACC + k];
                         base[sl * DPD_NACC + k] = 0.0;
                     }

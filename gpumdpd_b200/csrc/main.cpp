@@ -32,7 +32,7 @@ int main(int argc, char** argv)
     // run, thermo and write_data settings are re-read from the text
     unsigned nsteps = 0;
     int atom_style = 0;
-    std::string out_data;
+    std::string out_data, spring_file;
     std::istringstream ls(text);
     std::string line;
     while (std::getline(ls, line)) {
@@ -44,6 +44,12 @@ int main(int argc, char** argv)
         if (k == "run") t >> nsteps;
         if (k == "atom_style") { t >> a; atom_style = a == "atomic" ? 0 : (a == "bond" ? 1 : 2); }
         if (k == "write_data") t >> out_data;
+        if (k == "fix") {
+            // fix ID groupID spring k x y z r0 [file_name file_frequency]
+            std::vector<std::string> w;
+            while (t >> a) w.push_back(a);
+            if (w.size() == 10 && w[2] == "spring") spring_file = w[8];
+        }
     }
     e = dpd_run(eng, nsteps);
     if (e) {
@@ -80,6 +86,23 @@ int main(int argc, char** argv)
                     r.p[3], r.p[4], r.p[5]);
     }
     fclose(th);
+    if (!spring_file.empty()) {
+        // src/fix/fix_spring.cu:118-128 (header) and 340-360 (rows)
+        std::vector<double> sr(6 * 2048);
+        int ns = 0;
+        dpd_get_spring_records(eng, sr.data(), 2048, &ns);
+        FILE* sf = fopen(spring_file.c_str(), "w");
+        if (sf) {
+            fprintf(sf, "%15s\t\t%15s\t\t%15s\t\t%15s\t\t%15s\t\t%15s\n", "step", "spring_force_x", "spring_force_y",
+                    "spring_force_z", "spring_force", "spring_erergy");
+            for (int k = 0; k < ns; k++) {
+                const double* r = &sr[6 * (size_t)k];
+                fprintf(sf, "%15lld\t\t%15g\t\t%15g\t\t%15g\t\t%15g\t\t%15g\n", (long long)r[0], r[1], r[2], r[3],
+                        r[4], r[5]);
+            }
+            fclose(sf);
+        }
+    }
     if (!out_data.empty()) dpd_write_data(eng, out_data.c_str());
     int64_t natoms = 0;
     dpd_get_info(eng, nullptr, nullptr, &natoms, nullptr);

@@ -82,6 +82,15 @@ class Engine:
         _check(self.lib.dpd_get_thermo(self.h, rows, max_rows, ctypes.byref(n)), self.lib, self.h)
         return _rows_to_dict(rows, n.value)
 
+    def spring_records(self, max_rows=2048):
+        """Rows {step, Fx, Fy, Fz, +-|F|, energy} of a `fix spring` with a record file
+        (an (n, 6) array; empty without one)."""
+        rows = np.empty((max_rows, 6))
+        n = ctypes.c_int()
+        _check(self.lib.dpd_get_spring_records(self.h, capi.ptr(rows), max_rows, ctypes.byref(n)),
+               self.lib, self.h)
+        return rows[: n.value]
+
     def state(self, forces=True, images=True):
         n = self.n_atoms
         x = np.empty((n, 3))

@@ -249,7 +249,38 @@ def binary_mixture(L, a_ab, rho=3.0, seed=0, a_same=25.0, gamma=4.5, kT=1.0, dt=
     return System([0, 0, 0], [L, L, L], [1.0, 1.0], types, x, v, run_in=run)
 
 
-def replica_sweep(n_rep=256, L_min=8.0, L_max=24.0, a_lo=25.0, a_hi=45.0, seed=99, nsteps=5000,
+def probe_fixes(L=9.0, rho=3.0, seed=23, radius=1.5, probe_mass=2.0, spring_k=50.0, spring_r0=0.2,
+                spring_file=("spring.txt", 2), rvcm=(3, 1, 0, 1), recenter_every=4, kT=1.0, dt=0.04,
+                nsteps=1000, skin=0.3, thermo=100, a_same=25.0, a_ab=30.0, gamma=4.5,
+                data="system.data", max_rho=10.0):
+    """Solvent (type 1) around a spherical probe cluster (type 2, mass `probe_mass`) with the
+    group fixes: a spring pulling the probe's centre of mass towards a point one unit
+    from the box centre (to within spring_r0), rvcm on everything (every rvcm[0] steps,
+    flags rvcm[1:]), and recenter of the probe to the box centre every `recenter_every`
+    steps.  The probe starts one unit on the other side of the centre."""
+    rng = np.random.default_rng(seed)
+    n = int(round(rho * L ** 3))
+    x = rng.uniform(0.0, L, size=(n, 3))
+    centre = np.full(3, L / 2.0)
+    probe_at = centre - np.array([1.0, 0.0, 0.0])
+    types = np.where(np.linalg.norm(x - probe_at, axis=1) < radius, 2, 1).astype(np.int32)
+    masses = [1.0, float(probe_mass)]
+    v = _velocities(rng, n, kT, np.where(types == 2, probe_mass, 1.0))
+    sx, sy, sz = centre + np.array([1.0, 0.0, 0.0])
+    spring = f"spring {spring_k} {sx} {sy} {sz} {spring_r0}"
+    if spring_file:
+        spring += f" {spring_file[0]} {spring_file[1]}"
+    fixes = (("md", "all", "nve"), ("spr", "probe", spring),
+             ("rv", "all", "rvcm " + " ".join(str(q) for q in rvcm)),
+             ("rc", "probe", f"recenter {recenter_every} {centre[0]} {centre[1]} {centre[2]}"))
+    run = run_in_text(skin=skin, dt=dt, thermo=thermo, run=nsteps, data=data, temp=kT,
+                      seed=(seed * 104729 + 3) % 1000003, max_rho=max_rho,
+                      coeffs=[(1, 1, a_same, gamma), (1, 2, a_ab, gamma), (2, 2, a_same, gamma)],
+                      groups=(("all", (1, 2)), ("probe", (2,))), fixes=fixes)
+    return System([0, 0, 0], [L, L, L], masses, types, x, v, run_in=run)
+
+
+def replica_sweep(n_rep=256,L_min=8.0, L_max=24.0, a_lo=25.0, a_hi=45.0, seed=99, nsteps=5000,
                   rdf=(3.0, 150, 100), skin=0.3, thermo=100):
     """Uneven replicas: a_AB uniformly spaced over [a_lo, a_hi]; L drawn log-uniform."""
     rng = np.random.default_rng(seed)

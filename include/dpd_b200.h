@@ -115,6 +115,12 @@ int dpd_sync(dpd_engine* eng);
  * Copies up to max_rows of the most recent rows; *n_rows receives the number copied. */
 int dpd_get_thermo(dpd_engine* eng, dpd_thermo* rows, int max_rows, int* n_rows);
 
+/* Records of `fix ... spring k x y z r0 file freq` (src/fix/fix_spring.cu:340-360, the
+ * rows it writes to its file): 6 doubles per row {step, Fx, Fy, Fz, +-|F|, energy}, every
+ * freq steps from the zero step on.  Copies up to max_rows of the most recent rows (the
+ * device keeps the last 2048); *n_rows = 0 without such a fix. */
+int dpd_get_spring_records(dpd_engine* eng, double* rows, int max_rows, int* n_rows);
+
 /* Current state by tag: x wrapped into the box, v, image counters, forces of the
  * last evaluated step (any pointer may be NULL). Replaces Dump/write_data reads of
  * d_pos/d_vel/d_force (src/system/dump.cu:23-201). */

@@ -257,6 +257,18 @@ typedef struct {
     int angle_style;     /* 0 none, 1 harmonic (src/force/angle_harmonic.cu) */
     int nangletypes;
     double angle_coeff[ORACLE_MAXT][2]; /* k, theta0 in degrees */
+    /* group fixes; masks are the group's types (bit type-1) */
+    int spring_on;       /* src/fix/fix_spring.cu:281-370 (post_force) */
+    uint32_t spring_mask;
+    double spring_k, spring_c[3], spring_r0;
+    int rvcm_on;         /* src/fix/fix_rvcm.cu:233-286 (end_of_step) */
+    uint32_t rvcm_mask;
+    uint32_t rvcm_freq;
+    int rvcm_flag[3];
+    int recenter_on;     /* src/fix/fix_recenter.cu:270-335 (end_of_step) */
+    uint32_t recenter_mask;
+    uint32_t recenter_freq;
+    double recenter_c[3];
 } oracle_ff;
 
 /* The angle list (type, tag_i, tag_j, tag_k per angle; j is the apex) of the next
@@ -529,6 +541,103 @@ static void thermo(int n, const int* type, const double* v, const double* L, con
 }
 
 /* ------------------------------------------------------------------------- */
+/* Group fixes.  Unwrapped positions are x + img L (the reference's uwpos).          */
+static double group_mass(int n, const int* type, const oracle_ff* ff, uint32_t mask)
+{
+    double m = 0.0;
+    for (int i = 0; i < n; i++)
+        if ((mask >> (type[i] - 1)) & 1u) m += ff->mass[type[i] - 1];
+    return m;
+}
+
+/* The record of the last spring evaluation: Fx, Fy, Fz, +-|F|, energy (the row the
+ * reference writes to the spring's file, src/fix/fix_spring.cu:340-360).              */
+static double spring_last[5];
+
+void oracle_spring_last(double* out)
+{
+    for (int k = 0; k < 5; k++) out[k] = spring_last[k];
+}
+
+/* fix spring, post_force: F = -k (r - r0) d / r with d = com - c (r = |d| > 1e-10) on the
+ * group's centre of mass, a share m_i / M to each member; not part of the virial.     */
+static void fix_spring(int n, const int* type, const double* x, const int* img, const double* L,
+                       const oracle_ff* ff, double* f)
+{
+    const uint32_t mask = ff->spring_mask;
+    const double M = group_mass(n, type, ff, mask);
+    if (!(M > 0)) return;
+    double com[3] = {0, 0, 0};
+    for (int i = 0; i < n; i++) {
+        if (!((mask >> (type[i] - 1)) & 1u)) continue;
+        const double m = ff->mass[type[i] - 1];
+        for (int d = 0; d < 3; d++) com[d] += m * (x[3 * i + d] + img[3 * i + d] * L[d]);
+    }
+    double dv[3], r2 = 0.0;
+    for (int d = 0; d < 3; d++) {
+        dv[d] = com[d] / M - ff->spring_c[d];
+        r2 += dv[d] * dv[d];
+    }
+    const double r = sqrt(r2);
+    for (int k = 0; k < 5; k++) spring_last[k] = 0.0;
+    if (!(r > 1.0e-10)) return;
+    const double dr = r - ff->spring_r0;
+    for (int d = 0; d < 3; d++) spring_last[d] = -ff->spring_k * dr * dv[d] / r;
+    spring_last[3] = sqrt(spring_last[0] * spring_last[0] + spring_last[1] * spring_last[1] +
+                          spring_last[2] * spring_last[2]) * (dr < 0.0 ? -1.0 : 1.0);
+    spring_last[4] = 0.5 * ff->spring_k * dr * dr;
+    for (int i = 0; i < n; i++) {
+        if (!((mask >> (type[i] - 1)) & 1u)) continue;
+        const double share = ff->mass[type[i] - 1] / M;
+        for (int d = 0; d < 3; d++) f[3 * i + d] += -ff->spring_k * dr * dv[d] / r * share;
+    }
+}
+
+/* fix rvcm and fix recenter, end_of_step of a step that is a multiple of their frequency. */
+static void fix_end_of_step(int n, const int* type, double* x, double* v, int* img, const double* lo,
+                            const double* L, const oracle_ff* ff, uint32_t step)
+{
+    if (ff->rvcm_on && ff->rvcm_freq && step % ff->rvcm_freq == 0) {
+        const uint32_t mask = ff->rvcm_mask;
+        const double M = group_mass(n, type, ff, mask);
+        double p[3] = {0, 0, 0};
+        for (int i = 0; i < n; i++) {
+            if (!((mask >> (type[i] - 1)) & 1u)) continue;
+            for (int d = 0; d < 3; d++) p[d] += ff->mass[type[i] - 1] * v[3 * i + d];
+        }
+        if (M > 0)
+            for (int i = 0; i < n; i++) {
+                if (!((mask >> (type[i] - 1)) & 1u)) continue;
+                for (int d = 0; d < 3; d++) v[3 * i + d] -= ff->rvcm_flag[d] * p[d] / M;
+            }
+    }
+    if (ff->recenter_on && ff->recenter_freq && step % ff->recenter_freq == 0) {
+        const uint32_t mask = ff->recenter_mask;
+        const double M = group_mass(n, type, ff, mask);
+        double com[3] = {0, 0, 0};
+        for (int i = 0; i < n; i++) {
+            if (!((mask >> (type[i] - 1)) & 1u)) continue;
+            const double m = ff->mass[type[i] - 1];
+            for (int d = 0; d < 3; d++) com[d] += m * (x[3 * i + d] + img[3 * i + d] * L[d]);
+        }
+        if (M > 0)
+            for (int i = 0; i < n; i++) {
+                if (!((mask >> (type[i] - 1)) & 1u)) continue;
+                for (int d = 0; d < 3; d++) {
+                    double q = x[3 * i + d] + (ff->recenter_c[d] - com[d] / M);
+                    const double hi = lo[d] + L[d];
+                    while (q >= hi || q < lo[d]) {
+                        const int k = (q >= hi) - (q < lo[d]);
+                        q -= L[d] * k;
+                        img[3 * i + d] += k;
+                    }
+                    x[3 * i + d] = q;
+                }
+            }
+    }
+}
+
+/* ------------------------------------------------------------------------- */
 /* Velocity-Verlet run with the reference's step order (src/main/utils.cuh:166-213
  * for step 0, :254-303 per step; src/fix/fix_nve.cu:42-86 and :131-149).
  * State in/out: x (wrapped into [lo, lo+L)), v, img (image counters, 3n ints).
@@ -552,6 +661,7 @@ int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int
         uint32_t s0 = first_step - 1;
         status |= oracle_forces(n, tag, type, x, v, lo, L, ff, s0, nbonds, bonds, f, rho_out,
                                 energy, virial);
+        if (ff->spring_on) fix_spring(n, type, x, img, L, ff, f);
         if (log_f && s0 % log_f == 0 && nlog < max_log) {
             thermo(n, type, v, L, ff, energy, virial, thermo_out + 12 * nlog);
             log_steps[nlog++] = (int)s0;
@@ -575,10 +685,12 @@ int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int
         }
         status |= oracle_forces(n, tag, type, x, v, lo, L, ff, step, nbonds, bonds, f, rho_out,
                                 energy, virial);
+        if (ff->spring_on) fix_spring(n, type, x, img, L, ff, f);
         for (int i = 0; i < n; i++) {
             double dtm = 0.5 * dt / ff->mass[type[i] - 1];
             for (int d = 0; d < 3; d++) v[3 * i + d] += dtm * f[3 * i + d];
         }
+        fix_end_of_step(n, type, x, v, img, lo, L, ff, step);
         if (log_f && step % log_f == 0 && nlog < max_log) {
             thermo(n, type, v, L, ff, energy, virial, thermo_out + 12 * nlog);
             log_steps[nlog++] = (int)step;

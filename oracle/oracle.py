@@ -23,6 +23,12 @@ class OracleFF(ctypes.Structure):
         ("bond_coeff", (ctypes.c_double * 4) * MAXT),
         ("angle_style", ctypes.c_int), ("nangletypes", ctypes.c_int),
         ("angle_coeff", (ctypes.c_double * 2) * MAXT),
+        ("spring_on", ctypes.c_int), ("spring_mask", ctypes.c_uint32), ("spring_k", ctypes.c_double),
+        ("spring_c", ctypes.c_double * 3), ("spring_r0", ctypes.c_double),
+        ("rvcm_on", ctypes.c_int), ("rvcm_mask", ctypes.c_uint32), ("rvcm_freq", ctypes.c_uint32),
+        ("rvcm_flag", ctypes.c_int * 3),
+        ("recenter_on", ctypes.c_int), ("recenter_mask", ctypes.c_uint32), ("recenter_freq", ctypes.c_uint32),
+        ("recenter_c", ctypes.c_double * 3),
     ]
 
 
@@ -45,6 +51,8 @@ def load():
     lib.oracle_saru.argtypes = [u32, u32, u32, ctypes.c_int32]
     lib.oracle_set_saru_double_tail.restype = None
     lib.oracle_set_saru_double_tail.argtypes = [i]
+    lib.oracle_spring_last.restype = None
+    lib.oracle_spring_last.argtypes = [vp]
     lib.oracle_set_angles.restype = None
     lib.oracle_set_angles.argtypes = [i, vp]
     lib.oracle_saru_batch.restype = None
@@ -143,7 +151,31 @@ def ff_from_run_in(text, masses):
             angles[int(t[1])] = (float(t[2]), float(t[3]))
     bc = [bonds[k] for k in sorted(bonds)]
     ac = [angles[k] for k in sorted(angles)]
-    return make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc, astyle, ac)
+    ff = make_ff(style, len(masses), coeffs, kT, dt, seed, masses, bstyle, bc, astyle, ac)
+    # groups and the group fixes (spring, rvcm, recenter)
+    groups = {t[1]: [int(v) for v in t[3:]] for t in raw if t[0] == "group" and len(t) > 3}
+    def mask(g):
+        m = 0
+        for ty in groups[g]:
+            m |= 1 << (ty - 1)
+        return m
+    for t in raw:
+        if t[0] != "fix" or len(t) < 4:
+            continue
+        if t[3] == "spring":
+            ff.spring_on, ff.spring_mask, ff.spring_k = 1, mask(t[2]), float(t[4])
+            for d in range(3):
+                ff.spring_c[d] = float(t[5 + d])
+            ff.spring_r0 = float(t[8])
+        elif t[3] == "rvcm":
+            ff.rvcm_on, ff.rvcm_mask, ff.rvcm_freq = 1, mask(t[2]), int(t[4])
+            for d in range(3):
+                ff.rvcm_flag[d] = int(t[5 + d])
+        elif t[3] == "recenter":
+            ff.recenter_on, ff.recenter_mask, ff.recenter_freq = 1, mask(t[2]), int(t[4])
+            for d in range(3):
+                ff.recenter_c[d] = float(t[5 + d])
+    return ff
 
 
 def set_saru_double_tail(on):
@@ -224,6 +256,14 @@ def run(ff, tags, types, x, v, lo, L, first_step, nsteps, log_f, bonds=None, zer
     thermo = {c: th[:nlog, k] for k, c in enumerate(cols)}
     thermo["step"] = ls[:nlog]
     return {"x": x, "v": v, "image": img, "f": f, "rho": rho, "thermo": thermo}
+
+
+def spring_last():
+    """{Fx, Fy, Fz, +-|F|, energy} of the last spring evaluation of `run`/`forces`."""
+    lib = load()
+    out = np.zeros(5)
+    lib.oracle_spring_last(_p(out))
+    return out
 
 
 def pairs_f64(tags, x, lo, L, cut):

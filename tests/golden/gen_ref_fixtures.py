@@ -75,6 +75,9 @@ def parse_thermo(path):
     return {h: data[:, q] for q, h in enumerate(head)}
 
 
+KEEP_FRAMES = {"probe_fixes": (0, 1, 3, 4, 10)}  # steps after an rvcm (3) and a recenter (4)
+
+
 def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
     run = system.run_in
     lines = [ln for ln in run.splitlines() if not ln.startswith(("run ", "thermo ", "read_data "))]
@@ -89,6 +92,8 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
             raise RuntimeError(f"{name}: reference failed\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
         frames = parse_trj(os.path.join(td, "all.trj"))
         thermo = parse_thermo(os.path.join(td, "thermo.txt"))
+        spring = os.path.join(td, "spring.txt")  # fix spring's record file, when it has one
+        spring = np.loadtxt(spring, skiprows=1, ndmin=2) if os.path.exists(spring) else None
     save = {"run_in": np.array("\n".join(lines)), "masses": system.masses, "lo": system.lo,
             "hi": system.hi}
     if system.bonds is not None:
@@ -96,7 +101,7 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
     if system.angles is not None:
         save["angles"] = system.angles
     for step in sorted(frames):
-        if step not in (0, 1, nsteps):
+        if step not in KEEP_FRAMES.get(name, (0, 1, nsteps)):
             continue
         fr = frames[step]
         order = np.argsort(fr["id"])
@@ -106,6 +111,8 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
         save[f"s{step}_type"] = fr["type"][order].astype(np.int32)
     for h, col in thermo.items():
         save[f"thermo_{h}"] = col
+    if spring is not None:
+        save["spring"] = spring
     np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), **save)
 
 
@@ -124,6 +131,9 @@ def systems():
     out["mix_rc"] = mix
     # harmonic angles on every consecutive triple of A5B5 chains (atom_style angle)
     out["angle_chains"] = inputs.angle_chains(L=8.0, seed=19, nsteps=10, angle_k=3.0, theta0=120.0)
+    # group fixes: spring on a probe cluster (record file every 2 steps), rvcm on all every
+    # 3 steps (x and z), recenter of the probe every 4 steps
+    out["probe_fixes"] = inputs.probe_fixes(L=9.0, seed=23, nsteps=10)
     return out
 
 

@@ -172,3 +172,32 @@ def test_inputs_generators():
     reps = inputs.replica_sweep(n_rep=8, nsteps=10)
     ns = [r.n for r in reps]
     assert min(ns) >= 3 * 8 ** 3 * 0.99 and max(ns) <= 3 * 24 ** 3 * 1.01
+
+
+def test_group_fix_checks():
+    """fix spring / rvcm / recenter parameters (validateParams of src/fix/fix_spring.cu:17-52,
+    fix_rvcm.cu:17-40, fix_recenter.cu:17-32) and the in-box checks of their preprocess."""
+    from gpumdpd_b200 import inputs
+    s = inputs.probe_fixes(L=6.0, seed=2, radius=1.0)
+    code, err = _create(s.run_in, s)
+    assert code in (0, -8), err
+    t = s.run_in
+    spring = [ln for ln in t.splitlines() if " spring " in ln][0]
+    rvcm = [ln for ln in t.splitlines() if " rvcm " in ln][0]
+    rec = [ln for ln in t.splitlines() if " recenter " in ln][0]
+    cases = [
+        (t.replace(spring, spring.rsplit(" ", 3)[0]), "illegal fix_spring command"),
+        (t.replace(spring, spring.replace("spring 50.0 4.0", "spring 50.0 9.5")), "out of the box in x"),
+        (t.replace(spring, spring.replace(" spring.txt 2", " spring.txt 0")), "illegal fix_spring command"),
+        (t.replace(rvcm, rvcm + " 1"), "illegal fix_rvcm command"),
+        (t.replace(rvcm, rvcm.replace("rvcm 3 1 0 1", "rvcm 3 2 0 1")), "illegal fix_rvcm command"),
+        (t.replace(rvcm, rvcm.replace("rvcm 3", "rvcm 0")), "illegal fix_rvcm command"),
+        (t.replace(rec, rec.replace("recenter 4 3.0 3.0 3.0", "recenter 4 3.0 3.0 7.0")), "out of the box in z"),
+        (t.replace(rec, rec.replace("recenter 4", "recenter x")), "illegal fix_recenter command"),
+        (t.replace(rec, rec.replace(" probe ", " nogroup ")), "Group 'nogroup' not found"),
+        (t + "fix spr2 probe spring 1.0 3.0 3.0 3.0 0.0\n", "at most one fix spring"),
+    ]
+    for text, msg in cases:
+        assert text != t
+        code, err = _create(text, s)
+        assert code == -1 and msg in err, (msg, err)

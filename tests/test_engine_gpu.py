@@ -265,3 +265,79 @@ def test_restart_continues_step_counter():
     d -= L * np.round(d / L)
     assert np.abs(d).max() < 1e-4
     assert list(b.thermo()["step"]) == list(range(21))
+
+
+def test_group_fixes_vs_reference_and_oracle(oracle_mod):
+    """fix spring / rvcm / recenter on the GPU against the reference's own run and the
+    oracle: states after steps 1, 3 (rvcm), 4 (recenter) and 10, both with the run split
+    at those steps (the fixes then act on the last step of a run and the next run starts
+    from the spring-carrying forces) and as one 10-step run; the spring's records."""
+    s, g = _golden_system("probe_fixes")
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    tags = np.arange(1, s.n + 1)
+    e = _engine_from(s)
+    L = _box(e)
+    e.run(0)
+    st = e.state()
+    f_ref = np.column_stack([g["s0_f" + c] for c in "xyz"])
+    assert force_err(st["f"], f_ref) < FORCE_TOL
+    x0 = np.column_stack([g["s0_" + c] for c in "xyz"])
+    v0 = np.column_stack([g["s0_v" + c] for c in "xyz"])
+    done = 0
+    for steps in (1, 3, 4, 10):
+        e.run(steps - done)
+        done = steps
+        got = e.state()
+        xr = np.column_stack([g[f"s{steps}_" + c] for c in "xyz"])
+        vr = np.column_stack([g[f"s{steps}_v" + c] for c in "xyz"])
+        fr = np.column_stack([g[f"s{steps}_f" + c] for c in "xyz"])
+        o = oracle_mod.run(ff, tags, s.types, x0, v0, s.lo, L, 1, steps, 1)
+        for xw, vw, fw in ((xr, vr, fr), (o["x"], o["v"], o["f"])):
+            dx = got["x"] - xw
+            dx -= L * np.round(dx / L)
+            assert np.abs(dx).max() < (2e-6 if steps == 1 else 5e-5), steps
+            assert np.abs(got["v"] - vw).max() < (2e-5 if steps == 1 else 5e-4), steps
+            assert force_err(got["f"], fw) < (2e-5 if steps == 1 else 3e-4), steps
+        if steps == 3:
+            p = (s.masses[s.types - 1][:, None] * got["v"]).sum(0)
+            assert abs(p[0]) < 1e-3 and abs(p[2]) < 1e-3
+    th = e.thermo()
+    np.testing.assert_allclose(th["temp"], g["thermo_temp"], rtol=1e-4, atol=1e-5)
+    np.testing.assert_allclose(th["pressure"], g["thermo_pressure"], rtol=2e-4, atol=2e-4)
+    rec = e.spring_records()
+    ref = g["spring"]
+    assert rec.shape == ref.shape
+    np.testing.assert_array_equal(rec[:, 0], ref[:, 0])
+    np.testing.assert_allclose(rec[:, 1:], ref[:, 1:], rtol=2e-4, atol=2e-4 * np.abs(ref[:, 1:5]).max())
+    # one uninterrupted run: the end-of-step fixes inside the captured step
+    e2 = _engine_from(s)
+    e2.run(10)
+    a, b = e2.state(), e.state()
+    dx = a["x"] - b["x"]
+    dx -= L * np.round(dx / L)
+    assert np.abs(dx).max() < 5e-5
+    assert np.abs(a["v"] - b["v"]).max() < 5e-4
+
+
+def test_group_fixes_in_a_batch(oracle_mod):
+    """A replica with the group fixes packed beside replicas without: each matches its
+    own single-engine run (the fixes act on their replica only)."""
+    from gpumdpd_b200 import Batch, inputs
+    systems = [inputs.binary_mixture(6.0, 30.0, seed=31, nsteps=10, thermo=1),
+               inputs.probe_fixes(L=9.0, seed=29, nsteps=10, thermo=1, spring_file=None),
+               inputs.plain_dpd(L=7.0, seed=32, nsteps=10, thermo=1)]
+    b = Batch([s.run_in for s in systems], [s.c_system() for s in systems])
+    b.run(6)
+    for r, s in enumerate(systems):
+        e = _engine_from(s)
+        e.run(6)
+        a, c = b.state(r), e.state()
+        L = _box(e)
+        dx = a["x"] - c["x"]
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < 1e-4, r
+        assert np.abs(a["v"] - c["v"]).max() < 1e-3, r
+    # the probe replica's rvcm (steps 3 and 6, flags x and z) left no x/z momentum
+    s = systems[1]
+    p = (s.masses[s.types - 1][:, None] * b.state(1)["v"]).sum(0)
+    assert abs(p[0]) < 1e-3 and abs(p[2]) < 1e-3

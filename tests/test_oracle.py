@@ -158,3 +158,45 @@ def test_oracle_pairs_f32_vs_f64(oracle_mod):
         d = xe[a - 1] - xe[b - 1]
         d -= Le * np.round(d / Le)
         assert abs(np.linalg.norm(d) - float(np.float32(cut))) < 1e-5
+
+
+def test_group_fixes_match_reference(oracle_mod):
+    """fix spring (post_force, the zero step included), rvcm and recenter (end_of_step)
+    over 10 steps from the reference's step-0 state: states after step 1, 3 (rvcm),
+    4 (recenter) and 10, and the rows of the spring's record file (every 2 steps)."""
+    g = load_golden("probe_fixes")
+    x, v, f0, ids, types = _state(g, 0)
+    ff = oracle_mod.ff_from_run_in(str(g["run_in"]), g["masses"])
+    assert ff.spring_on and ff.rvcm_on and ff.recenter_on
+    L = g["hi"] - g["lo"]
+    m = g["masses"][types - 1]
+    o0 = oracle_mod.forces(ff, ids, types, x, v, g["lo"], L, 0)
+    # the dumped step-0 force includes the spring's share
+    assert force_err(o0["f"], f0) > 1e-4
+    z = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, 0, 1)
+    assert force_err(z["f"], f0) < 1e-5
+    for steps in (1, 3, 4, 10):
+        o = oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, steps, 1)
+        xr, vr, fr, _, _ = _state(g, steps)
+        dx = o["x"] - xr
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < (2e-6 if steps == 1 else 5e-5), steps
+        assert np.abs(o["v"] - vr).max() < (2e-5 if steps == 1 else 5e-4), steps
+        assert force_err(o["f"], fr) < (2e-5 if steps == 1 else 3e-4), steps
+        if steps == 3:  # rvcm with flags 1 0 1 at step 3: no x or z momentum left
+            p_ref = (m[:, None] * vr).sum(0)
+            p_o = (m[:, None] * o["v"]).sum(0)
+            assert abs(p_ref[0]) < 1e-3 and abs(p_ref[2]) < 1e-3 and abs(p_ref[1]) > 1e-2
+            assert abs(p_o[0]) < 1e-9 and abs(p_o[2]) < 1e-9
+        if steps == 4:  # recenter at step 4: the probe's centre of mass is at the target
+            grp = types == 2
+            com = (m[grp, None] * (o["x"] + o["image"] * L)[grp]).sum(0) / m[grp].sum()
+            np.testing.assert_allclose(com, list(ff.recenter_c), atol=1e-9)
+    rows = g["spring"]
+    assert list(rows[:, 0]) == [0, 2, 4, 6, 8, 10]
+    for row in rows:
+        # the spring of step s acts before that step's end_of_step fixes (a recenter at
+        # step 4 or 8 comes after the record)
+        oracle_mod.run(ff, ids, types, x, v, g["lo"], L, 1, int(row[0]), 1)
+        want = oracle_mod.spring_last()
+        np.testing.assert_allclose(row[1:], want, rtol=2e-4, atol=2e-4 * np.abs(want[:4]).max())
