@@ -111,6 +111,29 @@ int dpd_get_thermo(dpd_engine* h, dpd_thermo* rows, int max_rows, int* n_rows)
     return h->eng.get_thermo(0, rows, max_rows, n_rows);
 }
 
+int dpd_dump_open(dpd_engine* h, const char* path, int64_t start, int64_t every, int flags)
+{
+    ENG_CHECK(h);
+    if (!path) return DPD_E_ARG;
+    const dpd::RunInput& in = h->eng.rep(0).in;
+    if (every <= 0) {
+        if (!in.dump) {
+            h->eng.err = "no dump command in the run.in";
+            return DPD_E_ARG;
+        }
+        return h->eng.dump_open(path, in.dump_start, in.dump_f, !in.dump_wrapped, in.dump_force, in.dump_vel);
+    }
+    if (start < 0 || start > 0xFFFFFFFFll || every > 0xFFFFFFFFll) return DPD_E_ARG;
+    return h->eng.dump_open(path, (uint32_t)start, (uint32_t)every, (flags & DPD_DUMP_UNWRAPPED) != 0,
+                            (flags & DPD_DUMP_FORCE) != 0, (flags & DPD_DUMP_VEL) != 0);
+}
+
+int dpd_dump_close(dpd_engine* h)
+{
+    ENG_CHECK(h);
+    return h->eng.dump_close();
+}
+
 int dpd_get_spring_records(dpd_engine* h, double* rows, int max_rows, int* n_rows)
 {
     ENG_CHECK(h);

@@ -11,6 +11,7 @@
 #include <atomic>
 #include <thread>
 
+#include "dump.h"
 #include "engine.h"
 #include "kernels.cuh"
 #include "kernels_aos.cuh"
@@ -47,6 +48,7 @@ int Engine::dalloc(T** p, size_t n)
 
 Engine::~Engine()
 {
+    dump_close();
     if (graph_) cudaGraphExecDestroy(graph_);
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : allocs_) cudaFreeAsync(p, stream_);
@@ -423,19 +425,6 @@ int Engine::alloc_and_upload()
     return DPD_OK;
 }
 
-// Host loop over [0, n) split across hardware threads (state conversion of millions of
-// particles on every upload/download).
-template <class F>
-static void parallel_for(int64_t n, F fn)
-{
-    int nt = (int)std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
-    if (n < 65536) nt = 1;
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; t++) th.emplace_back([=] { fn(n * t / nt, n * (t + 1) / nt); });
-    fn(0, n / nt);
-    for (auto& x : th) x.join();
-}
-
 int Engine::staging()
 {
     if (h_pos_) return DPD_OK;
@@ -765,23 +754,33 @@ int Engine::run_async(uint32_t nsteps)
 {
     const int nrep = (int)reps_.size();
     const int g = (nrep + 255) / 256;
-    if (zero_pending_) {
-        // zero step at next_step_, then nsteps steps
-        const uint32_t target = next_step_ + nsteps;
-        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 1, 1, b_.build_flag, b_.phase);
+    // steps first..last: the zero step at next_step_ then nsteps steps, or nsteps steps.
+    // A trajectory frame needs the state at the end of its step, so a run with dumps is
+    // split into segments that end on dump steps (each later segment starts with the
+    // initial half kick and drift that the fused integrate leaves to the next step).
+    bool zero = zero_pending_;
+    const uint32_t first = next_step_;
+    const uint32_t last = zero ? next_step_ + nsteps : next_step_ - 1 + nsteps;
+    if (!zero && nsteps == 0) return DPD_OK;
+    uint32_t s = first;
+    for (;;) {
+        uint32_t end = last;
+        if (dump_) end = std::min(end, next_dump(s));
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, end, zero ? 1 : 0, zero ? 1 : 0,
+                                             b_.build_flag, b_.phase);
+        if (!zero) enqueue_integrate_initial(stream_);
         CK(cudaGetLastError());
-        for (uint32_t k = 0; k <= nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
-        next_step_ = target + 1;
-        zero_pending_ = false;
-    } else {
-        if (nsteps == 0) return DPD_OK;
-        const uint32_t target = next_step_ - 1 + nsteps;
-        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 0, 0, b_.build_flag, b_.phase);
-        enqueue_integrate_initial(stream_);
-        CK(cudaGetLastError());
-        for (uint32_t k = 0; k < nsteps; k++) CK(cudaGraphLaunch(graph_, stream_));
-        next_step_ = target + 1;
+        for (uint32_t k = s; k <= end; k++) CK(cudaGraphLaunch(graph_, stream_));
+        zero = false;
+        if (dump_ && dump_due(end)) {
+            int e = dump_frame(end);
+            if (e) return e;
+        }
+        if (end == last) break;
+        s = end + 1;
     }
+    next_step_ = last + 1;
+    zero_pending_ = false;
     return DPD_OK;
 }
 
@@ -1044,6 +1043,18 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
     const bool spring = f && b_.fixo && R.ff.spring.on && R.ff.spring.mask;
     if (spring) CK(cudaMemcpyAsync(&fo, b_.fixo + rep, sizeof(FixOut), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
+    if (!slots_to_tags(rep, pos, vel, img, frc, spring ? fo.spring_a : nullptr, x, v, image, f)) {
+        err = "corrupt tag in device state";
+        return DPD_E_STATE;
+    }
+    return DPD_OK;
+}
+
+bool Engine::slots_to_tags(int rep, const float4* pos, const float4* vel, const int4* img, const float4* frc,
+                           const float* spring_a, double* x, double* v, int* image, double* f) const
+{
+    const Replica& R = reps_[rep];
+    const RepDesc& d = R.desc;
     std::atomic<int> bad{0};
     parallel_for(d.n_real, [&](int64_t k0, int64_t k1) {
     for (int64_t k = k0; k < k1; k++) {
@@ -1054,36 +1065,31 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
             bad = 1;
             continue;
         }
+        const int t0 = tw & ((1 << DPD_TYPE_BITS) - 1);
         const size_t o = 3 * (size_t)(tag - 1);
         int code;
         memcpy(&code, &pos[k].w, 4);
         const int c[3] = {code & DPD_MAX_NC, (code >> DPD_CELL_BITS) & DPD_MAX_NC, (code >> (2 * DPD_CELL_BITS)) & DPD_MAX_NC};
-        const float off[3] = {pos[k].x, pos[k].y, pos[k].z};
-        const float vv[3] = {vel[k].x, vel[k].y, vel[k].z};
-        const float ff[3] = {frc[k].x, frc[k].y, frc[k].z};
-        const int im[3] = {img[k].x, img[k].y, img[k].z};
         for (int q = 0; q < 3; q++) {
             // exact position of the FP32 state; offsets may have drifted past the cell
             // (and the box) since the last build, so wrap into [lo, lo + L)
-            double xa = (double)c[q] * (double)d.w[q] + (double)off[q];
+            const float off = q == 0 ? pos[k].x : (q == 1 ? pos[k].y : pos[k].z);
+            double xa = (double)c[q] * (double)d.w[q] + (double)off;
             const double L = R.box_len[q];
             const double wrap = std::floor(xa / L);
             xa -= wrap * L;
             if (xa >= L) xa -= L;
             if (x) x[o + q] = d.lo[q] + xa;
-            if (v) v[o + q] = vv[q];
-            if (f) f[o + q] = ff[q];
-            if (spring && ((R.ff.spring.mask >> (tw & ((1 << DPD_TYPE_BITS) - 1))) & 1u))
-                f[o + q] += (double)fo.spring_a[q] * R.sys.masses[tw & ((1 << DPD_TYPE_BITS) - 1)];
-            if (image) image[o + q] = im[q] + (int)wrap;
+            if (v) v[o + q] = q == 0 ? vel[k].x : (q == 1 ? vel[k].y : vel[k].z);
+            if (f) {
+                f[o + q] = q == 0 ? frc[k].x : (q == 1 ? frc[k].y : frc[k].z);
+                if (spring_a && ((R.ff.spring.mask >> t0) & 1u)) f[o + q] += (double)spring_a[q] * R.sys.masses[t0];
+            }
+            if (image) image[o + q] = (q == 0 ? img[k].x : (q == 1 ? img[k].y : img[k].z)) + (int)wrap;
         }
     }
     });
-    if (bad) {
-        err = "corrupt tag in device state";
-        return DPD_E_STATE;
-    }
-    return DPD_OK;
+    return !bad;
 }
 
 int Engine::set_state(int rep, const double* x, const double* v)

@@ -2,14 +2,31 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dpd_b200.h"
 #include "dpd_common.h"
 #include "dpd_io.h"
+#include "dump.h"
 
 namespace dpd {
+
+// Host loop over [0, n) split across hardware threads (state conversion of millions of
+// particles on every upload/download).
+template <class F>
+inline void parallel_for(int64_t n, F fn)
+{
+    int nt = (int)std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    if (n < 65536) nt = 1;
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back([=] { fn(n * t / nt, n * (t + 1) / nt); });
+    fn(0, n / nt);
+    for (auto& x : th) x.join();
+}
 
 struct Replica {
     RunInput in;
@@ -78,6 +95,14 @@ public:
     int list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds);
     // spring records {step, Fx, Fy, Fz, +-|F|, energy} of a replica (newest DPD_RING_ROWS)
     int spring_records(int rep, double* rows, int max_rows, int* n_rows);
+    // trajectory frames of replica 0 in the reference's all.trj format, written by a host
+    // thread from snapshots while the device keeps stepping (dump.cu)
+    int dump_open(const std::string& path, uint32_t start, uint32_t every, bool unwrapped, bool force,
+                  bool vel);
+    int dump_close();
+    // FP32 slots of a replica (host copies) to FP64 arrays in tag order; false on a bad tag
+    bool slots_to_tags(int rep, const float4* pos, const float4* vel, const int4* img, const float4* frc,
+                       const float* spring_a, double* x, double* v, int* image, double* f) const;
     int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
                          int n, uint32_t step, float* d_force, float* d_pe, float* d_virial);
 
@@ -104,6 +129,9 @@ private:
     void enqueue_build(cudaStream_t s, bool list = true);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
+    int dump_frame(uint32_t step);
+    bool dump_due(uint32_t step) const;
+    uint32_t next_dump(uint32_t s) const;
     int cur_parity();
     int staging();
     int cuda_fail(cudaError_t e, const char* what);
@@ -131,6 +159,7 @@ private:
     bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
+    std::unique_ptr<DumpWriter> dump_;
 };
 
 int make_replica(const std::string& run_in, const std::string& data_path, const std::string& base_dir,

@@ -1,7 +1,8 @@
 // main.cpp -- gpudpd_b200: drop-in replacement of the reference executable's driver
 // (src/main/main.cu:15-72, src/main/utils.cuh:117-387).  Reads ./run.in, runs the
 // timestep on the GPU through libdpd_b200.so, writes thermo.txt with the reference's
-// columns (src/compute/thermo.cu:39-62,122-214) and the data file of write_data.
+// columns (src/compute/thermo.cu:39-62,122-214), the data file of write_data, the
+// all.trj frames of dump (src/system/dump.cu) and the record file of fix spring.
 #include <chrono>
 #include <cstdio>
 #include <fstream>
@@ -33,6 +34,7 @@ int main(int argc, char** argv)
     unsigned nsteps = 0;
     int atom_style = 0;
     std::string out_data, spring_file;
+    bool dump = false;
     std::istringstream ls(text);
     std::string line;
     while (std::getline(ls, line)) {
@@ -44,6 +46,7 @@ int main(int argc, char** argv)
         if (k == "run") t >> nsteps;
         if (k == "atom_style") { t >> a; atom_style = a == "atomic" ? 0 : (a == "bond" ? 1 : 2); }
         if (k == "write_data") t >> out_data;
+        if (k == "dump") dump = true;
         if (k == "fix") {
             // fix ID groupID spring k x y z r0 [file_name file_frequency]
             std::vector<std::string> w;
@@ -51,7 +54,14 @@ int main(int argc, char** argv)
             if (w.size() == 10 && w[2] == "spring") spring_file = w[8];
         }
     }
+    // trajectory frames to all.trj with the run.in's dump settings (src/system/dump.cu:5-8)
+    if (dump && dpd_dump_open(eng, "all.trj", 0, 0, 0)) {
+        fprintf(stderr, "ERROR: %s\n", dpd_last_error(eng));
+        dpd_destroy(eng);
+        return 1;
+    }
     e = dpd_run(eng, nsteps);
+    if (!e && dump) e = dpd_dump_close(eng);
     if (e) {
         fprintf(stderr, "ERROR: %s\n", dpd_last_error(eng));
         dpd_destroy(eng);

@@ -82,6 +82,15 @@ class Engine:
         _check(self.lib.dpd_get_thermo(self.h, rows, max_rows, ctypes.byref(n)), self.lib, self.h)
         return _rows_to_dict(rows, n.value)
 
+    def dump_open(self, path, start=0, every=0, unwrapped=False, force=False, vel=False):
+        """Write trajectory frames (the reference's all.trj format) to `path` during later
+        runs; every=0 takes the settings of the run.in's dump command."""
+        flags = (1 if unwrapped else 0) | (2 if force else 0) | (4 if vel else 0)
+        _check(self.lib.dpd_dump_open(self.h, str(path).encode(), int(start), int(every), flags), self.lib, self.h)
+
+    def dump_close(self):
+        _check(self.lib.dpd_dump_close(self.h), self.lib, self.h)
+
     def spring_records(self, max_rows=2048):
         """Rows {step, Fx, Fy, Fz, +-|F|, energy} of a `fix spring` with a record file
         (an (n, 6) array; empty without one)."""

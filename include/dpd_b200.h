@@ -115,6 +115,21 @@ int dpd_sync(dpd_engine* eng);
  * Copies up to max_rows of the most recent rows; *n_rows receives the number copied. */
 int dpd_get_thermo(dpd_engine* eng, dpd_thermo* rows, int max_rows, int* n_rows);
 
+/* Trajectory frames in the reference's all.trj format (Dump::dump, src/system/dump.cu:23-201):
+ * `ITEM:` headers, then `id type x y z [fx fy fz] [vx vy vz]` per atom in tag order with
+ * nine decimals, at step 0 when start is 0 and at every step >= start with
+ * (step - start) % every == 0 (src/main/utils.cuh:198-202,293-297).  every <= 0 takes
+ * start, frequency and columns from the run.in's `dump` command (DPD_E_ARG without one).
+ * flags: DPD_DUMP_UNWRAPPED (image-unwrapped positions), DPD_DUMP_FORCE, DPD_DUMP_VEL.
+ * Frames are snapshotted on the device and written by a host thread while the run goes
+ * on; dpd_dump_close (or dpd_destroy) waits for the last frame.  Velocities are written
+ * whenever DPD_DUMP_VEL is set (the reference's dump refreshes them only with forces). */
+#define DPD_DUMP_UNWRAPPED 1
+#define DPD_DUMP_FORCE 2
+#define DPD_DUMP_VEL 4
+int dpd_dump_open(dpd_engine* eng, const char* path, int64_t start, int64_t every, int flags);
+int dpd_dump_close(dpd_engine* eng);
+
 /* Records of `fix ... spring k x y z r0 file freq` (src/fix/fix_spring.cu:340-360, the
  * rows it writes to its file): 6 doubles per row {step, Fx, Fy, Fz, +-|F|, energy}, every
  * freq steps from the zero step on.  Copies up to max_rows of the most recent rows (the

@@ -1,0 +1,154 @@
+"""The gpudpd_b200 executable against the reference's own executable on the same run.in and
+data file: thermo.txt, the all.trj frames of a `dump` command, the record file of a
+`fix spring` and the data file of `write_data`.
+
+Stated tolerances: step-0 values agree to the reference's FP32 precision (positions 1e-6,
+forces 1e-5 of the RMS force, thermo 2e-5 relative); later frames within the FP32
+trajectory tolerances of the 10-step parity tests (positions 5e-5 after 10 steps)."""
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "gpumdpd_b200", "gpudpd_b200")
+STOCK = os.path.join(ROOT, "oracle", "_ref", "gpudpd_single")
+
+
+def parse_trj(path):
+    frames = {}
+    lines = open(path).read().splitlines()
+    k = 0
+    while k < len(lines):
+        assert lines[k] == "ITEM: TIMESTEP"
+        step = int(lines[k + 1])
+        assert lines[k + 2] == "ITEM: NUMBER OF ATOMS"
+        n = int(lines[k + 3])
+        assert lines[k + 4] == "ITEM: BOX BOUNDS pp pp pp"
+        box = np.array([[float(v) for v in lines[k + 5 + q].split()] for q in range(3)])
+        cols = lines[k + 8].split()[2:]
+        data = np.array([[float(v) for v in ln.split()] for ln in lines[k + 9: k + 9 + n]])
+        frames[step] = {"box": box, "cols": cols, **{c: data[:, q] for q, c in enumerate(cols)}}
+        k += 9 + n
+    return frames
+
+
+def _run(binary, system, run_in, files):
+    with tempfile.TemporaryDirectory() as td:
+        open(os.path.join(td, "run.in"), "w").write(run_in)
+        system.write_data(os.path.join(td, "system.data"))
+        p = subprocess.run([binary], cwd=td, capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+        return {f: open(os.path.join(td, f)).read() for f in files if os.path.exists(os.path.join(td, f))}
+
+
+def _thermo(text):
+    lines = [ln for ln in text.split("\n") if ln.strip()]
+    head = lines[0].split()
+    rows = np.array([[float(v) for v in ln.split()] for ln in lines[1:]])
+    return head, {k: rows[:, i] for i, k in enumerate(head)}
+
+
+def _case(wrapped):
+    from gpumdpd_b200 import inputs
+    s = inputs.probe_fixes(L=9.0, seed=41, nsteps=10, thermo=1)
+    run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in)
+    run_in += f"dump 0 5 {'wrapped' if wrapped else 'unwrapped'} force_yes vel_yes\nwrite_data out.data\n"
+    return s, run_in
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="gpudpd_b200 not built")
+@pytest.mark.parametrize("wrapped", [True, False])
+def test_cli_outputs_match_reference_executable(wrapped):
+    s, run_in = _case(wrapped)
+    files = ["thermo.txt", "all.trj", "spring.txt", "out.data"]
+    ours = _run(CLI, s, run_in, files)
+    assert set(ours) == set(files)
+    fr = parse_trj_text(ours["all.trj"])
+    assert sorted(fr) == [0, 5, 10]
+    for st, f in fr.items():
+        assert f["cols"] == ["id", "type", "x", "y", "z", "fx", "fy", "fz", "vx", "vy", "vz"]
+        np.testing.assert_array_equal(f["id"], np.arange(1, s.n + 1))
+        np.testing.assert_array_equal(f["type"], s.types)
+        np.testing.assert_allclose(f["box"], np.column_stack([s.lo, s.hi]))
+    x0 = np.column_stack([fr[0][c] for c in "xyz"])
+    np.testing.assert_allclose(x0, s.x, atol=2e-6)
+    head, th = _thermo(ours["thermo.txt"])
+    assert list(th["step"]) == list(range(11))
+    spring = np.loadtxt(ours["spring.txt"].splitlines()[1:], ndmin=2)
+    assert list(spring[:, 0]) == [0, 2, 4, 6, 8, 10]
+    assert "Atoms" in ours["out.data"] and "Velocities" in ours["out.data"]
+    if not os.path.exists(STOCK):
+        pytest.skip("reference build (oracle/build_ref.sh SINGLE) not present")
+    ref = _run(STOCK, s, run_in, files)
+    rhead, rth = _thermo(ref["thermo.txt"])
+    assert head == rhead
+    for k in ("temp", "pair_pe", "pressure"):
+        assert th[k][0] == pytest.approx(rth[k][0], rel=2e-5, abs=2e-6)
+        np.testing.assert_allclose(th[k], rth[k], rtol=2e-3, atol=2e-3)
+    rfr = parse_trj_text(ref["all.trj"])
+    assert sorted(rfr) == sorted(fr)
+    for st in fr:
+        assert rfr[st]["cols"] == fr[st]["cols"]
+        d = np.column_stack([fr[st][c] - rfr[st][c] for c in "xyz"])
+        if wrapped:
+            d -= (s.hi - s.lo) * np.round(d / (s.hi - s.lo))
+        assert np.abs(d).max() < (2e-6 if st == 0 else 5e-5), st
+        f = np.column_stack([fr[st]["f" + c] for c in "xyz"])
+        rf = np.column_stack([rfr[st]["f" + c] for c in "xyz"])
+        rms = np.sqrt((rf ** 2).sum(1).mean())
+        assert np.linalg.norm(f - rf, axis=1).max() / rms < (1e-5 if st == 0 else 3e-4), st
+        v = np.column_stack([fr[st]["v" + c] for c in "xyz"])
+        rv = np.column_stack([rfr[st]["v" + c] for c in "xyz"])
+        assert np.abs(v - rv).max() < (1e-6 if st == 0 else 5e-4), st
+    rspring = np.loadtxt(ref["spring.txt"].splitlines()[1:], ndmin=2)
+    np.testing.assert_array_equal(spring[:, 0], rspring[:, 0])
+    np.testing.assert_allclose(spring[:, 1:], rspring[:, 1:], rtol=2e-4, atol=2e-4 * np.abs(rspring[:, 1:5]).max())
+
+
+def parse_trj_text(text):
+    with tempfile.NamedTemporaryFile("w", suffix=".trj", delete=False) as f:
+        f.write(text)
+    try:
+        return parse_trj(f.name)
+    finally:
+        os.unlink(f.name)
+
+
+def test_engine_dump_frames_match_states(tmp_path):
+    """Frames written during one run (snapshots taken while the device keeps stepping)
+    equal the states of the same steps read between split runs, and the dump does not
+    change the trajectory."""
+    from gpumdpd_b200 import Engine, inputs
+    s = inputs.binary_mixture(8.0, 35.0, seed=12, nsteps=12, thermo=4)
+    path = tmp_path / "t.trj"
+    e = Engine(s.run_in, system=s.c_system())
+    e.dump_open(path, start=2, every=4, unwrapped=True, force=True, vel=True)
+    e.run(0)
+    e.run(12)
+    e.dump_close()
+    fr = parse_trj(str(path))
+    assert sorted(fr) == [2, 6, 10]
+    ref = Engine(s.run_in, system=s.c_system())
+    ref.run(0)
+    done = 0
+    L = s.hi - s.lo
+    for st in (2, 6, 10):
+        ref.run(st - done)
+        done = st
+        g = ref.state()
+        xu = g["x"] + g["image"] * L
+        x = np.column_stack([fr[st][c] for c in "xyz"])
+        assert np.abs(x - xu).max() < 1e-4, st
+        f = np.column_stack([fr[st]["f" + c] for c in "xyz"])
+        assert np.abs(f - g["f"]).max() < 1e-3 * np.abs(g["f"]).max(), st
+    ref.run(2)
+    a, b = e.state(), ref.state()
+    dx = a["x"] - b["x"]
+    dx -= L * np.round(dx / L)
+    assert np.abs(dx).max() < 1e-4
