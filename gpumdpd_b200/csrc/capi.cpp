@@ -128,6 +128,20 @@ int dpd_dump_open(dpd_engine* h, const char* path, int64_t start, int64_t every,
                             (flags & DPD_DUMP_FORCE) != 0, (flags & DPD_DUMP_VEL) != 0);
 }
 
+int dpd_write_restart(dpd_engine* h, const char* path)
+{
+    ENG_CHECK(h);
+    if (!path) return DPD_E_ARG;
+    return h->eng.write_restart(path);
+}
+
+int dpd_read_restart(dpd_engine* h, const char* path)
+{
+    ENG_CHECK(h);
+    if (!path) return DPD_E_ARG;
+    return h->eng.read_restart(path);
+}
+
 int dpd_dump_close(dpd_engine* h)
 {
     ENG_CHECK(h);

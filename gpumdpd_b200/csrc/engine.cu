@@ -766,8 +766,9 @@ int Engine::run_async(uint32_t nsteps)
     for (;;) {
         uint32_t end = last;
         if (dump_) end = std::min(end, next_dump(s));
-        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, end, zero ? 1 : 0, zero ? 1 : 0,
-                                             b_.build_flag, b_.phase);
+        k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, end, zero ? 1 : 0,
+                                             zero || force_build_ ? 1 : 0, b_.build_flag, b_.phase);
+        force_build_ = false;
         if (!zero) enqueue_integrate_initial(stream_);
         CK(cudaGetLastError());
         for (uint32_t k = s; k <= end; k++) CK(cudaGraphLaunch(graph_, stream_));

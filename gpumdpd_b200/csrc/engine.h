@@ -100,6 +100,10 @@ public:
     int dump_open(const std::string& path, uint32_t start, uint32_t every, bool unwrapped, bool force,
                   bool vel);
     int dump_close();
+    // exact checkpoint of every replica's FP32 state, forces and step counters; resume
+    // into an engine made from the same run.in and system (restart.cu)
+    int write_restart(const std::string& path);
+    int read_restart(const std::string& path);
     // FP32 slots of a replica (host copies) to FP64 arrays in tag order; false on a bad tag
     bool slots_to_tags(int rep, const float4* pos, const float4* vel, const int4* img, const float4* frc,
                        const float* spring_a, double* x, double* v, int* image, double* f) const;
@@ -146,6 +150,7 @@ private:
     bool any_mdpd_ = false, any_dpd_ = false, bonds_ = false, rdf_ = false;
     bool any_spring_ = false, any_eos_ = false;  // some replica has a spring / an rvcm or recenter
     bool zero_pending_ = true;
+    bool force_build_ = false;  // the next run starts with a list build (after a restart)
     uint32_t next_step_ = 0;
     std::vector<void*> allocs_;
     float4 *h_pos_ = nullptr, *h_vel_ = nullptr, *h_frc_ = nullptr;  // pinned staging

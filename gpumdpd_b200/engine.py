@@ -91,6 +91,14 @@ class Engine:
     def dump_close(self):
         _check(self.lib.dpd_dump_close(self.h), self.lib, self.h)
 
+    def write_restart(self, path):
+        """Exact checkpoint: FP32 state, forces of the last step, step counter, fix results."""
+        _check(self.lib.dpd_write_restart(self.h, str(path).encode()), self.lib, self.h)
+
+    def read_restart(self, path):
+        """Resume from a checkpoint of an engine made from the same run.in and system."""
+        _check(self.lib.dpd_read_restart(self.h, str(path).encode()), self.lib, self.h)
+
     def spring_records(self, max_rows=2048):
         """Rows {step, Fx, Fy, Fz, +-|F|, energy} of a `fix spring` with a record file
         (an (n, 6) array; empty without one)."""

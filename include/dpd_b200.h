@@ -130,6 +130,17 @@ int dpd_get_thermo(dpd_engine* eng, dpd_thermo* rows, int max_rows, int* n_rows)
 int dpd_dump_open(dpd_engine* eng, const char* path, int64_t start, int64_t every, int flags);
 int dpd_dump_close(dpd_engine* eng);
 
+/* Exact checkpoint and resume (new; the reference restarts from a write_data file at
+ * step 0, which replays its random-force stream, src/force/pair_dpd.cu:213).  The file
+ * holds the FP32 state as the engine keeps it (cell codes and offsets, velocities, image
+ * counters), the forces of the last evaluated step, the step counter and the fix results
+ * of every replica.  dpd_read_restart loads it into an engine created from the same run.in
+ * and system (DPD_E_ARG when atom count, types or cell grid differ); the next dpd_run
+ * continues with the following step.  Thermo rows, spring records and RDF sums restart
+ * empty. */
+int dpd_write_restart(dpd_engine* eng, const char* path);
+int dpd_read_restart(dpd_engine* eng, const char* path);
+
 /* Records of `fix ... spring k x y z r0 file freq` (src/fix/fix_spring.cu:340-360, the
  * rows it writes to its file): 6 doubles per row {step, Fx, Fy, Fz, +-|F|, energy}, every
  * freq steps from the zero step on.  Copies up to max_rows of the most recent rows (the

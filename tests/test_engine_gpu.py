@@ -341,3 +341,44 @@ def test_group_fixes_in_a_batch(oracle_mod):
     s = systems[1]
     p = (s.masses[s.types - 1][:, None] * b.state(1)["v"]).sum(0)
     assert abs(p[0]) < 1e-3 and abs(p[2]) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["probe_fixes", "diblock", "mdpd"])
+def test_restart_continues_the_run(tmp_path, name):
+    """A checkpoint after 20 steps loaded into a fresh engine gives back the same state
+    bit for bit (positions, velocities, forces with the spring's share), the step counter
+    continues (thermo rows at 25 and 30) and the next 10 steps track the uninterrupted run
+    to FP32 summation order (the random force continues at step 21, not at step 0)."""
+    from gpumdpd_b200 import DpdError, inputs
+    if name == "probe_fixes":
+        s = inputs.probe_fixes(L=9.0, seed=51, nsteps=100, thermo=5, spring_file=None)
+    elif name == "diblock":
+        s = inputs.diblock_melt(L=8.0, seed=52, nsteps=100, thermo=5)
+    else:
+        s = inputs.mdpd_slab(Lx=8.0, Ly=8.0, Lz=24.0, z0=8.0, z1=16.0, seed=53, nsteps=100, thermo=5)
+    path = tmp_path / "ck.bin"
+    a = _engine_from(s)
+    a.run(20)
+    a.write_restart(path)
+    b = _engine_from(s)
+    b.read_restart(path)
+    sa, sb = a.state(), b.state()
+    for k in ("x", "v", "f", "image"):
+        np.testing.assert_array_equal(sa[k], sb[k])
+    assert b.info()["step"] == a.info()["step"]
+    a.run(10)
+    b.run(10)
+    sa, sb = a.state(), b.state()
+    L = _box(a)
+    dx = sa["x"] - sb["x"]
+    dx -= L * np.round(dx / L)
+    assert np.abs(dx).max() < 1e-4
+    assert force_err(sb["f"], sa["f"]) < 1e-4
+    assert list(b.thermo()["step"]) == [25, 30]
+    np.testing.assert_allclose(b.thermo()["temp"], a.thermo()["temp"][-2:], rtol=1e-3)
+    # a different system is refused
+    from gpumdpd_b200 import inputs as inp
+    other = inp.plain_dpd(L=7.0, seed=3)
+    c = _engine_from(other)
+    with pytest.raises(DpdError):
+        c.read_restart(path)
