@@ -128,6 +128,13 @@ int dpd_dump_open(dpd_engine* h, const char* path, int64_t start, int64_t every,
                             (flags & DPD_DUMP_FORCE) != 0, (flags & DPD_DUMP_VEL) != 0);
 }
 
+int dpd_get_compute(dpd_engine* h, const char* id, double* rows, int max_rows, int* n_cols, int* n_rows)
+{
+    ENG_CHECK(h);
+    if (!id || !rows || max_rows < 0) return DPD_E_ARG;
+    return h->eng.compute_rows(0, id, rows, max_rows, n_cols, n_rows);
+}
+
 int dpd_write_restart(dpd_engine* h, const char* path)
 {
     ENG_CHECK(h);

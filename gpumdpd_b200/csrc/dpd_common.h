@@ -3,7 +3,7 @@
 #include <stdint.h>
 
 #define DPD_MAX_TYPES 32
-#define DPD_NACC 32          // FP64 accumulators per replica and slot
+#define DPD_NACC 48          // FP64 accumulators per replica and slot
 #define DPD_NACC_THERMO 20   // the first DPD_NACC_THERMO feed the thermo row
 #define DPD_ACC_SLOTS 32     // atomic spreading slots per replica
 #define DPD_THERMO_FIELDS 17 // doubles per logged thermo row
@@ -26,8 +26,10 @@ enum {
     // group-fix sums, consumed (and zeroed) by the fix reductions of the same step
     ACC_SPRING_COM = 20,  // 3: sum over the spring group of m x_unwrapped
     ACC_RVCM_P = 23,      // 3: sum over the rvcm group of m v
-    ACC_RECENTER_COM = 26 // 3: sum over the recenter group of m x_unwrapped
+    ACC_RECENTER_COM = 26, // 3: sum over the recenter group of m x_unwrapped
+    ACC_GC = 32            // 3 per group compute (DPD_MAX_GC of them), consumed by k_advance
 };
+#define DPD_MAX_GC 4
 
 // status bits (per replica, device)
 enum {
@@ -73,6 +75,7 @@ struct RepDesc {
     int rdf_ta, rdf_tb, rdf_nbins;
     float rdf_rmax;
     int rdf_off;    // offset into the RDF histogram array (nbins per replica)
+    int gc_n;       // group computes of this replica (table at gc[r * DPD_MAX_GC])
 };
 
 // Per-replica group fixes (src/fix/fix_spring.cu, fix_rvcm.cu, fix_recenter.cu).
@@ -85,6 +88,17 @@ struct FixDesc {
     double rvcm_m, recenter_m, recenter_c[3];
     double L[3];           // box lengths of the cell grid (unwrapped = lo + c w + o + img L)
     uint32_t spring_file_f; // spring record every this many steps (0 = none)
+};
+
+// Group computes (temp, rho, msd, tf), DPD_MAX_GC per replica (device).
+struct GCDesc {
+    int kind;         // 1 temp, 2 rho, 3 msd, 4 tf
+    uint32_t mask;    // the group's types (bit type-1)
+    uint32_t freq;
+    int ring;         // row ring of this compute (global index)
+    double norm;      // temp 1/(3 Ng - 3); rho 1/volume; msd 1/Ng
+    double region[6]; // rho: xlo xhi ylo yhi zlo zhi
+    double L[3];      // box lengths of the cell grid
 };
 
 // Per-replica results of the fix reductions of the current step (device).

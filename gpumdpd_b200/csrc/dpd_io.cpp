@@ -619,7 +619,7 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             ff.integ_mask |= bit;
         }
     }
-    // computes, src/compute/compute.cu:60-115: temp (per group) and rdf (new)
+    // computes, src/compute/compute.cu:60-115: temp, rho, msd, tf (per group) and rdf (new)
     std::set<std::string> cids;
     for (size_t k = 0; k < in.lines.size(); k++) {
         const auto& t = in.lines[k];
@@ -630,16 +630,33 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
         cids.insert(t[1]);
         if (!ff.groups.count(t[2])) return fail(err, line, "Group '" + t[2] + "' not found!");
         long long iv;
-        if (t[3] == "temp") {
-            if (t.size() != 6 || !parse_int(t[4], 1, 4294967295ll, iv))
-                return fail(err, line, "illegal compute_temp command: compute ID groupID temp frequency filename");
-            ComputeTemp c;
+        if (t[3] == "temp" || t[3] == "msd" || t[3] == "tf" || t[3] == "rho") {
+            // validateParams of src/compute/compute_temp.cu:17-30, compute_msd.cu:17-30,
+            // compute_tf.cu:17-30, compute_rho.cu:17-37; region checks of compute_rho.cu:42-75
+            const bool rho = t[3] == "rho";
+            const std::string msg = "illegal compute_" + t[3] + " command: compute ID groupID " + t[3] +
+                                    (rho ? " frequency xlo xhi ylo yhi zlo zhi filename" : " frequency filename");
+            if (t.size() != (rho ? 12u : 6u) || !parse_int(t[4], 1, 4294967295ll, iv)) return fail(err, line, msg);
+            GroupCompute c;
             c.id = t[1];
             c.group = t[2];
+            c.kind = t[3] == "temp" ? GC_TEMP : (t[3] == "msd" ? GC_MSD : (t[3] == "tf" ? GC_TF : GC_RHO));
             c.frequency = (unsigned)iv;
-            c.file = t[5];
+            c.file = t.back();
             for (int ty : ff.groups[t[2]]) c.type_mask |= 1u << (ty - 1);
-            ff.temps.push_back(c);
+            if (rho) {
+                for (int q = 0; q < 6; q++)
+                    if (!parse_double(t[5 + q], c.region[q])) return fail(err, line, msg);
+                const char* nm[3] = {"x", "y", "z"};
+                for (int d = 0; d < 3; d++) {
+                    if (c.region[2 * d] < sys.lo[d])
+                        return fail(err, line, msg + ": " + nm[d] + "lo < box." + nm[d] + "lo");
+                    if (c.region[2 * d + 1] > sys.hi[d])
+                        return fail(err, line, msg + ": " + nm[d] + "hi > box." + nm[d] + "hi");
+                }
+            }
+            if (ff.gcs.size() >= 4) return fail(err, line, "this engine takes at most 4 temp/rho/msd/tf computes");
+            ff.gcs.push_back(c);
         } else if (t[3] == "rdf") {
             // compute ID groupID rdf typeA typeB rmax nbins every filename
             ComputeRdf c;
@@ -658,7 +675,7 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             if (!ff.rdfs.empty()) return fail(err, line, "only one rdf compute is supported");
             ff.rdfs.push_back(c);
         } else {
-            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp and rdf)");
+            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp, rho, msd, tf and rdf)");
         }
     }
     return DPD_OK;

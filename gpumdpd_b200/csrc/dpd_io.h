@@ -39,10 +39,17 @@ struct SystemData {
     bool has_velocities = false;
 };
 
-struct ComputeTemp {
+// Group computes written to a file every `frequency` steps (src/compute/compute_temp.cu,
+// compute_rho.cu, compute_msd.cu, compute_tf.cu): the group's temperature, its number
+// density inside a box region, its mean squared displacement from the initial unwrapped
+// positions, and its total force.
+enum { GC_TEMP = 1, GC_RHO = 2, GC_MSD = 3, GC_TF = 4 };
+struct GroupCompute {
     std::string id, group, file;
+    int kind = GC_TEMP;
     unsigned frequency = 1;
     uint32_t type_mask = 0;
+    double region[6] = {0, 0, 0, 0, 0, 0};  // rho: xlo xhi ylo yhi zlo zhi
 };
 
 struct ComputeRdf {
@@ -90,7 +97,7 @@ struct ForceField {
     FixSpring spring;
     FixRvcm rvcm;
     FixRecenter recenter;
-    std::vector<ComputeTemp> temps;
+    std::vector<GroupCompute> gcs;
     std::vector<ComputeRdf> rdfs;
 };
 

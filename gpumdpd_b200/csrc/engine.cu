@@ -79,7 +79,7 @@ int Engine::layout()
     nmax_ = 16;
     maxb_ = 0;
     int tag_base = 0, coeff_off = 0, mass_off = 0, bond_off = 0, rdf_off = 0;
-    any_mdpd_ = any_dpd_ = bonds_ = rdf_ = false;
+    any_mdpd_ = any_dpd_ = bonds_ = rdf_ = any_gc_ = false;
     for (size_t r = 0; r < reps_.size(); r++) {
         Replica& R = reps_[r];
         RepDesc& d = R.desc;
@@ -152,6 +152,8 @@ int Engine::layout()
             d.rdf_rmax = (float)c.rmax;
             rdf_ = true;
         }
+        d.gc_n = (int)R.ff.gcs.size();
+        if (d.gc_n) any_gc_ = true;
         d.rdf_off = rdf_off;
         rdf_off += R.ff.rdfs.empty() ? 0 : R.ff.rdfs[0].nbins;
         // neighbour capacity: src/force/neigh_list.cu:14-17
@@ -413,6 +415,51 @@ int Engine::alloc_and_upload()
             CK(cudaStreamSynchronize(stream_));
         }
     }
+    // group computes: descriptors, initial unwrapped positions by global tag, row rings
+    gc_ring_base_.assign(nrep, 0);
+    if (any_gc_) {
+        std::vector<GCDesc> gd((size_t)nrep * DPD_MAX_GC);
+        memset(gd.data(), 0, sizeof(GCDesc) * gd.size());
+        std::vector<float4> uw0;
+        int ring = 0;
+        for (int r = 0; r < nrep; r++) {
+            const Replica& R = reps_[r];
+            gc_ring_base_[r] = ring;
+            for (size_t k = 0; k < R.ff.gcs.size(); k++) {
+                const GroupCompute& c = R.ff.gcs[k];
+                GCDesc& g = gd[(size_t)r * DPD_MAX_GC + k];
+                g.kind = c.kind;
+                g.mask = c.type_mask;
+                g.freq = c.frequency;
+                g.ring = ring++;
+                int64_t ng = 0;
+                for (int i = 0; i < R.sys.n_atoms; i++) ng += (c.type_mask >> (R.sys.type[i] - 1)) & 1u;
+                for (int q = 0; q < 6; q++) g.region[q] = c.region[q];
+                for (int q = 0; q < 3; q++) g.L[q] = R.box_len[q];
+                if (c.kind == GC_TEMP) g.norm = ng > 1 ? 1.0 / (3.0 * ng - 3.0) : 0.0;
+                if (c.kind == GC_MSD) g.norm = ng > 0 ? 1.0 / ng : 0.0;
+                if (c.kind == GC_RHO)
+                    g.norm = 1.0 / ((c.region[1] - c.region[0]) * (c.region[3] - c.region[2]) * (c.region[5] - c.region[4]));
+            }
+            // initial unwrapped positions: the data file's positions wrapped into the box
+            for (int i = 0; i < R.sys.n_atoms; i++) {
+                float q[3];
+                for (int k = 0; k < 3; k++) {
+                    double x = R.sys.x[3 * (size_t)i + k] - R.desc.lo[k];
+                    x -= R.box_len[k] * std::floor(x / R.box_len[k]);
+                    q[k] = (float)(R.desc.lo[k] + x);
+                }
+                uw0.push_back(make_float4(q[0], q[1], q[2], 0.0f));
+            }
+        }
+        if ((st = dalloc(&b_.gc, gd.size()))) return st;
+        if ((st = dalloc(&b_.uw0, uw0.size()))) return st;
+        if ((st = dalloc(&b_.gc_ring, (size_t)ring * DPD_RING_ROWS * 4))) return st;
+        if ((st = dalloc(&b_.gc_count, ring))) return st;
+        CK(cudaMemcpyAsync(b_.gc, gd.data(), sizeof(GCDesc) * gd.size(), cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(b_.uw0, uw0.data(), sizeof(float4) * uw0.size(), cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+    }
     std::vector<RepState> rs(nrep);
     for (auto& s : rs) {
         memset(&s, 0, sizeof(s));
@@ -596,6 +643,10 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     a.fix = b.fix;
     a.fixo = b.fixo;
     a.spring_ring = b.spring_ring;
+    a.gc = b.gc;
+    a.uw0 = b.uw0;
+    a.gc_ring = b.gc_ring;
+    a.gc_count = b.gc_count;
     return a;
 }
 
@@ -701,7 +752,7 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
         pdl_launch(k_fix_sums<1>, gp, 256, s, sa);
         pdl_launch(k_fix_reduce<1>, gr, 256, s, sa);
     }
-    if (any_spring_ || any_eos_) {
+    if (any_spring_ || any_eos_ || any_gc_) {
         pdl_launch(k_integrate_nolog<true>, gp, 256, s, sa);
         pdl_launch(k_integrate_logsteps<true>, std::min(gp, 148 * 4), 256, s, sa);
     } else {
@@ -715,7 +766,7 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
 {
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, (int)reps_.size());
     sa.mode = 1;
-    if (any_spring_ || any_eos_) k_integrate<true><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+    if (any_spring_ || any_eos_ || any_gc_) k_integrate<true><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
     else k_integrate<false><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
 }
 
@@ -930,6 +981,10 @@ int64_t Engine::estimate_bytes(const std::vector<const Replica*>& reps)
     bytes += nrep * ((int64_t)DPD_ACC_SLOTS * DPD_NACC * 8 + (int64_t)DPD_RING_ROWS * DPD_THERMO_FIELDS * 8);
     bytes += nang * 16 + (nang / 32) * 4 + nrep * 32 * 8;  // angle table, warp replicas, coefficients
     bytes += nrep * (int64_t)(sizeof(FixDesc) + sizeof(FixOut));  // group fixes (upper bound)
+    for (const Replica* R : reps)  // group computes: descriptors, x0, rows
+        if (!R->ff.gcs.empty())
+            bytes += (int64_t)sizeof(GCDesc) * DPD_MAX_GC + 16 * (int64_t)R->sys.n_atoms +
+                     (int64_t)R->ff.gcs.size() * (DPD_RING_ROWS * 32 + 4);
     for (const Replica* R : reps)
         if (R->ff.spring.on && R->ff.spring.file_freq) {
             bytes += nrep * (int64_t)DPD_RING_ROWS * 6 * 8;
@@ -986,6 +1041,35 @@ int Engine::get_thermo(int rep, dpd_thermo* rows, int max_rows, int* n_rows)
         for (int c = 0; c < 3; c++) t.momentum[c] = row[12 + c];
         t.angle_pe = row[16];
     }
+    if (n_rows) *n_rows = n;
+    return DPD_OK;
+}
+
+int Engine::compute_rows(int rep, const std::string& id, double* rows, int max_rows, int* n_cols, int* n_rows)
+{
+    if (rep < 0 || rep >= (int)reps_.size() || max_rows < 0) return DPD_E_ARG;
+    const Replica& R = reps_[rep];
+    int k = -1;
+    for (size_t q = 0; q < R.ff.gcs.size(); q++)
+        if (R.ff.gcs[q].id == id) k = (int)q;
+    if (k < 0) {
+        err = "no temp/rho/msd/tf compute with ID " + id;
+        return DPD_E_ARG;
+    }
+    const int ring = gc_ring_base_[rep] + k;
+    int count = 0;
+    CK(cudaMemcpyAsync(&count, b_.gc_count + ring, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    std::vector<double> buf((size_t)DPD_RING_ROWS * 4);
+    CK(cudaMemcpyAsync(buf.data(), b_.gc_ring + (size_t)ring * DPD_RING_ROWS * 4, sizeof(double) * buf.size(),
+                       cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const int nc = R.ff.gcs[k].kind == GC_TF ? 4 : 2;
+    const int n = std::min(std::min(count, DPD_RING_ROWS), max_rows);
+    for (int q = 0; q < n; q++) {
+        const double* src = buf.data() + 4 * (size_t)((count - n + q) % DPD_RING_ROWS);
+        for (int c = 0; c < nc; c++) rows[(size_t)q * nc + c] = src[c];
+    }
+    if (n_cols) *n_cols = nc;
     if (n_rows) *n_rows = n;
     return DPD_OK;
 }

@@ -65,6 +65,10 @@ struct DeviceBuffers {
     FixDesc* fix = nullptr;     // per replica group fixes (allocated when any replica has one)
     FixOut* fixo = nullptr;
     double* spring_ring = nullptr;  // spring records (allocated when a spring writes a file)
+    GCDesc* gc = nullptr;           // group computes (allocated when any replica has one)
+    float4* uw0 = nullptr;
+    double* gc_ring = nullptr;
+    int* gc_count = nullptr;
 };
 
 class Engine {
@@ -93,6 +97,9 @@ public:
     int write_data(int rep, const std::string& path);
     int set_tuning(const dpd_tuning* t);
     int list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds);
+    // rows {step, value} (temp, rho, msd) or {step, fx, fy, fz} (tf) of a group compute
+    // of a replica, by compute ID (newest DPD_RING_ROWS); *n_cols = 2 or 4
+    int compute_rows(int rep, const std::string& id, double* rows, int max_rows, int* n_cols, int* n_rows);
     // spring records {step, Fx, Fy, Fz, +-|F|, energy} of a replica (newest DPD_RING_ROWS)
     int spring_records(int rep, double* rows, int max_rows, int* n_rows);
     // trajectory frames of replica 0 in the reference's all.trj format, written by a host
@@ -149,6 +156,8 @@ private:
     int P_ = 0, C_ = 0, nmax_ = 16, maxb_ = 0;
     bool any_mdpd_ = false, any_dpd_ = false, bonds_ = false, rdf_ = false;
     bool any_spring_ = false, any_eos_ = false;  // some replica has a spring / an rvcm or recenter
+    bool any_gc_ = false;                         // some replica has a temp/rho/msd/tf compute
+    std::vector<int> gc_ring_base_;               // first compute ring of each replica
     bool zero_pending_ = true;
     bool force_build_ = false;  // the next run starts with a list build (after a restart)
     uint32_t next_step_ = 0;

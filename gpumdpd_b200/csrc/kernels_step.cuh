@@ -33,7 +33,21 @@ struct StepArgs {
     const FixDesc* fix;    // [nrep] group fixes (null when no replica has one)
     FixOut* fixo;          // [nrep]
     double* spring_ring;   // [nrep][DPD_RING_ROWS][6] spring records (null: none)
+    const GCDesc* gc;      // [nrep][DPD_MAX_GC] group computes (null when none)
+    const float4* uw0;     // [atoms of all replicas] initial unwrapped positions by global tag
+    double* gc_ring;       // [computes][DPD_RING_ROWS][4] rows {step, values}
+    int* gc_count;         // [computes] rows written
 };
+
+// group computes due at the current step of a replica (bit k: compute k), evaluated with
+// the end-of-step state after the thermo (src/main/utils.cuh:191-194, 290-291)
+__device__ __forceinline__ int gc_due(const StepArgs& a, const RepDesc& d, const RepState& st, int r)
+{
+    int due = 0;
+    for (int k = 0; k < d.gc_n; k++)
+        if ((st.step % a.gc[r * DPD_MAX_GC + k].freq) == 0u) due |= 1 << k;
+    return due;
+}
 
 // end-of-step fixes due at the current step of a replica: bit 0 rvcm, bit 1 recenter
 // (src/main/utils.cuh:287: Fix_end_of_step after the final half kick of steps >= 1)
@@ -651,12 +665,18 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
 // only moves the offsets.
 // LOGM: 2 = any step; 0 = every step except logged mode-0 steps (no FP64 sums: fewer
 // registers); 1 = logged mode-0 steps only.  0 and 1 together cover every slot once.
-template <int LOGM, bool FIX>
+// A step is logged when the thermo or (EXT) a group compute is due.  EXT adds the group
+// fixes and the group computes.
+template <int LOGM, bool EXT>
 __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
 {
     int r = -1;
     bool log = false;
+    int gcd = 0;
     double accv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double gv[3 * DPD_MAX_GC];
+    if (EXT && LOGM != 0)
+        for (int k = 0; k < 3 * DPD_MAX_GC; k++) gv[k] = 0.0;
     if (s < a.P) {
         // the particle's three streams are requested first (every slot < P is valid
         // memory), so their latency overlaps the replica-state reads
@@ -673,7 +693,8 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
         const bool work = active && s < d.p_end;
         const bool fin = a.mode == 0 && !st.zero_pending;
         log = a.mode == 0 && active && (st.step % (uint32_t)d.log_f) == 0u;
-        if ((LOGM == 0 && log) || (LOGM == 1 && !log)) return;  // warp-uniform
+        if (EXT && a.mode == 0 && active && d.gc_n) gcd = gc_due(a, d, st, r);
+        if ((LOGM == 0 && (log || gcd)) || (LOGM == 1 && !(log || gcd))) return;  // warp-uniform
         if (LOGM == 0) log = false;
         const bool init = a.mode == 1 ? true : st.step < st.target;
         const uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
@@ -687,7 +708,7 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
             float4 fe = f;
             int eos = 0;
             bool shifted = false;
-            if (FIX) {
+            if (EXT && a.fix) {
                 // group fixes: the spring's share m_i F / M joins the force of both half
                 // kicks (post_force); a due rvcm or recenter (end_of_step) has had its
                 // final half kick in k_fix_sums<1> and acts here before the thermo sums
@@ -732,7 +753,51 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                 accv[8] = mm * vy;
                 accv[9] = mm * vz;
             }
-            if (FIX && shifted && !(init && integ)) posp[s] = p;
+            if (EXT && LOGM != 0 && gcd) {
+                // group computes on the end-of-step state: src/compute/compute_temp.cu:74-173
+                // (kinetic energy), compute_rho.cu:109-207 (count inside the region, wrapped
+                // positions), compute_msd.cu:80-175 (|x_unwrapped - x0_unwrapped|^2),
+                // compute_tf.cu:80-181 (force, the spring's share included)
+#pragma unroll
+                for (int k = 0; k < DPD_MAX_GC; k++) {
+                    if (!((gcd >> k) & 1)) continue;
+                    const GCDesc& g = a.gc[r * DPD_MAX_GC + k];
+                    if (!((g.mask >> t0) & 1u)) continue;
+                    if (g.kind == 1) {
+                        gv[3 * k] = 0.5 * (double)m.x * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+                    } else if (g.kind == 4) {
+                        gv[3 * k] = fe.x;
+                        gv[3 * k + 1] = fe.y;
+                        gv[3 * k + 2] = fe.z;
+                    } else {
+                        const int code = __float_as_int(p.w);
+                        const float o[3] = {p.x, p.y, p.z};
+                        double xa[3];
+#pragma unroll
+                        for (int q = 0; q < 3; q++)
+                            xa[q] = (double)((code >> (q * DPD_CELL_BITS)) & DPD_MAX_NC) * (double)d.w[q] + (double)o[q];
+                        if (g.kind == 2) {
+                            bool in = true;
+#pragma unroll
+                            for (int q = 0; q < 3; q++) {
+                                double w = xa[q] - floor(xa[q] / g.L[q]) * g.L[q];
+                                if (w >= g.L[q]) w -= g.L[q];
+                                w += d.lo[q];
+                                in = in && w >= g.region[2 * q] && w < g.region[2 * q + 1];
+                            }
+                            gv[3 * k] = in ? 1.0 : 0.0;
+                        } else {
+                            const int4 im = a.buf.img[par][s];
+                            const float4 x0 = a.uw0[d.tag_base + (int)((uint32_t)__float_as_int(v.w) >> DPD_TYPE_BITS) - 1];
+                            const double dx = d.lo[0] + xa[0] + (double)im.x * g.L[0] - x0.x;
+                            const double dy = d.lo[1] + xa[1] + (double)im.y * g.L[1] - x0.y;
+                            const double dz = d.lo[2] + xa[2] + (double)im.z * g.L[2] - x0.z;
+                            gv[3 * k] = dx * dx + dy * dy + dz * dz;
+                        }
+                    }
+                }
+            }
+            if (EXT && shifted && !(init && integ)) posp[s] = p;
             if (init) {
                 if (integ) {
                     v.x = __fmaf_rn(dtm, fe.x, v.x);
@@ -772,35 +837,44 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                                 ACC_KIN + 4, ACC_KIN + 5, ACC_MOM + 0, ACC_MOM + 1, ACC_MOM + 2};
         acc_flush_warp<10>(accv, fields, r, a.acc);
     }
+    if (EXT && LOGM != 0 && gcd) {
+        int fields[3 * DPD_MAX_GC];
+#pragma unroll
+        for (int k = 0; k < 3 * DPD_MAX_GC; k++) fields[k] = ACC_GC + k;
+        acc_flush_warp<3 * DPD_MAX_GC>(gv, fields, r, a.acc);
+    }
 }
 
-template <bool FIX>
+template <bool EXT>
 __global__ void __launch_bounds__(256) k_integrate(StepArgs a)
 {
     griddep_wait();
-    integrate_slot<2, FIX>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    integrate_slot<2, EXT>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-template <bool FIX>
+template <bool EXT>
 __global__ void __launch_bounds__(256) k_integrate_nolog(StepArgs a)
 {
     griddep_wait();
-    integrate_slot<0, FIX>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    integrate_slot<0, EXT>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // logged steps: a small grid-stride launch that returns at once when no replica logs
-template <bool FIX>
+// (thermo or a group compute due)
+template <bool EXT>
 __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
 {
     griddep_wait();
     int any = 0;
     for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
         const RepState st = a.rstate[r];
-        any |= rep_active(st) && (st.step % (uint32_t)a.reps[r].log_f) == 0u;
+        if (!rep_active(st)) continue;
+        any |= (st.step % (uint32_t)a.reps[r].log_f) == 0u;
+        if (EXT && a.reps[r].gc_n) any |= gc_due(a, a.reps[r], st, r);
     }
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, FIX>(a, vb * 256 + threadIdx.x);
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, EXT>(a, vb * 256 + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1059,6 +1133,31 @@ __global__ void k_advance(StepArgs a)
                 row[15] = (double)st.status;
                 row[16] = sum[ACC_ANGLE_PE];
                 st.nlog++;
+            }
+            if (a.gc && d.gc_n) {
+                const int due = gc_due(a, d, st, r);
+                double* base = a.acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC;
+                for (int k = 0; k < d.gc_n; k++) {
+                    if (!((due >> k) & 1)) continue;
+                    const GCDesc& g = a.gc[r * DPD_MAX_GC + k];
+                    double s3[3] = {0.0, 0.0, 0.0};
+                    for (int sl = 0; sl < DPD_ACC_SLOTS; sl++)
+                        for (int q = 0; q < 3; q++) {
+                            s3[q] += base[sl * DPD_NACC + ACC_GC + 3 * k + q];
+                            base[sl * DPD_NACC + ACC_GC + 3 * k + q] = 0.0;
+                        }
+                    double* row = a.gc_ring + ((size_t)g.ring * DPD_RING_ROWS + (a.gc_count[g.ring] % DPD_RING_ROWS)) * 4;
+                    row[0] = (double)st.step;
+                    if (g.kind == 4) {
+                        row[1] = s3[0];
+                        row[2] = s3[1];
+                        row[3] = s3[2];
+                    } else {
+                        row[1] = (g.kind == 1 ? 2.0 : 1.0) * s3[0] * g.norm;
+                        row[2] = row[3] = 0.0;
+                    }
+                    a.gc_count[g.ring]++;
+                }
             }
             st.step++;
             st.zero_pending = 0;

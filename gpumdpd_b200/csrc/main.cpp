@@ -2,7 +2,8 @@
 // (src/main/main.cu:15-72, src/main/utils.cuh:117-387).  Reads ./run.in, runs the
 // timestep on the GPU through libdpd_b200.so, writes thermo.txt with the reference's
 // columns (src/compute/thermo.cu:39-62,122-214), the data file of write_data, the
-// all.trj frames of dump (src/system/dump.cu) and the record file of fix spring.
+// all.trj frames of dump (src/system/dump.cu), the record file of fix spring and the
+// files of the temp, rho, msd and tf computes.
 #include <chrono>
 #include <cstdio>
 #include <fstream>
@@ -35,6 +36,8 @@ int main(int argc, char** argv)
     int atom_style = 0;
     std::string out_data, spring_file;
     bool dump = false;
+    struct Comp { std::string id, style, file; };
+    std::vector<Comp> comps;  // temp, rho, msd, tf computes and their files
     std::istringstream ls(text);
     std::string line;
     while (std::getline(ls, line)) {
@@ -47,6 +50,12 @@ int main(int argc, char** argv)
         if (k == "atom_style") { t >> a; atom_style = a == "atomic" ? 0 : (a == "bond" ? 1 : 2); }
         if (k == "write_data") t >> out_data;
         if (k == "dump") dump = true;
+        if (k == "compute") {
+            std::vector<std::string> w;
+            while (t >> a) w.push_back(a);
+            if (w.size() >= 3 && (w[2] == "temp" || w[2] == "rho" || w[2] == "msd" || w[2] == "tf"))
+                comps.push_back({w[0], w[2], w.back()});
+        }
         if (k == "fix") {
             // fix ID groupID spring k x y z r0 [file_name file_frequency]
             std::vector<std::string> w;
@@ -112,6 +121,26 @@ int main(int argc, char** argv)
             }
             fclose(sf);
         }
+    }
+    // group compute files: src/compute/compute_temp.cu:34-40,160-170 and the same in
+    // compute_rho.cu, compute_msd.cu, compute_tf.cu
+    for (const Comp& c : comps) {
+        std::vector<double> cr(4 * 2048);
+        int nc = 0, nr = 0;
+        if (dpd_get_compute(eng, c.id.c_str(), cr.data(), 2048, &nc, &nr)) continue;
+        FILE* cf = fopen(c.file.c_str(), "w");
+        if (!cf) continue;
+        if (c.style == "tf")
+            fprintf(cf, "%15s\t\t%15s\t\t%15s\t\t%15s\n", "step", "tf_x", "tf_y", "tf_z");
+        else
+            fprintf(cf, "%15s\t\t%15s\n", "step", c.style.c_str());
+        for (int q = 0; q < nr; q++) {
+            const double* r = &cr[(size_t)q * nc];
+            fprintf(cf, "%15lld", (long long)r[0]);
+            for (int j = 1; j < nc; j++) fprintf(cf, "\t\t%15g", r[j]);
+            fprintf(cf, "\n");
+        }
+        fclose(cf);
     }
     if (!out_data.empty()) dpd_write_data(eng, out_data.c_str());
     int64_t natoms = 0;

@@ -198,6 +198,9 @@ int Engine::read_restart(const std::string& path)
         if (!reps_[r].ff.rdfs.empty()) nbins += reps_[r].ff.rdfs[0].nbins;
     }
     if (nbins > 0) CK(cudaMemsetAsync(b_.rdf_hist, 0, sizeof(unsigned long long) * nbins, stream_));
+    int ngc = 0;
+    for (auto& R : reps_) ngc += (int)R.ff.gcs.size();
+    if (ngc > 0) CK(cudaMemsetAsync(b_.gc_count, 0, sizeof(int) * ngc, stream_));
     CK(cudaMemcpyAsync(b_.rstate, rs.data(), sizeof(RepState) * nrep, cudaMemcpyHostToDevice, stream_));
     if (b_.fixo) CK(cudaMemcpyAsync(b_.fixo, fos.data(), sizeof(FixOut) * nrep, cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));

@@ -91,6 +91,15 @@ class Engine:
     def dump_close(self):
         _check(self.lib.dpd_dump_close(self.h), self.lib, self.h)
 
+    def compute(self, compute_id, max_rows=2048):
+        """Rows of a temp/rho/msd/tf group compute: (n, 2) {step, value} or (n, 4)
+        {step, fx, fy, fz}."""
+        rows = np.empty((max_rows, 4))
+        nc, n = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.dpd_get_compute(self.h, str(compute_id).encode(), capi.ptr(rows), max_rows,
+                                        ctypes.byref(nc), ctypes.byref(n)), self.lib, self.h)
+        return rows.reshape(-1)[: n.value * nc.value].reshape(n.value, nc.value)
+
     def write_restart(self, path):
         """Exact checkpoint: FP32 state, forces of the last step, step counter, fix results."""
         _check(self.lib.dpd_write_restart(self.h, str(path).encode()), self.lib, self.h)

@@ -141,6 +141,15 @@ int dpd_dump_close(dpd_engine* eng);
 int dpd_write_restart(dpd_engine* eng, const char* path);
 int dpd_read_restart(dpd_engine* eng, const char* path);
 
+/* Rows of a group compute by its ID (`compute ID group temp|rho|msd|tf freq ... file`,
+ * src/compute/compute_temp.cu, compute_rho.cu, compute_msd.cu, compute_tf.cu), the values
+ * the reference writes to its file every freq steps from the zero step on: {step, T} with
+ * T = 2 KE / (3 Ng - 3); {step, count in the region / region volume} (wrapped positions);
+ * {step, mean |x - x0|^2} over the group (unwrapped, x0 the data file's positions);
+ * {step, Fx, Fy, Fz} summed over the group.  *n_cols = 2 or 4; rows row-major, up to
+ * max_rows of the most recent (the device keeps 2048). */
+int dpd_get_compute(dpd_engine* eng, const char* id, double* rows, int max_rows, int* n_cols, int* n_rows);
+
 /* Records of `fix ... spring k x y z r0 file freq` (src/fix/fix_spring.cu:340-360, the
  * rows it writes to its file): 6 doubles per row {step, Fx, Fy, Fz, +-|F|, energy}, every
  * freq steps from the zero step on.  Copies up to max_rows of the most recent rows (the

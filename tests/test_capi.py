@@ -79,7 +79,7 @@ BAD = [
     ("fix_params", lambda t: t.replace("fix md all nve", "fix md all nve 1"), "illegal fix_nve command"),
     ("fix_dup_id", lambda t: t + "fix md all nve\n", "already registered"),
     ("dump_args", lambda t: t + "dump 0 10 wrapped force_no\n", "illegal dump command"),
-    ("compute_bad", lambda t: t + "compute c all msd 1 x.txt\n", "Compute type 'msd' not found"),
+    ("compute_bad", lambda t: t + "compute c all foo 1 x.txt\n", "Compute type 'foo' not found"),
     ("angle", lambda t: t.replace("atom_style atomic", "atom_style angle") + "bond_style harmonic\n", "angle_style command is missing"),
 ]
 
@@ -200,4 +200,29 @@ def test_group_fix_checks():
     for text, msg in cases:
         assert text != t
         code, err = _create(text, s)
+        assert code == -1 and msg in err, (msg, err)
+
+
+def test_group_compute_checks(base):
+    """compute temp/rho/msd/tf parameters (validateParams of src/compute/compute_*.cu) and
+    the rho region checks (compute_rho.cu:42-75)."""
+    t = base.run_in
+    ok = t + "compute ct all temp 1 t.txt\ncompute cr all rho 5 0 5 0 5 0 5 r.txt\n" \
+             "compute cm all msd 10 m.txt\ncompute cf all tf 2 f.txt\n"
+    code, err = _create(ok, base)
+    assert code in (0, -8), err
+    L = base.hi[0]
+    cases = [
+        (t + "compute ct all temp 1\n", "illegal compute_temp command"),
+        (t + "compute ct all temp 0 t.txt\n", "illegal compute_temp command"),
+        (t + "compute cm all msd 1 m.txt x\n", "illegal compute_msd command"),
+        (t + "compute cf all tf x f.txt\n", "illegal compute_tf command"),
+        (t + "compute cr all rho 1 0 5 0 5 0 r.txt\n", "illegal compute_rho command"),
+        (t + "compute cr all rho 1 -1 5 0 5 0 5 r.txt\n", "xlo < box.xlo"),
+        (t + f"compute cr all rho 1 0 5 0 5 0 {L + 1} r.txt\n", "zhi > box.zhi"),
+        (t + "compute ct all temp 1 t.txt\ncompute ct all msd 1 m.txt\n", "already registered"),
+        (t + "".join(f"compute c{k} all temp 1 t{k}.txt\n" for k in range(5)), "at most 4"),
+    ]
+    for text, msg in cases:
+        code, err = _create(text, base)
         assert code == -1 and msg in err, (msg, err)

@@ -59,14 +59,20 @@ def _case(wrapped):
     s = inputs.probe_fixes(L=9.0, seed=41, nsteps=10, thermo=1)
     run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in)
     run_in += f"dump 0 5 {'wrapped' if wrapped else 'unwrapped'} force_yes vel_yes\nwrite_data out.data\n"
+    run_in += ("compute ct probe temp 2 temp.txt\ncompute cr all rho 1 0.0 4.5 0.0 9.0 2.0 7.0 rho.txt\n"
+               "compute cm all msd 5 msd.txt\ncompute cf probe tf 1 tf.txt\n")
     return s, run_in
+
+
+COMPUTE_FILES = {"temp.txt": [0, 2, 4, 6, 8, 10], "rho.txt": list(range(11)), "msd.txt": [0, 5, 10],
+                 "tf.txt": list(range(11))}
 
 
 @pytest.mark.skipif(not os.path.exists(CLI), reason="gpudpd_b200 not built")
 @pytest.mark.parametrize("wrapped", [True, False])
 def test_cli_outputs_match_reference_executable(wrapped):
     s, run_in = _case(wrapped)
-    files = ["thermo.txt", "all.trj", "spring.txt", "out.data"]
+    files = ["thermo.txt", "all.trj", "spring.txt", "out.data"] + list(COMPUTE_FILES)
     ours = _run(CLI, s, run_in, files)
     assert set(ours) == set(files)
     fr = parse_trj_text(ours["all.trj"])
@@ -83,6 +89,11 @@ def test_cli_outputs_match_reference_executable(wrapped):
     spring = np.loadtxt(ours["spring.txt"].splitlines()[1:], ndmin=2)
     assert list(spring[:, 0]) == [0, 2, 4, 6, 8, 10]
     assert "Atoms" in ours["out.data"] and "Velocities" in ours["out.data"]
+    comp = {f: _thermo(ours[f]) for f in COMPUTE_FILES}
+    for f, steps in COMPUTE_FILES.items():
+        assert list(comp[f][1]["step"]) == steps, f
+    assert comp["tf.txt"][0] == ["step", "tf_x", "tf_y", "tf_z"]
+    assert comp["msd.txt"][1]["msd"][0] < 1e-10
     if not os.path.exists(STOCK):
         pytest.skip("reference build (oracle/build_ref.sh SINGLE) not present")
     ref = _run(STOCK, s, run_in, files)
@@ -106,6 +117,26 @@ def test_cli_outputs_match_reference_executable(wrapped):
         v = np.column_stack([fr[st]["v" + c] for c in "xyz"])
         rv = np.column_stack([rfr[st]["v" + c] for c in "xyz"])
         assert np.abs(v - rv).max() < (1e-6 if st == 0 else 5e-4), st
+    # group computes: same headers and steps; step-0 values to FP32 precision (the rho count
+    # may differ by a particle sitting on a region face), later rows within the trajectory
+    # tolerance
+    for f in COMPUTE_FILES:
+        h, c = comp[f]
+        rh, rc = _thermo(ref[f])
+        assert h == rh, f
+        np.testing.assert_array_equal(c["step"], rc["step"])
+    vol = 4.5 * 9.0 * 5.0
+    assert np.abs(comp["rho.txt"][1]["rho"] - _thermo(ref["rho.txt"])[1]["rho"]).max() * vol <= 1.5
+    t, rt = comp["temp.txt"][1]["temp"], _thermo(ref["temp.txt"])[1]["temp"]
+    assert t[0] == pytest.approx(rt[0], rel=1e-5)
+    np.testing.assert_allclose(t, rt, rtol=1e-3)
+    msd, rmsd = comp["msd.txt"][1]["msd"], _thermo(ref["msd.txt"])[1]["msd"]
+    np.testing.assert_allclose(msd, rmsd, rtol=1e-3, atol=1e-6)
+    tfc, rtf = comp["tf.txt"][1], _thermo(ref["tf.txt"])[1]
+    fscale = np.abs(np.column_stack([fr[0]["f" + c] for c in "xyz"])).max()
+    for c in ("tf_x", "tf_y", "tf_z"):
+        assert abs(tfc[c][0] - rtf[c][0]) < 1e-4 * fscale
+        np.testing.assert_allclose(tfc[c], rtf[c], atol=2e-2 * fscale)
     rspring = np.loadtxt(ref["spring.txt"].splitlines()[1:], ndmin=2)
     np.testing.assert_array_equal(spring[:, 0], rspring[:, 0])
     np.testing.assert_allclose(spring[:, 1:], rspring[:, 1:], rtol=2e-4, atol=2e-4 * np.abs(rspring[:, 1:5]).max())

@@ -382,3 +382,45 @@ def test_restart_continues_the_run(tmp_path, name):
     c = _engine_from(other)
     with pytest.raises(DpdError):
         c.read_restart(path)
+
+
+def test_group_computes_match_state(oracle_mod):
+    """temp, rho, msd and tf computes (rows written on the device inside the captured step)
+    against the same quantities evaluated from the engine's state read at those steps."""
+    from gpumdpd_b200 import inputs
+    s = inputs.probe_fixes(L=9.0, seed=61, nsteps=12, thermo=4, spring_file=None)
+    s.run_in += ("compute ct probe temp 3 temp.txt\n"
+                 "compute cr all rho 2 0.0 4.5 0.0 9.0 2.0 7.0 rho.txt\n"
+                 "compute cm all msd 4 msd.txt\n"
+                 "compute cf probe tf 1 tf.txt\n")
+    e = _engine_from(s)
+    e.run(0)
+    states = {0: e.state()}
+    for st in range(1, 13):
+        e.run(1)
+        states[st] = e.state()
+    m = s.masses[s.types - 1]
+    probe = s.types == 2
+    L = _box(e)
+    ct, cr, cm, cf = (e.compute(c) for c in ("ct", "cr", "cm", "cf"))
+    assert list(ct[:, 0]) == [0, 3, 6, 9, 12]
+    assert list(cr[:, 0]) == list(range(0, 13, 2))
+    assert list(cm[:, 0]) == [0, 4, 8, 12]
+    assert list(cf[:, 0]) == list(range(13)) and cf.shape[1] == 4
+    for step, val in ct:
+        v = states[int(step)]["v"][probe]
+        want = (m[probe, None] * v ** 2).sum() / (3 * probe.sum() - 3)
+        assert val == pytest.approx(want, rel=1e-5)
+    for step, val in cr:
+        x = states[int(step)]["x"]
+        inside = (x[:, 0] >= 0.0) & (x[:, 0] < 4.5) & (x[:, 2] >= 2.0) & (x[:, 2] < 7.0)
+        assert abs(val * 4.5 * 9.0 * 5.0 - inside.sum()) <= 2  # boundary rounding
+    x0 = s.x
+    for step, val in cm:
+        g = states[int(step)]
+        d = g["x"] + g["image"] * L - x0
+        assert val == pytest.approx((d ** 2).sum(1).mean(), rel=1e-4, abs=1e-9)
+    for row in cf:
+        f = states[int(row[0])]["f"][probe].sum(0)
+        scale = np.abs(states[int(row[0])]["f"]).max()
+        np.testing.assert_allclose(row[1:], f, atol=1e-4 * scale)
