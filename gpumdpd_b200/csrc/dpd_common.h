@@ -39,6 +39,8 @@ enum {
     ST_FENE_BROKEN = 8,
     ST_BOND_OVERFLOW = 16,
     ST_BAD_INPUT = 32,  // an AoS input carried an id or type outside the system
+    ST_WALL_ORDER = 64, // fix two_wall: the high wall is not above the low wall
+    ST_CONTACT_BOX = 128, // compute wall_contact: contact region outside the box
 };
 
 // Per-replica constant description (device copy, read through the L1 cache).
@@ -88,6 +90,15 @@ struct FixDesc {
     double rvcm_m, recenter_m, recenter_c[3];
     double L[3];           // box lengths of the cell grid (unwrapped = lo + c w + o + img L)
     uint32_t spring_file_f; // spring record every this many steps (0 = none)
+    // wall fixes (src/fix/fix_move.cu, fix_wall_reflect.cu, fix_two_wall.cu)
+    int n_move, n_reflect, n_twowall;
+    uint32_t move_mask[4];
+    float move_v[4][3];
+    uint32_t refl_mask[4];
+    int refl_dir[4];
+    float refl_lo[4], refl_hi[4];
+    uint32_t tw_mask[2], tw_lo[2], tw_hi[2];
+    int tw_dir[2];
 };
 
 // Group computes (temp, rho, msd, tf), DPD_MAX_GC per replica (device).
@@ -99,6 +110,11 @@ struct GCDesc {
     double norm;      // temp 1/(3 Ng - 3); rho 1/volume; msd 1/Ng
     double region[6]; // rho: xlo xhi ylo yhi zlo zhi
     double L[3];      // box lengths of the cell grid
+    uint32_t wall_mask; // wall_contact: the wall group's types
+    int wall_side;      // +1: lo wall (its maximum), -1: hi wall (its minimum)
+    int wall_dir;
+    float cutoff;
+    float box_lo, box_hi;  // the box along wall_dir
 };
 
 // Per-replica results of the fix reductions of the current step (device).

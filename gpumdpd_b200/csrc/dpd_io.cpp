@@ -610,8 +610,52 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             for (int d = 0; d < 3; d++) ff.recenter.c[d] = c[d];
             continue;
         }
+        auto direction = [](const std::string& s) { return s == "x" ? 0 : (s == "y" ? 1 : (s == "z" ? 2 : -1)); };
+        if (t[3] == "move") {
+            // src/fix/fix_move.cu:17-30
+            const char* msg = "illegal fix_move command: fix ID groupID move v_x v_y v_z";
+            FixMove m;
+            if (np != 3) return fail(err, line, msg);
+            for (int d = 0; d < 3; d++)
+                if (!parse_double(t[4 + d], m.v[d])) return fail(err, line, msg);
+            if (ff.moves.size() >= 4) return fail(err, line, "this engine takes at most 4 fix move");
+            m.mask = group_mask(t[2]);
+            ff.moves.push_back(m);
+            continue;
+        }
+        if (t[3] == "wall_reflect") {
+            // src/fix/fix_wall_reflect.cu:17-45 and the in-box check of :50-80
+            const char* msg = "illegal fix_wall_reflect command: fix ID groupID wall_reflect lo_wall_pos hi_wall_pos wall_direction";
+            FixWallReflect w;
+            if (np != 3 || !parse_double(t[4], w.lo) || !parse_double(t[5], w.hi)) return fail(err, line, msg);
+            if (w.lo >= w.hi) return fail(err, line, std::string(msg) + ": lo_wall_pos should lower than hi_wall_pos");
+            w.dir = direction(t[6]);
+            if (w.dir < 0) return fail(err, line, std::string(msg) + ": Invalid fix_wall_reflect direction");
+            if (w.lo < sys.lo[w.dir] || w.hi > sys.hi[w.dir]) return fail(err, line, "Wall position is out of the box!");
+            if (ff.reflects.size() >= 4) return fail(err, line, "this engine takes at most 4 fix wall_reflect");
+            w.mask = group_mask(t[2]);
+            ff.reflects.push_back(w);
+            continue;
+        }
+        if (t[3] == "two_wall") {
+            // src/fix/fix_two_wall.cu:17-40
+            const char* msg = "illegal fix_two_wall command: fix ID groupID two_wall lo_wall_name hi_wall_name direction";
+            FixTwoWall w;
+            if (np != 3) return fail(err, line, msg);
+            for (int q = 4; q <= 5; q++)
+                if (!ff.groups.count(t[q])) return fail(err, line, "Group '" + t[q] + "' not found!");
+            w.dir = direction(t[6]);
+            if (w.dir < 0) return fail(err, line, std::string(msg) + ": Invalid fix_two_wall direction");
+            if (ff.twowalls.size() >= 2) return fail(err, line, "this engine takes at most 2 fix two_wall");
+            w.mask = group_mask(t[2]);
+            w.lo_mask = group_mask(t[4]);
+            w.hi_mask = group_mask(t[5]);
+            ff.twowalls.push_back(w);
+            continue;
+        }
         if (t[3] != "nve")
-            return fail(err, line, "Fix type '" + t[3] + "' not found! (this engine implements nve, spring, rvcm, recenter)");
+            return fail(err, line, "Fix type '" + t[3] + "' not found! (this engine implements nve, spring, rvcm, recenter, "
+                                   "move, wall_reflect, two_wall)");
         if (t.size() != 4) return fail(err, line, "illegal fix_nve command: fix ID groupID nve");
         for (int ty : ff.groups[t[2]]) {
             uint32_t bit = 1u << (ty - 1);
@@ -657,6 +701,26 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             }
             if (ff.gcs.size() >= 4) return fail(err, line, "this engine takes at most 4 temp/rho/msd/tf computes");
             ff.gcs.push_back(c);
+        } else if (t[3] == "wall_contact") {
+            // src/compute/compute_wall_contact.cu:17-45
+            const std::string msg = "illegal compute_wall_contact command: compute ID groupID wall_contact frequency "
+                                    "wall_groupname lo/hi wall_direction cutoff filename";
+            GroupCompute c;
+            if (t.size() != 10 || !parse_int(t[4], 1, 4294967295ll, iv)) return fail(err, line, msg);
+            if (!ff.groups.count(t[5])) return fail(err, line, "Group '" + t[5] + "' not found!");
+            if (t[6] != "lo" && t[6] != "hi") return fail(err, line, msg);
+            c.wall_dir = t[7] == "x" ? 0 : (t[7] == "y" ? 1 : (t[7] == "z" ? 2 : -1));
+            if (c.wall_dir < 0 || !parse_double(t[8], c.cutoff)) return fail(err, line, msg);
+            c.id = t[1];
+            c.group = t[2];
+            c.kind = GC_WALL;
+            c.frequency = (unsigned)iv;
+            c.file = t[9];
+            c.wall_side = t[6] == "lo" ? 1 : -1;
+            for (int ty : ff.groups[t[2]]) c.type_mask |= 1u << (ty - 1);
+            for (int ty : ff.groups[t[5]]) c.wall_mask |= 1u << (ty - 1);
+            if (ff.gcs.size() >= 4) return fail(err, line, "this engine takes at most 4 temp/rho/msd/tf/wall_contact computes");
+            ff.gcs.push_back(c);
         } else if (t[3] == "rdf") {
             // compute ID groupID rdf typeA typeB rmax nbins every filename
             ComputeRdf c;
@@ -675,7 +739,7 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             if (!ff.rdfs.empty()) return fail(err, line, "only one rdf compute is supported");
             ff.rdfs.push_back(c);
         } else {
-            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp, rho, msd, tf and rdf)");
+            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp, rho, msd, tf, wall_contact and rdf)");
         }
     }
     return DPD_OK;

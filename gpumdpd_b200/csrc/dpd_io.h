@@ -43,13 +43,34 @@ struct SystemData {
 // compute_rho.cu, compute_msd.cu, compute_tf.cu): the group's temperature, its number
 // density inside a box region, its mean squared displacement from the initial unwrapped
 // positions, and its total force.
-enum { GC_TEMP = 1, GC_RHO = 2, GC_MSD = 3, GC_TF = 4 };
+enum { GC_TEMP = 1, GC_RHO = 2, GC_MSD = 3, GC_TF = 4, GC_WALL = 5 };
 struct GroupCompute {
     std::string id, group, file;
     int kind = GC_TEMP;
     unsigned frequency = 1;
     uint32_t type_mask = 0;
     double region[6] = {0, 0, 0, 0, 0, 0};  // rho: xlo xhi ylo yhi zlo zhi
+    // wall_contact (src/compute/compute_wall_contact.cu): group atoms within `cutoff` of
+    // the wall group's extreme position along `dir` (side +1: its maximum, lo wall; -1:
+    // its minimum, hi wall)
+    uint32_t wall_mask = 0;
+    int wall_side = 1, wall_dir = 2;
+    double cutoff = 0;
+};
+
+// Wall fixes (src/fix/fix_move.cu, fix_wall_reflect.cu, fix_two_wall.cu); several of each.
+struct FixMove {      // initial_integrate: v = V and x += V dt for the group
+    uint32_t mask = 0;
+    double v[3] = {0, 0, 0};
+};
+struct FixWallReflect { // post_integrate: mirror group atoms outside [lo, hi] along dir
+    uint32_t mask = 0;
+    int dir = 2;
+    double lo = 0, hi = 0;
+};
+struct FixTwoWall {   // post_integrate: the same between max(lo-wall group) and min(hi-wall group)
+    uint32_t mask = 0, lo_mask = 0, hi_mask = 0;
+    int dir = 2;
 };
 
 struct ComputeRdf {
@@ -98,6 +119,9 @@ struct ForceField {
     FixRvcm rvcm;
     FixRecenter recenter;
     std::vector<GroupCompute> gcs;
+    std::vector<FixMove> moves;
+    std::vector<FixWallReflect> reflects;
+    std::vector<FixTwoWall> twowalls;
     std::vector<ComputeRdf> rdfs;
 };
 

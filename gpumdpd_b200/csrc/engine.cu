@@ -368,7 +368,7 @@ int Engine::alloc_and_upload()
     {
         std::vector<FixDesc> fd(nrep);
         bool spring_file = false;
-        any_spring_ = any_eos_ = false;
+        any_spring_ = any_eos_ = any_motion_ = any_twowall_ = false;
         for (int r = 0; r < nrep; r++) {
             const Replica& R = reps_[r];
             FixDesc& f = fd[r];
@@ -406,8 +406,31 @@ int Engine::alloc_and_upload()
                 f.recenter_m = gmass(f.recenter_mask);
                 any_eos_ = true;
             }
+            f.n_move = (int)R.ff.moves.size();
+            for (int k = 0; k < f.n_move; k++) {
+                f.move_mask[k] = R.ff.moves[k].mask;
+                for (int q = 0; q < 3; q++) f.move_v[k][q] = (float)R.ff.moves[k].v[q];
+            }
+            f.n_reflect = (int)R.ff.reflects.size();
+            for (int k = 0; k < f.n_reflect; k++) {
+                const FixWallReflect& w = R.ff.reflects[k];
+                f.refl_mask[k] = w.mask;
+                f.refl_dir[k] = w.dir;
+                f.refl_lo[k] = (float)w.lo;
+                f.refl_hi[k] = (float)w.hi;
+            }
+            f.n_twowall = (int)R.ff.twowalls.size();
+            for (int k = 0; k < f.n_twowall; k++) {
+                const FixTwoWall& w = R.ff.twowalls[k];
+                f.tw_mask[k] = w.mask;
+                f.tw_lo[k] = w.lo_mask;
+                f.tw_hi[k] = w.hi_mask;
+                f.tw_dir[k] = w.dir;
+            }
+            if (f.n_move || f.n_reflect) any_motion_ = true;
+            if (f.n_twowall) any_twowall_ = true;
         }
-        if (any_spring_ || any_eos_) {
+        if (any_spring_ || any_eos_ || any_motion_ || any_twowall_) {
             if ((st = dalloc(&b_.fix, nrep))) return st;
             if ((st = dalloc(&b_.fixo, nrep))) return st;
             if (spring_file && (st = dalloc(&b_.spring_ring, (size_t)nrep * DPD_RING_ROWS * 6))) return st;
@@ -417,6 +440,7 @@ int Engine::alloc_and_upload()
     }
     // group computes: descriptors, initial unwrapped positions by global tag, row rings
     gc_ring_base_.assign(nrep, 0);
+    any_wallc_ = false;
     if (any_gc_) {
         std::vector<GCDesc> gd((size_t)nrep * DPD_MAX_GC);
         memset(gd.data(), 0, sizeof(GCDesc) * gd.size());
@@ -440,6 +464,16 @@ int Engine::alloc_and_upload()
                 if (c.kind == GC_MSD) g.norm = ng > 0 ? 1.0 / ng : 0.0;
                 if (c.kind == GC_RHO)
                     g.norm = 1.0 / ((c.region[1] - c.region[0]) * (c.region[3] - c.region[2]) * (c.region[5] - c.region[4]));
+                if (c.kind == GC_WALL) {
+                    g.norm = 1.0;
+                    g.wall_mask = c.wall_mask;
+                    g.wall_side = c.wall_side;
+                    g.wall_dir = c.wall_dir;
+                    g.cutoff = (float)c.cutoff;
+                    g.box_lo = (float)R.sys.lo[c.wall_dir];
+                    g.box_hi = (float)R.sys.hi[c.wall_dir];
+                    any_wallc_ = true;
+                }
             }
             // initial unwrapped positions: the data file's positions wrapped into the box
             for (int i = 0; i < R.sys.n_atoms; i++) {
@@ -460,6 +494,7 @@ int Engine::alloc_and_upload()
         CK(cudaMemcpyAsync(b_.uw0, uw0.data(), sizeof(float4) * uw0.size(), cudaMemcpyHostToDevice, stream_));
         CK(cudaStreamSynchronize(stream_));
     }
+    if ((any_twowall_ || any_wallc_) && (st = dalloc(&b_.wall_ext, (size_t)nrep * 8))) return st;
     std::vector<RepState> rs(nrep);
     for (auto& s : rs) {
         memset(&s, 0, sizeof(s));
@@ -647,6 +682,7 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     a.uw0 = b.uw0;
     a.gc_ring = b.gc_ring;
     a.gc_count = b.gc_count;
+    a.wall_ext = b.wall_ext;
     return a;
 }
 
@@ -752,22 +788,38 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
         pdl_launch(k_fix_sums<1>, gp, 256, s, sa);
         pdl_launch(k_fix_reduce<1>, gr, 256, s, sa);
     }
-    if (any_spring_ || any_eos_ || any_gc_) {
+    if (any_wallc_) {
+        // wall_contact computes: wall extents of the end-of-step positions
+        pdl_launch(k_wall_reset<1>, gr, 256, s, sa);
+        pdl_launch(k_wall_extent<1>, gp, 256, s, sa);
+    }
+    if (ext()) {
         pdl_launch(k_integrate_nolog<true>, gp, 256, s, sa);
         pdl_launch(k_integrate_logsteps<true>, std::min(gp, 148 * 4), 256, s, sa);
     } else {
         pdl_launch(k_integrate_nolog<false>, gp, 256, s, sa);
         pdl_launch(k_integrate_logsteps<false>, std::min(gp, 148 * 4), 256, s, sa);
     }
+    if (any_twowall_) enqueue_two_wall(s, sa);
     pdl_launch(k_advance, gr, 256, s, sa);
+}
+
+// fix two_wall after a drift: wall extents, then the reflection of the group
+void Engine::enqueue_two_wall(cudaStream_t s, const StepArgs& sa)
+{
+    const int gp = (P_ + 255) / 256, gr = ((int)reps_.size() + 255) / 256;
+    pdl_launch(k_wall_reset<0>, gr, 256, s, sa);
+    pdl_launch(k_wall_extent<0>, gp, 256, s, sa);
+    pdl_launch(k_two_wall, gp, 256, s, sa);
 }
 
 void Engine::enqueue_integrate_initial(cudaStream_t s)
 {
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, (int)reps_.size());
     sa.mode = 1;
-    if (any_spring_ || any_eos_ || any_gc_) k_integrate<true><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+    if (ext()) k_integrate<true><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
     else k_integrate<false><<<(P_ + 255) / 256, 256, 0, s>>>(sa);
+    if (any_twowall_) enqueue_two_wall(s, sa);
 }
 
 int Engine::build_graph()
@@ -874,6 +926,14 @@ int Engine::sync_and_check()
         }
         if (s & ST_BOND_MISSING) {
             err = "bond partner not found in replica " + std::to_string(r);
+            return DPD_E_STATE;
+        }
+        if (s & ST_WALL_ORDER) {
+            err = "The high wall is positioned lower than the low wall (fix two_wall, replica " + std::to_string(r) + ")";
+            return DPD_E_STATE;
+        }
+        if (s & ST_CONTACT_BOX) {
+            err = "contact region out of the box (compute wall_contact, replica " + std::to_string(r) + ")";
             return DPD_E_STATE;
         }
         if (s & ST_BAD_INPUT) {

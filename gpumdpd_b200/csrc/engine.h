@@ -13,6 +13,8 @@
 #include "dpd_io.h"
 #include "dump.h"
 
+struct StepArgs;  // kernels_step.cuh
+
 namespace dpd {
 
 // Host loop over [0, n) split across hardware threads (state conversion of millions of
@@ -69,6 +71,7 @@ struct DeviceBuffers {
     float4* uw0 = nullptr;
     double* gc_ring = nullptr;
     int* gc_count = nullptr;
+    int* wall_ext = nullptr;        // wall extents (fix two_wall, compute wall_contact)
 };
 
 class Engine {
@@ -156,7 +159,11 @@ private:
     int P_ = 0, C_ = 0, nmax_ = 16, maxb_ = 0;
     bool any_mdpd_ = false, any_dpd_ = false, bonds_ = false, rdf_ = false;
     bool any_spring_ = false, any_eos_ = false;  // some replica has a spring / an rvcm or recenter
-    bool any_gc_ = false;                         // some replica has a temp/rho/msd/tf compute
+    bool any_gc_ = false;                         // some replica has a temp/rho/msd/tf/wall_contact compute
+    bool any_motion_ = false, any_twowall_ = false, any_wallc_ = false;  // fix move/wall_reflect, two_wall, wall_contact
+    // the integrate variant with group fixes and computes
+    bool ext() const { return any_spring_ || any_eos_ || any_gc_ || any_motion_ || any_twowall_; }
+    void enqueue_two_wall(cudaStream_t s, const ::StepArgs& sa);
     std::vector<int> gc_ring_base_;               // first compute ring of each replica
     bool zero_pending_ = true;
     bool force_build_ = false;  // the next run starts with a list build (after a restart)

@@ -37,7 +37,42 @@ struct StepArgs {
     const float4* uw0;     // [atoms of all replicas] initial unwrapped positions by global tag
     double* gc_ring;       // [computes][DPD_RING_ROWS][4] rows {step, values}
     int* gc_count;         // [computes] rows written
+    int* wall_ext;         // [nrep][8] wall extents, order-preserving ints: two_wall k at
+                           // 2k (max of its lo wall), 2k+1 (min of its hi wall); wall_contact
+                           // compute k at 4+k
 };
+
+// order-preserving int image of a float (atomicMax / atomicMin on positions)
+__device__ __forceinline__ int ford(float f)
+{
+    const int b = __float_as_int(f);
+    return b >= 0 ? b : b ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ford_inv(int b) { return __int_as_float(b >= 0 ? b : b ^ 0x7fffffff); }
+
+// position of a slot along axis q wrapped into [lo, lo + L) (the reference's d_pos)
+__device__ __forceinline__ float wrapped_coord(const RepDesc& d, double L, const float4& p, int q)
+{
+    const int code = __float_as_int(p.w);
+    const float o = q == 0 ? p.x : (q == 1 ? p.y : p.z);
+    double xa = (double)((code >> (q * DPD_CELL_BITS)) & DPD_MAX_NC) * (double)d.w[q] + (double)o;
+    xa -= floor(xa / L) * L;
+    if (xa >= L) xa -= L;
+    return (float)(d.lo[q] + xa);
+}
+
+__device__ __forceinline__ void add_axis(float4& p, int q, float dx)
+{
+    if (q == 0) p.x += dx;
+    else if (q == 1) p.y += dx;
+    else p.z += dx;
+}
+__device__ __forceinline__ void flip_axis(float4& v, int q)
+{
+    if (q == 0) v.x = -v.x;
+    else if (q == 1) v.y = -v.y;
+    else v.z = -v.z;
+}
 
 // group computes due at the current step of a replica (bit k: compute k), evaluated with
 // the end-of-step state after the thermo (src/main/utils.cuh:191-194, 290-291)
@@ -765,6 +800,16 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                     if (!((g.mask >> t0) & 1u)) continue;
                     if (g.kind == 1) {
                         gv[3 * k] = 0.5 * (double)m.x * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+                    } else if (g.kind == 5) {
+                        // src/compute/compute_wall_contact.cu:60-100,186-290: atoms within the
+                        // cutoff of the wall group's extreme position
+                        const float bound = ford_inv(a.wall_ext[r * 8 + 4 + k]);
+                        const float cb = g.wall_side > 0 ? bound + g.cutoff : bound - g.cutoff;
+                        if (g.wall_side > 0 ? cb > g.box_hi : cb < g.box_lo)
+                            atomicOr(&a.rstate[r].status, ST_CONTACT_BOX);
+                        const float xw = wrapped_coord(d, g.L[g.wall_dir], p, g.wall_dir);
+                        const bool in = g.wall_side > 0 ? (xw >= bound && xw < cb) : (xw >= cb && xw < bound);
+                        gv[3 * k] = in ? 1.0 : 0.0;
                     } else if (g.kind == 4) {
                         gv[3 * k] = fe.x;
                         gv[3 * k + 1] = fe.y;
@@ -797,7 +842,7 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                     }
                 }
             }
-            if (EXT && shifted && !(init && integ)) posp[s] = p;
+            if (EXT && shifted && !init) posp[s] = p;
             if (init) {
                 if (integ) {
                     v.x = __fmaf_rn(dtm, fe.x, v.x);
@@ -806,6 +851,35 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
                     p.x = __fmaf_rn(dt, v.x, p.x);
                     p.y = __fmaf_rn(dt, v.y, p.y);
                     p.z = __fmaf_rn(dt, v.z, p.z);
+                }
+                bool moved = integ || shifted;
+                if (EXT && a.fix) {
+                    // fix move (initial_integrate, src/fix/fix_move.cu:33-80): v = V, x += V dt;
+                    // then fix wall_reflect (post_integrate, src/fix/fix_wall_reflect.cu:84-125):
+                    // a group atom past a wall is mirrored back, its normal velocity reversed
+                    const FixDesc& fd = a.fix[r];
+                    for (int k = 0; k < fd.n_move; k++)
+                        if ((fd.move_mask[k] >> t0) & 1u) {
+                            v.x = fd.move_v[k][0];
+                            v.y = fd.move_v[k][1];
+                            v.z = fd.move_v[k][2];
+                            p.x += fd.move_v[k][0] * dt;
+                            p.y += fd.move_v[k][1] * dt;
+                            p.z += fd.move_v[k][2] * dt;
+                            moved = true;
+                        }
+                    for (int k = 0; k < fd.n_reflect; k++)
+                        if ((fd.refl_mask[k] >> t0) & 1u) {
+                            const int q = fd.refl_dir[k];
+                            const float xw = wrapped_coord(d, fd.L[q], p, q);
+                            if (xw < fd.refl_lo[k] || xw > fd.refl_hi[k]) {
+                                add_axis(p, q, 2.0f * ((xw < fd.refl_lo[k] ? fd.refl_lo[k] : fd.refl_hi[k]) - xw));
+                                flip_axis(v, q);
+                                moved = true;
+                            }
+                        }
+                }
+                if (moved) {
                     if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z) || !isfinite(v.x) ||
                         !isfinite(v.y) || !isfinite(v.z))
                         atomicOr(&a.rstate[r].status, ST_NONFINITE);
@@ -875,6 +949,131 @@ __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, EXT>(a, vb * 256 + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------------
+// Wall extents: the maximum position of a lo-wall group and the minimum of a hi-wall
+// group along the wall axis (src/fix/fix_two_wall.cu:145-180 and
+// src/compute/compute_wall_contact.cu:186-225 take them with thrust max/min_element).
+// PH 0: the two_wall groups, after the drift; PH 1: the wall groups of wall_contact
+// computes due this step, before the integrate (the end-of-step positions).
+template <int PH>
+__global__ void k_wall_reset(StepArgs a)
+{
+    griddep_wait();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.nrep) return;
+    int* e = a.wall_ext + r * 8;
+    if (PH == 0) {
+        for (int k = 0; k < 2; k++) {
+            e[2 * k] = ford(-INFINITY);
+            e[2 * k + 1] = ford(INFINITY);
+        }
+    } else {
+        for (int k = 0; k < DPD_MAX_GC; k++) {
+            const bool lo = !a.gc || a.gc[r * DPD_MAX_GC + k].wall_side > 0;
+            e[4 + k] = ford(lo ? -INFINITY : INFINITY);
+        }
+    }
+}
+
+template <int PH>
+__global__ void __launch_bounds__(256) k_wall_extent(StepArgs a)
+{
+    griddep_wait();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;  // warp-uniform
+    const int r = a.warp_rep[s >> 5];
+    const RepState st = a.rstate[r];
+    if (!rep_active(st)) return;
+    const RepDesc& d = a.reps[r];
+    const int lane = threadIdx.x & 31;
+    const int par = *a.parity;
+    const bool real = s < d.p_end;
+    float4 p = make_float4(0, 0, 0, 0);
+    int t0 = 0;
+    if (real) {
+        p = a.buf.pos[par][s];
+        t0 = type0_of(a.buf.vel[par][s].w);
+    }
+    if (PH == 0) {
+        if (!a.fix) return;
+        const FixDesc& fd = a.fix[r];
+        for (int k = 0; k < fd.n_twowall; k++) {
+            const int q = fd.tw_dir[k];
+            const bool inlo = real && ((fd.tw_lo[k] >> t0) & 1u), inhi = real && ((fd.tw_hi[k] >> t0) & 1u);
+            const float xw = (inlo || inhi) ? wrapped_coord(d, fd.L[q], p, q) : 0.0f;
+            const int mx = __reduce_max_sync(0xffffffffu, inlo ? ford(xw) : INT_MIN);
+            const int mn = __reduce_min_sync(0xffffffffu, inhi ? ford(xw) : INT_MAX);
+            if (lane == 0) {
+                if (mx != INT_MIN) atomicMax(&a.wall_ext[r * 8 + 2 * k], mx);
+                if (mn != INT_MAX) atomicMin(&a.wall_ext[r * 8 + 2 * k + 1], mn);
+            }
+        }
+    } else {
+        if (!a.gc || a.mode != 0 || !d.gc_n) return;
+        const int due = gc_due(a, d, st, r);
+        for (int k = 0; k < d.gc_n; k++) {
+            const GCDesc& g = a.gc[r * DPD_MAX_GC + k];
+            if (g.kind != 5 || !((due >> k) & 1)) continue;
+            const bool in = real && ((g.wall_mask >> t0) & 1u);
+            const float xw = in ? wrapped_coord(d, g.L[g.wall_dir], p, g.wall_dir) : 0.0f;
+            if (g.wall_side > 0) {
+                const int mx = __reduce_max_sync(0xffffffffu, in ? ford(xw) : INT_MIN);
+                if (lane == 0 && mx != INT_MIN) atomicMax(&a.wall_ext[r * 8 + 4 + k], mx);
+            } else {
+                const int mn = __reduce_min_sync(0xffffffffu, in ? ford(xw) : INT_MAX);
+                if (lane == 0 && mn != INT_MAX) atomicMin(&a.wall_ext[r * 8 + 4 + k], mn);
+            }
+        }
+    }
+}
+
+// fix two_wall, post_integrate (src/fix/fix_two_wall.cu:84-125, 183-200): group atoms
+// below the lo wall's maximum or above the hi wall's minimum are mirrored back with the
+// normal velocity reversed; then the list-rebuild check of the moved atoms.
+__global__ void __launch_bounds__(256) k_two_wall(StepArgs a)
+{
+    griddep_wait();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P || !a.fix) return;
+    const int r = a.warp_rep[s >> 5];
+    const RepState st = a.rstate[r];
+    const RepDesc& d = a.reps[r];
+    if (!rep_active(st) || s >= d.p_end) return;
+    const bool init = a.mode == 1 ? true : st.step < st.target;
+    if (!init) return;  // no drift this launch: nothing to correct
+    const FixDesc& fd = a.fix[r];
+    if (!fd.n_twowall) return;
+    const int par = *a.parity;
+    float4 p = a.buf.pos[par][s];
+    float4 v = a.buf.vel[par][s];
+    const int t0 = type0_of(v.w);
+    bool moved = false;
+    for (int k = 0; k < fd.n_twowall; k++) {
+        if (!((fd.tw_mask[k] >> t0) & 1u)) continue;
+        const float lo = ford_inv(a.wall_ext[r * 8 + 2 * k]), hi = ford_inv(a.wall_ext[r * 8 + 2 * k + 1]);
+        if (hi <= lo) atomicOr(&a.rstate[r].status, ST_WALL_ORDER);
+        const int q = fd.tw_dir[k];
+        const float xw = wrapped_coord(d, fd.L[q], p, q);
+        if (xw < lo || xw > hi) {
+            add_axis(p, q, 2.0f * ((xw < lo ? lo : hi) - xw));
+            flip_axis(v, q);
+            moved = true;
+        }
+    }
+    if (!moved) return;
+    a.buf.pos[par][s] = p;
+    a.buf.vel[par][s] = v;
+    const uint32_t next = a.mode == 1 ? st.step : st.step + 1u;
+    if ((next % (uint32_t)d.nl_f) == 0u && !d.skin_zero) {
+        const float4 q = a.last4[s];
+        const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        if (!(__fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))) < d.hskin2)) {
+            const uint32_t ph = *a.phase + (a.mode == 1 ? 0u : 1u);
+            a.build_flag[ph & 1] = 1;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------

@@ -280,6 +280,35 @@ def probe_fixes(L=9.0, rho=3.0, seed=23, radius=1.5, probe_mass=2.0, spring_k=50
     return System([0, 0, 0], [L, L, L], masses, types, x, v, run_in=run)
 
 
+def wall_channel(L=8.0, Lz=14.0, rho=3.0, wall=1.0, v_top=0.5, walls="two_wall", seed=71, kT=1.0, dt=0.04,
+                 nsteps=1000, skin=0.3, thermo=100, a_ll=25.0, a_lw=30.0, gamma=4.5, contact=1.0,
+                 data="system.data", max_rho=10.0):
+    """Liquid (type 1) between two particle walls along z: a frozen lo wall (type 2) in
+    [0, wall) and a hi wall (type 3) in [Lz - wall, Lz) moved along x at v_top by fix move
+    (Couette).  The liquid is integrated by fix nve and kept between the walls by fix
+    two_wall (walls="two_wall") or by fix wall_reflect at the wall faces ("reflect");
+    compute wall_contact counts liquid atoms within `contact` of the lo wall."""
+    rng = np.random.default_rng(seed)
+    n = int(round(rho * L * L * Lz))
+    x = np.column_stack([rng.uniform(0, L, n), rng.uniform(0, L, n), rng.uniform(0, Lz, n)])
+    types = np.where(x[:, 2] < wall, 2, np.where(x[:, 2] >= Lz - wall, 3, 1)).astype(np.int32)
+    v = _velocities(rng, n, kT, np.ones(n))
+    v[types != 1] = 0.0
+    fixes = [("md", "liquid", "nve"), ("mv", "top", f"move {v_top} 0.0 0.0")]
+    if walls == "two_wall":
+        fixes.append(("tw", "liquid", "two_wall bottom top z"))
+    else:
+        fixes.append(("wr", "liquid", f"wall_reflect {wall} {Lz - wall} z"))
+    computes = (("cwc", "liquid", "wall_contact", 1, "bottom", "lo", "z", contact, "wall_contact.txt"),)
+    c = [(1, 1, a_ll, gamma), (1, 2, a_lw, gamma), (1, 3, a_lw, gamma), (2, 2, a_ll, gamma), (2, 3, a_ll, gamma),
+         (3, 3, a_ll, gamma)]
+    run = run_in_text(skin=skin, dt=dt, thermo=thermo, run=nsteps, data=data, temp=kT,
+                      seed=(seed * 7907 + 11) % 1000003, max_rho=max_rho, coeffs=c,
+                      groups=(("liquid", (1,)), ("bottom", (2,)), ("top", (3,))), fixes=tuple(fixes),
+                      computes=computes)
+    return System([0, 0, 0], [L, L, Lz], [1.0, 1.0, 1.0], types, x, v, run_in=run)
+
+
 def replica_sweep(n_rep=256,L_min=8.0, L_max=24.0, a_lo=25.0, a_hi=45.0, seed=99, nsteps=5000,
                   rdf=(3.0, 150, 100), skin=0.3, thermo=100):
     """Uneven replicas: a_AB uniformly spaced over [a_lo, a_hi]; L drawn log-uniform."""

@@ -269,6 +269,17 @@ typedef struct {
     uint32_t recenter_mask;
     uint32_t recenter_freq;
     double recenter_c[3];
+    uint32_t integ_mask; /* types integrated by fix nve; 0 = every type */
+    int n_move;          /* src/fix/fix_move.cu:33-100 (initial_integrate) */
+    uint32_t move_mask[4];
+    double move_v[4][3];
+    int n_reflect;       /* src/fix/fix_wall_reflect.cu:84-140 (post_integrate) */
+    uint32_t refl_mask[4];
+    int refl_dir[4];
+    double refl_lo[4], refl_hi[4];
+    int n_twowall;       /* src/fix/fix_two_wall.cu:84-200 (post_integrate) */
+    uint32_t tw_mask[2], tw_lo[2], tw_hi[2];
+    int tw_dir[2];
 } oracle_ff;
 
 /* The angle list (type, tag_i, tag_j, tag_k per angle; j is the apex) of the next
@@ -637,6 +648,64 @@ static void fix_end_of_step(int n, const int* type, double* x, double* v, int* i
     }
 }
 
+/* fix move (initial_integrate after fix nve's drift): v = V, x += V dt; then the
+ * post_integrate walls: fix wall_reflect mirrors group atoms outside [lo, hi] along its
+ * axis and reverses that velocity component; fix two_wall does the same between the
+ * maximum position of its lo-wall group and the minimum of its hi-wall group.         */
+static void wrap_coord(double* x, int* img, const double* lo, const double* L, int i, int d)
+{
+    double p = x[3 * i + d];
+    const double hi = lo[d] + L[d];
+    while (p >= hi || p < lo[d]) {
+        const int k = (p >= hi) - (p < lo[d]);
+        p -= L[d] * k;
+        img[3 * i + d] += k;
+    }
+    x[3 * i + d] = p;
+}
+
+static void wall_fixes(int n, const int* type, double* x, double* v, int* img, const double* lo,
+                       const double* L, const oracle_ff* ff)
+{
+    for (int k = 0; k < ff->n_move; k++)
+        for (int i = 0; i < n; i++) {
+            if (!((ff->move_mask[k] >> (type[i] - 1)) & 1u)) continue;
+            for (int d = 0; d < 3; d++) {
+                v[3 * i + d] = ff->move_v[k][d];
+                x[3 * i + d] += ff->move_v[k][d] * ff->dt;
+                wrap_coord(x, img, lo, L, i, d);
+            }
+        }
+    for (int k = 0; k < ff->n_reflect; k++) {
+        const int d = ff->refl_dir[k];
+        for (int i = 0; i < n; i++) {
+            if (!((ff->refl_mask[k] >> (type[i] - 1)) & 1u)) continue;
+            const double p = x[3 * i + d];
+            if (p < ff->refl_lo[k] || p > ff->refl_hi[k]) {
+                x[3 * i + d] = p + 2.0 * ((p < ff->refl_lo[k] ? ff->refl_lo[k] : ff->refl_hi[k]) - p);
+                v[3 * i + d] = -v[3 * i + d];
+            }
+        }
+    }
+    for (int k = 0; k < ff->n_twowall; k++) {
+        const int d = ff->tw_dir[k];
+        double wlo = -INFINITY, whi = INFINITY;
+        for (int i = 0; i < n; i++) {
+            const uint32_t bit = 1u << (type[i] - 1);
+            if (ff->tw_lo[k] & bit) wlo = fmax(wlo, x[3 * i + d]);
+            if (ff->tw_hi[k] & bit) whi = fmin(whi, x[3 * i + d]);
+        }
+        for (int i = 0; i < n; i++) {
+            if (!((ff->tw_mask[k] >> (type[i] - 1)) & 1u)) continue;
+            const double p = x[3 * i + d];
+            if (p < wlo || p > whi) {
+                x[3 * i + d] = p + 2.0 * ((p < wlo ? wlo : whi) - p);
+                v[3 * i + d] = -v[3 * i + d];
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Velocity-Verlet run with the reference's step order (src/main/utils.cuh:166-213
  * for step 0, :254-303 per step; src/fix/fix_nve.cu:42-86 and :131-149).
@@ -671,6 +740,8 @@ int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int
         uint32_t step = first_step + (uint32_t)s;
         for (int i = 0; i < n; i++) {
             double dtm = 0.5 * dt / ff->mass[type[i] - 1];
+            const uint32_t bit = 1u << (type[i] - 1);
+            if (ff->integ_mask && !(ff->integ_mask & bit)) continue;
             for (int d = 0; d < 3; d++) {
                 v[3 * i + d] += dtm * f[3 * i + d];
                 double p = x[3 * i + d] + dt * v[3 * i + d];
@@ -683,11 +754,13 @@ int oracle_run(int n, const int* tag, const int* type, double* x, double* v, int
                 x[3 * i + d] = p;
             }
         }
+        wall_fixes(n, type, x, v, img, lo, L, ff);
         status |= oracle_forces(n, tag, type, x, v, lo, L, ff, step, nbonds, bonds, f, rho_out,
                                 energy, virial);
         if (ff->spring_on) fix_spring(n, type, x, img, L, ff, f);
         for (int i = 0; i < n; i++) {
             double dtm = 0.5 * dt / ff->mass[type[i] - 1];
+            if (ff->integ_mask && !(ff->integ_mask & (1u << (type[i] - 1)))) continue;
             for (int d = 0; d < 3; d++) v[3 * i + d] += dtm * f[3 * i + d];
         }
         fix_end_of_step(n, type, x, v, img, lo, L, ff, step);

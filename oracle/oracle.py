@@ -29,6 +29,12 @@ class OracleFF(ctypes.Structure):
         ("rvcm_flag", ctypes.c_int * 3),
         ("recenter_on", ctypes.c_int), ("recenter_mask", ctypes.c_uint32), ("recenter_freq", ctypes.c_uint32),
         ("recenter_c", ctypes.c_double * 3),
+        ("integ_mask", ctypes.c_uint32),
+        ("n_move", ctypes.c_int), ("move_mask", ctypes.c_uint32 * 4), ("move_v", (ctypes.c_double * 3) * 4),
+        ("n_reflect", ctypes.c_int), ("refl_mask", ctypes.c_uint32 * 4), ("refl_dir", ctypes.c_int * 4),
+        ("refl_lo", ctypes.c_double * 4), ("refl_hi", ctypes.c_double * 4),
+        ("n_twowall", ctypes.c_int), ("tw_mask", ctypes.c_uint32 * 2), ("tw_lo", ctypes.c_uint32 * 2),
+        ("tw_hi", ctypes.c_uint32 * 2), ("tw_dir", ctypes.c_int * 2),
     ]
 
 
@@ -175,6 +181,24 @@ def ff_from_run_in(text, masses):
             ff.recenter_on, ff.recenter_mask, ff.recenter_freq = 1, mask(t[2]), int(t[4])
             for d in range(3):
                 ff.recenter_c[d] = float(t[5 + d])
+        elif t[3] == "nve":
+            ff.integ_mask |= mask(t[2])
+        elif t[3] == "move":
+            k = ff.n_move
+            ff.move_mask[k] = mask(t[2])
+            for d in range(3):
+                ff.move_v[k][d] = float(t[4 + d])
+            ff.n_move = k + 1
+        elif t[3] == "wall_reflect":
+            k = ff.n_reflect
+            ff.refl_mask[k], ff.refl_lo[k], ff.refl_hi[k] = mask(t[2]), float(t[4]), float(t[5])
+            ff.refl_dir[k] = "xyz".index(t[6])
+            ff.n_reflect = k + 1
+        elif t[3] == "two_wall":
+            k = ff.n_twowall
+            ff.tw_mask[k], ff.tw_lo[k], ff.tw_hi[k] = mask(t[2]), mask(t[4]), mask(t[5])
+            ff.tw_dir[k] = "xyz".index(t[6])
+            ff.n_twowall = k + 1
     return ff
 
 

@@ -94,6 +94,9 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
         thermo = parse_thermo(os.path.join(td, "thermo.txt"))
         spring = os.path.join(td, "spring.txt")  # fix spring's record file, when it has one
         spring = np.loadtxt(spring, skiprows=1, ndmin=2) if os.path.exists(spring) else None
+        # files of computes (step + values per row)
+        extra = {f[:-4]: np.loadtxt(os.path.join(td, f), skiprows=1, ndmin=2) for f in os.listdir(td)
+                 if f.endswith(".txt") and f not in ("thermo.txt", "spring.txt")}
     save = {"run_in": np.array("\n".join(lines)), "masses": system.masses, "lo": system.lo,
             "hi": system.hi}
     if system.bonds is not None:
@@ -113,6 +116,8 @@ def run_reference(name, system, out_dir, nsteps=10, binary="gpudpd_single"):
         save[f"thermo_{h}"] = col
     if spring is not None:
         save["spring"] = spring
+    for k, rows in extra.items():
+        save[f"file_{k}"] = rows
     np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), **save)
 
 
@@ -134,6 +139,10 @@ def systems():
     # group fixes: spring on a probe cluster (record file every 2 steps), rvcm on all every
     # 3 steps (x and z), recenter of the probe every 4 steps
     out["probe_fixes"] = inputs.probe_fixes(L=9.0, seed=23, nsteps=10)
+    # particle walls: a frozen bottom wall, a top wall moved by fix move, the liquid kept
+    # between them by fix two_wall or fix wall_reflect; compute wall_contact on the bottom
+    out["wall_channel"] = inputs.wall_channel(seed=71, nsteps=10)
+    out["wall_reflect"] = inputs.wall_channel(seed=73, nsteps=10, walls="reflect")
     return out
 
 

@@ -226,3 +226,34 @@ def test_group_compute_checks(base):
     for text, msg in cases:
         code, err = _create(text, base)
         assert code == -1 and msg in err, (msg, err)
+
+
+def test_wall_fix_checks():
+    """fix move / wall_reflect / two_wall and compute wall_contact parameters
+    (src/fix/fix_move.cu:17-30, fix_wall_reflect.cu:17-80, fix_two_wall.cu:17-40,
+    src/compute/compute_wall_contact.cu:17-45)."""
+    from gpumdpd_b200 import inputs
+    s = inputs.wall_channel(L=6.0, Lz=10.0, seed=3)
+    t = s.run_in
+    code, err = _create(t, s)
+    assert code in (0, -8), err
+    r = inputs.wall_channel(L=6.0, Lz=10.0, seed=3, walls="reflect")
+    code, err = _create(r.run_in, r)
+    assert code in (0, -8), err
+    cases = [
+        (t.replace("move 0.5 0.0 0.0", "move 0.5 0.0"), "illegal fix_move command"),
+        (t.replace("two_wall bottom top z", "two_wall bottom top w"), "Invalid fix_two_wall direction"),
+        (t.replace("two_wall bottom top z", "two_wall bottom nowall z"), "Group 'nowall' not found"),
+        (t.replace("two_wall bottom top z", "two_wall bottom top"), "illegal fix_two_wall command"),
+        (t + "fix wr liquid wall_reflect 5.0 2.0 z\n", "lo_wall_pos should lower than hi_wall_pos"),
+        (t + "fix wr liquid wall_reflect -1.0 2.0 z\n", "Wall position is out of the box!"),
+        (t + "fix wr liquid wall_reflect 1.0 2.0 q\n", "Invalid fix_wall_reflect direction"),
+        (t.replace("wall_contact 1 bottom lo z 1.0", "wall_contact 1 bottom mid z 1.0"), "illegal compute_wall_contact"),
+        (t.replace("wall_contact 1 bottom lo z 1.0", "wall_contact 1 nowall lo z 1.0"), "Group 'nowall' not found"),
+        (t.replace("wall_contact 1 bottom lo z 1.0 wall_contact.txt", "wall_contact 1 bottom lo z 1.0"),
+         "illegal compute_wall_contact"),
+    ]
+    for text, msg in cases:
+        assert text != t
+        code, err = _create(text, s)
+        assert code == -1 and msg in err, (msg, err)

@@ -424,3 +424,43 @@ def test_group_computes_match_state(oracle_mod):
         f = states[int(row[0])]["f"][probe].sum(0)
         scale = np.abs(states[int(row[0])]["f"]).max()
         np.testing.assert_allclose(row[1:], f, atol=1e-4 * scale)
+
+
+@pytest.mark.parametrize("name", ["wall_channel", "wall_reflect"])
+def test_walls_vs_reference_and_oracle(oracle_mod, name):
+    """fix move (top wall), fix two_wall / wall_reflect (liquid) and compute wall_contact
+    (bottom wall) against the reference's own run and the oracle: states after steps 1,
+    4 and 10 (the run split so the post-integrate walls also follow the initial half kick
+    of a continued run) and the wall_contact rows."""
+    s, g = _golden_system(name)
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    tags = np.arange(1, s.n + 1)
+    e = _engine_from(s)
+    L = _box(e)
+    x0 = np.column_stack([g["s0_" + c] for c in "xyz"])
+    v0 = np.column_stack([g["s0_v" + c] for c in "xyz"])
+    e.run(0)
+    done = 0
+    for steps in (1, 4, 10):
+        e.run(steps - done)
+        done = steps
+        got = e.state()
+        o = oracle_mod.run(ff, tags, s.types, x0, v0, s.lo, L, 1, steps, 1)
+        refs = [(o["x"], o["v"], o["f"])]
+        if f"s{steps}_x" in g:
+            refs.append((np.column_stack([g[f"s{steps}_" + c] for c in "xyz"]),
+                         np.column_stack([g[f"s{steps}_v" + c] for c in "xyz"]),
+                         np.column_stack([g[f"s{steps}_f" + c] for c in "xyz"])))
+        for xw, vw, fw in refs:
+            dx = got["x"] - xw
+            dx -= L * np.round(dx / L)
+            assert np.abs(dx).max() < (2e-6 if steps == 1 else 5e-5), steps
+            assert np.abs(got["v"] - vw).max() < (2e-5 if steps == 1 else 5e-4), steps
+            assert force_err(got["f"], fw) < (2e-5 if steps == 1 else 3e-4), steps
+    top = s.types == 3
+    np.testing.assert_allclose(e.state()["v"][top], np.tile([0.5, 0.0, 0.0], (top.sum(), 1)))
+    wc = e.compute("cwc")
+    ref = g["file_wall_contact"]
+    np.testing.assert_array_equal(wc[:, 0], ref[:, 0])
+    assert wc[0, 1] == ref[0, 1]
+    assert np.abs(wc[:, 1] - ref[:, 1]).max() <= 1

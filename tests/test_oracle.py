@@ -5,7 +5,8 @@ import pytest
 
 from conftest import force_err, load_golden
 
-SYSTEMS = ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc", "angle_chains"]
+SYSTEMS = ["dpd_c1", "dpd_random_only", "mdpd_slab", "diblock", "mix_rc", "angle_chains", "wall_channel",
+           "wall_reflect"]
 
 
 def _state(g, step):
@@ -80,7 +81,8 @@ def test_step0_thermo_matches_reference(oracle_mod, name):
         assert th["angle_pe"][0] == pytest.approx(g["thermo_angle_pe"][0], rel=rtol, abs=2e-6)
 
 
-@pytest.mark.parametrize("name", ["dpd_c1", "mdpd_slab", "diblock", "dpd_c1_double", "angle_chains"])
+@pytest.mark.parametrize("name", ["dpd_c1", "mdpd_slab", "diblock", "dpd_c1_double", "angle_chains",
+                                  "wall_channel", "wall_reflect"])
 def test_trajectory_matches_reference(oracle_mod, name):
     """10 velocity-Verlet steps (src/main/utils.cuh:254-303) from the reference's step-0
     state: positions and forces at step 1 and 10 track the reference."""
