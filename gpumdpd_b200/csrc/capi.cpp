@@ -149,6 +149,13 @@ int dpd_read_restart(dpd_engine* h, const char* path)
     return h->eng.read_restart(path);
 }
 
+int dpd_compute_dump_open(dpd_engine* h, const char* id, const char* path)
+{
+    ENG_CHECK(h);
+    if (!id) return DPD_E_ARG;
+    return h->eng.compute_dump_open(id, path ? path : "");
+}
+
 int dpd_dump_close(dpd_engine* h)
 {
     ENG_CHECK(h);

@@ -701,6 +701,16 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             }
             if (ff.gcs.size() >= 4) return fail(err, line, "this engine takes at most 4 temp/rho/msd/tf computes");
             ff.gcs.push_back(c);
+        } else if (t[3] == "dump") {
+            // src/compute/compute_dump.cu:17-30
+            if (t.size() != 6 || !parse_int(t[4], 1, 4294967295ll, iv))
+                return fail(err, line, "illegal compute_dump command: compute ID groupID dump frequency filename");
+            ComputeDump c;
+            c.id = t[1];
+            c.frequency = (unsigned)iv;
+            c.file = t[5];
+            for (int ty : ff.groups[t[2]]) c.mask |= 1u << (ty - 1);
+            ff.cdumps.push_back(c);
         } else if (t[3] == "wall_contact") {
             // src/compute/compute_wall_contact.cu:17-45
             const std::string msg = "illegal compute_wall_contact command: compute ID groupID wall_contact frequency "
@@ -739,7 +749,7 @@ int parse_force_field(const RunInput& in, const SystemData& sys, ForceField& ff,
             if (!ff.rdfs.empty()) return fail(err, line, "only one rdf compute is supported");
             ff.rdfs.push_back(c);
         } else {
-            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp, rho, msd, tf, wall_contact and rdf)");
+            return fail(err, line, "Compute type '" + t[3] + "' not found! (this engine implements temp, rho, msd, tf, wall_contact, dump and rdf)");
         }
     }
     return DPD_OK;

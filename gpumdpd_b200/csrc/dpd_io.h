@@ -58,6 +58,14 @@ struct GroupCompute {
     double cutoff = 0;
 };
 
+// compute ID groupID dump frequency filename (src/compute/compute_dump.cu): wrapped
+// positions of the group every `frequency` steps from the zero step on.
+struct ComputeDump {
+    std::string id, file;
+    uint32_t mask = 0;
+    unsigned frequency = 1;
+};
+
 // Wall fixes (src/fix/fix_move.cu, fix_wall_reflect.cu, fix_two_wall.cu); several of each.
 struct FixMove {      // initial_integrate: v = V and x += V dt for the group
     uint32_t mask = 0;
@@ -119,6 +127,7 @@ struct ForceField {
     FixRvcm rvcm;
     FixRecenter recenter;
     std::vector<GroupCompute> gcs;
+    std::vector<ComputeDump> cdumps;
     std::vector<FixMove> moves;
     std::vector<FixWallReflect> reflects;
     std::vector<FixTwoWall> twowalls;

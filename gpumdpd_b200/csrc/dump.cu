@@ -1,5 +1,6 @@
 // dump.cu -- trajectory frames of replica 0 in the reference's all.trj format
-// (src/system/dump.cu:23-201): LAMMPS-style frames with id type x y z [fx fy fz]
+// (src/system/dump.cu:23-201), and the group frames of a dump compute
+// (src/compute/compute_dump.cu): LAMMPS-style frames with id type x y z [fx fy fz]
 // [vx vy vz], positions wrapped or unwrapped, nine decimals.  Frames are taken at the
 // reference's dump steps (step 0 when start is 0, from src/main/utils.cuh:198-202; then
 // step >= start with (step - start) % every == 0, :293-297).  Unlike the reference,
@@ -31,33 +32,42 @@ __global__ void k_snapshot(const int* parity, const float4* pos0, const float4* 
     ofrc[s] = force4[p0 + s];
 }
 
-bool Engine::dump_due(uint32_t step) const
+bool Engine::dump_due(const DumpWriter* w, uint32_t step)
 {
-    if (!dump_) return false;
-    if (step == 0) return dump_->start == 0;
-    return step >= dump_->start && (step - dump_->start) % dump_->every == 0;
+    if (step == 0) return w->start == 0;
+    return step >= w->start && (step - w->start) % w->every == 0;
 }
 
-uint32_t Engine::next_dump(uint32_t s) const
+uint32_t Engine::next_dump(const DumpWriter* w, uint32_t s)
 {
-    if (s == 0 && dump_->start == 0) return 0;
-    const uint64_t start = dump_->start, every = dump_->every;
+    if (s == 0 && w->start == 0) return 0;
+    const uint64_t start = w->start, every = w->every;
     const uint64_t d0 = std::max<uint64_t>(std::max<uint64_t>(s, 1), start);
     const uint64_t d = start + (d0 - start + every - 1) / every * every;
     return d > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)d;
 }
 
 // Format one frame (tag order) and append it to the file.  Lines are formatted in
-// parallel chunks and written in order.
-static bool write_frame(FILE* fp, const Replica& R, uint32_t step, const double* x, const int* img,
-                        const double* v, const double* f, bool unwrapped, bool force, bool vel)
+// parallel chunks and written in order.  A compute dump (w.group != 0) lists the group's
+// atoms with wrapped positions (src/compute/compute_dump.cu:60-130).
+static bool write_frame(FILE* fp, const Replica& R, const DumpWriter& w, uint32_t step, const double* x,
+                        const int* img, const double* v, const double* f)
 {
     const int n = R.sys.n_atoms;
+    auto member = [&](int i) { return !w.group || ((w.group >> (R.sys.type[i] - 1)) & 1u); };
+    int nout = n;
+    if (w.group) {
+        nout = 0;
+        for (int i = 0; i < n; i++) nout += member(i);
+    }
     fprintf(fp, "ITEM: TIMESTEP\n%u\n", step);
-    fprintf(fp, "ITEM: NUMBER OF ATOMS\n%d\n", n);
+    fprintf(fp, "ITEM: NUMBER OF ATOMS\n%d\n", nout);
     fprintf(fp, "ITEM: BOX BOUNDS pp pp pp\n");
     for (int k = 0; k < 3; k++) fprintf(fp, "%.9f %.9f\n", R.sys.lo[k], R.sys.hi[k]);
-    fprintf(fp, "ITEM: ATOMS id type x y z%s%s\n", force ? " fx fy fz" : "", vel ? " vx vy vz" : "");
+    if (w.group)
+        fprintf(fp, "ITEM: ATOMS id %stype x y z\n", w.mol ? "mol " : "");
+    else
+        fprintf(fp, "ITEM: ATOMS id type x y z%s%s\n", w.force ? " fx fy fz" : "", w.vel ? " vx vy vz" : "");
     const int nchunk = n < 65536 ? 1 : 64;
     std::vector<std::string> out(nchunk);
     parallel_for(nchunk, [&](int64_t c0, int64_t c1) {
@@ -67,15 +77,21 @@ static bool write_frame(FILE* fp, const Replica& R, uint32_t step, const double*
             s.reserve((size_t)(i1 - i0) * 128);
             char buf[320];
             for (int i = i0; i < i1; i++) {
+                if (!member(i)) continue;
                 double p[3];
                 for (int q = 0; q < 3; q++)
-                    p[q] = unwrapped ? x[3 * (size_t)i + q] + (double)img[3 * (size_t)i + q] * R.box_len[q]
-                                     : x[3 * (size_t)i + q];
-                int len = snprintf(buf, sizeof(buf), "%d %d %.9f %.9f %.9f", i + 1, R.sys.type[i], p[0], p[1], p[2]);
-                if (force)
+                    p[q] = w.unwrapped ? x[3 * (size_t)i + q] + (double)img[3 * (size_t)i + q] * R.box_len[q]
+                                       : x[3 * (size_t)i + q];
+                int len;
+                if (w.group && w.mol)
+                    len = snprintf(buf, sizeof(buf), "%d %d %d %.9f %.9f %.9f", i + 1,
+                                   R.sys.mol.empty() ? 0 : R.sys.mol[i], R.sys.type[i], p[0], p[1], p[2]);
+                else
+                    len = snprintf(buf, sizeof(buf), "%d %d %.9f %.9f %.9f", i + 1, R.sys.type[i], p[0], p[1], p[2]);
+                if (w.force)
                     len += snprintf(buf + len, sizeof(buf) - len, " %.9f %.9f %.9f", f[3 * (size_t)i],
                                     f[3 * (size_t)i + 1], f[3 * (size_t)i + 2]);
-                if (vel)
+                if (w.vel)
                     len += snprintf(buf + len, sizeof(buf) - len, " %.9f %.9f %.9f", v[3 * (size_t)i],
                                     v[3 * (size_t)i + 1], v[3 * (size_t)i + 2]);
                 buf[len++] = '\n';
@@ -88,17 +104,30 @@ static bool write_frame(FILE* fp, const Replica& R, uint32_t step, const double*
     return fflush(fp) == 0;
 }
 
+static void free_writer(DumpWriter* w)
+{
+    if (w->file) fclose(w->file);
+    w->file = nullptr;
+    if (w->copy) cudaStreamSynchronize(w->copy);
+    for (int k = 0; k < 2; k++) {
+        for (void* p : {(void*)w->dpos[k], (void*)w->dvel[k], (void*)w->dfrc[k], (void*)w->dimg[k], (void*)w->dfo[k]})
+            if (p) cudaFree(p);
+        for (void* p : {(void*)w->hpos[k], (void*)w->hvel[k], (void*)w->hfrc[k], (void*)w->himg[k], (void*)w->hfo[k]})
+            if (p) cudaFreeHost(p);
+        if (w->taken[k]) cudaEventDestroy(w->taken[k]);
+        if (w->copied[k]) cudaEventDestroy(w->copied[k]);
+    }
+    if (w->copy) cudaStreamDestroy(w->copy);
+}
+
 int Engine::dump_open(const std::string& path, uint32_t start, uint32_t every, bool unwrapped, bool force,
                       bool vel)
 {
-    if (dump_) {
-        err = "a trajectory dump is already open";
-        return DPD_E_STATE;
-    }
-    if (every == 0 || reps_.empty()) {
-        err = "dump frequency must be positive";
-        return DPD_E_ARG;
-    }
+    for (auto& w : dumps_)
+        if (w->id.empty()) {
+            err = "a trajectory dump is already open";
+            return DPD_E_STATE;
+        }
     std::unique_ptr<DumpWriter> w(new DumpWriter());
     w->path = path;
     w->start = start;
@@ -106,25 +135,52 @@ int Engine::dump_open(const std::string& path, uint32_t start, uint32_t every, b
     w->unwrapped = unwrapped;
     w->force = force;
     w->vel = vel;
-    w->file = fopen(path.c_str(), "w");
+    return dump_start(std::move(w));
+}
+
+int Engine::compute_dump_open(const std::string& id, const std::string& path)
+{
+    if (reps_.empty()) return DPD_E_STATE;
+    const Replica& R = reps_[0];
+    const ComputeDump* c = nullptr;
+    for (auto& q : R.ff.cdumps)
+        if (q.id == id) c = &q;
+    if (!c) {
+        err = "no dump compute with ID " + id;
+        return DPD_E_ARG;
+    }
+    for (auto& w : dumps_)
+        if (w->id == id) {
+            err = "the dump compute " + id + " is already open";
+            return DPD_E_STATE;
+        }
+    std::unique_ptr<DumpWriter> w(new DumpWriter());
+    w->path = path.empty() ? c->file : path;
+    w->id = id;
+    w->start = 0;
+    w->every = c->frequency;
+    w->group = c->mask ? c->mask : 0xFFFFFFFFu;
+    w->mol = R.in.atom_style != 0;
+    return dump_start(std::move(w));
+}
+
+// open the file, allocate the two snapshot slots and start the writer thread
+int Engine::dump_start(std::unique_ptr<DumpWriter> w)
+{
+    if (w->every == 0 || reps_.empty()) {
+        err = "dump frequency must be positive";
+        return DPD_E_ARG;
+    }
+    w->file = fopen(w->path.c_str(), "w");
     if (!w->file) {
-        err = "cannot open dump file " + path;
+        err = "cannot open dump file " + w->path;
         return DPD_E_IO;
     }
     const RepDesc& d = reps_[0].desc;
     w->ns = d.p_cap_end - d.p_begin;
     const size_t n = (size_t)w->ns;
     auto fail = [&](cudaError_t e, const char* what) {
-        fclose(w->file);
-        for (int k = 0; k < 2; k++) {
-            for (void* p : {(void*)w->dpos[k], (void*)w->dvel[k], (void*)w->dfrc[k], (void*)w->dimg[k], (void*)w->dfo[k]})
-                if (p) cudaFree(p);
-            for (void* p : {(void*)w->hpos[k], (void*)w->hvel[k], (void*)w->hfrc[k], (void*)w->himg[k], (void*)w->hfo[k]})
-                if (p) cudaFreeHost(p);
-            if (w->taken[k]) cudaEventDestroy(w->taken[k]);
-            if (w->copied[k]) cudaEventDestroy(w->copied[k]);
-        }
-        if (w->copy) cudaStreamDestroy(w->copy);
+        free_writer(w.get());
         return cuda_fail(e, what);
     };
     cudaError_t e;
@@ -167,8 +223,7 @@ int Engine::dump_open(const std::string& path, uint32_t start, uint32_t every, b
                                       spring ? wp->hfo[slot]->spring_a : nullptr, x.data(), v.data(), img.data(),
                                       f.data())) {
                 error = "corrupt tag in a dump snapshot";
-            } else if (!write_frame(wp->file, *R, wp->step[slot], x.data(), img.data(), v.data(), f.data(),
-                                    wp->unwrapped, wp->force, wp->vel)) {
+            } else if (!write_frame(wp->file, *R, *wp, wp->step[slot], x.data(), img.data(), v.data(), f.data())) {
                 error = "cannot write dump file " + wp->path;
             }
             {
@@ -179,13 +234,12 @@ int Engine::dump_open(const std::string& path, uint32_t start, uint32_t every, b
             wp->cv.notify_all();
         }
     });
-    dump_ = std::move(w);
+    dumps_.push_back(std::move(w));
     return DPD_OK;
 }
 
-int Engine::dump_frame(uint32_t step)
+int Engine::dump_frame(DumpWriter* w, uint32_t step)
 {
-    DumpWriter* w = dump_.get();
     const int slot = w->next_slot;
     {
         std::unique_lock<std::mutex> lk(w->mu);
@@ -229,34 +283,27 @@ int Engine::dump_frame(uint32_t step)
 
 int Engine::dump_close()
 {
-    if (!dump_) return DPD_OK;
-    DumpWriter* w = dump_.get();
-    {
-        std::lock_guard<std::mutex> lk(w->mu);
-        w->stop = true;
-    }
-    w->cv.notify_all();
-    if (w->thread.joinable()) w->thread.join();
     int rc = DPD_OK;
-    if (!w->error.empty()) {
-        err = w->error;
-        rc = DPD_E_IO;
+    for (auto& wu : dumps_) {
+        DumpWriter* w = wu.get();
+        {
+            std::lock_guard<std::mutex> lk(w->mu);
+            w->stop = true;
+        }
+        w->cv.notify_all();
+        if (w->thread.joinable()) w->thread.join();
+        if (!w->error.empty() && rc == DPD_OK) {
+            err = w->error;
+            rc = DPD_E_IO;
+        }
+        if (w->file && fclose(w->file) != 0 && rc == DPD_OK) {
+            err = "cannot close dump file " + w->path;
+            rc = DPD_E_IO;
+        }
+        w->file = nullptr;
+        free_writer(w);
     }
-    if (w->file && fclose(w->file) != 0 && rc == DPD_OK) {
-        err = "cannot close dump file " + w->path;
-        rc = DPD_E_IO;
-    }
-    if (w->copy) cudaStreamSynchronize(w->copy);
-    for (int k = 0; k < 2; k++) {
-        for (void* p : {(void*)w->dpos[k], (void*)w->dvel[k], (void*)w->dfrc[k], (void*)w->dimg[k], (void*)w->dfo[k]})
-            if (p) cudaFree(p);
-        for (void* p : {(void*)w->hpos[k], (void*)w->hvel[k], (void*)w->hfrc[k], (void*)w->himg[k], (void*)w->hfo[k]})
-            if (p) cudaFreeHost(p);
-        cudaEventDestroy(w->taken[k]);
-        cudaEventDestroy(w->copied[k]);
-    }
-    if (w->copy) cudaStreamDestroy(w->copy);
-    dump_.reset();
+    dumps_.clear();
     return rc;
 }
 

@@ -19,9 +19,12 @@ namespace dpd {
 
 struct DumpWriter {
     std::string path;
+    std::string id;                    // "" for the dump command, else the compute's ID
     FILE* file = nullptr;
     uint32_t start = 0, every = 1;
     bool unwrapped = false, force = false, vel = false;
+    uint32_t group = 0;                // compute dump: the group's types (0 = every atom)
+    bool mol = false;                  // compute dump of a molecular system: id mol type x y z
     int ns = 0;                        // slots of replica 0 (a multiple of 32)
     float4 *dpos[2] = {}, *dvel[2] = {}, *dfrc[2] = {};
     int4* dimg[2] = {};

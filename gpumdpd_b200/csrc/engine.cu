@@ -868,7 +868,7 @@ int Engine::run_async(uint32_t nsteps)
     uint32_t s = first;
     for (;;) {
         uint32_t end = last;
-        if (dump_) end = std::min(end, next_dump(s));
+        for (auto& w : dumps_) end = std::min(end, next_dump(w.get(), s));
         k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, end, zero ? 1 : 0,
                                              zero || force_build_ ? 1 : 0, b_.build_flag, b_.phase);
         force_build_ = false;
@@ -876,10 +876,11 @@ int Engine::run_async(uint32_t nsteps)
         CK(cudaGetLastError());
         for (uint32_t k = s; k <= end; k++) CK(cudaGraphLaunch(graph_, stream_));
         zero = false;
-        if (dump_ && dump_due(end)) {
-            int e = dump_frame(end);
-            if (e) return e;
-        }
+        for (auto& w : dumps_)
+            if (dump_due(w.get(), end)) {
+                int e = dump_frame(w.get(), end);
+                if (e) return e;
+            }
         if (end == last) break;
         s = end + 1;
     }

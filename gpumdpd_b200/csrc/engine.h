@@ -109,7 +109,9 @@ public:
     // thread from snapshots while the device keeps stepping (dump.cu)
     int dump_open(const std::string& path, uint32_t start, uint32_t every, bool unwrapped, bool force,
                   bool vel);
-    int dump_close();
+    // the frames of a `compute ID group dump freq file` of replica 0 (to its file, or path)
+    int compute_dump_open(const std::string& id, const std::string& path);
+    int dump_close();  // every open trajectory
     // exact checkpoint of every replica's FP32 state, forces and step counters; resume
     // into an engine made from the same run.in and system (restart.cu)
     int write_restart(const std::string& path);
@@ -143,9 +145,10 @@ private:
     void enqueue_build(cudaStream_t s, bool list = true);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
-    int dump_frame(uint32_t step);
-    bool dump_due(uint32_t step) const;
-    uint32_t next_dump(uint32_t s) const;
+    int dump_frame(DumpWriter* w, uint32_t step);
+    int dump_start(std::unique_ptr<DumpWriter> w);
+    static bool dump_due(const DumpWriter* w, uint32_t step);
+    static uint32_t next_dump(const DumpWriter* w, uint32_t s);
     int cur_parity();
     int staging();
     int cuda_fail(cudaError_t e, const char* what);
@@ -180,7 +183,7 @@ private:
     bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
-    std::unique_ptr<DumpWriter> dump_;
+    std::vector<std::unique_ptr<DumpWriter>> dumps_;
 };
 
 int make_replica(const std::string& run_in, const std::string& data_path, const std::string& base_dir,

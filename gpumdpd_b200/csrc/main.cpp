@@ -37,7 +37,8 @@ int main(int argc, char** argv)
     std::string out_data, spring_file;
     bool dump = false;
     struct Comp { std::string id, style, file; };
-    std::vector<Comp> comps;  // temp, rho, msd, tf computes and their files
+    std::vector<Comp> comps;  // temp, rho, msd, tf, wall_contact computes and their files
+    std::vector<std::string> cdumps;  // dump computes
     std::istringstream ls(text);
     std::string line;
     while (std::getline(ls, line)) {
@@ -53,8 +54,10 @@ int main(int argc, char** argv)
         if (k == "compute") {
             std::vector<std::string> w;
             while (t >> a) w.push_back(a);
-            if (w.size() >= 3 && (w[2] == "temp" || w[2] == "rho" || w[2] == "msd" || w[2] == "tf"))
+            if (w.size() >= 3 && (w[2] == "temp" || w[2] == "rho" || w[2] == "msd" || w[2] == "tf" ||
+                                  w[2] == "wall_contact"))
                 comps.push_back({w[0], w[2], w.back()});
+            if (w.size() >= 3 && w[2] == "dump") cdumps.push_back(w[0]);
         }
         if (k == "fix") {
             // fix ID groupID spring k x y z r0 [file_name file_frequency]
@@ -69,8 +72,14 @@ int main(int argc, char** argv)
         dpd_destroy(eng);
         return 1;
     }
+    for (const std::string& id : cdumps)
+        if (dpd_compute_dump_open(eng, id.c_str(), nullptr)) {
+            fprintf(stderr, "ERROR: %s\n", dpd_last_error(eng));
+            dpd_destroy(eng);
+            return 1;
+        }
     e = dpd_run(eng, nsteps);
-    if (!e && dump) e = dpd_dump_close(eng);
+    if (!e && (dump || !cdumps.empty())) e = dpd_dump_close(eng);
     if (e) {
         fprintf(stderr, "ERROR: %s\n", dpd_last_error(eng));
         dpd_destroy(eng);

@@ -88,6 +88,12 @@ class Engine:
         flags = (1 if unwrapped else 0) | (2 if force else 0) | (4 if vel else 0)
         _check(self.lib.dpd_dump_open(self.h, str(path).encode(), int(start), int(every), flags), self.lib, self.h)
 
+    def compute_dump_open(self, compute_id, path=None):
+        """Write the frames of the run.in's `compute ID group dump freq file` (to `path`, or
+        the compute's file)."""
+        _check(self.lib.dpd_compute_dump_open(self.h, str(compute_id).encode(),
+                                              str(path).encode() if path else None), self.lib, self.h)
+
     def dump_close(self):
         _check(self.lib.dpd_dump_close(self.h), self.lib, self.h)
 

@@ -128,6 +128,12 @@ int dpd_get_thermo(dpd_engine* eng, dpd_thermo* rows, int max_rows, int* n_rows)
 #define DPD_DUMP_FORCE 2
 #define DPD_DUMP_VEL 4
 int dpd_dump_open(dpd_engine* eng, const char* path, int64_t start, int64_t every, int flags);
+/* The frames of the run.in's `compute ID groupID dump frequency filename`
+ * (src/compute/compute_dump.cu:40-130): the group's atoms, `id type x y z` (atom_style
+ * atomic) or `id mol type x y z`, wrapped positions, every frequency steps from the zero
+ * step on, to `path` (NULL: the compute's file name).  Written like dpd_dump_open's. */
+int dpd_compute_dump_open(dpd_engine* eng, const char* id, const char* path);
+/* Wait for the last frame of every open trajectory and close them. */
 int dpd_dump_close(dpd_engine* eng);
 
 /* Exact checkpoint and resume (new; the reference restarts from a write_data file at

@@ -183,3 +183,66 @@ def test_engine_dump_frames_match_states(tmp_path):
     dx = a["x"] - b["x"]
     dx -= L * np.round(dx / L)
     assert np.abs(dx).max() < 1e-4
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="gpudpd_b200 not built")
+@pytest.mark.parametrize("walls", ["two_wall", "reflect"])
+def test_cli_walls_match_reference_executable(walls):
+    """Particle walls (fix move, two_wall / wall_reflect), compute wall_contact and a group
+    dump compute of the liquid, against the reference executable."""
+    from gpumdpd_b200 import inputs
+    s = inputs.wall_channel(seed=81, nsteps=10, thermo=1, walls=walls)
+    run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in)
+    run_in += "compute cd liquid dump 5 liquid.trj\n"
+    files = ["thermo.txt", "wall_contact.txt", "liquid.trj"]
+    ours = _run(CLI, s, run_in, files)
+    assert set(ours) == set(files)
+    fr = parse_trj_text(ours["liquid.trj"])
+    assert sorted(fr) == [0, 5, 10]
+    liquid = np.flatnonzero(s.types == 1) + 1
+    for st, f in fr.items():
+        assert f["cols"] == ["id", "type", "x", "y", "z"]
+        np.testing.assert_array_equal(f["id"], liquid)
+    h, wc = _thermo(ours["wall_contact.txt"])
+    assert h == ["step", "wall_contact"] and list(wc["step"]) == list(range(11))
+    if not os.path.exists(STOCK):
+        pytest.skip("reference build (oracle/build_ref.sh SINGLE) not present")
+    ref = _run(STOCK, s, run_in, files)
+    rh, rwc = _thermo(ref["wall_contact.txt"])
+    assert rh == h
+    assert wc["wall_contact"][0] == rwc["wall_contact"][0]
+    assert np.abs(wc["wall_contact"] - rwc["wall_contact"]).max() <= 1
+    rfr = parse_trj_text(ref["liquid.trj"])
+    assert sorted(rfr) == sorted(fr)
+    for st in fr:
+        np.testing.assert_array_equal(rfr[st]["id"], fr[st]["id"])
+        d = np.column_stack([fr[st][c] - rfr[st][c] for c in "xyz"])
+        d -= (s.hi - s.lo) * np.round(d / (s.hi - s.lo))
+        assert np.abs(d).max() < (2e-6 if st == 0 else 5e-5), st
+    _, th = _thermo(ours["thermo.txt"])
+    _, rth = _thermo(ref["thermo.txt"])
+    assert th["temp"][0] == pytest.approx(rth["temp"][0], rel=2e-5)
+    np.testing.assert_allclose(th["temp"], rth["temp"], rtol=2e-3)
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="gpudpd_b200 not built")
+def test_cli_molecular_compute_dump():
+    """A dump compute of a bonded system lists id mol type x y z (compute_dump.cu:110-128)."""
+    from gpumdpd_b200 import inputs
+    s = inputs.diblock_melt(L=6.0, seed=83, nsteps=4, thermo=2)
+    run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in)
+    run_in = run_in.replace("group all type 1 2", "group all type 1 2\ngroup heads type 1")
+    run_in += "compute cd heads dump 2 heads.trj\n"
+    ours = _run(CLI, s, run_in, ["heads.trj"])
+    fr = parse_trj_text(ours["heads.trj"])
+    assert sorted(fr) == [0, 2, 4]
+    assert fr[0]["cols"] == ["id", "mol", "type", "x", "y", "z"]
+    np.testing.assert_array_equal(fr[0]["id"], np.flatnonzero(s.types == 1) + 1)
+    np.testing.assert_array_equal(fr[0]["mol"], s.mol[s.types == 1])
+    if os.path.exists(STOCK):
+        ref = _run(STOCK, s, run_in, ["heads.trj"])
+        rfr = parse_trj_text(ref["heads.trj"])
+        assert sorted(rfr) == sorted(fr)
+        np.testing.assert_array_equal(rfr[0]["mol"], fr[0]["mol"])
+        np.testing.assert_allclose(np.column_stack([fr[0][c] for c in "xyz"]),
+                                   np.column_stack([rfr[0][c] for c in "xyz"]), atol=2e-6)
