@@ -184,7 +184,7 @@ def run_ours(args, world, rank, local):
     system = make_system(args)
     eng = Engine(system.run_in, system=system.c_system())
     pair_variant = 8 if args.pair_variant is None else args.pair_variant
-    eng.set_tuning(pair_variant=pair_variant, cell_order=1)
+    eng.set_tuning(pair_variant=pair_variant, cell_order=1, build_variant=args.build_variant)
     eng.run(0)
     eng.run(args.warmup)
     ls = eng.list_stats()
@@ -243,6 +243,7 @@ def run_ours(args, world, rank, local):
                    "n_bonds": 0 if system.bonds is None else len(system.bonds), "box": system.box.tolist(),
                    "dt": 0.04, "skin": args.skin, "mean_half_list": ls["mean_half_list"],
                    "list_builds_per_step": builds_per_step, "pair_variant": pair_variant,
+                   "build_variant": args.build_variant,
                    "tuned": tuned, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state+list > 1 GB)"},
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -252,9 +253,10 @@ def run_ours(args, world, rank, local):
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "clocks": clk.summary(),
-        # per step: 9 list-build kernels (each returns at once unless a build is flagged),
-        # the pair kernel(s), integrate, advance; plus 2 before the graph
-        "gpu_launches": int(args.steps * (11 + (2 if pair_variant in (7, 8) else 1)) + 2),
+        # per step: 7 list-build kernels (each returns at once unless a build is flagged),
+        # the pair kernel(s), the integrate pair (non-log steps + log steps), advance; plus
+        # 2 before the graph
+        "gpu_launches": int(args.steps * (10 + (2 if pair_variant in (7, 8, 9) else 1)) + 2),
         "impl": "ours",
     }
     del th, st2
@@ -499,6 +501,8 @@ def main():
     ap.add_argument("--tune", action="store_true", help="run the autotuner first (skin and pair schedule)")
     ap.add_argument("--pair-variant", type=int, default=None,
                     help="pair-kernel schedule (default: the engine's choice)")
+    ap.add_argument("--build-variant", type=int, default=0,
+                    help="list-build kernel (0: ranges in registers; 1, 2: in shared memory)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and served lines")
     ap.add_argument("--slab-steps", type=int, default=20000)

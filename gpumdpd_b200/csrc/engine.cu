@@ -720,6 +720,9 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
     } else if (variant == 8) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5>, grid, 256, s, a);
         pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 4), 256, s, a);
+    } else if (variant == 9) {
+        pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5, true>, grid, 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 4), 256, s, a);
     }
     else pdl_launch(k_pair_q<STYLE, BONDS, 4, false>, grid, 256, s, a);
 }
@@ -730,7 +733,7 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
 // warp schedule, 4 blocks/SM; 5: flattened, 3 blocks/SM; 6: the flattened schedule with
 // the list build fused into it (DPD; mDPD falls back to 4); 7 and 8 (the default): the
 // flattened schedule as two launches, non-log steps without FP64 sums at 6 (7) or 5 (8)
-// blocks/SM, log steps at 4
+// blocks/SM, log steps at 4; 9: as 8 with the i-side forces summed per owner in the warp
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -752,7 +755,11 @@ void Engine::enqueue_build(cudaStream_t s, bool list)
     pdl_launch(k_scan_add, gc, 256, s, ba);
     pdl_launch(k_permute, gp, 256, s, ba);
     pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
-    if (list) pdl_launch(k_build_nlist, gp, 256, s, ba);
+    if (list) {
+        if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
+        else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);
+        else pdl_launch(k_build_nlist, gp, 256, s, ba);
+    }
 }
 
 void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
@@ -1438,9 +1445,9 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 8 || t->cell_order < 0 || t->cell_order > 1 ||
-        t->pair_block < 0) {
-        err = "dpd_set_tuning: pair_variant must be 0..6, cell_order 0 or 1";
+    if (t->pair_variant < 0 || t->pair_variant > 9 || t->cell_order < 0 || t->cell_order > 1 ||
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 2) {
+        err = "dpd_set_tuning: pair_variant must be 0..9, build_variant 0..2, cell_order 0 or 1";
         return DPD_E_ARG;
     }
     tune_ = *t;

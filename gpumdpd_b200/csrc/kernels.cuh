@@ -438,3 +438,72 @@ __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
     if (!build_on(a)) return;
     build_nlist_slot(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
+
+// The same list with the 14 cell ranges kept in shared memory instead of registers
+// ([stencil cell][thread], conflict-free): fewer registers per thread, so more warps per
+// SM hide the candidate-gather latency.  Identical entries in identical order.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_build_nlist_s(BuildArgs a)
+{
+    __shared__ int2 s_rng[14][256];
+    griddep_wait();
+    if (!build_on(a)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int tid = threadIdx.x;
+    if (s >= a.P) return;
+    const int r = a.warp_rep[s >> 5];
+    const RepDesc& d = a.reps[r];
+    if (s >= d.p_end || a.rstate[r].step > a.rstate[r].target) {
+        a.ncount[s] = 0;
+        return;
+    }
+    const float4* pos = a.buf.pos[*a.parity];
+    const float4 pi = pos[s];
+    const int code = __float_as_int(pi.w);
+    const int cx = cell_x(code), cy = cell_y(code), cz = cell_z(code);
+    const int ncx = d.nc[0], ncy = d.nc[1], ncz = d.nc[2];
+    for (int st = 0; st < 14; st++) {
+        const int ox = st ? c_half[st - 1][0] : 0, oy = st ? c_half[st - 1][1] : 0, oz = st ? c_half[st - 1][2] : 0;
+        int nx = cx + ox; nx += nx < 0 ? ncx : 0; nx -= nx >= ncx ? ncx : 0;
+        int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
+        int nz = cz + oz; nz += nz < 0 ? ncz : 0; nz -= nz >= ncz ? ncz : 0;
+        const int key = d.c_begin + __ldg(a.crank + d.c_begin + (nx * ncy + ny) * ncz + nz);
+        s_rng[st][tid] = make_int2(st ? __ldg(a.cstart + key) : s + 1, __ldg(a.cstart + key + 1));
+    }
+    const float cut2 = d.cut2;
+    const float wx = d.w[0], wy = d.w[1], wz = d.w[2];
+    int* out = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+    int count = 0;
+    for (int st = 0; st < 14; st++) {
+        const int ox = st ? c_half[st - 1][0] : 0, oy = st ? c_half[st - 1][1] : 0, oz = st ? c_half[st - 1][2] : 0;
+        const float sx = __int2float_rn(-ox) * wx, sy = __int2float_rn(-oy) * wy, sz = __int2float_rn(-oz) * wz;
+        const int tagbits = ((1 - ox) * 9 + (1 - oy) * 3 + (1 - oz)) << DPD_CODE_SHIFT;
+        const int2 rg = s_rng[st][tid];
+        for (int j0 = rg.x; j0 < rg.y; j0 += 4) {
+            float4 pj[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (j0 + u < rg.y) pj[u] = pos[j0 + u];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (j0 + u < rg.y) {
+                    const float dx = __fadd_rn(__fsub_rn(pi.x, pj[u].x), sx);
+                    const float dy = __fadd_rn(__fsub_rn(pi.y, pj[u].y), sy);
+                    const float dz = __fadd_rn(__fsub_rn(pi.z, pj[u].z), sz);
+                    float r2 = __fmul_rn(dx, dx);
+                    r2 = __fmaf_rn(dy, dy, r2);
+                    r2 = __fmaf_rn(dz, dz, r2);
+                    if (r2 <= cut2) {
+                        if (count < a.nmax) out[(size_t)count * 32] = (j0 + u) | tagbits;
+                        count++;
+                    }
+                }
+            }
+        }
+    }
+    if (count > a.nmax) {
+        atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+        count = a.nmax;
+    }
+    a.ncount[s] = count;
+}

@@ -535,7 +535,10 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 // LOGM: 2 = any step; 0 = non-log steps only (no FP64 sums: fewer registers, more
 // warps per SM); 1 = log steps only.  0 and 1 are launched together, each returning at
 // once on the other kind of step.
-template <int STYLE, bool BONDS, int LOGM = 2>
+// SEG: the i-side forces of an iteration are summed per owner in registers first (the flat
+// entries of one owner sit in consecutive lanes: a segmented warp scan), so one float4
+// reduction per owner and iteration reaches L2 instead of one per pair.
+template <int STYLE, bool BONDS, int LOGM = 2, bool SEG = false>
 __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
 {
     __shared__ int s_start[8][33];
@@ -611,6 +614,7 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
             if (STYLE == 1) rho_j = __ldg(a.rho + j);
         }
         if (t0 + 32 + lane < total) locate(t0 + 32 + lane, l_nx, ent_nx);
+        float ix = 0.0f, iy = 0.0f, iz = 0.0f;
         if (valid) {
             const float4 pil = s_pi[warp][l];
             float dx, dy, dz;
@@ -624,9 +628,34 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
                                     : pair_force<STYLE, false>(crow, r2, dx, dy, dz, vv, vj, s_rho[warp][l], rho_j, seed, step, fx, fy, fz, accv);
                 if (ok) {
                     atomicAdd(&a.force4[j], make_float4(-fx, -fy, -fz, 0.0f));
-                    atomicAdd(&a.force4[wbase + l], make_float4(fx, fy, fz, 0.0f));
+                    if (SEG) {
+                        ix = fx;
+                        iy = fy;
+                        iz = fz;
+                    } else {
+                        atomicAdd(&a.force4[wbase + l], make_float4(fx, fy, fz, 0.0f));
+                    }
                 }
             }
+        }
+        if (SEG) {
+            // lanes past the end get keys of their own: they never join a segment
+            const int key = valid ? l : 32 + lane;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float tx = __shfl_up_sync(0xffffffffu, ix, o);
+                const float ty = __shfl_up_sync(0xffffffffu, iy, o);
+                const float tz = __shfl_up_sync(0xffffffffu, iz, o);
+                const int tk = __shfl_up_sync(0xffffffffu, key, o);
+                if (lane >= o && tk == key) {
+                    ix += tx;
+                    iy += ty;
+                    iz += tz;
+                }
+            }
+            const int nk = __shfl_down_sync(0xffffffffu, key, 1);
+            if (valid && (lane == 31 || nk != key) && (ix != 0.0f || iy != 0.0f || iz != 0.0f))
+                atomicAdd(&a.force4[wbase + l], make_float4(ix, iy, iz, 0.0f));
         }
     }
     if (BONDS && work) {
@@ -649,17 +678,17 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat(StepArgs a)
     pair_flat_warp<STYLE, BONDS>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-template <int STYLE, bool BONDS, int LOGM, int MINB>
+template <int STYLE, bool BONDS, int LOGM, int MINB, bool SEG = false>
 __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 {
     griddep_wait();
-    pair_flat_warp<STYLE, BONDS, LOGM>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    pair_flat_warp<STYLE, BONDS, LOGM, SEG>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // The log-step half of the split schedule as a small grid-stride launch: every block
 // first checks whether any replica logs this step (the common answer is no, and then the
 // launch costs one wave of tiny blocks instead of a full grid of early exits).
-template <int STYLE, bool BONDS>
+template <int STYLE, bool BONDS, bool SEG = false>
 __global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
 {
     griddep_wait();
@@ -671,7 +700,7 @@ __global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-        pair_flat_warp<STYLE, BONDS, 1>(a, vb * 256 + threadIdx.x);
+        pair_flat_warp<STYLE, BONDS, 1, SEG>(a, vb * 256 + threadIdx.x);
         __syncwarp();  // the warp's shared slots are reused by the next virtual block
     }
 }

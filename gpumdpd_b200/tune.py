@@ -13,7 +13,7 @@ import re
 from .engine import Batch, Engine
 
 SKINS = (0.0, 0.1, 0.2, 0.3)
-VARIANTS = (1, 4, 6, 8)
+VARIANTS = (1, 4, 6, 8, 9)
 
 
 def with_skin(run_in, skin):

@@ -85,9 +85,13 @@ typedef struct dpd_tuning {
                               4-5 = flattened warp schedule (small skins),
                               6 = flattened with the list build fused (DPD),
                               7-8 = flattened, log and non-log steps split (8 is
-                              the default)                                        */
+                              the default), 9 = as 8 with the i-side forces summed
+                              per owner in the warp before the reduction         */
     int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
-    int reserved[5];
+    int build_variant;     /* list build: 0 = cell ranges in registers, 4
+                              blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
+                              8 blocks/SM                                         */
+    int reserved[4];
 } dpd_tuning;
 
 /* ---- plain engine: replaces main()/read_info/preprocess/zero_step/simulation

@@ -93,7 +93,7 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 @pytest.mark.parametrize("name", ["mdpd_slab", "diblock", "mix_rc"])
 def test_pair_schedules_agree_with_oracle(oracle_mod, name, variant):
     """Every pair-kernel schedule the tuner may pick gives the oracle's step-0 forces and
@@ -464,3 +464,22 @@ def test_walls_vs_reference_and_oracle(oracle_mod, name):
     np.testing.assert_array_equal(wc[:, 0], ref[:, 0])
     assert wc[0, 1] == ref[0, 1]
     assert np.abs(wc[:, 1] - ref[:, 1]).max() <= 1
+
+
+@pytest.mark.parametrize("build_variant", [1, 2])
+@pytest.mark.parametrize("name", ["dpd", "diblock", "small_box"])
+def test_build_variants_give_the_same_list(oracle_mod, name, build_variant):
+    """The list-build kernels with the cell ranges in shared memory build the same half
+    list (bit-exact tag-pair sets) and the same step-0 forces as the register version."""
+    s = _systems()[name]
+    a = _engine_from(s)
+    a.run(0)
+    b = _engine_from(s)
+    b.set_tuning(pair_variant=8, cell_order=1, build_variant=build_variant)
+    b.run(0)
+    got = set(map(tuple, b.neighbors().tolist()))
+    assert got == set(map(tuple, a.neighbors().tolist()))
+    assert force_err(b.state()["f"], a.state()["f"]) < 1e-5
+    b.run(5)
+    a.run(5)
+    assert force_err(b.state()["f"], a.state()["f"]) < 1e-4
