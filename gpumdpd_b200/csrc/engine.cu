@@ -883,6 +883,10 @@ int Engine::run_async(uint32_t nsteps)
         CK(cudaGetLastError());
         for (uint32_t k = s; k <= end; k++) CK(cudaGraphLaunch(graph_, stream_));
         zero = false;
+        // the host's step counter follows each segment, so a failed frame write leaves
+        // it where the device stopped
+        next_step_ = end + 1;
+        zero_pending_ = false;
         for (auto& w : dumps_)
             if (dump_due(w.get(), end)) {
                 int e = dump_frame(w.get(), end);
@@ -891,8 +895,6 @@ int Engine::run_async(uint32_t nsteps)
         if (end == last) break;
         s = end + 1;
     }
-    next_step_ = last + 1;
-    zero_pending_ = false;
     return DPD_OK;
 }
 
