@@ -40,6 +40,15 @@ def workload_name(args):
     return f"{args.workload}_skin{args.skin}"
 
 
+def build_launches(system, skin):
+    """Kernels of one list build: counting pass, scan (one launch when the cells fit one
+    4096-element block, else three), permutation (with the parity flip up to 1184 blocks
+    of 256 slots, else a separate flip), list."""
+    cells = int(np.prod(np.floor(system.box / (1.0 + skin)))) + 1
+    slots = system.n + 31
+    return 3 + (1 if cells <= 4096 else 3) + (0 if (slots + 255) // 256 <= 148 * 8 else 1)
+
+
 def make_system(args):
     from gpumdpd_b200 import inputs
     if args.workload == "melt":
@@ -253,10 +262,11 @@ def run_ours(args, world, rank, local):
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "clocks": clk.summary(),
-        # per step: 7 list-build kernels (each returns at once unless a build is flagged),
-        # the pair kernel(s), the integrate pair (non-log steps + log steps), advance; plus
-        # 2 before the graph
-        "gpu_launches": int(args.steps * (10 + (2 if pair_variant in (7, 8, 9) else 1)) + 2),
+        # per step: the list-build kernels (counting pass, 1 or 3 scan launches, permutation,
+        # list; each returns at once unless a build is flagged), the pair kernel(s), the
+        # integrate pair (non-log steps + log steps), advance; plus 2 before the graph
+        "gpu_launches": int(args.steps * (build_launches(system, args.skin) + 3 +
+                                          (2 if pair_variant in (7, 8, 9) else 1)) + 2),
         "impl": "ours",
     }
     del th, st2

@@ -265,6 +265,7 @@ int Engine::alloc_and_upload()
     DA(b_.cell_lin, C_);
     DA(b_.cnt, C_);
     DA(b_.cstart, C_ + 1);
+    DA(b_.ticket, 1);
     DA(b_.skey, P_);
     DA(b_.srank, P_);
     int64_t ntag = 0;
@@ -638,6 +639,7 @@ static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int 
     a.nlist = b.nlist;
     a.rstate = b.rstate;
     a.blocksum = b.blocksum;
+    a.ticket = b.ticket;
     return a;
 }
 
@@ -750,11 +752,19 @@ void Engine::enqueue_build(cudaStream_t s, bool list)
     const int gc = (C_ + 255) / 256;
     const int nsb = (C_ + 4095) / 4096;
     pdl_launch(k_bin_count, gp, 256, s, ba);
-    pdl_launch(k_scan_blocks, nsb, 1024, s, ba);
-    pdl_launch(k_scan_sums, 1, 1024, s, ba, nsb);
-    pdl_launch(k_scan_add, gc, 256, s, ba);
-    pdl_launch(k_permute, gp, 256, s, ba);
-    pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
+    if (nsb == 1) {
+        pdl_launch(k_scan_blocks<true>, 1, 1024, s, ba);
+    } else {
+        pdl_launch(k_scan_blocks<false>, nsb, 1024, s, ba);
+        pdl_launch(k_scan_sums, 1, 1024, s, ba, nsb);
+        pdl_launch(k_scan_add, gc, 256, s, ba);
+    }
+    if (gp <= 148 * 8) {
+        pdl_launch(k_permute<true>, gp, 256, s, ba, nrep);
+    } else {
+        pdl_launch(k_permute<false>, gp, 256, s, ba, nrep);
+        pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
+    }
     if (list) {
         if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
         else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);

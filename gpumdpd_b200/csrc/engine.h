@@ -59,6 +59,7 @@ struct DeviceBuffers {
     int *cell_rep = nullptr, *cell_lin = nullptr;
     int *cnt = nullptr, *cstart = nullptr, *skey = nullptr, *srank = nullptr, *tag2idx = nullptr;
     int *ncount = nullptr, *nlist = nullptr, *blocksum = nullptr;
+    unsigned int* ticket = nullptr;  // k_permute's last-block counter
     double *acc = nullptr, *ring = nullptr;
     unsigned long long* rdf_hist = nullptr;
     int* build_flag = nullptr;

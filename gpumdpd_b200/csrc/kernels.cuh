@@ -136,9 +136,10 @@ struct PBuf {
     int2* bonds[2];
 };
 
-// Neighbour-list build: counting sort of slots by (re-binned) cell, per-cell order by
-// tag, permutation into the other buffer, parity flip, then the half list.  All
-// kernels return at once unless the build flag of this phase is set.
+// Neighbour-list build: counting sort of slots by (re-binned) cell (in-cell order: the
+// order the counting atomics drew), permutation into the other buffer with the parity
+// flip by its last block, then the half list.  All kernels return at once unless the
+// build flag of this phase is set.
 struct BuildArgs {
     const RepDesc* reps;
     const int* warp_rep;
@@ -163,6 +164,7 @@ struct BuildArgs {
     int* nlist;
     RepState* rstate;
     int* blocksum;
+    unsigned int* ticket;   // blocks of the permutation done (reset by the last one)
 };
 
 __device__ __forceinline__ bool build_on(const BuildArgs& a)
@@ -236,6 +238,9 @@ __global__ void k_bin_count(BuildArgs a)
 
 // exclusive scan of cnt[0..C) into cstart[0..C], three passes (block scan of 4096
 // elements, scan of block sums in one block, add back).
+// SINGLE: the whole scan fits one block (C <= 4096): the block's scan is the result, and
+// it writes the total, so the two passes over the block sums are not launched.
+template <bool SINGLE>
 __global__ void k_scan_blocks(BuildArgs a)
 {
     griddep_wait();
@@ -265,7 +270,10 @@ __global__ void k_scan_blocks(BuildArgs a)
         if (idx < a.C) a.cstart[idx] = run;
         run += v[k];
     }
-    if (threadIdx.x == 1023) a.blocksum[blockIdx.x] = sh[1023];
+    if (threadIdx.x == 1023) {
+        if (SINGLE) a.cstart[a.C] = sh[1023];
+        else a.blocksum[blockIdx.x] = sh[1023];
+    }
 }
 
 __global__ void k_scan_sums(BuildArgs a, int nblocks)
@@ -305,12 +313,8 @@ __global__ void k_scan_add(BuildArgs a)
 // pass drew), re-binning positions; the new positions are also the reference positions
 // of the displacement check (last4).  Reads are coalesced; the writes of a warp land in
 // a few neighbouring cells.
-__global__ void k_permute(BuildArgs a)
+__device__ __forceinline__ void permute_slot(const BuildArgs& a, const int s)
 {
-    griddep_wait();
-    if (!build_on(a)) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.P) return;
     const int par = *a.parity, nxt = par ^ 1;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
@@ -337,6 +341,35 @@ __global__ void k_permute(BuildArgs a)
     if (!d.skin_zero) a.last4[dst] = p;  // skin 0 rebuilds unconditionally: no skin check
     for (int k = 0; k < a.maxb; k++)
         a.buf.bonds[nxt][(size_t)k * a.P + dst] = a.buf.bonds[par][(size_t)k * a.P + s];
+}
+
+// The permutation.  FLIP (small grids, where a launch costs more than the work): the
+// last block to finish (a ticket counter) also flips the parity, counts the build of
+// every replica and resets the ticket.  Every block has read the parity before it takes
+// its ticket, and the list build that follows waits for the whole grid.  Large grids
+// leave the flip to k_flip: the ticket's fence in every block costs more than a launch.
+template <bool FLIP>
+__global__ void k_permute(BuildArgs a, int nrep)
+{
+    griddep_wait();
+    if (!build_on(a)) return;  // grid-uniform
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < a.P) permute_slot(a, s);
+    if (!FLIP) return;
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (last) {
+        for (int r = threadIdx.x; r < nrep; r += blockDim.x) a.rstate[r].nbuild++;
+        if (threadIdx.x == 0) {
+            *a.parity ^= 1;
+            *a.ticket = 0u;
+        }
+    }
 }
 
 __global__ void k_flip(BuildArgs a, int nrep)
