@@ -128,3 +128,28 @@ def test_rdf_of_a_served_job():
     assert ns >= 6
     assert np.isfinite(g).all()
     assert g[-10:].mean() == pytest.approx(1.0, abs=0.15)
+
+
+def test_jobs_with_fixes_and_walls_in_the_mix():
+    """Jobs with group fixes (spring, rvcm, recenter) and particle walls (move, two_wall)
+    share a cohort with a plain job: each finishes with the state of its run alone, to
+    FP32 summation order after 20 steps."""
+    from gpumdpd_b200 import inputs
+    from gpumdpd_b200.server import Server
+    systems = [inputs.probe_fixes(L=9.0, seed=5, nsteps=20, thermo=5, spring_file=None),
+               inputs.wall_channel(L=8.0, Lz=12.0, seed=6, nsteps=20, thermo=5),
+               inputs.plain_dpd(L=7.0, seed=7, nsteps=20, thermo=5)]
+    srv = Server(hbm_budget_bytes=8e9, chunk_steps=8)
+    ids = [srv.submit(s) for s in systems]
+    srv.drain()
+    for jid, s in zip(ids, systems):
+        r = srv.result(jid)
+        assert r["status"] == "done", r
+        _, st, steps = _alone(s)
+        assert r["steps"] == steps
+        fin = srv.state(jid)
+        L = s.hi - s.lo
+        dx = fin["x"] - st["x"]
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < 1e-3
+        assert np.abs(fin["v"] - st["v"]).max() < 1e-2
