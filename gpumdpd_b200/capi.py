@@ -19,7 +19,7 @@ DPD_ERRORS = {
 # every symbol declared in include/dpd_b200.h
 EXPORTED = [
     "dpd_create", "dpd_create_from_system", "dpd_run", "dpd_sync", "dpd_get_thermo", "dpd_get_spring_records",
-    "dpd_dump_open", "dpd_compute_dump_open", "dpd_dump_close", "dpd_write_restart", "dpd_read_restart", "dpd_get_compute",
+    "dpd_dump_open", "dpd_compute_dump_open", "dpd_dump_close", "dpd_bond_compute_aos", "dpd_nve_aos", "dpd_write_restart", "dpd_read_restart", "dpd_get_compute",
     "dpd_get_state", "dpd_set_state", "dpd_get_density", "dpd_get_cells", "dpd_get_neighbors",
     "dpd_compute_rdf", "dpd_rdf_config", "dpd_rdf_result", "dpd_get_info", "dpd_set_tuning",
     "dpd_write_data", "dpd_time_steps", "dpd_get_list_stats", "dpd_last_error", "dpd_destroy", "dpd_pair_compute_aos",
@@ -110,6 +110,8 @@ def load():
         "dpd_get_spring_records": (i, [vp, vp, i, P(i)]),
         "dpd_dump_open": (i, [vp, cp, i64, i64, i]),
         "dpd_dump_close": (i, [vp]),
+        "dpd_bond_compute_aos": (i, [vp, vp, vp, i, vp, vp, vp]),
+        "dpd_nve_aos": (i, [vp, i, vp, i, vp, vp, vp, vp, vp]),
         "dpd_compute_dump_open": (i, [vp, cp, cp]),
         "dpd_write_restart": (i, [vp, cp]),
         "dpd_get_compute": (i, [vp, cp, vp, i, P(i), P(i)]),

@@ -162,6 +162,20 @@ int dpd_dump_close(dpd_engine* h)
     return h->eng.dump_close();
 }
 
+int dpd_bond_compute_aos(dpd_engine* h, const float* d_pos, const int* d_bondlist, int n_bonds, float* d_force,
+                         float* d_bond_pe, float* d_virial)
+{
+    ENG_CHECK(h);
+    return h->eng.bond_compute_aos(d_pos, d_bondlist, n_bonds, d_force, d_bond_pe, d_virial);
+}
+
+int dpd_nve_aos(dpd_engine* h, int phase, const int* d_group, int n_group, const int* d_type, float* d_pos,
+                float* d_uwpos, float* d_vel, const float* d_force)
+{
+    ENG_CHECK(h);
+    return h->eng.nve_aos(phase, d_group, n_group, d_type, d_pos, d_uwpos, d_vel, d_force);
+}
+
 int dpd_get_spring_records(dpd_engine* h, double* rows, int max_rows, int* n_rows)
 {
     ENG_CHECK(h);

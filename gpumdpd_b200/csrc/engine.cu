@@ -1468,6 +1468,108 @@ int Engine::set_tuning(const dpd_tuning* t)
 
 // Pair::compute_force on the reference's AoS device buffers (see kernels_aos.cuh).  Bonds
 // are left to the caller's own bond style, as the reference computes them separately.
+// status of the AoS bond / nve kernels: they run on the legacy default stream, in order
+// with the caller's own kernels; the status is read back after each call
+int Engine::aos_check(const char* what)
+{
+    CK(cudaGetLastError());
+    int stt = 0;
+    CK(cudaMemcpyAsync(&stt, aos_status_, sizeof(int), cudaMemcpyDeviceToHost, cudaStreamLegacy));
+    CK(cudaStreamSynchronize(cudaStreamLegacy));
+    if (stt) {
+        CK(cudaMemsetAsync(aos_status_, 0, sizeof(int), cudaStreamLegacy));
+        if (stt & ST_FENE_BROKEN) {
+            err = std::string(what) + ": FENE bond stretched beyond R0";
+            return DPD_E_NUMERIC;
+        }
+        err = std::string(what) + ": an atom id, index or type outside the engine's system";
+        return DPD_E_ARG;
+    }
+    return DPD_OK;
+}
+
+int Engine::bond_compute_aos(const float* d_pos, const int* d_bondlist, int n_bonds, float* d_force,
+                             float* d_bond_pe, float* d_virial)
+{
+    if (reps_.size() != 1) {
+        err = "the AoS bond entry point works on a single-system engine";
+        return DPD_E_STATE;
+    }
+    const Replica& R = reps_[0];
+    if (R.ff.bond_style == 0 || R.ff.bond_coeff.empty()) {
+        err = "the engine's run.in has no bond_style";
+        return DPD_E_STATE;
+    }
+    if (n_bonds < 0 || (n_bonds > 0 && (!d_pos || !d_bondlist || !d_force))) {
+        err = "null device pointer or negative bond count";
+        return DPD_E_ARG;
+    }
+    int st;
+    if (!aos_status_ && (st = dalloc(&aos_status_, 1))) return st;
+    CK(cudaStreamSynchronize(stream_));  // the status word was zeroed on the engine's stream
+    AosBondArgs b;
+    for (int k = 0; k < 3; k++) {
+        b.L[k] = (float)R.sys.hi[k] - (float)R.sys.lo[k];
+        b.hL[k] = 0.5f * b.L[k];
+    }
+    b.style = R.ff.bond_style;
+    b.ntypes = (int)R.ff.bond_coeff.size();
+    b.coef = b_.bondc + R.desc.bond_off;
+    b.n_atoms = R.sys.n_atoms;
+    b.status = aos_status_;
+    if (n_bonds > 0) {
+        const int g = (n_bonds + 255) / 256;
+        if (d_bond_pe || d_virial)
+            k_bond_aos<true><<<g, 256, 0, cudaStreamLegacy>>>(b, d_pos, d_bondlist, n_bonds, d_force, d_bond_pe, d_virial);
+        else
+            k_bond_aos<false><<<g, 256, 0, cudaStreamLegacy>>>(b, d_pos, d_bondlist, n_bonds, d_force, nullptr, nullptr);
+    }
+    return aos_check("bond force");
+}
+
+int Engine::nve_aos(int phase, const int* d_group, int n_group, const int* d_type, float* d_pos, float* d_uwpos,
+                    float* d_vel, const float* d_force)
+{
+    if (reps_.size() != 1) {
+        err = "the AoS nve entry point works on a single-system engine";
+        return DPD_E_STATE;
+    }
+    if ((phase != 0 && phase != 1) || n_group < 0 ||
+        (n_group > 0 && (!d_group || !d_type || !d_pos || !d_vel || !d_force))) {
+        err = "phase must be 0 (initial) or 1 (final); null device pointer or negative count";
+        return DPD_E_ARG;
+    }
+    const Replica& R = reps_[0];
+    int st;
+    if (!aos_status_ && (st = dalloc(&aos_status_, 1))) return st;
+    if (!aos_mass_) {
+        if ((st = dalloc(&aos_mass_, R.sys.n_atomtypes))) return st;
+        std::vector<float> m(R.sys.n_atomtypes);
+        for (int t = 0; t < R.sys.n_atomtypes; t++) m[t] = (float)R.sys.masses[t];
+        CK(cudaMemcpyAsync(aos_mass_, m.data(), sizeof(float) * m.size(), cudaMemcpyHostToDevice, stream_));
+    }
+    CK(cudaStreamSynchronize(stream_));
+    AosNveArgs b;
+    b.dt = (float)R.in.dt;
+    for (int k = 0; k < 3; k++) {
+        b.lo[k] = (float)R.sys.lo[k];
+        b.hi[k] = (float)R.sys.hi[k];
+        b.L[k] = b.hi[k] - b.lo[k];
+    }
+    b.ntypes = R.sys.n_atomtypes;
+    b.mass = aos_mass_;
+    b.n_atoms = R.sys.n_atoms;
+    b.status = aos_status_;
+    if (n_group > 0) {
+        const int g = (n_group + 255) / 256;
+        if (phase == 0)
+            k_nve_aos<0><<<g, 256, 0, cudaStreamLegacy>>>(b, d_group, n_group, d_type, d_pos, d_uwpos, d_vel, d_force);
+        else
+            k_nve_aos<1><<<g, 256, 0, cudaStreamLegacy>>>(b, d_group, n_group, d_type, d_pos, d_uwpos, d_vel, d_force);
+    }
+    return aos_check("nve");
+}
+
 int Engine::pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
                              int n, uint32_t step, float* d_force, float* d_pe, float* d_virial)
 {

@@ -122,6 +122,11 @@ public:
                        const float* spring_a, double* x, double* v, int* image, double* f) const;
     int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,
                          int n, uint32_t step, float* d_force, float* d_pe, float* d_virial);
+    // the bond force and fix nve on the reference's AoS buffers (kernels_aos.cuh)
+    int bond_compute_aos(const float* d_pos, const int* d_bondlist, int n_bonds, float* d_force,
+                         float* d_bond_pe, float* d_virial);
+    int nve_aos(int phase, const int* d_group, int n_group, const int* d_type, float* d_pos, float* d_uwpos,
+                float* d_vel, const float* d_force);
 
     int n_rep() const { return (int)reps_.size(); }
     const Replica& rep(int r) const { return reps_[r]; }
@@ -181,6 +186,9 @@ private:
     int* angle_wrep_ = nullptr;   // replica of each warp of the angle table
     int nang_ = 0;                // angle table length (padded to whole warps per replica)
     float *pe_slot_ = nullptr, *vir_slot_ = nullptr;  // per-atom PE/virial of the AoS entry
+    int* aos_status_ = nullptr;    // status bits of the AoS bond / nve kernels (device)
+    float* aos_mass_ = nullptr;    // masses per type for the AoS nve kernel (device)
+    int aos_check(const char* what);
     bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;

@@ -170,3 +170,118 @@ __global__ void k_aos_done(int* build_flag, const uint32_t* phase)
 {
     build_flag[(*phase) & 1] = 0;
 }
+
+// ---------------------------------------------------------------------------------
+// Bond::compute_force on the reference's AoS buffers (src/force/bond_harmonic.cu:167-402):
+// one thread per entry of the bond list {type, id_i, id_j}; displacement x_i - x_j with
+// the reference's minimum image (d -= L((d >= L/2) - (d < -L/2))), harmonic E = k(r-r0)^2,
+// F_i = -2k(r-r0)/r d, or this engine's FENE; forces added to both atoms; on log steps the
+// bond's energy (one value per bond, as the reference's d_bond_pe) and half the virial
+// r_a F_b to each atom.
+struct AosBondArgs {
+    float L[3], hL[3];
+    int style;       // 1 harmonic, 2 fene
+    int ntypes;
+    const float4* coef;  // per bond type: harmonic {k, r0}; fene {K, R0, eps, sigma}
+    int n_atoms;
+    int* status;     // device int: bit ST_BOND_MISSING (an id outside the system), ST_FENE_BROKEN
+};
+
+template <bool LOG>
+__global__ void k_bond_aos(AosBondArgs b, const float* __restrict__ pos, const int* __restrict__ bl, int nb,
+                           float* force, float* bond_pe, float* virial)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nb) return;
+    const int ty = bl[3 * q], ia = bl[3 * q + 1] - 1, ja = bl[3 * q + 2] - 1;
+    if (ty < 1 || ty > b.ntypes || ia < 0 || ia >= b.n_atoms || ja < 0 || ja >= b.n_atoms) {
+        atomicOr(b.status, ST_BOND_MISSING);
+        return;
+    }
+    float d[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float x = pos[3 * ia + k] - pos[3 * ja + k];
+        x = x - b.L[k] * (float)((x >= b.hL[k]) - (x < -b.hL[k]));
+        d[k] = x;
+    }
+    const float r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const float4 c = b.coef[ty - 1];
+    float fbond = 0.0f, e = 0.0f;
+    if (b.style == 1) {
+        const float r = sqrtf(r2);
+        fbond = r > 0.0f ? -2.0f * c.x * (r - c.y) / r : 0.0f;
+        e = c.x * (r - c.y) * (r - c.y);
+    } else {
+        float rr = r2 / (c.y * c.y);
+        if (rr >= 1.0f) {
+            atomicOr(b.status, ST_FENE_BROKEN);
+            rr = 0.999f;
+        }
+        fbond = -c.x / (1.0f - rr);
+        e = -0.5f * c.x * c.y * c.y * logf(1.0f - rr);
+        if (c.z > 0.0f && r2 < 1.2599210498948732f * c.w * c.w) {
+            const float sr2 = c.w * c.w / r2;
+            const float sr6 = sr2 * sr2 * sr2;
+            fbond += 48.0f * c.z * sr6 * (sr6 - 0.5f) / r2;
+            e += 4.0f * c.z * sr6 * (sr6 - 1.0f) + c.z;
+        }
+    }
+    const float f[3] = {d[0] * fbond, d[1] * fbond, d[2] * fbond};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        atomicAdd(force + 3 * ia + k, f[k]);
+        atomicAdd(force + 3 * ja + k, -f[k]);
+    }
+    if (LOG) {
+        if (bond_pe) bond_pe[q] = e;
+        if (virial) {
+            const float v6[6] = {0.5f * d[0] * f[0], 0.5f * d[0] * f[1], 0.5f * d[0] * f[2],
+                                 0.5f * d[1] * f[1], 0.5f * d[1] * f[2], 0.5f * d[2] * f[2]};
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+                atomicAdd(virial + 6 * ia + k, v6[k]);
+                atomicAdd(virial + 6 * ja + k, v6[k]);
+            }
+        }
+    }
+}
+
+// fix nve on the reference's AoS buffers (src/fix/fix_nve.cu:30-152), one thread per atom
+// of the group's index list: PHASE 0 the initial half kick v += dt/2 f/m, the drift
+// x += dt v wrapped into [lo, hi) and the unwrapped position uw += dt v; PHASE 1 the
+// final half kick.  The same FP32 operations as the reference's kernels.
+struct AosNveArgs {
+    float dt;
+    float lo[3], hi[3], L[3];
+    int ntypes;
+    const float* mass;  // per type
+    int n_atoms;
+    int* status;        // device int: bit ST_BAD_INPUT (an index or type outside the system)
+};
+
+template <int PHASE>
+__global__ void k_nve_aos(AosNveArgs b, const int* __restrict__ group, int ng, const int* __restrict__ type,
+                          float* pos, float* uwpos, float* vel, const float* __restrict__ force)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ng) return;
+    const int i = group[q];
+    if (i < 0 || i >= b.n_atoms || type[i] < 1 || type[i] > b.ntypes) {
+        atomicOr(b.status, ST_BAD_INPUT);
+        return;
+    }
+    const float dtm = (0.5f * b.dt) * (1.0f / b.mass[type[i] - 1]);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float v = __fmaf_rn(dtm, force[3 * i + k], vel[3 * i + k]);
+        vel[3 * i + k] = v;
+        if (PHASE == 0) {
+            float p = __fmaf_rn(b.dt, v, pos[3 * i + k]);
+            for (int it = 0; it < 64 && (p >= b.hi[k] || p < b.lo[k]); it++)
+                p -= b.L[k] * (float)((p >= b.hi[k]) - (p < b.lo[k]));
+            pos[3 * i + k] = p;
+            if (uwpos) uwpos[3 * i + k] = __fmaf_rn(b.dt, v, uwpos[3 * i + k]);
+        }
+    }
+}

@@ -190,6 +190,16 @@ class Engine:
     def write_data(self, path):
         _check(self.lib.dpd_write_data(self.h, path.encode()), self.lib, self.h)
 
+    def bond_compute_aos(self, d_pos, d_bondlist, n_bonds, d_force, d_bond_pe=None, d_virial=None):
+        """Bond::compute_force on AoS device buffers (integer device addresses)."""
+        _check(self.lib.dpd_bond_compute_aos(self.h, d_pos, d_bondlist, int(n_bonds), d_force, d_bond_pe, d_virial),
+               self.lib, self.h)
+
+    def nve_aos(self, phase, d_group, n_group, d_type, d_pos, d_uwpos, d_vel, d_force):
+        """fix nve's initial (phase 0) or final (phase 1) step on AoS device buffers."""
+        _check(self.lib.dpd_nve_aos(self.h, int(phase), d_group, int(n_group), d_type, d_pos, d_uwpos, d_vel,
+                                    d_force), self.lib, self.h)
+
     def pair_compute_aos(self, d_pos, d_vel, d_id, d_type, n, step, d_force, d_pe=None, d_virial=None):
         """Pair::compute_force on AoS device buffers (integer device addresses)."""
         _check(self.lib.dpd_pair_compute_aos(self.h, d_pos, d_vel, d_id, d_type, int(n), int(step), d_force,

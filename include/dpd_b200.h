@@ -160,6 +160,24 @@ int dpd_read_restart(dpd_engine* eng, const char* path);
  * max_rows of the most recent (the device keeps 2048). */
 int dpd_get_compute(dpd_engine* eng, const char* id, double* rows, int max_rows, int* n_cols, int* n_rows);
 
+/* Bond::compute_force on the reference's own device buffers (Bond_harmonic, src/force/
+ * bond_harmonic.cu:167-402): d_bondlist holds n_bonds entries {type, id_i, id_j} (1-based
+ * ids, atom index = id - 1), d_pos the FP32 AoS positions, d_force the forces the bond
+ * force is added to.  On log steps pass d_bond_pe (per bond, overwritten) and/or d_virial
+ * (6 per atom, half of each bond's r_a F_b added to both atoms); NULL otherwise.  The bond
+ * style and coefficients are the engine's run.in's (harmonic, or this engine's fene).
+ * Runs on the legacy default stream, in order with the caller's kernels. */
+int dpd_bond_compute_aos(dpd_engine* eng, const float* d_pos, const int* d_bondlist, int n_bonds,
+                         float* d_force, float* d_bond_pe, float* d_virial);
+
+/* Fix nve on the reference's own device buffers (src/fix/fix_nve.cu:30-152) for the atom
+ * indices of a group (d_group, n_group): phase 0 the initial half kick and drift (positions
+ * wrapped into the box, d_uwpos advanced when not NULL), phase 1 the final half kick.  dt,
+ * masses and box are the engine's run.in and system's.  Legacy default stream, like
+ * dpd_bond_compute_aos. */
+int dpd_nve_aos(dpd_engine* eng, int phase, const int* d_group, int n_group, const int* d_type, float* d_pos,
+                float* d_uwpos, float* d_vel, const float* d_force);
+
 /* Records of `fix ... spring k x y z r0 file freq` (src/fix/fix_spring.cu:340-360, the
  * rows it writes to its file): 6 doubles per row {step, Fx, Fy, Fz, +-|F|, energy}, every
  * freq steps from the zero step on.  Copies up to max_rows of the most recent rows (the

@@ -9,9 +9,10 @@
 # force-included on the command line instead of editing any source.
 #
 # Usage: oracle/build_ref.sh [SINGLE|DOUBLE|SHIM]   (default SINGLE, the reference's default)
-#   SHIM: the SINGLE build plus gpumdpd_b200/shim/pair_dpd_b200.cu (pair_style dpd/b200 and
-#   mdpd/b200, which hand the reference's device buffers to libdpd_b200), linked against
-#   the in-tree libdpd_b200.so -> oracle/_ref/gpudpd_single_b200.
+#   SHIM: the SINGLE build plus the plugins of gpumdpd_b200/shim/ (pair_style dpd/b200 and
+#   mdpd/b200, bond_style harmonic/b200, fix nve/b200, which hand the reference's device
+#   buffers to libdpd_b200), linked against the in-tree libdpd_b200.so
+#   -> oracle/_ref/gpudpd_single_b200.
 set -euo pipefail
 MODE="${1:-SINGLE}"
 PREC="$MODE"
@@ -46,8 +47,13 @@ for p in "${pids[@]}"; do wait "$p"; done
 lower="$(echo "$PREC" | tr 'A-Z' 'a-z')"
 if [ "$MODE" = "SHIM" ]; then
     REPO="$(cd "$HERE/.." && pwd)"
-    nvcc "${FLAGS[@]}" -I"$REPO/include" -dc "$REPO/gpumdpd_b200/shim/pair_dpd_b200.cu" -o "$OBJ/shim_pair_dpd_b200.o"
-    nvcc "${FLAGS[@]}" "${objs[@]}" "$OBJ/shim_pair_dpd_b200.o" -L"$REPO/gpumdpd_b200" -ldpd_b200 \
+    shims=()
+    for src in "$REPO"/gpumdpd_b200/shim/*.cu; do
+        o="$OBJ/shim_$(basename "$src" .cu).o"
+        nvcc "${FLAGS[@]}" -I"$REPO/include" -dc "$src" -o "$o"
+        shims+=("$o")
+    done
+    nvcc "${FLAGS[@]}" "${objs[@]}" "${shims[@]}" -L"$REPO/gpumdpd_b200" -ldpd_b200 \
         -Xlinker -rpath -Xlinker '$ORIGIN/../../gpumdpd_b200' -o "$OUT/gpudpd_single_b200"
     echo "built $OUT/gpudpd_single_b200"
     exit 0

@@ -68,3 +68,41 @@ def test_reference_loop_with_b200_pair_style(name):
         np.testing.assert_allclose(b[early], a[early], rtol=1e-3, atol=1e-5)
     assert ours["temp"].mean() == pytest.approx(stock["temp"].mean(), rel=2e-2)
     assert ours["pressure"].mean() == pytest.approx(stock["pressure"].mean(), rel=2e-2)
+
+
+def _plugins(run_in, style, which):
+    """The run.in with the chosen stock styles replaced by their b200 plugins."""
+    if "pair" in which:
+        run_in = run_in.replace(f"pair_style {style} ", f"pair_style {style}/b200 ")
+    if "bond" in which:
+        run_in = run_in.replace("bond_style harmonic", "bond_style harmonic/b200")
+    if "nve" in which:
+        run_in = re.sub(r"(?m)^(fix \S+ \S+) nve$", r"\1 nve/b200", run_in)
+    return run_in
+
+
+@pytest.mark.skipif(not (os.path.exists(STOCK) and os.path.exists(SHIM)),
+                    reason="reference builds (oracle/build_ref.sh SINGLE and SHIM) not present")
+@pytest.mark.parametrize("name,which", [("diblock", ("bond",)), ("diblock", ("nve",)),
+                                        ("diblock", ("pair", "bond", "nve")), ("angles", ("bond", "nve")),
+                                        ("dpd", ("nve",)), ("mdpd", ("pair", "nve"))])
+def test_reference_loop_with_b200_bond_and_nve(name, which):
+    """bond_style harmonic/b200 (dpd_bond_compute_aos) and fix nve/b200 (dpd_nve_aos) in
+    the reference's own loop, alone and together with the pair plugin: the thermo rows
+    (bond PE included) follow the stock executable's.  The bond force and the integrator
+    repeat the stock FP32 operations, so with the stock pair style the rows agree to the
+    printed precision until FP32 atomics reorder sums."""
+    s, run_in, style = _case(name)
+    stock = _run(STOCK, s, run_in)
+    text = _plugins(run_in, style, which)
+    assert text != run_in
+    ours = _run(SHIM, s, text)
+    assert np.array_equal(stock["step"], ours["step"])
+    keys = ["temp", "pair_pe", "pressure"] + (["bond_pe"] if "bond_pe" in stock else [])
+    for k in keys:
+        a, b = stock[k], ours[k]
+        assert abs(a[0] - b[0]) <= 1e-5 * abs(a[0]) + 2e-6, (k, a[0], b[0])
+        early = stock["step"] <= 20
+        np.testing.assert_allclose(b[early], a[early], rtol=1e-3, atol=1e-5)
+    assert ours["temp"].mean() == pytest.approx(stock["temp"].mean(), rel=2e-2)
+    assert ours["pressure"].mean() == pytest.approx(stock["pressure"].mean(), rel=2e-2)
