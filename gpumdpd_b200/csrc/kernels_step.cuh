@@ -1401,28 +1401,30 @@ __global__ void k_advance(StepArgs a)
 
 // ---------------------------------------------------------------------------------
 // RDF sampling (new; no reference counterpart): histogram of minimum-image distances
-// from particles of type ta to particles of type tb within rmax, sampled on steps
-// that are multiples of rdf_every, from the end-of-step positions.  Candidate cells
-// are the last build's cells around the particle's cell plus one layer (particles
-// drift by less than a cell between builds); each build cell is visited once.
+// from particles of type ta to particles of type tb within rmax, sampled on steps that
+// are multiples of rdf_every, from the end-of-step positions.  Candidate cells are the
+// last build's cells within rmax of the particle's cell; when the list is not rebuilt at
+// every step (skin > 0 or nl_f > 1) particles may have drifted since the build, and one
+// more layer of cells is searched.  With a build this step (skin 0, nl_f 1: the sample
+// sees the build's positions) cells farther than rmax from the particle itself are
+// skipped.  A warp takes its 32 slots one after the other; for each type-ta particle the
+// lanes share out the stencil's cells (one cell per lane and turn), so the lanes stay busy
+// whatever the cell sizes.  Each warp keeps its histogram and its stencil (the cell
+// offsets, packed, when there are at most DPD_RDF_MAXCELLS) in shared memory.
 #define DPD_RDF_MAXBINS 512
+#define DPD_RDF_MAXCELLS 512
 __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
 {
     griddep_wait();
     __shared__ unsigned int hs[8][DPD_RDF_MAXBINS];
+    __shared__ int stab[8][DPD_RDF_MAXCELLS];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int r = -1;
-    bool on = false;
-    if (s < a.P) {
-        r = a.warp_rep[s >> 5];
-        const RepDesc& d = a.reps[r];
-        const RepState st = a.rstate[r];
-        on = d.rdf_every > 0 && rep_active(st) && (st.step % (uint32_t)d.rdf_every) == 0u;
-    }
-    // every warp is single-replica, so `on` is warp-uniform
-    if (!on) return;
+    if ((s & ~31) >= a.P) return;  // warp-uniform
+    const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
+    const RepState st = a.rstate[r];
+    if (!(d.rdf_every > 0 && rep_active(st) && (st.step % (uint32_t)d.rdf_every) == 0u)) return;  // warp-uniform
     const int par = *a.parity;
     const float4* pos = a.buf.pos[par];
     const float4* vel = a.buf.vel[par];
@@ -1430,46 +1432,109 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
     for (int b = lane; b < nb; b += 32) hs[warp][b] = 0u;
     __syncwarp();
     if (s == d.p_begin) atomicAdd((unsigned long long*)&a.rstate[r].rdf_samples, 1ull);
-    if (s < d.p_end) {
-        const float4 pi = pos[s];
-        const int ti = type0_of(vel[s].w) + 1;
-        if (ti == d.rdf_ta) {
-            const int ci = __float_as_int(pi.w);
-            const int cx = cell_x(ci), cy = cell_y(ci), cz = cell_z(ci);
-            const float rmax2 = d.rdf_rmax * d.rdf_rmax;
-            const float inv_dr = (float)d.rdf_nbins / d.rdf_rmax;
-            int lo3[3], hi3[3];
-            for (int k = 0; k < 3; k++) {
-                int nr = (int)ceilf(d.rdf_rmax * d.inv_w[k]) + 1;
-                if (2 * nr + 1 >= d.nc[k]) {
-                    lo3[k] = -(d.nc[k] / 2);
-                    hi3[k] = d.nc[k] - 1 - d.nc[k] / 2;
-                } else {
-                    lo3[k] = -nr;
-                    hi3[k] = nr;
+    const float rmax2 = d.rdf_rmax * d.rdf_rmax;
+    const float inv_dr = (float)d.rdf_nbins / d.rdf_rmax;
+    int lo3[3], n3[3];
+    const bool fresh = d.skin_zero && d.nl_f == 1;
+    bool local = true;  // the searched cells are nearer than half the grid in every axis
+    for (int k = 0; k < 3; k++) {
+        // 1e-6: a ratio rounded down to an integer still covers the last layer
+        const int nr = (int)ceilf(d.rdf_rmax * d.inv_w[k] * 1.000001f) + (fresh ? 0 : 1);
+        if (2 * nr + 1 >= d.nc[k]) {
+            lo3[k] = -(d.nc[k] / 2);
+            n3[k] = d.nc[k];
+            local = false;
+        } else {
+            lo3[k] = -nr;
+            n3[k] = 2 * nr + 1;
+        }
+    }
+    const bool prune = fresh && local;
+    const int ncand = n3[0] * n3[1] * n3[2];
+    const bool tabled = ncand <= DPD_RDF_MAXCELLS;
+    // cell offset c of the stencil, packed as (ox+512) | (oy+512)<<10 | (oz+512)<<20
+    auto decode = [&](int c) {
+        return (lo3[0] + c / (n3[1] * n3[2]) + 512) | ((lo3[1] + (c / n3[2]) % n3[1] + 512) << 10) |
+               ((lo3[2] + c % n3[2] + 512) << 20);
+    };
+    if (tabled)
+        for (int c = lane; c < ncand; c += 32) stab[warp][c] = decode(c);
+    __syncwarp();
+    const int w0 = s & ~31;
+    for (int q = 0; q < 32; q++) {
+        const int si = w0 + q;
+        if (si >= d.p_end) break;  // warp-uniform
+        const float4 vi = vel[si];
+        if (type0_of(vi.w) + 1 != d.rdf_ta) continue;  // warp-uniform
+        const float4 pi = pos[si];
+        const int ci = __float_as_int(pi.w);
+        const int cx = cell_x(ci), cy = cell_y(ci), cz = cell_z(ci);
+        // the stencil in chunks of 32 cells, one per lane; the chunk's candidates are
+        // shared out over the lanes as one flat sequence (owner cell by a binary search
+        // over the lanes' scanned counts)
+        for (int c0 = 0; c0 < ncand; c0 += 32) {
+            const int c = c0 + lane;
+            int beg = 0, cnt = 0;
+            float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+            if (c < ncand) {
+                const int pk = tabled ? stab[warp][c] : decode(c);
+                const int ox = (pk & 1023) - 512, oy = ((pk >> 10) & 1023) - 512, oz = ((pk >> 20) & 1023) - 512;
+                bool keep = true;
+                if (prune) {
+                    // distance from the particle to the near face of that cell
+                    const float gx = ox > 0 ? (float)ox * d.w[0] - pi.x : (ox < 0 ? pi.x - (float)(ox + 1) * d.w[0] : 0.0f);
+                    const float gy = oy > 0 ? (float)oy * d.w[1] - pi.y : (oy < 0 ? pi.y - (float)(oy + 1) * d.w[1] : 0.0f);
+                    const float gz = oz > 0 ? (float)oz * d.w[2] - pi.z : (oz < 0 ? pi.z - (float)(oz + 1) * d.w[2] : 0.0f);
+                    keep = gx * gx + gy * gy + gz * gz < rmax2;
+                }
+                if (keep) {
+                    // |offset| < nc: one wrap at most
+                    int nx = cx + ox; nx += nx < 0 ? d.nc[0] : 0; nx -= nx >= d.nc[0] ? d.nc[0] : 0;
+                    int ny = cy + oy; ny += ny < 0 ? d.nc[1] : 0; ny -= ny >= d.nc[1] ? d.nc[1] : 0;
+                    int nz = cz + oz; nz += nz < 0 ? d.nc[2] : 0; nz -= nz >= d.nc[2] ? d.nc[2] : 0;
+                    const int key = d.c_begin + a.crank[d.c_begin + (nx * d.nc[1] + ny) * d.nc[2] + nz];
+                    beg = a.cstart[key];
+                    cnt = a.cstart[key + 1] - beg;
+                    sx = __int2float_rn(-ox) * d.w[0];
+                    sy = __int2float_rn(-oy) * d.w[1];
+                    sz = __int2float_rn(-oz) * d.w[2];
                 }
             }
-            for (int ox = lo3[0]; ox <= hi3[0]; ox++) {
-                const int nx = ((cx + ox) % d.nc[0] + d.nc[0]) % d.nc[0];
-                for (int oy = lo3[1]; oy <= hi3[1]; oy++) {
-                    const int ny = ((cy + oy) % d.nc[1] + d.nc[1]) % d.nc[1];
-                    for (int oz = lo3[2]; oz <= hi3[2]; oz++) {
-                        const int nz = ((cz + oz) % d.nc[2] + d.nc[2]) % d.nc[2];
-                        const int key = d.c_begin + a.crank[d.c_begin + (nx * d.nc[1] + ny) * d.nc[2] + nz];
-                        const int jb = a.cstart[key], je = a.cstart[key + 1];
-                        for (int j = jb; j < je; j++) {
-                            if (j == s) continue;
-                            const float4 vj = __ldg(vel + j);
-                            if (type0_of(vj.w) + 1 != d.rdf_tb) continue;
-                            const float4 pj = __ldg(pos + j);
-                            float dx, dy, dz;
-                            disp3(d, ci, pi, pj, dx, dy, dz);
-                            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-                            if (r2 < rmax2) {
-                                int bin = (int)(sqrtf(r2) * inv_dr);
-                                if (bin < nb) atomicAdd(&hs[warp][bin], 1u);
-                            }
-                        }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int start = incl - cnt;
+            for (int t0 = 0; t0 < total; t0 += 32) {
+                const int t = t0 + lane;
+                int l = 0;  // the last lane whose start is <= t
+#pragma unroll
+                for (int stp = 16; stp >= 1; stp >>= 1) {
+                    const int sv = __shfl_sync(0xffffffffu, start, l + stp);
+                    if (sv <= t) l += stp;
+                }
+                const int j = __shfl_sync(0xffffffffu, beg, l) + (t - __shfl_sync(0xffffffffu, start, l));
+                const float hx = __shfl_sync(0xffffffffu, sx, l), hy = __shfl_sync(0xffffffffu, sy, l),
+                            hz = __shfl_sync(0xffffffffu, sz, l);
+                if (t < total && j != si) {
+                    const float4 pj = __ldg(pos + j);
+                    float dx, dy, dz;
+                    if (local) {
+                        // (o_i - o_j) + (c_i - c_j) w with c_j = c_i + offset: the nearest
+                        // image for every pair this search can reach
+                        dx = __fadd_rn(__fsub_rn(pi.x, pj.x), hx);
+                        dy = __fadd_rn(__fsub_rn(pi.y, pj.y), hy);
+                        dz = __fadd_rn(__fsub_rn(pi.z, pj.z), hz);
+                    } else {
+                        disp3(d, ci, pi, pj, dx, dy, dz);
+                    }
+                    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+                    if (r2 < rmax2 && type0_of(__ldg(&vel[j].w)) + 1 == d.rdf_tb) {
+                        const int bin = (int)(sqrtf(r2) * inv_dr);
+                        if (bin < nb) atomicAdd(&hs[warp][bin], 1u);
                     }
                 }
             }
