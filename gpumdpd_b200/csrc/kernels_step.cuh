@@ -1403,11 +1403,11 @@ __global__ void k_advance(StepArgs a)
 // RDF sampling (new; no reference counterpart): histogram of minimum-image distances
 // from particles of type ta to particles of type tb within rmax, sampled on steps that
 // are multiples of rdf_every, from the end-of-step positions.  Candidate cells are the
-// last build's cells within rmax of the particle's cell; when the list is not rebuilt at
-// every step (skin > 0 or nl_f > 1) particles may have drifted since the build, and one
-// more layer of cells is searched.  With a build this step (skin 0, nl_f 1: the sample
-// sees the build's positions) cells farther than rmax from the particle itself are
-// skipped.  A warp takes its 32 slots one after the other; for each type-ta particle the
+// last build's cells within reach of the particle: rmax with a build this step (skin 0,
+// nl_f 1: the sample sees the build's positions); rmax + skin when the displacement check
+// runs every step (nl_f 1: no particle has moved skin/2 since the build); otherwise one
+// more layer of cells.  In the first two cases cells farther than rmax (+ skin/2 for the
+// candidate's drift) from the particle itself are skipped.  A warp takes its 32 slots one after the other; for each type-ta particle the
 // lanes share out the stencil's cells (one cell per lane and turn), so the lanes stay busy
 // whatever the cell sizes.  Each warp keeps its histogram and its stencil (the cell
 // offsets, packed, when there are at most DPD_RDF_MAXCELLS) in shared memory.
@@ -1436,10 +1436,13 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
     const float inv_dr = (float)d.rdf_nbins / d.rdf_rmax;
     int lo3[3], n3[3];
     const bool fresh = d.skin_zero && d.nl_f == 1;
+    const bool bounded = !d.skin_zero && d.nl_f == 1;
+    const float hskin = bounded ? sqrtf(d.hskin2) : 0.0f;  // the drift bound, skin/2
     bool local = true;  // the searched cells are nearer than half the grid in every axis
     for (int k = 0; k < 3; k++) {
         // 1e-6: a ratio rounded down to an integer still covers the last layer
-        const int nr = (int)ceilf(d.rdf_rmax * d.inv_w[k] * 1.000001f) + (fresh ? 0 : 1);
+        const int nr = fresh || bounded ? (int)ceilf((d.rdf_rmax + 2.0f * hskin) * d.inv_w[k] * 1.000001f)
+                                        : (int)ceilf(d.rdf_rmax * d.inv_w[k] * 1.000001f) + 1;
         if (2 * nr + 1 >= d.nc[k]) {
             lo3[k] = -(d.nc[k] / 2);
             n3[k] = d.nc[k];
@@ -1449,7 +1452,8 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
             n3[k] = 2 * nr + 1;
         }
     }
-    const bool prune = fresh && local;
+    const bool prune = (fresh || bounded) && local;
+    const float reach2 = (d.rdf_rmax + hskin) * (d.rdf_rmax + hskin);
     const int ncand = n3[0] * n3[1] * n3[2];
     const bool tabled = ncand <= DPD_RDF_MAXCELLS;
     // cell offset c of the stencil, packed as (ox+512) | (oy+512)<<10 | (oz+512)<<20
@@ -1485,7 +1489,7 @@ __global__ void __launch_bounds__(256) k_rdf(StepArgs a)
                     const float gx = ox > 0 ? (float)ox * d.w[0] - pi.x : (ox < 0 ? pi.x - (float)(ox + 1) * d.w[0] : 0.0f);
                     const float gy = oy > 0 ? (float)oy * d.w[1] - pi.y : (oy < 0 ? pi.y - (float)(oy + 1) * d.w[1] : 0.0f);
                     const float gz = oz > 0 ? (float)oz * d.w[2] - pi.z : (oz < 0 ? pi.z - (float)(oz + 1) * d.w[2] : 0.0f);
-                    keep = gx * gx + gy * gy + gz * gz < rmax2;
+                    keep = gx * gx + gy * gy + gz * gz < reach2;
                 }
                 if (keep) {
                     // |offset| < nc: one wrap at most

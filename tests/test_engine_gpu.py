@@ -487,13 +487,16 @@ def test_build_variants_give_the_same_list(oracle_mod, name, build_variant):
     assert force_err(b.state()["f"], a.state()["f"]) < 1e-4
 
 
-@pytest.mark.parametrize("skin", [0.0, 0.3])
-def test_rdf_samples_over_a_run_vs_oracle(oracle_mod, skin):
+@pytest.mark.parametrize("skin,nl_f", [(0.0, 1), (0.3, 1), (0.3, 2)])
+def test_rdf_samples_over_a_run_vs_oracle(oracle_mod, skin, nl_f):
     """The RDF accumulated over samples every 2 steps equals the mean of the oracle's RDFs
-    of the states at those steps: at skin 0 (a build each step, the cells within rmax of
-    the particle are searched) and at skin 0.3 (one more layer of cells for the drift)."""
+    of the states at those steps: at skin 0 (a build each step: the cells within rmax of
+    the particle), at skin 0.3 checked every step (reach rmax + skin) and checked every
+    other step (one more layer of cells)."""
     from gpumdpd_b200 import inputs
     s = inputs.binary_mixture(14.0, 30.0, seed=23, nsteps=0, rdf=(3.0, 60, 2), skin=skin)
+    s.run_in = re.sub(r"(?m)^neighbor (\S+) (\S+) (\S+) 1$", rf"neighbor \1 \2 \3 {nl_f}", s.run_in)
+    assert f" {nl_f}\n" in [ln for ln in s.run_in.splitlines(True) if ln.startswith("neighbor")][0]
     e = _engine_from(s)
     gs = []
     e.run(0)
