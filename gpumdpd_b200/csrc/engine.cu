@@ -923,6 +923,12 @@ int Engine::read_rstate(std::vector<RepState>& st)
     return DPD_OK;
 }
 
+int Engine::rstate_async(RepState* host)
+{
+    CK(cudaMemcpyAsync(host, b_.rstate, sizeof(RepState) * reps_.size(), cudaMemcpyDeviceToHost, stream_));
+    return DPD_OK;
+}
+
 int Engine::sync_and_check()
 {
     CK(cudaStreamSynchronize(stream_));
@@ -931,35 +937,41 @@ int Engine::sync_and_check()
     int e = read_rstate(st);
     if (e) return e;
     for (size_t r = 0; r < st.size(); r++) {
-        int s = st[r].status;
-        if (s & ST_LIST_OVERFLOW) {
-            err = "neighbour list overflow in replica " + std::to_string(r) + ": increase max_rho in the neighbor command";
-            return DPD_E_OVERFLOW;
-        }
-        if (s & ST_NONFINITE) {
-            err = "non-finite position or velocity in replica " + std::to_string(r);
-            return DPD_E_NUMERIC;
-        }
-        if (s & ST_FENE_BROKEN) {
-            err = "FENE bond stretched beyond R0 in replica " + std::to_string(r);
-            return DPD_E_NUMERIC;
-        }
-        if (s & ST_BOND_MISSING) {
-            err = "bond partner not found in replica " + std::to_string(r);
-            return DPD_E_STATE;
-        }
-        if (s & ST_WALL_ORDER) {
-            err = "The high wall is positioned lower than the low wall (fix two_wall, replica " + std::to_string(r) + ")";
-            return DPD_E_STATE;
-        }
-        if (s & ST_CONTACT_BOX) {
-            err = "contact region out of the box (compute wall_contact, replica " + std::to_string(r) + ")";
-            return DPD_E_STATE;
-        }
-        if (s & ST_BAD_INPUT) {
-            err = "an atom id or type in the AoS input is outside the engine's system";
-            return DPD_E_ARG;
-        }
+        const int code = status_error(st[r].status, (int)r);
+        if (code) return code;
+    }
+    return DPD_OK;
+}
+
+int Engine::status_error(int s, int r)
+{
+    if (s & ST_LIST_OVERFLOW) {
+        err = "neighbour list overflow in replica " + std::to_string(r) + ": increase max_rho in the neighbor command";
+        return DPD_E_OVERFLOW;
+    }
+    if (s & ST_NONFINITE) {
+        err = "non-finite position or velocity in replica " + std::to_string(r);
+        return DPD_E_NUMERIC;
+    }
+    if (s & ST_FENE_BROKEN) {
+        err = "FENE bond stretched beyond R0 in replica " + std::to_string(r);
+        return DPD_E_NUMERIC;
+    }
+    if (s & ST_BOND_MISSING) {
+        err = "bond partner not found in replica " + std::to_string(r);
+        return DPD_E_STATE;
+    }
+    if (s & ST_WALL_ORDER) {
+        err = "The high wall is positioned lower than the low wall (fix two_wall, replica " + std::to_string(r) + ")";
+        return DPD_E_STATE;
+    }
+    if (s & ST_CONTACT_BOX) {
+        err = "contact region out of the box (compute wall_contact, replica " + std::to_string(r) + ")";
+        return DPD_E_STATE;
+    }
+    if (s & ST_BAD_INPUT) {
+        err = "an atom id or type in the AoS input is outside the engine's system";
+        return DPD_E_ARG;
     }
     return DPD_OK;
 }

@@ -139,6 +139,11 @@ public:
     // per-replica step limits: replica r evaluates no step beyond limit[r]
     int set_limits(const std::vector<uint32_t>& limit);
     int read_rstate(std::vector<RepState>& st);
+    // enqueue a copy of every replica's state word into host memory (pinned, n_rep entries)
+    // on the engine's stream, after the work enqueued so far
+    int rstate_async(RepState* host);
+    // the error of a device status word of replica r (DPD_OK when clean)
+    int status_error(int status, int r);
     cudaStream_t stream() const { return stream_; }
     // device bytes init() would allocate for these replicas (no CUDA calls)
     static int64_t estimate_bytes(const std::vector<const Replica*>& reps);

@@ -6,9 +6,10 @@
 //      memory of the admitted set fits the budget; admitted jobs of similar length
 //      (steps within a factor 2) become one cohort: one packed engine (one launch per
 //      stage for all of them, the step captured in a CUDA graph) on its own CUDA stream;
-//   2. keeps every cohort's stream fed with chunks of steps: a cohort whose chunk has
-//      completed gets its next one at once, without waiting for the others, so the
-//      cohorts' kernels overlap on the device;
+//   2. keeps every cohort's stream fed with chunks of steps, two in flight: while one
+//      runs, the next is queued behind it, and a completed chunk is checked from a copy
+//      of the replicas' state words taken on the stream after it, so the stream never
+//      waits for the host; the cohorts' kernels overlap on the device;
 //   3. retires the jobs that reached their `run N`: their thermo rows, final state and
 //      RDF are copied out, and a cohort's device memory returns to the budget when its
 //      last job has finished.
@@ -53,6 +54,13 @@ struct Job {
     int64_t rdf_samples = 0;
 };
 
+// A chunk of steps in flight: an event after it and the replicas' state words copied
+// (pinned host memory) on the stream after it.
+struct Chunk {
+    cudaEvent_t ev = nullptr;
+    RepState* rs = nullptr;
+};
+
 struct Cohort {
     std::unique_ptr<dpd::Engine> eng;
     std::vector<int64_t> jobs;  // job id of each replica
@@ -60,8 +68,18 @@ struct Cohort {
     uint32_t max_steps = 0;     // longest job in the cohort
     uint32_t issued = 0;        // steps issued after the zero step
     bool started = false;
-    bool inflight = false;      // a chunk is enqueued and not yet checked
+    Chunk slot[2];
+    std::deque<int> pending;    // slots of the enqueued chunks not yet checked, oldest first
+    int next_slot = 0;
     int64_t bytes = 0;
+    ~Cohort()
+    {
+        if (eng) cudaStreamSynchronize(eng->stream());
+        for (Chunk& k : slot) {
+            if (k.ev) cudaEventDestroy(k.ev);
+            if (k.rs) cudaFreeHost(k.rs);
+        }
+    }
 };
 
 // list capacity and bonds per atom of one job, as the engine's layout computes them
@@ -192,6 +210,11 @@ int dpd_server::make_cohort(const std::vector<int64_t>& ids)
         }
         return fail(e, "admitting " + std::to_string(ids.size()) + " job(s): " + msg);
     }
+    for (Chunk& k : c->slot) {
+        if (cudaEventCreateWithFlags(&k.ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost((void**)&k.rs, sizeof(RepState) * ids.size()) != cudaSuccess)
+            return fail(DPD_E_CUDA, "cannot create a cohort's chunk events");
+    }
     c->bytes = c->eng->device_bytes();
     used_bytes += c->bytes;
     for (int64_t id : ids) {
@@ -248,43 +271,64 @@ int dpd_server::advance()
         err = "cohort failed: " + c.eng->err;
         if (!first_err) first_err = rc;
     };
+    auto all_done = [](const Cohort& c) {
+        return std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; });
+    };
     for (auto& cp : cohorts) {
         Cohort& c = *cp;
-        if (c.inflight) {
-            if (cudaStreamQuery(c.eng->stream()) == cudaErrorNotReady) continue;
-            c.inflight = false;
+        // completed chunks, oldest first: errors from their status words, finished jobs
+        bool failed = false;
+        while (!c.pending.empty()) {
+            const Chunk& k = c.slot[c.pending.front()];
+            const cudaError_t q = cudaEventQuery(k.ev);
+            if (q == cudaErrorNotReady) break;
+            c.pending.pop_front();
             progressed = true;
-            int rc = c.eng->sync_and_check();
-            std::vector<RepState> st;
-            if (!rc) rc = c.eng->read_rstate(st);
+            int rc = DPD_OK;
+            if (q != cudaSuccess) {
+                c.eng->err = std::string("CUDA error in a chunk: ") + cudaGetErrorString(q);
+                rc = DPD_E_CUDA;
+            }
+            for (size_t r = 0; r < c.jobs.size() && !rc; r++)
+                if (!c.finished[r]) rc = c.eng->status_error(k.rs[r].status, (int)r);
             if (rc) {
                 fail_cohort(c, rc);
-                continue;
+                cudaStreamSynchronize(c.eng->stream());
+                c.pending.clear();
+                failed = true;
+                break;
             }
             for (size_t r = 0; r < c.jobs.size(); r++) {
                 if (c.finished[r]) continue;
-                if (st[r].step > jobs[c.jobs[r]].steps) {
+                if (k.rs[r].step > jobs[c.jobs[r]].steps) {
                     retire_job(c, (int)r, c.jobs[r]);
                     c.finished[r] = true;
                 }
             }
         }
-        if (std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; })) continue;
-        const uint32_t n = std::min<uint32_t>((uint32_t)chunk, c.max_steps - c.issued);
-        const int rc = c.eng->run_async(n);  // the first call also runs the zero step
-        if (rc) {
-            fail_cohort(c, rc);
-            continue;
+        if (failed) continue;
+        // keep two chunks in flight until the longest job's steps are issued
+        while (c.pending.size() < 2 && !all_done(c) && (!c.started || c.issued < c.max_steps)) {
+            const uint32_t n = std::min<uint32_t>((uint32_t)chunk, c.max_steps - c.issued);
+            Chunk& k = c.slot[c.next_slot];
+            int rc = c.eng->run_async(n);  // the first call also runs the zero step
+            if (!rc) rc = c.eng->rstate_async(k.rs);
+            if (!rc && cudaEventRecord(k.ev, c.eng->stream()) != cudaSuccess) rc = DPD_E_CUDA;
+            if (rc) {
+                fail_cohort(c, rc);
+                break;
+            }
+            c.pending.push_back(c.next_slot);
+            c.next_slot ^= 1;
+            c.started = true;
+            c.issued += n;
+            progressed = true;
         }
-        c.started = true;
-        c.issued += n;
-        c.inflight = true;
-        progressed = true;
     }
     // release cohorts whose jobs have all finished
     for (size_t k = 0; k < cohorts.size();) {
         Cohort& c = *cohorts[k];
-        if (!c.inflight && std::all_of(c.finished.begin(), c.finished.end(), [](bool b) { return b; })) {
+        if (c.pending.empty() && all_done(c)) {
             used_bytes -= c.bytes;
             cohorts.erase(cohorts.begin() + k);
         } else {
