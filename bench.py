@@ -49,6 +49,15 @@ def build_launches(system, skin):
     return 3 + (1 if cells <= 4096 else 3) + (0 if (slots + 255) // 256 <= 148 * 8 else 1)
 
 
+def step_launches(system, pair_variant):
+    """Kernels of one step after the list build: on small grids (up to 1184 blocks of 256
+    slots) the pair pass and the integrate with the bookkeeping are one launch each; else
+    the pair kernel(s), the integrate pair (non-log steps + log steps) and advance."""
+    if (system.n + 31 + 255) // 256 <= 148 * 8 and pair_variant == 8:
+        return 2
+    return (2 if pair_variant in (7, 8, 9) else 1) + 3
+
+
 def make_system(args):
     from gpumdpd_b200 import inputs
     if args.workload == "melt":
@@ -265,8 +274,8 @@ def run_ours(args, world, rank, local):
         # per step: the list-build kernels (counting pass, 1 or 3 scan launches, permutation,
         # list; each returns at once unless a build is flagged), the pair kernel(s), the
         # integrate pair (non-log steps + log steps), advance; plus 2 before the graph
-        "gpu_launches": int(args.steps * (build_launches(system, args.skin) + 3 +
-                                          (2 if pair_variant in (7, 8, 9) else 1)) + 2),
+        "gpu_launches": int(args.steps * (build_launches(system, args.skin) +
+                                          step_launches(system, pair_variant)) + 2),
         "impl": "ours",
     }
     del th, st2

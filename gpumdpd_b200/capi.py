@@ -65,7 +65,7 @@ class dpd_thermo(ctypes.Structure):
 class dpd_tuning(ctypes.Structure):
     _fields_ = [
         ("pair_block", ctypes.c_int), ("pair_variant", ctypes.c_int), ("cell_order", ctypes.c_int),
-        ("build_variant", ctypes.c_int), ("reserved", ctypes.c_int * 4),
+        ("build_variant", ctypes.c_int), ("launch_mode", ctypes.c_int), ("reserved", ctypes.c_int * 3),
     ]
 
 

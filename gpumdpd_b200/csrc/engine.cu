@@ -266,6 +266,7 @@ int Engine::alloc_and_upload()
     DA(b_.cnt, C_);
     DA(b_.cstart, C_ + 1);
     DA(b_.ticket, 1);
+    DA(b_.ticket2, 1);
     DA(b_.skey, P_);
     DA(b_.srank, P_);
     int64_t ntag = 0;
@@ -685,6 +686,7 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     a.gc_ring = b.gc_ring;
     a.gc_count = b.gc_count;
     a.wall_ext = b.wall_ext;
+    a.ticket = b.ticket2;
     return a;
 }
 
@@ -777,7 +779,9 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     const int nrep = (int)reps_.size();
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
     const int gp = (P_ + 255) / 256;
-    const int variant = tune_.pair_variant;
+    // small grids: fewer, larger launches (the pair pass and the integrate each in one)
+    const bool small = tune_.launch_mode == 2 || (tune_.launch_mode == 0 && gp <= 148 * 8);
+    const int variant = small && tune_.pair_variant == 8 ? 4 : tune_.pair_variant;
     // schedule 6: the DPD list build runs inside the pair kernel
     const bool fused = variant == 6 && !any_mdpd_;
     enqueue_build(s, !fused);
@@ -809,6 +813,12 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
         // wall_contact computes: wall extents of the end-of-step positions
         pdl_launch(k_wall_reset<1>, gr, 256, s, sa);
         pdl_launch(k_wall_extent<1>, gp, 256, s, sa);
+    }
+    if (small && !any_twowall_) {
+        // the step's bookkeeping runs in the integrate's last block
+        if (ext()) pdl_launch(k_integrate_adv<true>, gp, 256, s, sa);
+        else pdl_launch(k_integrate_adv<false>, gp, 256, s, sa);
+        return;
     }
     if (ext()) {
         pdl_launch(k_integrate_nolog<true>, gp, 256, s, sa);
@@ -1470,8 +1480,9 @@ int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
     if (t->pair_variant < 0 || t->pair_variant > 9 || t->cell_order < 0 || t->cell_order > 1 ||
-        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 2) {
-        err = "dpd_set_tuning: pair_variant must be 0..9, build_variant 0..2, cell_order 0 or 1";
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 2 || t->launch_mode < 0 ||
+        t->launch_mode > 2) {
+        err = "dpd_set_tuning: pair_variant must be 0..9, build_variant 0..2, cell_order 0 or 1, launch_mode 0..2";
         return DPD_E_ARG;
     }
     tune_ = *t;

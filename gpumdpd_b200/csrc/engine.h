@@ -60,6 +60,7 @@ struct DeviceBuffers {
     int *cnt = nullptr, *cstart = nullptr, *skey = nullptr, *srank = nullptr, *tag2idx = nullptr;
     int *ncount = nullptr, *nlist = nullptr, *blocksum = nullptr;
     unsigned int* ticket = nullptr;  // k_permute's last-block counter
+    unsigned int* ticket2 = nullptr; // k_integrate_adv's last-block counter
     double *acc = nullptr, *ring = nullptr;
     unsigned long long* rdf_hist = nullptr;
     int* build_flag = nullptr;

@@ -33,6 +33,7 @@ struct StepArgs {
     const FixDesc* fix;    // [nrep] group fixes (null when no replica has one)
     FixOut* fixo;          // [nrep]
     double* spring_ring;   // [nrep][DPD_RING_ROWS][6] spring records (null: none)
+    unsigned int* ticket;  // blocks of k_integrate_adv done (reset by the last one)
     const GCDesc* gc;      // [nrep][DPD_MAX_GC] group computes (null when none)
     const float4* uw0;     // [atoms of all replicas] initial unwrapped positions by global tag
     double* gc_ring;       // [computes][DPD_RING_ROWS][4] rows {step, values}
@@ -1327,11 +1328,9 @@ __global__ void __launch_bounds__(256) k_angle(StepArgs a, const int4* __restric
 // ---------------------------------------------------------------------------------
 // End of step bookkeeping, one thread per replica: thermo row of a logged step
 // (src/compute/thermo.cu:274-306, 479-520), step counter, build flag of this phase.
-__global__ void k_advance(StepArgs a)
+__device__ __forceinline__ void advance_rep(const StepArgs& a, const int r)
 {
-    griddep_wait();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < a.nrep) {
+    {
         RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
         if (rep_active(st)) {
@@ -1392,10 +1391,47 @@ __global__ void k_advance(StepArgs a)
             a.rstate[r] = st;
         }
     }
-    if (r == 0) {
-        uint32_t ph = *a.phase;
-        a.build_flag[ph & 1] = 0;
-        *a.phase = ph + 1u;
+}
+
+// the step's phase: this phase's build flag cleared, the phase counter advanced
+__device__ __forceinline__ void advance_phase(const StepArgs& a)
+{
+    const uint32_t ph = *a.phase;
+    a.build_flag[ph & 1] = 0;
+    *a.phase = ph + 1u;
+}
+
+__global__ void k_advance(StepArgs a)
+{
+    griddep_wait();
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < a.nrep) advance_rep(a, r);
+    if (r == 0) advance_phase(a);
+}
+
+// Small grids, where a launch costs more than the work: the whole velocity-Verlet step
+// (any step, logged or not) in one launch whose last block (a ticket counter) also does
+// the step's bookkeeping of every replica.  Every block's writes and FP64 sums are done
+// and fenced before it takes its ticket.
+template <bool EXT>
+__global__ void __launch_bounds__(256) k_integrate_adv(StepArgs a)
+{
+    griddep_wait();
+    integrate_slot<2, EXT>(a, blockIdx.x * blockDim.x + threadIdx.x);
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) advance_rep(a, r);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        advance_phase(a);
+        *a.ticket = 0u;
     }
 }
 

@@ -91,7 +91,11 @@ typedef struct dpd_tuning {
     int build_variant;     /* list build: 0 = cell ranges in registers, 4
                               blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
                               8 blocks/SM                                         */
-    int reserved[4];
+    int launch_mode;       /* 0 = small grids (up to 1184 blocks of 256 slots) run the
+                              pair pass (schedule 8) and the integrate each as one
+                              launch, the step's bookkeeping in the integrate's
+                              last block; 1 = never; 2 = always                   */
+    int reserved[3];
 } dpd_tuning;
 
 /* ---- plain engine: replaces main()/read_info/preprocess/zero_step/simulation

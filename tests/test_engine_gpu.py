@@ -511,3 +511,38 @@ def test_rdf_samples_over_a_run_vs_oracle(oracle_mod, skin, nl_f):
     # FP32 distances against FP64 ones: a pair within ~1e-7 of a bin edge may land in the
     # neighbouring bin (a few counts in 1e4-1e5 per bin)
     np.testing.assert_allclose(g, go, rtol=2e-3, atol=2e-3)
+
+
+@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "probe_fixes"])
+def test_small_grid_launches_match_split_launches(oracle_mod, name):
+    """Small grids run the pair pass and the integrate (with the step's bookkeeping in its
+    last block) as one launch each; the split launches of large grids (launch_mode 1) give
+    the same thermo rows and state, to FP32 summation order, over logged and non-logged
+    steps, with the group fixes and computes too."""
+    from gpumdpd_b200 import inputs
+    if name == "probe_fixes":
+        s = inputs.probe_fixes(L=9.0, seed=77, nsteps=20, thermo=3, spring_file=None)
+        s.run_in += "compute ct probe temp 2 t.txt\n"
+    else:
+        s = _systems()[name]
+        s.run_in = re.sub(r"(?m)^thermo \d+$", "thermo 3", s.run_in)
+    runs = []
+    for mode in (0, 1):
+        e = _engine_from(s)
+        e.set_tuning(pair_variant=8, cell_order=1, launch_mode=mode)
+        e.run(0)
+        e.run(7)
+        e.run(5)
+        runs.append((e.thermo(), e.state(), e.compute("ct") if name == "probe_fixes" else None, e.info()))
+    (ta, sa, ca, ia), (tb, sb, cb, ib) = runs
+    assert ia["step"] == ib["step"] == 12  # the last evaluated step
+    np.testing.assert_array_equal(ta["step"], tb["step"])
+    np.testing.assert_allclose(ta["temp"], tb["temp"], rtol=1e-4)
+    np.testing.assert_allclose(ta["pressure"], tb["pressure"], rtol=1e-4, atol=1e-4)
+    L = s.hi - s.lo
+    dx = sa["x"] - sb["x"]
+    dx -= L * np.round(dx / L)
+    assert np.abs(dx).max() < 1e-4
+    if ca is not None:
+        np.testing.assert_array_equal(ca[:, 0], cb[:, 0])
+        np.testing.assert_allclose(ca[:, 1], cb[:, 1], rtol=1e-4)
