@@ -49,6 +49,18 @@ def build_launches(system, skin):
     return 3 + (1 if cells <= 4096 else 3) + (0 if (slots + 255) // 256 <= 148 * 8 else 1)
 
 
+def pair_kernel_name(system, pair_variant):
+    """The pair kernel the engine launches for this system: on tiny grids (up to 148 blocks
+    of 256 slots) one thread per list entry, on small grids (up to 1184) the flattened
+    schedule as one launch, else the flattened schedule split by log steps."""
+    gp = (system.n + 31 + 255) // 256
+    if pair_variant == 8 and gp <= 148:
+        return "k_pair_entry (thread per list entry, tiny grids)"
+    if pair_variant == 8 and gp <= 148 * 8:
+        return "k_pair_flat (flattened pair schedule, one launch on small grids)"
+    return "k_pair_flat_split + k_pair_flat_logsteps (flattened pair schedule)"
+
+
 def step_launches(system, pair_variant):
     """Kernels of one step after the list build: on small grids (up to 1184 blocks of 256
     slots) the pair pass and the integrate with the bookkeeping are one launch each; else
@@ -244,6 +256,11 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    # state (two parity buffers of position, velocity, image and bond partners) + half list
+    foot = n * (2 * (48 + 8 * maxb) + 4 * 48 + 16)
+    l2 = (f"inputs larger than L2 (state+list ~{foot / 1e9:.2f} GB)" if foot > 126e6 else
+          f"inputs smaller than L2 (state+list ~{foot / 1e6:.1f} MB): L2-resident, no flush; "
+          "a latency-bound small system, not the headline workload")
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
@@ -263,11 +280,11 @@ def run_ours(args, world, rank, local):
                    "list_builds_per_step": builds_per_step, "pair_variant": pair_variant,
                    "build_variant": args.build_variant,
                    "tuned": tuned, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state+list > 1 GB)"},
+                   "l2": l2},
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "chunk_steps": chunk, "path": "dpd_set_state + dpd_run + dpd_get_state (C ABI, host buffers)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "k_pair_flat (flattened pair schedule, DPD + bonds)",
+                     "traffic": traffic, "kernel": pair_kernel_name(system, pair_variant),
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
         "clocks": clk.summary(),

@@ -727,6 +727,8 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
     } else if (variant == 9) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5, true>, grid, 256, s, a);
         pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 4), 256, s, a);
+    } else if (variant == 10) {
+        pdl_launch(k_pair_entry<STYLE, BONDS>, (a.nmax * (a.P >> 5) + 7) / 8, 256, s, a);
     }
     else pdl_launch(k_pair_q<STYLE, BONDS, 4, false>, grid, 256, s, a);
 }
@@ -737,7 +739,8 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
 // warp schedule, 4 blocks/SM; 5: flattened, 3 blocks/SM; 6: the flattened schedule with
 // the list build fused into it (DPD; mDPD falls back to 4); 7 and 8 (the default): the
 // flattened schedule as two launches, non-log steps without FP64 sums at 6 (7) or 5 (8)
-// blocks/SM, log steps at 4; 9: as 8 with the i-side forces summed per owner in the warp
+// blocks/SM, log steps at 4; 9: as 8 with the i-side forces summed per owner in the warp;
+// 10: one thread per list entry (small grids)
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -746,7 +749,7 @@ static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const
 }
 
 // The list-build chain; every kernel returns at once unless this phase's flag is set.
-void Engine::enqueue_build(cudaStream_t s, bool list)
+void Engine::enqueue_build(cudaStream_t s, bool list, bool wide)
 {
     const int nrep = (int)reps_.size();
     BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
@@ -768,7 +771,8 @@ void Engine::enqueue_build(cudaStream_t s, bool list)
         pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
     }
     if (list) {
-        if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
+        if (wide && gp <= 148 * 8) pdl_launch(k_build_wide, (14 * P_ + 255) / 256, 256, s, ba);
+        else if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
         else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);
         else pdl_launch(k_build_nlist, gp, 256, s, ba);
     }
@@ -780,11 +784,17 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
     const int gp = (P_ + 255) / 256;
     // small grids: fewer, larger launches (the pair pass and the integrate each in one)
-    const bool small = tune_.launch_mode == 2 || (tune_.launch_mode == 0 && gp <= 148 * 8);
-    const int variant = small && tune_.pair_variant == 8 ? 4 : tune_.pair_variant;
+    const bool small = tune_.launch_mode == 2 || ((tune_.launch_mode == 0 || tune_.launch_mode == 3) && gp <= 148 * 8);
+    // tiny grids (at most one block of 256 slots per SM): the list build with a thread per
+    // (slot, stencil cell) and the pair pass with a thread per list entry; past that their
+    // idle lanes cost more than the parallelism gains.  launch_mode 3 leaves them out: an
+    // engine that shares the GPU with others (a server's cohorts) gains more from leaving
+    // SMs to them than from spreading its own few pairs
+    const bool tiny = small && gp <= 148 && tune_.launch_mode != 3;
+    const int variant = small && tune_.pair_variant == 8 ? (tiny ? 10 : 4) : tune_.pair_variant;
     // schedule 6: the DPD list build runs inside the pair kernel
     const bool fused = variant == 6 && !any_mdpd_;
-    enqueue_build(s, !fused);
+    enqueue_build(s, !fused, (tiny && tune_.build_variant == 0) || tune_.build_variant == 3);
     if (any_mdpd_) pdl_launch(k_density, gp, 256, s, sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
     if (fused) {
@@ -1479,10 +1489,10 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 9 || t->cell_order < 0 || t->cell_order > 1 ||
-        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 2 || t->launch_mode < 0 ||
-        t->launch_mode > 2) {
-        err = "dpd_set_tuning: pair_variant must be 0..9, build_variant 0..2, cell_order 0 or 1, launch_mode 0..2";
+    if (t->pair_variant < 0 || t->pair_variant > 10 || t->cell_order < 0 || t->cell_order > 1 ||
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 3 || t->launch_mode < 0 ||
+        t->launch_mode > 3) {
+        err = "dpd_set_tuning: pair_variant must be 0..10, build_variant 0..3, cell_order 0 or 1, launch_mode 0..3";
         return DPD_E_ARG;
     }
     tune_ = *t;
@@ -1620,7 +1630,7 @@ int Engine::pair_compute_aos(const float* d_pos, const float* d_vel, const int* 
     StepArgs sa = step_args(b_, P_, nmax_, maxb_, 1);
     const int gp = (P_ + 255) / 256;
     k_aos_in<<<(n + 255) / 256, 256, 0, stream_>>>(sa, d_pos, d_vel, d_id, d_type, n, step, aos_built_ ? 0 : 1);
-    enqueue_build(stream_);
+    enqueue_build(stream_, true, tune_.build_variant == 3);
     if (any_mdpd_) k_density<<<gp, 256, 0, stream_>>>(sa);
     const bool peratom = d_pe || d_virial;
     if (d.style == 0) {

@@ -154,7 +154,7 @@ private:
     int alloc_and_upload();
     int upload_particles();
     void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
-    void enqueue_build(cudaStream_t s, bool list = true);
+    void enqueue_build(cudaStream_t s, bool list = true, bool wide = false);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
     int dump_frame(DumpWriter* w, uint32_t step);

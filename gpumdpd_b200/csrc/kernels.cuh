@@ -356,6 +356,7 @@ __global__ void k_permute(BuildArgs a, int nrep)
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < a.P) permute_slot(a, s);
     if (!FLIP) return;
+    if (s < a.P) a.ncount[s] = 0;  // k_build_wide counts with atomics
     __shared__ bool last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -470,6 +471,59 @@ __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
     griddep_wait();
     if (!build_on(a)) return;
     build_nlist_slot(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Small grids, where one thread per particle leaves most of the GPU idle and each thread's
+// 14 cell ranges form a long serial chain: the same half list with one thread per (slot,
+// stencil cell), the 14 threads of a slot appending to its list through an atomic count
+// (zeroed by k_permute<true>, which always precedes it).  The same entries and the same
+// predicate; their order within a slot's list is the order the atomics drew, and a count
+// above nmax is left in place (every reader clamps it) with the overflow flagged.
+__global__ void __launch_bounds__(256) k_build_wide(BuildArgs a)
+{
+    griddep_wait();
+    if (!build_on(a)) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 14 * a.P) return;
+    const int st = t / a.P, s = t - st * a.P;  // consecutive threads: consecutive slots
+    const int r = a.warp_rep[s >> 5];
+    const RepDesc& d = a.reps[r];
+    if (s >= d.p_end || a.rstate[r].step > a.rstate[r].target) return;  // no list
+    const float4* pos = a.buf.pos[*a.parity];
+    const float4 pi = pos[s];
+    const int code = __float_as_int(pi.w);
+    const int ox = st ? c_half[st - 1][0] : 0, oy = st ? c_half[st - 1][1] : 0, oz = st ? c_half[st - 1][2] : 0;
+    int nx = cell_x(code) + ox; nx += nx < 0 ? d.nc[0] : 0; nx -= nx >= d.nc[0] ? d.nc[0] : 0;
+    int ny = cell_y(code) + oy; ny += ny < 0 ? d.nc[1] : 0; ny -= ny >= d.nc[1] ? d.nc[1] : 0;
+    int nz = cell_z(code) + oz; nz += nz < 0 ? d.nc[2] : 0; nz -= nz >= d.nc[2] ? d.nc[2] : 0;
+    const int key = d.c_begin + __ldg(a.crank + d.c_begin + (nx * d.nc[1] + ny) * d.nc[2] + nz);
+    const int jb = st ? __ldg(a.cstart + key) : s + 1, je = __ldg(a.cstart + key + 1);
+    const float sx = __int2float_rn(-ox) * d.w[0], sy = __int2float_rn(-oy) * d.w[1], sz = __int2float_rn(-oz) * d.w[2];
+    const int tagbits = ((1 - ox) * 9 + (1 - oy) * 3 + (1 - oz)) << DPD_CODE_SHIFT;
+    const float cut2 = d.cut2;
+    int* out = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+    for (int j0 = jb; j0 < je; j0 += 4) {
+        float4 pj[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (j0 + u < je) pj[u] = pos[j0 + u];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (j0 + u < je) {
+                const float dx = __fadd_rn(__fsub_rn(pi.x, pj[u].x), sx);
+                const float dy = __fadd_rn(__fsub_rn(pi.y, pj[u].y), sy);
+                const float dz = __fadd_rn(__fsub_rn(pi.z, pj[u].z), sz);
+                float r2 = __fmul_rn(dx, dx);
+                r2 = __fmaf_rn(dy, dy, r2);
+                r2 = __fmaf_rn(dz, dz, r2);
+                if (r2 <= cut2) {
+                    const int k = atomicAdd(a.ncount + s, 1);
+                    if (k < a.nmax) out[(size_t)k * 32] = (j0 + u) | tagbits;
+                    else atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+                }
+            }
+        }
+    }
 }
 
 // The same list with the 14 cell ranges kept in shared memory instead of registers

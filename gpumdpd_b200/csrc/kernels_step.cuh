@@ -357,6 +357,76 @@ __global__ void __launch_bounds__(256) k_pair(StepArgs a)
 }
 
 // ---------------------------------------------------------------------------------
+// Pair force for small grids: one thread per list entry.  Warp w takes line k of the
+// warp-interleaved list (the k-th entries of 32 slots) with k = w / (P/32), so the few
+// pairs of a small system spread over the whole GPU instead of a few warps walking them
+// in turn, and the warps past the longest list return at once.  Both sides of a pair are
+// float4 reductions; the bonds of a slot are taken by its k = 0 thread.
+template <int STYLE, bool BONDS>
+__global__ void __launch_bounds__(256) k_pair_entry(StepArgs a)
+{
+    griddep_wait();
+    __shared__ float4 tab[8][27];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = a.P >> 5;
+    const int line = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int k = line / nw, wslot = line - k * nw;
+    int r = -1;
+    bool wactive = false, log = false;
+    uint32_t step = 0;
+    if (k < a.nmax) {
+        r = a.warp_rep[wslot];
+        const RepState st = a.rstate[r];
+        const RepDesc& d = a.reps[r];
+        wactive = rep_active(st) && d.style == STYLE;
+        step = st.step;
+        log = wactive && (step % (uint32_t)d.log_f) == 0u;
+        if (wactive) fill_shift(tab[warp], d, lane);
+    }
+    __syncwarp();
+    double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int s = wslot * 32 + lane;
+    if (wactive && s < a.reps[r].p_end) {
+        const RepDesc& d = a.reps[r];
+        const int par = *a.parity;
+        const float4* pos = a.buf.pos[par];
+        if (k < min(a.ncount[s], a.nmax)) {
+            const float4* vel = a.buf.vel[par];
+            const int ent = __ldg(a.nlist + ((size_t)wslot * a.nmax + k) * 32 + lane);
+            const int j = ent & DPD_J_MASK;
+            const float4 pi = pos[s], pj = __ldg(pos + j);
+            float dx, dy, dz;
+            pair_disp(tab[warp], ent, pi, pj, dx, dy, dz);
+            const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+            if (r2 <= d.rcmax2) {
+                const float4 vi = vel[s], vj = __ldg(vel + j);
+                const float rho_i = STYLE == 1 ? a.rho[s] : 0.0f, rho_j = STYLE == 1 ? __ldg(a.rho + j) : 0.0f;
+                const float4* crow = a.coeff + d.coeff_off + type0_of(vi.w) * d.ntypes * 3;
+                float gx, gy, gz;
+                const bool ok = log ? pair_force<STYLE, true>(crow, r2, dx, dy, dz, vi, vj, rho_i, rho_j, d.seed, step, gx, gy, gz, accv)
+                                    : pair_force<STYLE, false>(crow, r2, dx, dy, dz, vi, vj, rho_i, rho_j, d.seed, step, gx, gy, gz, accv);
+                if (ok) {
+                    atomicAdd(&a.force4[j], make_float4(-gx, -gy, -gz, 0.0f));
+                    atomicAdd(&a.force4[s], make_float4(gx, gy, gz, 0.0f));
+                }
+            }
+        }
+        if (BONDS && k == 0) {
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+            const float4 pi = pos[s];
+            if (log) bond_loop<true>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+            else bond_loop<false>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
+            atomicAdd(&a.force4[s], make_float4(fx, fy, fz, 0.0f));
+        }
+    }
+    if (__syncthreads_or(log)) {
+        const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
+                               ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+        acc_flush<8>(accv, fields, log ? r : -1, a.acc);
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Pair force, warp pair-queue schedule.  Thread-per-particle loops diverge on the
 // ~130-instruction Saru evaluation (only the pairs inside rc need it), so each warp
 // first filters its 32 particles' list candidates (DPD_U per lane per iteration, loads

@@ -106,7 +106,6 @@ struct dpd_server {
     double budget = 0;
     int chunk = 100;
     dpd_tuning tune{};
-    bool has_tune = false;
     std::map<int64_t, Job> jobs;
     std::deque<int64_t> queue;
     std::vector<std::unique_ptr<Cohort>> cohorts;
@@ -198,7 +197,7 @@ int dpd_server::make_cohort(const std::vector<int64_t>& ids)
     }
     c->finished.assign(ids.size(), false);
     c->eng = std::make_unique<dpd::Engine>();
-    int e = c->eng->init(std::move(reps), has_tune ? &tune : nullptr);
+    int e = c->eng->init(std::move(reps), &tune);
     if (!e) e = c->eng->set_limits(limits);
     const double t = now();
     if (e) {
@@ -355,8 +354,12 @@ int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning
     s->chunk = chunk_steps;
     if (tune) {
         s->tune = *tune;
-        s->has_tune = true;
+    } else {  // the engine defaults
+        s->tune.cell_order = 1;
+        s->tune.pair_variant = 8;
     }
+    // cohorts run side by side: no tiny-grid kernels (launch_mode 3 for 0)
+    if (s->tune.launch_mode == 0) s->tune.launch_mode = 3;
     *out = s;
     return DPD_OK;
 }

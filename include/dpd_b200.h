@@ -86,15 +86,23 @@ typedef struct dpd_tuning {
                               6 = flattened with the list build fused (DPD),
                               7-8 = flattened, log and non-log steps split (8 is
                               the default), 9 = as 8 with the i-side forces summed
-                              per owner in the warp before the reduction         */
+                              per owner in the warp before the reduction,
+                              10 = one thread per list entry                     */
     int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
     int build_variant;     /* list build: 0 = cell ranges in registers, 4
                               blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
-                              8 blocks/SM                                         */
+                              8 blocks/SM; 3 = a thread per (slot, stencil cell)
+                              (grids up to 1184 blocks; larger ones use 0)        */
     int launch_mode;       /* 0 = small grids (up to 1184 blocks of 256 slots) run the
-                              pair pass (schedule 8) and the integrate each as one
-                              launch, the step's bookkeeping in the integrate's
-                              last block; 1 = never; 2 = always                   */
+                              pair pass as one launch (schedule 4 in place of 8) and
+                              the integrate as one, the step's bookkeeping in the
+                              integrate's last block; tiny ones (up to 148 blocks)
+                              also build the list with a thread per (slot, stencil
+                              cell) (in place of build variant 0) and run the pair
+                              pass with a thread per list entry (schedule 10);
+                              1 = never; 2 = always; 3 = as 0 without the tiny-grid
+                              kernels (the server's cohorts: engines that share
+                              the GPU run better on fewer, fuller blocks)         */
     int reserved[3];
 } dpd_tuning;
 
@@ -284,6 +292,8 @@ typedef struct dpd_job_result {
     dpd_thermo last;
 } dpd_job_result;
 
+/* `tune` (NULL: the engine defaults) applies to every cohort; its launch_mode 0 runs
+ * as 3, since the cohorts share the GPU. */
 int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning* tune,
                       dpd_server** out);
 /* Submit a job (copies the inputs); *job_id receives its id. */

@@ -93,7 +93,7 @@ def test_step0_forces_vs_oracle_and_reference(oracle_mod, name):
     assert th["pressure"][0] == pytest.approx(g["thermo_pressure"][0], rel=2e-5)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
 @pytest.mark.parametrize("name", ["mdpd_slab", "diblock", "mix_rc"])
 def test_pair_schedules_agree_with_oracle(oracle_mod, name, variant):
     """Every pair-kernel schedule the tuner may pick gives the oracle's step-0 forces and
@@ -242,11 +242,14 @@ def test_long_run_statistics_vs_oracle(oracle_mod):
         assert abs(a.mean() - b.mean()) < 4 * err, key
 
 
-def test_overflow_is_reported_not_silent():
-    """A neighbour capacity below need is an error status, never a silent truncation."""
+@pytest.mark.parametrize("launch_mode", [0, 1])
+def test_overflow_is_reported_not_silent(launch_mode):
+    """A neighbour capacity below need is an error status, never a silent truncation, from
+    the small-grid list build (a thread per slot and stencil cell) and the large-grid one."""
     from gpumdpd_b200 import DpdError, inputs
     s = inputs.plain_dpd(L=8.0, seed=3, max_rho=0.2)
     e = _engine_from(s)
+    e.set_tuning(pair_variant=8, cell_order=1, launch_mode=launch_mode)
     with pytest.raises(DpdError) as ex:
         e.run(0)
     assert ex.value.code == -5
@@ -468,16 +471,18 @@ def test_walls_vs_reference_and_oracle(oracle_mod, name):
     assert np.abs(wc[:, 1] - ref[:, 1]).max() <= 1
 
 
-@pytest.mark.parametrize("build_variant", [1, 2])
+@pytest.mark.parametrize("build_variant,launch_mode", [(1, 0), (2, 0), (0, 1), (3, 1)])
 @pytest.mark.parametrize("name", ["dpd", "diblock", "small_box"])
-def test_build_variants_give_the_same_list(oracle_mod, name, build_variant):
-    """The list-build kernels with the cell ranges in shared memory build the same half
-    list (bit-exact tag-pair sets) and the same step-0 forces as the register version."""
+def test_build_variants_give_the_same_list(oracle_mod, name, build_variant, launch_mode):
+    """The list-build kernels with the cell ranges in shared memory, and the large-grid
+    thread-per-slot build (launch_mode 1), build the same half list (bit-exact tag-pair
+    sets) and the same step-0 forces as the small-grid build with a thread per slot and
+    stencil cell that these systems get by default."""
     s = _systems()[name]
     a = _engine_from(s)
     a.run(0)
     b = _engine_from(s)
-    b.set_tuning(pair_variant=8, cell_order=1, build_variant=build_variant)
+    b.set_tuning(pair_variant=8, cell_order=1, build_variant=build_variant, launch_mode=launch_mode)
     b.run(0)
     got = set(map(tuple, b.neighbors().tolist()))
     assert got == set(map(tuple, a.neighbors().tolist()))
@@ -513,36 +518,41 @@ def test_rdf_samples_over_a_run_vs_oracle(oracle_mod, skin, nl_f):
     np.testing.assert_allclose(g, go, rtol=2e-3, atol=2e-3)
 
 
-@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "probe_fixes"])
+@pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "probe_fixes", "dpd_41k"])
 def test_small_grid_launches_match_split_launches(oracle_mod, name):
     """Small grids run the pair pass and the integrate (with the step's bookkeeping in its
-    last block) as one launch each; the split launches of large grids (launch_mode 1) give
-    the same thermo rows and state, to FP32 summation order, over logged and non-logged
-    steps, with the group fixes and computes too."""
+    last block) as one launch each, and tiny ones (up to 148 blocks of 256 slots; all but
+    the 41k-particle box here) build the list with a thread per (slot, stencil cell) and
+    run the pair pass with a thread per list entry; the split launches of large grids
+    (launch_mode 1) give the same thermo rows and state, to FP32 summation order, over
+    logged and non-logged steps, with the group fixes and computes too."""
     from gpumdpd_b200 import inputs
     if name == "probe_fixes":
         s = inputs.probe_fixes(L=9.0, seed=77, nsteps=20, thermo=3, spring_file=None)
         s.run_in += "compute ct probe temp 2 t.txt\n"
+    elif name == "dpd_41k":
+        s = inputs.plain_dpd(L=24.0, seed=78, nsteps=20, thermo=3)
     else:
         s = _systems()[name]
         s.run_in = re.sub(r"(?m)^thermo \d+$", "thermo 3", s.run_in)
     runs = []
-    for mode in (0, 1):
+    for mode in (1, 0, 3):  # split launches; small-grid launches with and without tiny-grid kernels
         e = _engine_from(s)
         e.set_tuning(pair_variant=8, cell_order=1, launch_mode=mode)
         e.run(0)
         e.run(7)
         e.run(5)
         runs.append((e.thermo(), e.state(), e.compute("ct") if name == "probe_fixes" else None, e.info()))
-    (ta, sa, ca, ia), (tb, sb, cb, ib) = runs
-    assert ia["step"] == ib["step"] == 12  # the last evaluated step
-    np.testing.assert_array_equal(ta["step"], tb["step"])
-    np.testing.assert_allclose(ta["temp"], tb["temp"], rtol=1e-4)
-    np.testing.assert_allclose(ta["pressure"], tb["pressure"], rtol=1e-4, atol=1e-4)
+    tb, sb, cb, ib = runs[0]
     L = s.hi - s.lo
-    dx = sa["x"] - sb["x"]
-    dx -= L * np.round(dx / L)
-    assert np.abs(dx).max() < 1e-4
-    if ca is not None:
-        np.testing.assert_array_equal(ca[:, 0], cb[:, 0])
-        np.testing.assert_allclose(ca[:, 1], cb[:, 1], rtol=1e-4)
+    for ta, sa, ca, ia in runs[1:]:
+        assert ia["step"] == ib["step"] == 12  # the last evaluated step
+        np.testing.assert_array_equal(ta["step"], tb["step"])
+        np.testing.assert_allclose(ta["temp"], tb["temp"], rtol=1e-4)
+        np.testing.assert_allclose(ta["pressure"], tb["pressure"], rtol=1e-4, atol=1e-4)
+        dx = sa["x"] - sb["x"]
+        dx -= L * np.round(dx / L)
+        assert np.abs(dx).max() < 1e-4
+        if ca is not None:
+            np.testing.assert_array_equal(ca[:, 0], cb[:, 0])
+            np.testing.assert_allclose(ca[:, 1], cb[:, 1], rtol=1e-4)
