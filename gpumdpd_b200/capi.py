@@ -18,7 +18,7 @@ DPD_ERRORS = {
 
 # every symbol declared in include/dpd_b200.h
 EXPORTED = [
-    "dpd_create", "dpd_create_from_system", "dpd_run", "dpd_sync", "dpd_get_thermo", "dpd_get_spring_records",
+    "dpd_create", "dpd_create_from_system", "dpd_create_fp64", "dpd_run", "dpd_sync", "dpd_get_thermo", "dpd_get_spring_records",
     "dpd_dump_open", "dpd_compute_dump_open", "dpd_dump_close", "dpd_bond_compute_aos", "dpd_nve_aos", "dpd_write_restart", "dpd_read_restart", "dpd_get_compute",
     "dpd_get_state", "dpd_set_state", "dpd_get_density", "dpd_get_cells", "dpd_get_neighbors",
     "dpd_compute_rdf", "dpd_rdf_config", "dpd_rdf_result", "dpd_get_info", "dpd_set_tuning",
@@ -104,6 +104,7 @@ def load():
     sig = {
         "dpd_create": (i, [cp, cp, cp, P(vp)]),
         "dpd_create_from_system": (i, [cp, P(dpd_system), P(vp)]),
+        "dpd_create_fp64": (i, [cp, cp, cp, P(dpd_system), P(vp)]),
         "dpd_run": (i, [vp, u32]),
         "dpd_sync": (i, [vp]),
         "dpd_get_thermo": (i, [vp, P(dpd_thermo), i, P(i)]),

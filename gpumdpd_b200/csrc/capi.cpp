@@ -6,9 +6,13 @@
 
 #include "../../include/dpd_b200.h"
 #include "engine.h"
+#include "fp64.h"
 
+// One handle type for both engines: `f64` is set for the FP64 parity mode, which answers
+// run, sync, thermo, state and info; every other call refuses it.
 struct dpd_engine {
     dpd::Engine eng;
+    std::unique_ptr<dpd::EngineF64> f64;
 };
 
 static thread_local std::string g_create_err;
@@ -86,28 +90,59 @@ int dpd_batch_create(int n_rep, const char* const* run_in_texts, const dpd_syste
     return DPD_OK;
 }
 
-#define ENG_CHECK(h)               \
-    if (!(h)) {                    \
+#define ENG_CHECK_ANY(h)              \
+    if (!(h)) {                       \
         g_create_err = "null engine"; \
-        return DPD_E_ARG;          \
+        return DPD_E_ARG;             \
     }
+#define ENG_CHECK(h)                                                    \
+    ENG_CHECK_ANY(h)                                                    \
+    if ((h)->f64) {                                                     \
+        (h)->f64->err = "not available in the FP64 parity mode";        \
+        return DPD_E_ARG;                                               \
+    }
+
+int dpd_create_fp64(const char* run_in_text, const char* data_path, const char* base_dir,
+                    const dpd_system* sys, dpd_engine** out)
+{
+    if (!run_in_text || !out) return set_create_err("null argument", DPD_E_ARG);
+    *out = nullptr;
+    dpd::Replica rep;
+    std::string err;
+    int e = sys ? dpd::make_replica_from_system(run_in_text, sys, rep, err)
+                : dpd::make_replica(run_in_text, data_path ? data_path : "", base_dir ? base_dir : "", rep, err);
+    if (e) return set_create_err(err, e);
+    // the engine first: a refused input makes no CUDA call
+    std::unique_ptr<dpd::EngineF64> f(new (std::nothrow) dpd::EngineF64);
+    if (!f) return set_create_err("out of host memory", DPD_E_NOMEM);
+    e = f->init(std::move(rep));
+    if (e) return set_create_err(f->err, e);
+    auto* h = new (std::nothrow) dpd_engine;
+    if (!h) return set_create_err("out of host memory", DPD_E_NOMEM);
+    h->f64 = std::move(f);
+    *out = h;
+    return DPD_OK;
+}
 
 int dpd_run(dpd_engine* h, uint32_t nsteps)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) return h->f64->run(nsteps);
     return h->eng.run(nsteps);
 }
 
 int dpd_sync(dpd_engine* h)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) return DPD_OK;  // its runs are synchronous
     return h->eng.sync_and_check();
 }
 
 int dpd_get_thermo(dpd_engine* h, dpd_thermo* rows, int max_rows, int* n_rows)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
     if (!rows || max_rows < 0) return DPD_E_ARG;
+    if (h->f64) return h->f64->get_thermo(rows, max_rows, n_rows);
     return h->eng.get_thermo(0, rows, max_rows, n_rows);
 }
 
@@ -185,13 +220,15 @@ int dpd_get_spring_records(dpd_engine* h, double* rows, int max_rows, int* n_row
 
 int dpd_get_state(dpd_engine* h, double* x, double* v, int* image, double* f)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) return h->f64->get_state(x, v, image, f);
     return h->eng.get_state(0, x, v, image, f);
 }
 
 int dpd_set_state(dpd_engine* h, const double* x, const double* v)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) return h->f64->set_state(x, v);
     return h->eng.set_state(0, x, v);
 }
 
@@ -235,7 +272,14 @@ int dpd_rdf_result(dpd_engine* h, double* g, int64_t* nsamples)
 
 int dpd_get_info(dpd_engine* h, int64_t* step, int64_t* n_builds, int64_t* n_atoms, int64_t* device_bytes)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) {  // cell grids are rebuilt every step: builds = steps
+        if (step) *step = h->f64->steps_done();
+        if (n_builds) *n_builds = h->f64->steps_done() + 1;
+        if (n_atoms) *n_atoms = h->f64->n_atoms();
+        if (device_bytes) *device_bytes = h->f64->device_bytes();
+        return DPD_OK;
+    }
     if (step) *step = h->eng.steps_done(0);
     if (n_builds) *n_builds = h->eng.n_builds();
     if (n_atoms) *n_atoms = h->eng.total_atoms();
@@ -271,6 +315,7 @@ int dpd_time_steps(dpd_engine* h, uint32_t nsteps, double* total_ms, double* pai
 const char* dpd_last_error(dpd_engine* h)
 {
     if (!h) return g_create_err.c_str();
+    if (h->f64) return h->f64->err.c_str();
     return h->eng.err.c_str();
 }
 

@@ -7,8 +7,8 @@
 // so the published steps and constants are kept; the float tail is evaluated with one
 // rounding per operation exactly as the reference's -DSINGLE build does:
 // u = (float)s * 2^-31 - 1, theta = sqrt(3)f * u.
-__device__ __forceinline__ float saru_theta(uint32_t seed1, uint32_t seed2, uint32_t seed,
-                                            uint32_t timestep)
+__device__ __forceinline__ uint32_t saru_bits(uint32_t seed1, uint32_t seed2, uint32_t seed,
+                                              uint32_t timestep)
 {
     uint32_t seed3 = seed + timestep;
     seed3 ^= (seed1 << 7) ^ (seed2 >> 6);
@@ -32,7 +32,24 @@ __device__ __forceinline__ float saru_theta(uint32_t seed1, uint32_t seed2, uint
         wstate += ((state << 4) + 0xAD90777Du) ^ (state + sum) ^ ((state >> 5) + 0x7E95761Eu);
     }
     uint32_t v = (state ^ (state >> 26)) + wstate;
-    uint32_t s = (v ^ (v >> 20)) * 0x6957f5a7u;
+    return (v ^ (v >> 20)) * 0x6957f5a7u;
+}
+
+__device__ __forceinline__ float saru_theta(uint32_t seed1, uint32_t seed2, uint32_t seed,
+                                            uint32_t timestep)
+{
+    const uint32_t s = saru_bits(seed1, seed2, seed, timestep);
     float u = __fmaf_rn(__uint2float_rn(s), 4.6566128730773926e-10f, -1.0f);
     return __fmul_rn(1.7320508075688772f, u);
+}
+
+// The tail of the reference's -DDOUBLE build (the same line with numtyp = double): the
+// product s * 2^-32 stays float (its constant is a float literal), an exact scaling of
+// (float)s; the affine map and sqrt(3) are double.
+__device__ __forceinline__ double saru_theta_f64(uint32_t seed1, uint32_t seed2, uint32_t seed,
+                                                 uint32_t timestep)
+{
+    const uint32_t s = saru_bits(seed1, seed2, seed, timestep);
+    const float a = __fmul_rn(__uint2float_rn(s), 2.3283064365386963e-10f);
+    return __dmul_rn(1.7320508075688772935274463, __fma_rn((double)a, 2.0, -1.0));
 }

@@ -40,12 +40,25 @@ def _rows_to_dict(rows, n):
 
 
 class Engine:
-    """One DPD system on the GPU (plain engine)."""
+    """One DPD system on the GPU (plain engine).
 
-    def __init__(self, run_in, data_path=None, base_dir=None, system=None):
+    precision="fp64" makes the FP64 parity engine (the reference's -DDOUBLE build): run,
+    thermo, state, set_state and info only; pair, bond and angle styles with fix nve."""
+
+    def __init__(self, run_in, data_path=None, base_dir=None, system=None, precision="fp32"):
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision must be 'fp32' or 'fp64'")
         self.lib = capi.load()
         self.h = ctypes.c_void_p()
-        if system is not None:
+        self.precision = precision
+        if precision == "fp64":
+            s = None
+            if system is not None:
+                s, self._keep = system
+            code = self.lib.dpd_create_fp64(run_in.encode(), data_path.encode() if data_path else None,
+                                            base_dir.encode() if base_dir else None,
+                                            ctypes.byref(s) if s is not None else None, ctypes.byref(self.h))
+        elif system is not None:
             s, self._keep = system
             code = self.lib.dpd_create_from_system(run_in.encode(), ctypes.byref(s), ctypes.byref(self.h))
         else:

@@ -273,6 +273,20 @@ int dpd_batch_get_state(dpd_engine* eng, int rep, double* x, double* v, int* ima
                         double* f);
 int dpd_batch_rdf_result(dpd_engine* eng, int rep, double* g, int64_t* nsamples);
 
+/* ---- FP64 parity mode: the reference's -DDOUBLE build (src/main/common.cuh:38-42,
+ *      numtyp = double) ------------------------------------------------------------
+ * An engine in double precision: wrapped FP64 positions in tag order, every pair taken
+ * from both sides (no force atomics, runs repeat bit for bit), the Saru tail of the
+ * -DDOUBLE build.  It separates precision effects from algorithm effects: against the
+ * -DDOUBLE build it agrees step by step to FP64 rounding.  Covers pair_style dpd/mdpd,
+ * bond_style harmonic/fene, angle_style harmonic, fix nve and thermo; other fixes,
+ * computes and dumps are refused at creation.  The handle answers dpd_run, dpd_sync,
+ * dpd_get_thermo, dpd_get_state, dpd_set_state, dpd_get_info, dpd_last_error and
+ * dpd_destroy; other calls return DPD_E_ARG.  sys != NULL: the system from arrays (as
+ * dpd_create_from_system), else the run.in's data file (as dpd_create). */
+int dpd_create_fp64(const char* run_in_text, const char* data_path, const char* base_dir,
+                    const dpd_system* sys, dpd_engine** out);
+
 /* ---- serving: continuous batching of DPD jobs -----------------------------------
  * A server owns a device-memory budget.  Jobs are submitted at any time; at each
  * scheduling point (every `chunk` steps) finished jobs are retired, their memory is

@@ -59,6 +59,35 @@ def test_valid_input_refuses_without_gpu(base):
     assert code == -8 and "no CPU fallback" in msg
 
 
+def _create_fp64(run_in, system):
+    from gpumdpd_b200 import capi
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    s, keep = system.c_system()
+    code = lib.dpd_create_fp64(run_in.encode(), None, None, ctypes.byref(s), ctypes.byref(h))
+    msg = lib.dpd_last_error(None).decode()
+    if code == 0:
+        lib.dpd_destroy(h)
+    return code, msg
+
+
+def test_fp64_mode_checks():
+    """The FP64 parity engine applies the same grammar checks, refuses the fixes, computes
+    and dumps it does not cover before touching a device, and has no CPU fallback."""
+    from gpumdpd_b200 import inputs
+    s = inputs.probe_fixes(L=9.0, seed=5, nsteps=10, thermo=1)
+    code, msg = _create_fp64(s.run_in, s)
+    assert code == -1 and "FP64 parity mode" in msg
+    b = inputs.plain_dpd(L=6.0, seed=1)
+    code, msg = _create_fp64(b.run_in.replace("run 1000\n", ""), b)
+    assert code == -1 and "run command is missing" in msg
+    code, msg = _create_fp64(b.run_in + "compute ct all temp 1 t.txt\n", b)
+    assert code == -1 and "FP64 parity mode" in msg
+    if _no_gpu():
+        code, msg = _create_fp64(b.run_in, b)
+        assert code == -8 and "no CPU fallback" in msg
+
+
 BAD = [
     ("unknown", lambda t: t + "foo 1 2\n", "unknown command foo"),
     ("no_run", lambda t: t.replace("run 1000\n", ""), "run command is missing"),

@@ -277,3 +277,32 @@ def test_fp32_engine_vs_reference_double_build(name):
         a, ea = _block_mean(ours[k][100:])
         b, eb = _block_mean(ref[k][100:])
         assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-3 * abs(b), (k, a, ea, b, eb)
+
+
+@pytest.mark.skipif(not os.path.exists(DOUBLE), reason="the reference's -DDOUBLE build not present")
+@pytest.mark.parametrize("name", ["dpd", "diblock"])
+def test_fp64_engine_vs_reference_double_build(name):
+    """The FP64 parity engine against the reference's -DDOUBLE build on the same input: the
+    thermo rows of the first 20 steps agree to thermo.txt's print precision (6 decimals; the
+    diblock's bond PE, about 1e4, to 2e-10 relative), where the FP32 engine parts from it
+    within a few steps; later the two FP64 trajectories part too (2e-8 relative in the bond
+    PE by step 35), and the 4000-step run means of T and P agree within their statistical
+    errors."""
+    from gpumdpd_b200 import Engine, inputs
+    if name == "dpd":
+        s = inputs.plain_dpd(L=10.0, seed=91, nsteps=4000, thermo=1)
+    else:
+        s = inputs.diblock_melt(L=10.0, seed=92, nsteps=4000, thermo=1)
+    run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in)
+    ref = _thermo(_run(DOUBLE, s, run_in, ["thermo.txt"])["thermo.txt"])[1]
+    e = Engine(s.run_in, system=s.c_system(), precision="fp64")
+    e.run(4000)
+    ours = e.thermo(max_rows=5000)
+    assert len(ours["step"]) == len(ref["temp"]) == 4001
+    cols = ["temp", "pressure"] + (["bond_pe"] if name == "diblock" else [])
+    for k in cols:
+        np.testing.assert_allclose(ours[k][:21], ref[k][:21], rtol=0, atol=2e-6)
+    for k in ("temp", "pressure"):
+        a, ea = _block_mean(ours[k][100:])
+        b, eb = _block_mean(ref[k][100:])
+        assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-3 * abs(b), (k, a, ea, b, eb)
