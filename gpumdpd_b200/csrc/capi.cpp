@@ -301,7 +301,8 @@ int dpd_set_tuning(dpd_engine* h, const dpd_tuning* t)
 
 int dpd_write_data(dpd_engine* h, const char* path)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) return path ? h->f64->write_data(path) : DPD_E_ARG;
     if (!path) return DPD_E_ARG;
     return h->eng.write_data(0, path);
 }

@@ -762,6 +762,16 @@ int EngineF64::get_state(double* x, double* v, int* image, double* f)
     return DPD_OK;
 }
 
+// the reference's write_data file of the current state (as the single-precision engine)
+int EngineF64::write_data(const std::string& path)
+{
+    SystemData s = R_.sys;
+    s.v.resize(s.x.size());
+    int e = get_state(s.x.data(), s.v.data(), nullptr, nullptr);
+    if (e) return e;
+    return write_data_file(path, R_.in.atom_style, s, err);
+}
+
 // new positions (image counts restart from zero) and/or velocities by tag; the next run
 // starts with a zero step
 int EngineF64::set_state(const double* x, const double* v)

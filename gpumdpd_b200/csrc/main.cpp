@@ -3,7 +3,9 @@
 // timestep on the GPU through libdpd_b200.so, writes thermo.txt with the reference's
 // columns (src/compute/thermo.cu:39-62,122-214), the data file of write_data, the
 // all.trj frames of dump (src/system/dump.cu), the record file of fix spring and the
-// files of the temp, rho, msd and tf computes.
+// files of the temp, rho, msd and tf computes.  `gpudpd_b200 --fp64 [run.in]` runs the
+// FP64 parity engine instead, the counterpart of the reference's -DDOUBLE build (thermo.txt
+// and write_data; the fixes, computes and dumps it does not cover are refused).
 #include <chrono>
 #include <cstdio>
 #include <fstream>
@@ -15,7 +17,12 @@
 
 int main(int argc, char** argv)
 {
-    std::string path = argc > 1 ? argv[1] : "run.in";
+    bool fp64 = false;
+    std::string path = "run.in";
+    for (int k = 1; k < argc; k++) {
+        if (std::string(argv[k]) == "--fp64") fp64 = true;
+        else path = argv[k];
+    }
     std::ifstream f(path);
     if (!f) {
         fprintf(stderr, "cannot open input file: %s\n", path.c_str());
@@ -26,7 +33,8 @@ int main(int argc, char** argv)
     const std::string text = ss.str();
     auto t0 = std::chrono::steady_clock::now();
     dpd_engine* eng = nullptr;
-    int e = dpd_create(text.c_str(), nullptr, nullptr, &eng);
+    int e = fp64 ? dpd_create_fp64(text.c_str(), nullptr, nullptr, nullptr, &eng)
+                 : dpd_create(text.c_str(), nullptr, nullptr, &eng);
     if (e) {
         fprintf(stderr, "ERROR: %s\n", dpd_last_error(nullptr));
         return 1;
@@ -85,7 +93,7 @@ int main(int argc, char** argv)
         dpd_destroy(eng);
         return 1;
     }
-    std::vector<dpd_thermo> rows(2048);
+    std::vector<dpd_thermo> rows(fp64 ? nsteps + 2 : 2048);
     int n = 0;
     dpd_get_thermo(eng, rows.data(), (int)rows.size(), &n);
     FILE* th = fopen("thermo.txt", "w");

@@ -38,11 +38,11 @@ def parse_trj(path):
     return frames
 
 
-def _run(binary, system, run_in, files):
+def _run(binary, system, run_in, files, args=()):
     with tempfile.TemporaryDirectory() as td:
         open(os.path.join(td, "run.in"), "w").write(run_in)
         system.write_data(os.path.join(td, "system.data"))
-        p = subprocess.run([binary], cwd=td, capture_output=True, text=True, timeout=600)
+        p = subprocess.run([binary, *args], cwd=td, capture_output=True, text=True, timeout=600)
         assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
         return {f: open(os.path.join(td, f)).read() for f in files if os.path.exists(os.path.join(td, f))}
 
@@ -306,3 +306,23 @@ def test_fp64_engine_vs_reference_double_build(name):
         a, ea = _block_mean(ours[k][100:])
         b, eb = _block_mean(ref[k][100:])
         assert abs(a - b) < 4 * np.hypot(ea, eb) + 1e-3 * abs(b), (k, a, ea, b, eb)
+
+
+@pytest.mark.skipif(not (os.path.exists(CLI) and os.path.exists(DOUBLE)),
+                    reason="gpudpd_b200 or the reference's -DDOUBLE build not present")
+def test_cli_fp64_vs_reference_double_executable():
+    """`gpudpd_b200 --fp64` in place of the reference's -DDOUBLE executable: the same
+    thermo.txt columns, rows agreeing to print precision over the first 20 steps, and a
+    write_data file with the same atoms."""
+    from gpumdpd_b200 import inputs
+    s = inputs.diblock_melt(L=8.0, seed=93, nsteps=60, thermo=1)
+    run_in = re.sub(r"(?m)^read_data .*$", "read_data system.data", s.run_in) + "write_data out.data\n"
+    ours = _run(CLI, s, run_in, ["thermo.txt", "out.data"], args=["--fp64"])
+    ref = _run(DOUBLE, s, run_in, ["thermo.txt", "out.data"])
+    ho, to = _thermo(ours["thermo.txt"])
+    hr, tr = _thermo(ref["thermo.txt"])
+    assert ho == hr
+    assert len(to["step"]) == len(tr["step"]) == 61
+    for k in hr:
+        np.testing.assert_allclose(to[k][:21], tr[k][:21], rtol=0, atol=2e-6, err_msg=k)
+    assert "out.data" in ours and len(ours["out.data"].splitlines()) == len(ref["out.data"].splitlines())
