@@ -303,6 +303,7 @@ def run_ours(args, world, rank, local):
         out["slab"] = run_slab(args)
         out["batched"] = run_batched(args)
         out["served"] = run_served(args)
+        out["fp64"] = run_fp64(args)
     if rank == 0:
         print(json.dumps(out))
 
@@ -471,6 +472,54 @@ def run_served(args):
             "plain_timing": f"device time per step over min({args.plain_steps}, steps) steps x steps, per job"}
 
 
+def time_reference_binary(binary, system, K):
+    """Runs a reference executable on `system` for 2K steps with thermo every K steps and
+    times steps K..2K on the host clock between its thermo lines (setup and file I/O
+    excluded).  Returns (seconds, None) or (None, the end of its output)."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        lines = [ln for ln in system.run_in.splitlines() if not ln.startswith(("run ", "thermo ", "read_data "))]
+        lines += [f"run {2 * K}", f"thermo {K}", "read_data system.data"]
+        open(os.path.join(td, "run.in"), "w").write("\n".join(lines) + "\n")
+        system.write_data(os.path.join(td, "system.data"))
+        p = subprocess.Popen([binary], cwd=td, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, bufsize=1)
+        stamps = {}
+        log = []
+        for line in p.stdout:
+            log.append(line)
+            tok = line.split()
+            if tok and tok[0].isdigit() and len(tok) >= 5:
+                stamps[int(tok[0])] = time.perf_counter()
+        rc = p.wait()
+    if rc != 0 or K not in stamps or 2 * K not in stamps:
+        return None, f"rc={rc}: " + "".join(log[-3:]).strip().replace("\n", " | ")
+    return stamps[2 * K] - stamps[K], None
+
+
+def run_fp64(args):
+    """The FP64 parity mode on C1 (plain DPD, 3000 particles): the FP64 engine's device time
+    per step (CUDA events) against the reference's -DDOUBLE build on the same input (host
+    clock between its thermo lines, as the reference arm)."""
+    from gpumdpd_b200 import Engine, inputs
+    s = inputs.plain_dpd(L=10.0, seed=2024, nsteps=10 ** 6, thermo=1000, skin=0.0)
+    e = Engine(s.run_in, system=s.c_system(), precision="fp64")
+    e.run(0)
+    e.run(50)
+    K = 2000
+    ms = e.time_steps(K)["total_ms"] / K
+    out = {"workload": f"plain_L10_N{s.n}_fp64", "particles": s.n, "ms_per_step": ms,
+           "value": s.n / (ms / 1000.0), "unit": "particle-steps/s", "dtype": "f64"}
+    binary = os.path.join(ROOT, "oracle", "_ref", "gpudpd_double")
+    if os.path.exists(binary):
+        dt, why = time_reference_binary(binary, s, K)
+        if dt is not None:
+            out["reference_double_ms_per_step"] = dt * 1000 / K
+            out["speedup_vs_reference_double"] = out["reference_double_ms_per_step"] / ms
+        else:
+            out["reference_double"] = f"failed {why}"
+    return out
+
+
 def run_reference(args, world, rank):
     """The reference's own CUDA build (oracle/_ref/gpudpd_single, built from its sources by
     oracle/build_ref.sh) on the same system: it reads run.in + a data file in its own
@@ -491,26 +540,10 @@ def run_reference(args, world, rank):
                           "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
-    import tempfile
-    with tempfile.TemporaryDirectory() as td:
-        lines = [ln for ln in system.run_in.splitlines() if not ln.startswith(("run ", "thermo ", "read_data "))]
-        lines += [f"run {2 * K}", f"thermo {K}", "read_data system.data"]
-        open(os.path.join(td, "run.in"), "w").write("\n".join(lines) + "\n")
-        system.write_data(os.path.join(td, "system.data"))
-        p = subprocess.Popen([binary], cwd=td, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, bufsize=1)
-        stamps = {}
-        log = []
-        for line in p.stdout:
-            log.append(line)
-            tok = line.split()
-            if tok and tok[0].isdigit() and len(tok) >= 5:
-                stamps[int(tok[0])] = time.perf_counter()
-        rc = p.wait()
-    if rc != 0 or K not in stamps or 2 * K not in stamps:
-        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed rc={rc}: "
-                          + "".join(log[-3:]).strip().replace("\n", " | ")}))
+    dt, why = time_reference_binary(binary, system, K)
+    if dt is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed {why}"}))
         return
-    dt = stamps[2 * K] - stamps[K]
     value = system.n * K / dt
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
            "steps": K, "warmup": K, "ms_per_step": dt * 1000 / K, "higher_is_better": True,

@@ -309,7 +309,12 @@ int dpd_write_data(dpd_engine* h, const char* path)
 
 int dpd_time_steps(dpd_engine* h, uint32_t nsteps, double* total_ms, double* pair_ms, int64_t* pair_launches)
 {
-    ENG_CHECK(h);
+    ENG_CHECK_ANY(h);
+    if (h->f64) {  // no separate pair timing in the parity mode
+        if (pair_ms) *pair_ms = 0.0;
+        if (pair_launches) *pair_launches = 0;
+        return h->f64->time_steps(nsteps, total_ms);
+    }
     return h->eng.time_steps(nsteps, total_ms, pair_ms, pair_launches);
 }
 

@@ -6,9 +6,9 @@
 // summation order is fixed), the mDPD density pass (src/force/pair_mdpd.cu:253-297), the
 // force pass, the final half kick (src/fix/fix_nve.cu:131-149) and on logged steps a
 // fixed-order reduction of the thermo sums (src/compute/thermo.cu:240-246,301-303,422-434,
-// 506-517).  The force pass gives one thread per atom all its pairs from both sides (27
-// cells), its bonds and its angles, so no atomics touch the forces and runs repeat
-// bit for bit.
+// 506-517).  The force pass gives one warp per atom all its pairs from both sides (a lane
+// per cell of the 27), its bonds and its angles, summed by a fixed butterfly, so no
+// atomics touch the forces and runs repeat bit for bit.
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -97,102 +97,112 @@ __global__ void k64_sort_cells(F64Args a, int ncell)
     }
 }
 
-// the 27 cells around atom i (nc >= 3 per dimension: no cell is visited twice); calls
-// fn(j, dx, dy, dz, r2) for every other atom j with r2 <= maxrc2
+// the c-th of the 27 cells around atom i (c = 9 (ox+1) + 3 (oy+1) + (oz+1); nc >= 3 per
+// dimension, so no cell is visited twice); calls fn(j, dx, dy, dz, r2) for every other
+// atom j there with r2 <= maxrc2, in index order
 template <class F>
-__device__ __forceinline__ void for_neighbours(const F64Args& a, int i, F&& fn)
+__device__ __forceinline__ void for_cell(const F64Args& a, int i, int c, F&& fn)
 {
     const double xi = a.x[3 * i], yi = a.x[3 * i + 1], zi = a.x[3 * i + 2];
-    int c[3];
-    cell_of(a, a.x + 3 * i, c);
-    for (int ox = -1; ox <= 1; ox++)
-        for (int oy = -1; oy <= 1; oy++)
-            for (int oz = -1; oz <= 1; oz++) {
-                const int cx = (c[0] + ox + a.nc[0]) % a.nc[0];
-                const int cy = (c[1] + oy + a.nc[1]) % a.nc[1];
-                const int cz = (c[2] + oz + a.nc[2]) % a.nc[2];
-                const int cell = (cx * a.nc[1] + cy) * a.nc[2] + cz;
-                const int* l = a.clist + (size_t)cell * a.cap;
-                const int m = min(a.cnt[cell], a.cap);
-                for (int p = 0; p < m; p++) {
-                    const int j = l[p];
-                    if (j == i) continue;
-                    const double dx = min_image(xi - a.x[3 * j], a.L[0]);
-                    const double dy = min_image(yi - a.x[3 * j + 1], a.L[1]);
-                    const double dz = min_image(zi - a.x[3 * j + 2], a.L[2]);
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    if (r2 <= a.maxrc2) fn(j, dx, dy, dz, r2);
-                }
-            }
+    int ci[3];
+    cell_of(a, a.x + 3 * i, ci);
+    const int cx = (ci[0] + c / 9 - 1 + a.nc[0]) % a.nc[0];
+    const int cy = (ci[1] + (c / 3) % 3 - 1 + a.nc[1]) % a.nc[1];
+    const int cz = (ci[2] + c % 3 - 1 + a.nc[2]) % a.nc[2];
+    const int cell = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+    const int* l = a.clist + (size_t)cell * a.cap;
+    const int m = min(a.cnt[cell], a.cap);
+    for (int p = 0; p < m; p++) {
+        const int j = l[p];
+        if (j == i) continue;
+        const double dx = min_image(xi - a.x[3 * j], a.L[0]);
+        const double dy = min_image(yi - a.x[3 * j + 1], a.L[1]);
+        const double dz = min_image(zi - a.x[3 * j + 2], a.L[2]);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= a.maxrc2) fn(j, dx, dy, dz, r2);
+    }
+}
+
+// sum over the warp by a fixed butterfly: the same order on every run
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 // mDPD local density, src/force/pair_mdpd.cu:253-297: rho_i = sum_{j != i}
-// 15/(2 pi rd^3) max(0, 1 - r/rd)^2 (pairs within the largest cutoff)
-__global__ void k64_density(F64Args a)
+// 15/(2 pi rd^3) max(0, 1 - r/rd)^2 (pairs within the largest cutoff).  One warp per
+// atom, lane c takes the c-th of the 27 cells.
+__global__ void __launch_bounds__(256) k64_density(F64Args a)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i >= a.n) return;  // warp-uniform
     const int ti = a.type[i];
     double rho = 0.0;
-    for_neighbours(a, i, [&](int j, double, double, double, double r2) {
-        const double rd = a.coeff[5 * tri(ti, a.type[j], a.ntypes) + 4];
-        double wd = 1.0 - sqrt(r2) / rd;
-        if (wd < 0.0) wd = 0.0;
-        rho += 15.0 / 2.0 / 3.14159265358979323846 / (rd * rd * rd) * wd * wd;
-    });
-    a.rho[i] = rho;
+    if (lane < 27)
+        for_cell(a, i, lane, [&](int j, double, double, double, double r2) {
+            const double rd = a.coeff[5 * tri(ti, a.type[j], a.ntypes) + 4];
+            double wd = 1.0 - sqrt(r2) / rd;
+            if (wd < 0.0) wd = 0.0;
+            rho += 15.0 / 2.0 / 3.14159265358979323846 / (rd * rd * rd) * wd * wd;
+        });
+    rho = warp_sum(rho);
+    if (lane == 0) a.rho[i] = rho;
 }
 
-// Forces on atom i: DPD / mDPD pairs (src/force/pair_dpd.cu:292-403, pair_mdpd.cu:
-// 399-521), bonds (src/force/bond_harmonic.cu:208-268; FENE + WCA as the FP32 engine) and
-// harmonic angles (src/force/angle_harmonic.cu:187-270).  On logged steps the atom's
-// share of the energies and of the virial: half of each pair and bond, a third of each
-// angle, as the reference splits them.
+// Forces on atom i, one warp per atom: lane c takes the DPD / mDPD pairs of the c-th of
+// the 27 cells (src/force/pair_dpd.cu:292-403, pair_mdpd.cu:399-521), the lanes share out
+// the atom's bonds (src/force/bond_harmonic.cu:208-268; FENE + WCA as the FP32 engine)
+// and harmonic angles (src/force/angle_harmonic.cu:187-270), and a fixed butterfly sums
+// the lanes.  On logged steps the atom's share of the energies and of the virial: half of
+// each pair and bond, a third of each angle, as the reference splits them.
 template <bool LOG>
-__global__ void k64_force(F64Args a, uint32_t step)
+__global__ void __launch_bounds__(256) k64_force(F64Args a, uint32_t step)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (i >= a.n) return;  // warp-uniform
     const int ti = a.type[i];
     const double vxi = a.v[3 * i], vyi = a.v[3 * i + 1], vzi = a.v[3 * i + 2];
     double fx = 0.0, fy = 0.0, fz = 0.0, pe = 0.0, bpe = 0.0, ape = 0.0;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     const double rho_i = a.style == 1 ? a.rho[i] : 0.0;
-    for_neighbours(a, i, [&](int j, double dx, double dy, double dz, double r2) {
-        const double* c = a.coeff + 5 * tri(ti, a.type[j], a.ntypes);
-        const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4];
-        if (!(r2 <= rc * rc)) return;
-        const double r = sqrt(r2);
-        if (r < 1.0e-10) return;
-        const double rinv = 1.0 / r;
-        const double dot = dx * (vxi - a.v[3 * j]) + dy * (vyi - a.v[3 * j + 1]) + dz * (vzi - a.v[3 * j + 2]);
-        const double wc = 1.0 - r / rc;
-        const uint32_t t1 = (uint32_t)min(i, j) + 1u, t2 = (uint32_t)max(i, j) + 1u;
-        const double theta = saru_theta_f64(t1, t2, a.seed, step);
-        const double sigma = sqrt(gamma) * a.sig_scale;
-        double fpair, e;
-        if (a.style == 0) {
-            fpair = A * wc - gamma * wc * wc * dot * rinv + sigma * wc * theta;
-            e = 0.5 * A * rc * wc * wc;
-        } else {
-            double wd = 1.0 - r / rd;
-            if (wd < 0.0) wd = 0.0;
-            const double rs = rho_i + a.rho[j];
-            fpair = A * wc + B * rs * wd - gamma * wc * wc * dot * rinv + sigma * wc * theta;
-            e = 0.5 * A * rc * wc * wc + 0.25 * B * rd * rs * wd * wd;
-        }
-        fpair *= rinv;
-        const double gx = dx * fpair, gy = dy * fpair, gz = dz * fpair;
-        fx += gx;
-        fy += gy;
-        fz += gz;
-        if (LOG) {
-            pe += 0.5 * e;
-            vir[0] += 0.5 * dx * gx; vir[1] += 0.5 * dx * gy; vir[2] += 0.5 * dx * gz;
-            vir[3] += 0.5 * dy * gy; vir[4] += 0.5 * dy * gz; vir[5] += 0.5 * dz * gz;
-        }
-    });
-    for (int b = a.bstart[i]; b < a.bstart[i + 1]; b++) {
+    if (lane < 27)
+        for_cell(a, i, lane, [&](int j, double dx, double dy, double dz, double r2) {
+            const double* c = a.coeff + 5 * tri(ti, a.type[j], a.ntypes);
+            const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4];
+            if (!(r2 <= rc * rc)) return;
+            const double r = sqrt(r2);
+            if (r < 1.0e-10) return;
+            const double rinv = 1.0 / r;
+            const double dot = dx * (vxi - a.v[3 * j]) + dy * (vyi - a.v[3 * j + 1]) + dz * (vzi - a.v[3 * j + 2]);
+            const double wc = 1.0 - r / rc;
+            const uint32_t t1 = (uint32_t)min(i, j) + 1u, t2 = (uint32_t)max(i, j) + 1u;
+            const double theta = saru_theta_f64(t1, t2, a.seed, step);
+            const double sigma = sqrt(gamma) * a.sig_scale;
+            double fpair, e;
+            if (a.style == 0) {
+                fpair = A * wc - gamma * wc * wc * dot * rinv + sigma * wc * theta;
+                e = 0.5 * A * rc * wc * wc;
+            } else {
+                double wd = 1.0 - r / rd;
+                if (wd < 0.0) wd = 0.0;
+                const double rs = rho_i + a.rho[j];
+                fpair = A * wc + B * rs * wd - gamma * wc * wc * dot * rinv + sigma * wc * theta;
+                e = 0.5 * A * rc * wc * wc + 0.25 * B * rd * rs * wd * wd;
+            }
+            fpair *= rinv;
+            const double gx = dx * fpair, gy = dy * fpair, gz = dz * fpair;
+            fx += gx;
+            fy += gy;
+            fz += gz;
+            if (LOG) {
+                pe += 0.5 * e;
+                vir[0] += 0.5 * dx * gx; vir[1] += 0.5 * dx * gy; vir[2] += 0.5 * dx * gz;
+                vir[3] += 0.5 * dy * gy; vir[4] += 0.5 * dy * gz; vir[5] += 0.5 * dz * gz;
+            }
+        });
+    for (int b = a.bstart[i] + lane; b < a.bstart[i + 1]; b += 32) {
         const int2 e2 = a.bent[b];
         const int j = e2.x;
         const double dx = min_image(a.x[3 * i] - a.x[3 * j], a.L[0]);
@@ -230,7 +240,7 @@ __global__ void k64_force(F64Args a, uint32_t step)
             vir[3] += 0.5 * dy * gy; vir[4] += 0.5 * dy * gz; vir[5] += 0.5 * dz * gz;
         }
     }
-    for (int t = a.astart[i]; t < a.astart[i + 1]; t++) {
+    for (int t = a.astart[i] + lane; t < a.astart[i + 1]; t += 32) {
         const int4 an = a.aent[t];
         double d1[3], d2[3];
 #pragma unroll
@@ -274,16 +284,28 @@ __global__ void k64_force(F64Args a, uint32_t step)
             vir[5] += third * (d1[2] * fi[2] + d2[2] * fk[2]);
         }
     }
-    a.f[3 * i] = fx;
-    a.f[3 * i + 1] = fy;
-    a.f[3 * i + 2] = fz;
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    if (lane == 0) {
+        a.f[3 * i] = fx;
+        a.f[3 * i + 1] = fy;
+        a.f[3 * i + 2] = fz;
+    }
     if (LOG) {
-        double* q = a.q + (size_t)NQ * i;
-        q[0] = pe;
-        q[1] = bpe;
-        q[2] = ape;
+        pe = warp_sum(pe);
+        bpe = warp_sum(bpe);
+        ape = warp_sum(ape);
 #pragma unroll
-        for (int k = 0; k < 6; k++) q[3 + k] = vir[k];
+        for (int k = 0; k < 6; k++) vir[k] = warp_sum(vir[k]);
+        if (lane == 0) {
+            double* q = a.q + (size_t)NQ * i;
+            q[0] = pe;
+            q[1] = bpe;
+            q[2] = ape;
+#pragma unroll
+            for (int k = 0; k < 6; k++) q[3 + k] = vir[k];
+        }
     }
 }
 
@@ -646,12 +668,13 @@ int EngineF64::eval_forces(uint32_t step, bool log)
     a.img = img_; a.type = type_; a.cnt = cnt_; a.clist = clist_; a.status = status_;
     a.bstart = bstart_; a.astart = astart_; a.bent = bent_; a.aent = aent_;
     const int g = (n_ + 255) / 256, gc = (ncell_ + 255) / 256;
+    const int gw = (int)(((size_t)n_ * 32 + 255) / 256);  // a warp per atom
     k64_clear<<<gc, 256, 0, stream_>>>(cnt_, ncell_);
     k64_bin<<<g, 256, 0, stream_>>>(a);
     k64_sort_cells<<<gc, 256, 0, stream_>>>(a, ncell_);
-    if (a.style == 1) k64_density<<<g, 256, 0, stream_>>>(a);
-    if (log) k64_force<true><<<g, 256, 0, stream_>>>(a, step);
-    else k64_force<false><<<g, 256, 0, stream_>>>(a, step);
+    if (a.style == 1) k64_density<<<gw, 256, 0, stream_>>>(a);
+    if (log) k64_force<true><<<gw, 256, 0, stream_>>>(a, step);
+    else k64_force<false><<<gw, 256, 0, stream_>>>(a, step);
     F64_CK(cudaGetLastError());
     return DPD_OK;
 }
@@ -759,6 +782,29 @@ int EngineF64::get_state(double* x, double* v, int* image, double* f)
     if (image) F64_CK(cudaMemcpyAsync(image, img_, sizeof(int) * n3, cudaMemcpyDeviceToHost, stream_));
     if (f) F64_CK(cudaMemcpyAsync(f, f_, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_));
     F64_CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
+// nsteps steps timed with CUDA events on the engine's stream
+int EngineF64::time_steps(uint32_t nsteps, double* total_ms)
+{
+    if (zero_pending_) {
+        int e = run(0);
+        if (e) return e;
+    }
+    cudaEvent_t e0, e1;
+    F64_CK(cudaEventCreate(&e0));
+    F64_CK(cudaEventCreate(&e1));
+    F64_CK(cudaEventRecord(e0, stream_));
+    int e = run(nsteps);
+    cudaEventRecord(e1, stream_);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e) return e;
+    if (total_ms) *total_ms = ms;
     return DPD_OK;
 }
 

@@ -30,6 +30,7 @@ public:
     int get_state(double* x, double* v, int* image, double* f);
     int set_state(const double* x, const double* v);
     int write_data(const std::string& path);
+    int time_steps(uint32_t nsteps, double* total_ms);
     int64_t steps_done() const { return zero_pending_ && next_step_ == 0 ? 0 : (int64_t)next_step_ - 1; }
     int64_t n_atoms() const { return n_; }
     int64_t device_bytes() const { return bytes_; }

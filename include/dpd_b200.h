@@ -282,7 +282,8 @@ int dpd_batch_rdf_result(dpd_engine* eng, int rep, double* g, int64_t* nsamples)
  * bond_style harmonic/fene, angle_style harmonic, fix nve and thermo; other fixes,
  * computes and dumps are refused at creation.  The handle answers dpd_run, dpd_sync,
  * dpd_get_thermo, dpd_get_state, dpd_set_state, dpd_get_info, dpd_write_data,
- * dpd_last_error and dpd_destroy; other calls return DPD_E_ARG.  sys != NULL: the system from arrays (as
+ * dpd_time_steps (total time only), dpd_last_error and dpd_destroy; other calls return
+ * DPD_E_ARG.  sys != NULL: the system from arrays (as
  * dpd_create_from_system), else the run.in's data file (as dpd_create). */
 int dpd_create_fp64(const char* run_in_text, const char* data_path, const char* base_dir,
                     const dpd_system* sys, dpd_engine** out);
