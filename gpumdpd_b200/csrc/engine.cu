@@ -1302,8 +1302,12 @@ int Engine::set_state(int rep, const double* x, const double* v)
         R.sys.x = xv;
         R.sys.v = vv;
     }
-    if (x) memcpy(R.sys.x.data(), x, sizeof(double) * n3);
-    if (v) memcpy(R.sys.v.data(), v, sizeof(double) * n3);
+    // host copies of a few hundred MB: one thread's memcpy would take tens of ms
+    auto pcopy = [n3](double* dst, const double* src) {
+        parallel_for((int64_t)n3, [&](int64_t i0, int64_t i1) { memcpy(dst + i0, src + i0, sizeof(double) * (i1 - i0)); });
+    };
+    if (x) pcopy(R.sys.x.data(), x);
+    if (v) pcopy(R.sys.v.data(), v);
     // full re-upload of every replica's particles (the host copies of the others are
     // refreshed first); the next run starts with a zero step and a list build
     for (int r = 0; r < (int)reps_.size(); r++) {
