@@ -23,15 +23,20 @@ namespace {
 
 enum { F64_NONFINITE = 1, F64_FENE = 2, F64_CELL_OVERFLOW = 4, F64_FAR = 8 };
 enum { NQ = 9, NSUM = 19, RED_BLOCKS = 256 };
+// pair table per type pair: A, B, gamma, rc, rd, sigma = sqrt(gamma) sqrt(2 kT)/sqrt(dt),
+// 1/rc, 1/rd, rc^2
+enum { NC = 9 };
 
 struct F64Args {
     int n, ntypes, style, bond_style, angle_style, cap;
     int nc[3];
     uint32_t seed, integ_mask;
-    double lo[3], L[3], w[3], dt, sig_scale, maxrc2;
+    double lo[3], L[3], w[3], dt, maxrc2;
     const double *coeff, *mass, *bondc, *anglec;
     double *x, *v, *f, *rho, *q;
-    int *img, *type, *cnt, *clist, *status;
+    int *img, *type, *cnt, *status;
+    double4* crec;  // cell records: position and atom index (exact in a double), cap per cell
+    int* ccode;  // each atom's cell as cx | cy << 10 | cz << 20, written by the binning
     const int *bstart, *astart;
     const int2* bent;
     const int4* aent;
@@ -74,22 +79,24 @@ __global__ void k64_bin(F64Args a)
     if (i >= a.n) return;
     int c[3];
     const int cell = cell_of(a, a.x + 3 * i, c);
+    a.ccode[i] = c[0] | (c[1] << 10) | (c[2] << 20);
     const int k = atomicAdd(a.cnt + cell, 1);
-    if (k < a.cap) a.clist[(size_t)cell * a.cap + k] = i;
+    if (k < a.cap)
+        a.crec[(size_t)cell * a.cap + k] = make_double4(a.x[3 * i], a.x[3 * i + 1], a.x[3 * i + 2], (double)i);
     else atomicOr(a.status, F64_CELL_OVERFLOW);
 }
 
-// each cell's atoms in index order: the pair sums then run in a fixed order
+// each cell's records in atom-index order: the pair sums then run in a fixed order
 __global__ void k64_sort_cells(F64Args a, int ncell)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    int* l = a.clist + (size_t)c * a.cap;
+    double4* l = a.crec + (size_t)c * a.cap;
     const int m = min(a.cnt[c], a.cap);
     for (int p = 1; p < m; p++) {
-        const int v = l[p];
+        const double4 v = l[p];
         int q = p - 1;
-        while (q >= 0 && l[q] > v) {
+        while (q >= 0 && l[q].w > v.w) {
             l[q + 1] = l[q];
             q--;
         }
@@ -104,20 +111,21 @@ template <class F>
 __device__ __forceinline__ void for_cell(const F64Args& a, int i, int c, F&& fn)
 {
     const double xi = a.x[3 * i], yi = a.x[3 * i + 1], zi = a.x[3 * i + 2];
-    int ci[3];
-    cell_of(a, a.x + 3 * i, ci);
-    const int cx = (ci[0] + c / 9 - 1 + a.nc[0]) % a.nc[0];
-    const int cy = (ci[1] + (c / 3) % 3 - 1 + a.nc[1]) % a.nc[1];
-    const int cz = (ci[2] + c % 3 - 1 + a.nc[2]) % a.nc[2];
+    const int code = a.ccode[i];
+    int cx = (code & 1023) + c / 9 - 1, cy = ((code >> 10) & 1023) + (c / 3) % 3 - 1, cz = (code >> 20) + c % 3 - 1;
+    cx += cx < 0 ? a.nc[0] : 0; cx -= cx >= a.nc[0] ? a.nc[0] : 0;
+    cy += cy < 0 ? a.nc[1] : 0; cy -= cy >= a.nc[1] ? a.nc[1] : 0;
+    cz += cz < 0 ? a.nc[2] : 0; cz -= cz >= a.nc[2] ? a.nc[2] : 0;
     const int cell = (cx * a.nc[1] + cy) * a.nc[2] + cz;
-    const int* l = a.clist + (size_t)cell * a.cap;
+    const double4* l = a.crec + (size_t)cell * a.cap;
     const int m = min(a.cnt[cell], a.cap);
     for (int p = 0; p < m; p++) {
-        const int j = l[p];
+        const double4 rj = l[p];
+        const int j = (int)rj.w;
         if (j == i) continue;
-        const double dx = min_image(xi - a.x[3 * j], a.L[0]);
-        const double dy = min_image(yi - a.x[3 * j + 1], a.L[1]);
-        const double dz = min_image(zi - a.x[3 * j + 2], a.L[2]);
+        const double dx = min_image(xi - rj.x, a.L[0]);
+        const double dy = min_image(yi - rj.y, a.L[1]);
+        const double dz = min_image(zi - rj.z, a.L[2]);
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 <= a.maxrc2) fn(j, dx, dy, dz, r2);
     }
@@ -142,8 +150,9 @@ __global__ void __launch_bounds__(256) k64_density(F64Args a)
     double rho = 0.0;
     if (lane < 27)
         for_cell(a, i, lane, [&](int j, double, double, double, double r2) {
-            const double rd = a.coeff[5 * tri(ti, a.type[j], a.ntypes) + 4];
-            double wd = 1.0 - sqrt(r2) / rd;
+            const double* c = a.coeff + NC * tri(ti, a.type[j], a.ntypes);
+            const double rd = c[4];
+            double wd = 1.0 - sqrt(r2) * c[7];
             if (wd < 0.0) wd = 0.0;
             rho += 15.0 / 2.0 / 3.14159265358979323846 / (rd * rd * rd) * wd * wd;
         });
@@ -169,23 +178,23 @@ __global__ void __launch_bounds__(256) k64_force(F64Args a, uint32_t step)
     const double rho_i = a.style == 1 ? a.rho[i] : 0.0;
     if (lane < 27)
         for_cell(a, i, lane, [&](int j, double dx, double dy, double dz, double r2) {
-            const double* c = a.coeff + 5 * tri(ti, a.type[j], a.ntypes);
-            const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4];
-            if (!(r2 <= rc * rc)) return;
-            const double r = sqrt(r2);
+            const double* c = a.coeff + NC * tri(ti, a.type[j], a.ntypes);
+            const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4], sigma = c[5];
+            if (!(r2 <= c[8])) return;
+            // 1/r by rsqrt and r/rc as r * (1/rc): within an ulp of the divisions
+            const double rinv = rsqrt(r2);
+            const double r = r2 * rinv;
             if (r < 1.0e-10) return;
-            const double rinv = 1.0 / r;
             const double dot = dx * (vxi - a.v[3 * j]) + dy * (vyi - a.v[3 * j + 1]) + dz * (vzi - a.v[3 * j + 2]);
-            const double wc = 1.0 - r / rc;
+            const double wc = 1.0 - r * c[6];
             const uint32_t t1 = (uint32_t)min(i, j) + 1u, t2 = (uint32_t)max(i, j) + 1u;
             const double theta = saru_theta_f64(t1, t2, a.seed, step);
-            const double sigma = sqrt(gamma) * a.sig_scale;
             double fpair, e;
             if (a.style == 0) {
                 fpair = A * wc - gamma * wc * wc * dot * rinv + sigma * wc * theta;
                 e = 0.5 * A * rc * wc * wc;
             } else {
-                double wd = 1.0 - r / rd;
+                double wd = 1.0 - r * c[7];
                 if (wd < 0.0) wd = 0.0;
                 const double rs = rho_i + a.rho[j];
                 fpair = A * wc + B * rs * wd - gamma * wc * wc * dot * rinv + sigma * wc * theta;
@@ -419,7 +428,7 @@ int EngineF64::fail(cudaError_t e, const char* what)
 
 EngineF64::~EngineF64()
 {
-    void* ptrs[] = {x_, v_, f_, rho_, q_, part_, sums_, img_, type_, cnt_, clist_, status_,
+    void* ptrs[] = {x_, v_, f_, rho_, q_, part_, sums_, img_, type_, cnt_, ccode_, crec_, status_,
                     bstart_, astart_, bent_, aent_, tab_};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -541,14 +550,22 @@ int EngineF64::init(Replica&& rep)
     // coefficient tables
     const int nt = R_.sys.n_atomtypes, ntri = nt * (nt + 1) / 2;
     const int nbt = std::max(R_.sys.n_bondtypes, 1), nat = std::max(R_.sys.n_angletypes, 1);
-    std::vector<double> tab((size_t)5 * ntri + nt + 4 * nbt + 2 * nat, 0.0);
-    for (int p = 0; p < ntri && p < (int)ff.coeff.size(); p++)
-        for (int k = 0; k < 5; k++) tab[5 * p + k] = ff.coeff[p][k];
-    for (int t = 0; t < nt; t++) tab[5 * ntri + t] = R_.sys.masses[t];
+    std::vector<double> tab((size_t)NC * ntri + nt + 4 * nbt + 2 * nat, 0.0);
+    // sqrt(2 kT) / sqrt(dt), src/force/pair_dpd.cu:577-578
+    const double sig_scale = std::sqrt(2.0 * ff.temp) / std::sqrt(in.dt);
+    for (int p = 0; p < ntri && p < (int)ff.coeff.size(); p++) {
+        double* c = &tab[(size_t)NC * p];
+        for (int k = 0; k < 5; k++) c[k] = ff.coeff[p][k];
+        c[5] = std::sqrt(c[2]) * sig_scale;
+        c[6] = c[3] > 0.0 ? 1.0 / c[3] : 0.0;
+        c[7] = c[4] > 0.0 ? 1.0 / c[4] : HUGE_VAL;  // no rd: w_d clamps to 0
+        c[8] = c[3] * c[3];
+    }
+    for (int t = 0; t < nt; t++) tab[NC * ntri + t] = R_.sys.masses[t];
     for (int b = 0; b < (int)ff.bond_coeff.size() && b < nbt; b++)
-        for (int k = 0; k < 4; k++) tab[5 * ntri + nt + 4 * b + k] = ff.bond_coeff[b][k];
+        for (int k = 0; k < 4; k++) tab[NC * ntri + nt + 4 * b + k] = ff.bond_coeff[b][k];
     for (int b = 0; b < (int)ff.angle_coeff.size() && b < nat; b++)
-        for (int k = 0; k < 2; k++) tab[5 * ntri + nt + 4 * nbt + 2 * b + k] = ff.angle_coeff[b][k];
+        for (int k = 0; k < 2; k++) tab[NC * ntri + nt + 4 * nbt + 2 * b + k] = ff.angle_coeff[b][k];
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -575,7 +592,8 @@ int EngineF64::init(Replica&& rep)
     F64_CK(dalloc64(&img_, 3 * n, bytes_));
     F64_CK(dalloc64(&type_, n, bytes_));
     F64_CK(dalloc64(&cnt_, (size_t)ncell_, bytes_));
-    F64_CK(dalloc64(&clist_, (size_t)ncell_ * cap_, bytes_));
+    F64_CK(dalloc64(&ccode_, n, bytes_));
+    F64_CK(dalloc64(&crec_, (size_t)ncell_ * cap_, bytes_));
     F64_CK(dalloc64(&status_, 1, bytes_));
     F64_CK(dalloc64(&bstart_, n + 1, bytes_));
     F64_CK(dalloc64(&astart_, n + 1, bytes_));
@@ -642,8 +660,6 @@ static F64Args make_args(const Replica& R, int n, const int nc[3], const double 
     a.seed = R.ff.seed;
     a.integ_mask = R.ff.integ_mask;
     a.dt = R.in.dt;
-    // sqrt(2 kT) / sqrt(dt), src/force/pair_dpd.cu:577-578
-    a.sig_scale = std::sqrt(2.0 * R.ff.temp) / std::sqrt(R.in.dt);
     double rcm = 0.0;
     for (auto& c : R.ff.coeff) rcm = std::max(rcm, c[3]);
     a.maxrc2 = rcm * rcm;
@@ -661,11 +677,11 @@ int EngineF64::eval_forces(uint32_t step, bool log)
     F64Args a = make_args(R_, n_, nc_, L_, cap_);
     const int nt = R_.sys.n_atomtypes, ntri = nt * (nt + 1) / 2, nbt = std::max(R_.sys.n_bondtypes, 1);
     a.coeff = tab_;
-    a.mass = tab_ + 5 * ntri;
-    a.bondc = tab_ + 5 * ntri + nt;
-    a.anglec = tab_ + 5 * ntri + nt + 4 * nbt;
+    a.mass = tab_ + NC * ntri;
+    a.bondc = tab_ + NC * ntri + nt;
+    a.anglec = tab_ + NC * ntri + nt + 4 * nbt;
     a.x = x_; a.v = v_; a.f = f_; a.rho = rho_; a.q = q_;
-    a.img = img_; a.type = type_; a.cnt = cnt_; a.clist = clist_; a.status = status_;
+    a.img = img_; a.type = type_; a.cnt = cnt_; a.crec = crec_; a.status = status_; a.ccode = ccode_;
     a.bstart = bstart_; a.astart = astart_; a.bent = bent_; a.aent = aent_;
     const int g = (n_ + 255) / 256, gc = (ncell_ + 255) / 256;
     const int gw = (int)(((size_t)n_ * 32 + 255) / 256);  // a warp per atom
@@ -685,7 +701,7 @@ int EngineF64::log_row(uint32_t step)
 {
     F64Args a = make_args(R_, n_, nc_, L_, cap_);
     const int nt = R_.sys.n_atomtypes, ntri = nt * (nt + 1) / 2;
-    a.mass = tab_ + 5 * ntri;
+    a.mass = tab_ + NC * ntri;
     a.v = v_; a.q = q_; a.type = type_;
     const int nb = std::min((int)RED_BLOCKS, (n_ + 255) / 256);
     k64_thermo_partial<<<nb, 256, 0, stream_>>>(a, part_);
@@ -736,7 +752,7 @@ int EngineF64::run(uint32_t nsteps)
 {
     F64Args a = make_args(R_, n_, nc_, L_, cap_);
     const int nt = R_.sys.n_atomtypes, ntri = nt * (nt + 1) / 2;
-    a.mass = tab_ + 5 * ntri;
+    a.mass = tab_ + NC * ntri;
     a.x = x_; a.v = v_; a.f = f_; a.img = img_; a.type = type_; a.status = status_;
     const int g = (n_ + 255) / 256;
     const uint32_t log_f = R_.in.log_f;

@@ -55,8 +55,9 @@ private:
     double* q_ = nullptr;        // per-atom log terms: pair, bond, angle PE, virial[6]
     double* part_ = nullptr;     // per-block partial sums of the thermo reduction
     double* sums_ = nullptr;     // reduced thermo sums
-    int *img_ = nullptr, *type_ = nullptr, *cnt_ = nullptr;
-    int *clist_ = nullptr, *status_ = nullptr;
+    int *img_ = nullptr, *type_ = nullptr, *cnt_ = nullptr, *ccode_ = nullptr;
+    int* status_ = nullptr;
+    double4* crec_ = nullptr;    // cell records (position, atom index), cap_ per cell
     int *bstart_ = nullptr, *astart_ = nullptr;
     int2* bent_ = nullptr;       // bond partner index, bond type (1-based)
     int4* aent_ = nullptr;       // angle atoms i, j (apex), k as indices, angle type (1-based)
