@@ -144,3 +144,35 @@ def test_fp64_handle_refuses_other_calls():
     assert "FP64 parity mode" in str(ex.value)
     e.run(2)
     assert e.info()["step"] == 2
+
+
+def test_fp64_fene_bonds_match_fp64_oracle(oracle_mod):
+    """FENE + WCA bonds (not in the reference): step-0 forces and bond PE, then ten steps,
+    against the FP64 oracle.  Bonds start at 0.9 with the WCA range 2^(1/6) 0.85 = 0.954, so
+    the repulsion acts.  The stiff FENE spring needs a shorter step than DPD's 0.04: with it,
+    bonds pass R0 within ten steps, an error in both."""
+    from gpumdpd_b200 import inputs
+    s = inputs.diblock_melt(L=10.0, seed=9, nsteps=10, bond_step=0.9, thermo=1, dt=0.005)
+    s.run_in = s.run_in.replace("bond_style harmonic", "bond_style fene").replace(
+        "bond_coeff 1 4.0 0.0", "bond_coeff 1 30.0 1.5 1.0 0.85")
+    assert "bond_style fene" in s.run_in and "bond_coeff 1 30.0 1.5 1.0 0.85" in s.run_in
+    e = _fp64(s)
+    e.run(0)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    L = s.hi - s.lo
+    oracle_mod.set_saru_double_tail(True)
+    try:
+        o0 = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, s.x, s.v, s.lo, L, 0, bonds=s.bonds)
+        o = oracle_mod.run(ff, np.arange(1, s.n + 1), s.types, s.x, s.v, s.lo, L, 1, 10, 1, bonds=s.bonds)
+    finally:
+        oracle_mod.set_saru_double_tail(False)
+    assert force_err(st["f"], o0["f"]) < 1e-12
+    assert e.thermo()["bond_pe"][0] == pytest.approx(o0["bond_pe"], rel=1e-12)
+    e.run(10)
+    st = e.state()
+    dx = st["x"] - o["x"]
+    dx -= L * np.round(dx / L)
+    assert np.abs(dx).max() < 1e-9
+    assert force_err(st["f"], o["f"]) < 1e-9
+    np.testing.assert_allclose(e.thermo()["bond_pe"], o["thermo"]["bond_pe"], rtol=1e-9)
