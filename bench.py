@@ -19,6 +19,7 @@ decomposed), launched by torch.distributed.run; value sums all ranks.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -40,13 +41,14 @@ def workload_name(args):
     return f"{args.workload}_skin{args.skin}"
 
 
-def build_launches(system, skin):
+def build_launches(system, skin, pair_variant=8):
     """Kernels of one list build: counting pass, scan (one launch when the cells fit one
     4096-element block, else three), permutation (with the parity flip up to 1184 blocks
-    of 256 slots, else a separate flip), list."""
+    of 256 slots, else a separate flip), list (none with the cell-tile schedule 11)."""
     cells = int(np.prod(np.floor(system.box / (1.0 + skin)))) + 1
     slots = system.n + 31
-    return 3 + (1 if cells <= 4096 else 3) + (0 if (slots + 255) // 256 <= 148 * 8 else 1)
+    return (2 if pair_variant == 11 else 3) + (1 if cells <= 4096 else 3) + \
+        (0 if (slots + 255) // 256 <= 148 * 8 else 1)
 
 
 def pair_kernel_name(system, pair_variant):
@@ -54,6 +56,8 @@ def pair_kernel_name(system, pair_variant):
     of 256 slots) one thread per list entry, on small grids (up to 1184) the flattened
     schedule as one launch, else the flattened schedule split by log steps."""
     gp = (system.n + 31 + 255) // 256
+    if pair_variant == 11:
+        return "k_tile + k_tile_logsteps (cell tiles staged in shared memory, no list)"
     if pair_variant == 8 and gp <= 148:
         return "k_pair_entry (thread per list entry, tiny grids)"
     if pair_variant == 8 and gp <= 148 * 8:
@@ -65,24 +69,109 @@ def step_launches(system, pair_variant):
     """Kernels of one step after the list build: on small grids (up to 1184 blocks of 256
     slots) the pair pass and the integrate with the bookkeeping are one launch each; else
     the pair kernel(s), the integrate pair (non-log steps + log steps) and advance."""
-    if (system.n + 31 + 255) // 256 <= 148 * 8 and pair_variant == 8:
+    small = (system.n + 31 + 255) // 256 <= 148 * 8
+    if small and pair_variant == 8:
         return 2
+    if pair_variant == 11:
+        return 2 + (1 if small else 3)
     return (2 if pair_variant in (7, 8, 9) else 1) + 3
 
 
-def make_system(args):
+def thermo_every(args):
+    """Thermo cadence of the headline run, shared by both arms: the reference prints a
+    thermo line every N steps and is timed between its lines at steps W and W+K, so N
+    divides both W and K; logged steps cost both engines their virial/energy variants."""
+    return math.gcd(args.warmup, args.steps)
+
+
+def make_system(args, thermo=1000):
     from gpumdpd_b200 import inputs
     if args.workload == "melt":
-        return inputs.diblock_melt(L=100.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
+        return inputs.diblock_melt(L=100.0, seed=7, nsteps=10 ** 6, thermo=thermo, skin=args.skin)
     if args.workload == "melt_mid":
-        return inputs.diblock_melt(L=60.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
+        return inputs.diblock_melt(L=60.0, seed=7, nsteps=10 ** 6, thermo=thermo, skin=args.skin)
     if args.workload == "melt_small":
-        return inputs.diblock_melt(L=30.0, seed=7, nsteps=10 ** 6, thermo=1000, skin=args.skin)
+        return inputs.diblock_melt(L=30.0, seed=7, nsteps=10 ** 6, thermo=thermo, skin=args.skin)
     if args.workload == "plain":
-        return inputs.plain_dpd(L=10.0, seed=2024, nsteps=10 ** 6, thermo=1000, skin=args.skin)
+        return inputs.plain_dpd(L=10.0, seed=2024, nsteps=10 ** 6, thermo=thermo, skin=args.skin)
     if args.workload == "slab":
-        return inputs.mdpd_slab(nsteps=10 ** 6, thermo=1000, skin=args.skin)
+        return inputs.mdpd_slab(nsteps=10 ** 6, thermo=thermo, skin=args.skin)
     raise SystemExit(f"unknown workload {args.workload}")
+
+
+def block_stats(series, nblocks=10):
+    """Mean and its standard error from block averages (consecutive blocks of equal
+    length; rows that do not fill a block are left out of the error estimate)."""
+    x = np.asarray(series, dtype=np.float64)
+    nb = min(nblocks, len(x) // 2)
+    if nb < 2:
+        return float(x.mean()), float("nan")
+    ln = len(x) // nb
+    b = x[: nb * ln].reshape(nb, ln).mean(axis=1)
+    return float(x.mean()), float(b.std(ddof=1) / math.sqrt(nb))
+
+
+def compare(a, b, nblocks=10):
+    """a (FP32 engine) against b (FP64 engine) for one observable's series over the same
+    window: both means, their difference, its combined standard error and the ratio."""
+    ma, sa = block_stats(a, nblocks)
+    mb, sb = block_stats(b, nblocks)
+    se = math.sqrt(sa * sa + sb * sb)
+    return {"fp32": round(ma, 6), "fp64": round(mb, 6), "err": round(ma - mb, 6),
+            "stderr": round(se, 6), "z": round((ma - mb) / se, 2) if se > 0 else None}
+
+
+def with_thermo(run_in, every):
+    import re
+    return re.sub(r"(?m)^thermo \d+$", f"thermo {int(every)}", run_in)
+
+
+def without_computes(run_in):
+    """The run.in without its `compute` lines (the FP64 parity engine runs the force field
+    and fix nve only; sampling computes do not change the trajectory)."""
+    return "".join(ln + "\n" for ln in run_in.splitlines() if not ln.startswith("compute "))
+
+
+def with_run(run_in, steps):
+    import re
+    return re.sub(r"(?m)^run \d+$", f"run {int(steps)}", run_in)
+
+
+def state_system(s, x, v, run_in):
+    """The system `s` at state (x, v) in tag order, with another run.in."""
+    from gpumdpd_b200 import inputs
+    return inputs.System(s.lo, s.hi, s.masses, s.types, x, v, bonds=s.bonds, n_bondtypes=s.n_bondtypes,
+                         mol=s.mol, run_in=run_in, atom_style=s.atom_style, angles=s.angles,
+                         n_angletypes=s.n_angletypes)
+
+
+def fp32_fp64_window(s, x, v, steps, every, fields=("temp", "pressure"), extra=None, tuning=None):
+    """Run the FP32 engine and the FP64 parity engine (the reference's -DDOUBLE
+    arithmetic, pinned to the FP64 oracle by the test suite) from the same state (x, v)
+    for `steps` steps with thermo every `every` steps; compare each field's mean over the
+    rows after the first.  `extra` maps a name to a function of the thermo dict giving
+    another series."""
+    from gpumdpd_b200 import Engine
+    run_in = with_run(with_thermo(without_computes(s.run_in), every), steps)
+    rows = {}
+    t = {}
+    for prec in ("fp32", "fp64"):
+        sysp = state_system(s, x, v, run_in)
+        e = Engine(run_in, system=sysp.c_system(), precision=prec)
+        if prec == "fp32" and tuning:
+            e.set_tuning(**tuning)
+        t0 = time.perf_counter()
+        e.run(steps)
+        t[prec] = time.perf_counter() - t0
+        rows[prec] = e.thermo()
+        e.close()
+    out = {}
+    for f in fields:
+        out[f] = compare(rows["fp32"][f][1:], rows["fp64"][f][1:])
+    for name, fn in (extra or {}).items():
+        out[name] = compare(fn(rows["fp32"])[1:], fn(rows["fp64"])[1:])
+    out["window"] = {"steps": steps, "thermo_every": every, "rows": int(len(rows["fp32"]["temp"]) - 1)}
+    return out
 
 
 class ClockSampler:
@@ -178,27 +267,41 @@ def barrier(world):
         dist.barrier()
 
 
-def algorithmic_bytes_per_particle(mean_half_list, maxb):
+def algorithmic_bytes_per_particle(mean_half_list, maxb, pair_variant=8):
     """Pair kernel, per particle-step: x,v of i (32 B) + force write (12 B) + list length
     (4 B) + list entries (4 B each); neighbour-j gathers are assumed cache-resident and not
-    counted.  The fused bonds add their partner table (8 B per slot)."""
+    counted.  The fused bonds add their partner table (8 B per slot).  The cell-tile
+    schedule (11) reads no list: 44 B + bonds."""
+    if pair_variant == 11:
+        return 44.0 + 8.0 * maxb
     return 48.0 + 4.0 * mean_half_list + 8.0 * maxb
 
 
-def cpu_baseline(system, nthreads, nsteps=2):
-    """FP64 oracle port of the reference algorithm on the host cores (bounded sample)."""
+def cpu_baseline(system, nthreads, nsteps=2, engine_state0=None):
+    """FP64 oracle port of the reference algorithm (pair forces with the Saru random force
+    on a half Verlet list, bonds, velocity Verlet) on the host cores: a bounded sample of
+    the workload.  Given the engine's state after its zero step, the oracle also checks
+    the engine's step-0 forces on that state (largest per-particle error over the RMS
+    force)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     ff = oracle.ff_from_run_in(system.run_in, system.masses)
     tags = np.arange(1, system.n + 1)
     t0 = time.perf_counter()
     oracle.bench_steps(ff, tags, system.types, system.x, system.v, system.lo, system.box, 1, nsteps,
-                       0.3, nthreads)
+                       0.3, nthreads, bonds=system.bonds)
     dt = time.perf_counter() - t0
-    return {"value": system.n * nsteps / dt, "unit": "particle-steps/s", "cores": nthreads,
-            "kind": "port",
-            "sample": f"full {system.n}-particle system, step-0 force + {nsteps} steps incl. one list "
-                      f"build, FP64, pair forces (bonds omitted), {nthreads} threads; {dt:.1f} s"}
+    out = {"value": system.n * nsteps / dt, "unit": "particle-steps/s", "cores": nthreads,
+           "kind": "port",
+           "sample": f"full {system.n}-particle system: step-0 forces + {nsteps} steps incl. one list "
+                     f"build, FP64, pair + bond forces, {nthreads} threads; {dt:.1f} s"}
+    if engine_state0 is not None:
+        o = oracle.forces(ff, tags, system.types, engine_state0["x"], engine_state0["v"], system.lo,
+                          system.box, 0, bonds=system.bonds)
+        rms = float(np.sqrt((np.linalg.norm(o["f"], axis=1) ** 2).mean()))
+        err = np.linalg.norm(engine_state0["f"] - o["f"], axis=1).max() / rms
+        out["step0_force_max_err_over_rms"] = float(err)
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -211,11 +314,13 @@ def run_ours(args, world, rank, local):
         args.skin = best["skin"]
         args.pair_variant = best["pair_variant"]
         tuned = {"best": best, "table": table}
-    system = make_system(args)
+    every = thermo_every(args)
+    system = make_system(args, thermo=every)
     eng = Engine(system.run_in, system=system.c_system())
     pair_variant = 8 if args.pair_variant is None else args.pair_variant
-    eng.set_tuning(pair_variant=pair_variant, cell_order=1, build_variant=args.build_variant)
+    eng.set_tuning(pair_variant=pair_variant, cell_order=1, build_variant=args.build_variant, tile=args.tile)
     eng.run(0)
+    st0 = eng.state(images=False) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     eng.run(args.warmup)
     ls = eng.list_stats()
     b0 = eng.info()["builds"]
@@ -241,13 +346,13 @@ def run_ours(args, world, rank, local):
     eng.set_state(x, v)
     eng.run(chunk)
     st2 = eng.state(forces=False, images=False)
-    th = eng.thermo(max_rows=4)
+    eng.thermo(max_rows=4)
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
     e2e = world * n * chunk / e2e_s
     h2d = n * 6 * 8 / chunk
     d2h = (n * 6 * 8 + 4 * 8 * 16) / chunk
     maxb = 2 if system.bonds is not None else 0
-    bpp = algorithmic_bytes_per_particle(ls["mean_half_list"], maxb)
+    bpp = algorithmic_bytes_per_particle(ls["mean_half_list"], maxb, pair_variant)
     per_launch_ms = pair_ms / max(res["pair_launches"], 1)
     achieved = n * bpp / (per_launch_ms / 1000.0) / 1e9
     peaks = {}
@@ -269,6 +374,7 @@ def run_ours(args, world, rank, local):
             traffic = t["dram_bytes_per_launch"]
     except Exception:
         pass
+    pairs_per_step = ls["pairs"]
     out = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -276,43 +382,62 @@ def run_ours(args, world, rank, local):
         "data": "synthetic (seeded generator, gpumdpd_b200/inputs.py)",
         "config": {"workload": workload_name(args), "n_particles": n,
                    "n_bonds": 0 if system.bonds is None else len(system.bonds), "box": system.box.tolist(),
-                   "dt": 0.04, "skin": args.skin, "mean_half_list": ls["mean_half_list"],
+                   "dt": 0.04, "skin": args.skin, "thermo_every": every,
+                   "mean_half_list": round(ls["mean_half_list"], 3),
                    "list_builds_per_step": builds_per_step, "pair_variant": pair_variant,
-                   "build_variant": args.build_variant,
-                   "tuned": tuned, "parallelism": f"replicas{world}",
-                   "l2": l2},
+                   "tile": args.tile if pair_variant == 11 else None,
+                   "tuned": tuned if isinstance(tuned, str) else "bench --tune",
+                   "parallelism": f"replicas{world}", "l2": l2},
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "chunk_steps": chunk, "path": "dpd_set_state + dpd_run + dpd_get_state (C ABI, host buffers)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": pair_kernel_name(system, pair_variant),
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                     # the kernel is issue-bound, not HBM-bound: the Saru chain's integer
+                     # operations per pair inside rc set the compute-side ceiling
+                     "binding": "instruction issue (Saru integer chain + gathers), not HBM",
+                     "pairs_per_step": pairs_per_step,
+                     "saru_int_ops_per_pair": 130},
         "clocks": clk.summary(),
         # per step: the list-build kernels (counting pass, 1 or 3 scan launches, permutation,
         # list; each returns at once unless a build is flagged), the pair kernel(s), the
         # integrate pair (non-log steps + log steps), advance; plus 2 before the graph
-        "gpu_launches": int(args.steps * (build_launches(system, args.skin) +
+        "gpu_launches": int(args.steps * (build_launches(system, args.skin, pair_variant) +
                                           step_launches(system, pair_variant)) + 2),
         "impl": "ours",
     }
-    del th, st2
-    eng.close()
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(system, os.cpu_count() or 1)
     if world == 1 and not args.no_extras:
-        out["slab"] = run_slab(args)
-        out["batched"] = run_batched(args)
-        out["served"] = run_served(args)
-        out["fp64"] = run_fp64(args)
+        # T and P of the headline system: the FP32 engine against the FP64 parity engine
+        # from the same (timed-run) state over the same window
+        out["accuracy"] = fp32_fp64_window(system, st2["x"], st2["v"], args.acc_steps, 5,
+                                           tuning={"pair_variant": pair_variant, "cell_order": 1})
+    eng.close()
+    del st, st2
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(system, os.cpu_count() or 1, engine_state0=st0)
+        del st0
+    detail = {}
+    if world == 1 and not args.no_extras:
+        for name, fn in (("slab", run_slab), ("batched", run_batched), ("served", run_served),
+                         ("fp64", run_fp64)):
+            summary, det = fn(args)
+            out[name] = summary
+            detail[name] = det
     if rank == 0:
-        print(json.dumps(out))
+        if detail and args.detail:
+            with open(args.detail, "w") as f:
+                json.dump(detail, f)
+            out["detail_file"] = os.path.basename(args.detail)
+        print(json.dumps(out), flush=True)
 
 
 def run_slab(args):
     """Many-body DPD liquid slab: box 40x40x120, density 6 in z in [40,80] (N = 384k), A=-40,
     B=25, rc=1, rd=0.75, gamma=4.5, kT=1, dt=0.01, two-pass density then force, 20k steps
     timed on the device; the z density profile (bins 0.5) of the final state and
-    gamma_s = (Lz/2)<P_zz - (P_xx+P_yy)/2> over the second half of the run."""
+    gamma_s = (Lz/2)<P_zz - (P_xx+P_yy)/2> over the second half of the run; then T, P and
+    gamma_s of the FP32 engine against the FP64 parity engine from the final state."""
     from gpumdpd_b200 import Engine, inputs, observables, tune
     s = inputs.mdpd_slab(nsteps=args.slab_steps, thermo=100)
     s.run_in = tune.with_skin(s.run_in, args.batch_skin)
@@ -324,7 +449,6 @@ def run_slab(args):
         k = min(500, args.slab_steps - done)
         total_ms += eng.time_steps(k)["total_ms"]
         done += k
-    r = {"total_ms": total_ms}
     th = eng.thermo()
     st = eng.state(forces=False, images=False)
     eng.close()
@@ -332,13 +456,18 @@ def run_slab(args):
     liq, vap = observables.slab_densities(c, rho, 40.0, 80.0, margin=5.0)
     half = len(th["step"]) // 2
     g, gerr = observables.surface_tension(th["p"], s.box[2], skip=half)
-    return {"workload": f"mdpd_slab_40x40x120_N{s.n}_skin{args.batch_skin}", "particles": s.n,
-            "steps": args.slab_steps, "value": s.n * args.slab_steps / (r["total_ms"] / 1000.0),
-            "unit": "particle-steps/s", "ms_per_step": r["total_ms"] / args.slab_steps,
-            "liquid_density": liq, "vapour_density": vap,
-            "surface_tension": g, "surface_tension_stderr": gerr,
-            "mean_temp_second_half": float(np.mean(th["temp"][half:])),
-            "density_profile_z0.5": [round(float(v), 3) for v in rho]}
+    lz = float(s.box[2])
+    acc = fp32_fp64_window(s, st["x"], st["v"], args.slab_acc_steps, 10,
+                           extra={"surface_tension": lambda t: 0.5 * lz * (t["p"][:, 5] - 0.5 * (t["p"][:, 0] + t["p"][:, 3]))})
+    value = s.n * args.slab_steps / (total_ms / 1000.0)
+    summary = {"workload": f"mdpd_slab_40x40x120_N{s.n}_skin{args.batch_skin}", "particles": s.n,
+               "steps": args.slab_steps, "value": value, "unit": "particle-steps/s",
+               "ms_per_step": total_ms / args.slab_steps, "liquid_density": round(liq, 4),
+               "vapour_density": round(vap, 4), "surface_tension": round(g, 4),
+               "surface_tension_stderr": round(gerr, 4),
+               "mean_temp_second_half": round(float(np.mean(th["temp"][half:])), 5),
+               "err_vs_fp64": acc}
+    return summary, {"density_profile_z0.5": [round(float(x), 4) for x in rho]}
 
 
 def plain_step_ms(system, steps):
@@ -349,17 +478,33 @@ def plain_step_ms(system, steps):
     eng.run(0)
     eng.run(3)
     r = eng.time_steps(steps)
-    th = eng.thermo()
     eng.close()
-    return r["total_ms"] / steps, th
+    return r["total_ms"] / steps
+
+
+def run_alone(system, precision="fp32"):
+    """A system alone from its initial state for its run.in's `run N` (thermo rows)."""
+    from gpumdpd_b200 import Engine
+    run_in = system.run_in if precision == "fp32" else without_computes(system.run_in)
+    import re
+    steps = int(re.search(r"(?m)^run (\d+)$", run_in).group(1))
+    e = Engine(run_in, system=system.c_system(), precision=precision)
+    e.run(steps)
+    th = e.thermo()
+    e.close()
+    return th
 
 
 def run_batched(args):
     """Batched sweep: uneven A/B mixtures (a_AB over 25..45, L log-uniform over 8..24) in one
     packed engine, one launch per stage and the step captured in a CUDA graph, against the
-    plain engine running the same replicas one at a time (device time per step summed)."""
+    plain engine running the same replicas one at a time (device time per step summed).
+    Accuracy: for 8 replicas (smallest, largest, a_AB extremes, 4 spread over the sweep)
+    the packed run's mean T and P against the plain FP32 engine and the FP64 parity engine
+    running the same replica alone from the same initial state over the same steps, each
+    with its block-averaged standard error (rows after the first fifth)."""
     from gpumdpd_b200 import Batch, inputs, tune
-    systems = inputs.replica_sweep(n_rep=args.replicas, nsteps=5000)
+    systems = inputs.replica_sweep(n_rep=args.replicas, nsteps=args.batch_steps, thermo=10)
     for s in systems:
         s.run_in = tune.with_skin(s.run_in, args.batch_skin)
     n_tot = sum(s.n for s in systems)
@@ -368,49 +513,60 @@ def run_batched(args):
     b.run(0)
     K = args.batch_steps
     total_ms, done = 0.0, 0
-    while done < K:  # the whole sweep (5000 steps), timed in graphs of at most 500 steps
+    while done < K:  # the whole sweep, timed in graphs of at most 500 steps
         k = min(500, K - done)
         total_ms += b.time_steps(k)["total_ms"]
         done += k
     batched = n_tot * K / (total_ms / 1000.0)
-    rows_b = [b.thermo(k) for k in range(len(systems))]
-    # per replica: mean pressure after the first fifth of the run, and the A-B RDF's first
-    # peak (height, position)
+    R = len(systems)
+    ns = np.array([s.n for s in systems])
+    sel = sorted({int(np.argmin(ns)), int(np.argmax(ns)), 0, R - 1} |
+                 {int(k) for k in np.linspace(0, R - 1, 6)[1:-1]})
+    rows_b = {k: b.thermo(k) for k in sel}
     per_rep = []
     for k, s in enumerate(systems):
-        th = rows_b[k]
+        th = b.thermo(k)
         skip = max(1, len(th["pressure"]) // 5)
-        g, ns = b.rdf(k, 150)
+        g, nsamp = b.rdf(k, 150)
         rmax = min(3.0, 0.5 * float(s.box[0]))
         ipk = int(np.argmax(g))
-        per_rep.append({"a_ab": round(25.0 + 20.0 * k / max(len(systems) - 1, 1), 3), "n": s.n,
+        per_rep.append({"a_ab": round(25.0 + 20.0 * k / max(R - 1, 1), 3), "n": s.n,
                         "mean_p": round(float(th["pressure"][skip:].mean()), 4),
                         "rdf_peak": round(float(g[ipk]), 4), "rdf_peak_r": round((ipk + 0.5) * rmax / 150, 3),
-                        "rdf_samples": ns})
-    rows_b = rows_b[:8]
+                        "rdf_samples": nsamp})
     b.close()
-    plain_ms = []
-    rows_p = []
-    for k, s in enumerate(systems):
-        ms, th = plain_step_ms(s, args.plain_steps)
-        plain_ms.append(ms)
-        if k < 8:
-            rows_p.append(th)
+    plain_ms = [plain_step_ms(s, args.plain_steps) for s in systems]
     plain = n_tot / (sum(plain_ms) / 1000.0)
-    # same physics: per-replica mean T and P over the rows both runs logged
-    dt_max = dp_max = 0.0
-    for tb, tp in zip(rows_b, rows_p):
-        m = min(len(tb["temp"]), len(tp["temp"]))
-        if m > 1:
-            dt_max = max(dt_max, abs(tb["temp"][1:m].mean() / tp["temp"][1:m].mean() - 1))
-            dp_max = max(dp_max, abs(tb["pressure"][1:m].mean() / tp["pressure"][1:m].mean() - 1))
-    return {"workload": f"{len(systems)}_replica_AB_sweep_L8-24_skin{args.batch_skin}", "replicas": len(systems),
-            "particles": n_tot, "value": batched, "unit": "particle-steps/s", "steps": K,
-            "plain_one_at_a_time": plain, "speedup_vs_plain": batched / plain,
-            "plain_steps_per_replica": args.plain_steps,
-            "matched_accuracy": {"same_kernels_and_precision": True,
-                                 "max_rel_diff_mean_T_first8": dt_max, "max_rel_diff_mean_P_first8": dp_max},
-            "per_replica": per_rep}
+    acc = []
+    for k in sel:
+        s = systems[k]
+        tb = rows_b[k]
+        tp = run_alone(s, "fp32")
+        t64 = run_alone(s, "fp64")
+        m = min(len(tb["temp"]), len(tp["temp"]), len(t64["temp"]))
+        skip = max(1, m // 5)
+        rec = {"replica": k, "n": s.n, "a_ab": round(25.0 + 20.0 * k / max(R - 1, 1), 3), "rows": m - skip}
+        for f in ("temp", "pressure"):
+            rec[f] = {"batched_vs_fp64": compare(tb[f][skip:m], t64[f][skip:m]),
+                      "batched_vs_plain": compare(tb[f][skip:m], tp[f][skip:m])}
+        acc.append(rec)
+
+    def worst(f, key):
+        r = max(acc, key=lambda a: abs(a[f][key]["z"] or 0.0))
+        c = r[f][key]
+        return {"replica": r["replica"], "err": c["err"], "stderr": c["stderr"], "z": c["z"],
+                "rel_err": round(c["err"] / c["fp64"], 6) if c["fp64"] else None}
+
+    summary = {"workload": f"{R}_replica_AB_sweep_L8-24_skin{args.batch_skin}", "replicas": R,
+               "particles": n_tot, "value": batched, "unit": "particle-steps/s", "steps": K,
+               "plain_one_at_a_time": plain, "speedup_vs_plain": batched / plain,
+               "plain_steps_per_replica": args.plain_steps,
+               "err_vs_fp64": {"replicas_checked": len(sel), "steps": K, "thermo_every": 10,
+                               "worst_temp": worst("temp", "batched_vs_fp64"),
+                               "worst_pressure": worst("pressure", "batched_vs_fp64")},
+               "batched_vs_plain": {"worst_temp": worst("temp", "batched_vs_plain"),
+                                    "worst_pressure": worst("pressure", "batched_vs_plain")}}
+    return summary, {"per_replica": per_rep, "accuracy": acc}
 
 
 def served_run(jobs, args, rate_label):
@@ -438,9 +594,9 @@ def served_run(jobs, args, rate_label):
     st = srv.stats()
     srv.close()
     pct = latency_percentiles(res)
-    return {"rate_jobs_per_s": rate_label, "value": work / makespan, "makespan_s": makespan,
-            "busy_s": st["busy_s"], "p50_latency_s": pct.get("p50"), "p99_latency_s": pct.get("p99"),
-            "particle_steps": work}, res, ids
+    return {"rate_jobs_per_s": rate_label, "value": work / makespan, "makespan_s": round(makespan, 3),
+            "busy_s": round(st["busy_s"], 3), "p50_latency_s": round(pct.get("p50"), 4),
+            "p99_latency_s": round(pct.get("p99"), 4), "particle_steps": work}, res, ids
 
 
 def run_served(args):
@@ -448,7 +604,9 @@ def run_served(args):
     log-uniform 1k-200k, A5B5 chains in 0-50% of beads, steps U[1k,20k], T/P/RDF
     requested) through the continuous-batching server under a 120 GB budget; aggregate
     particle-steps/s over the makespan and p50/p99 job latency, against the plain engine
-    running the same jobs one at a time (device time per step x steps, per job)."""
+    running the same jobs one at a time (device time per step x steps, per job).
+    Accuracy: the 4 cheapest jobs' served mean T and P (with their block standard errors)
+    against the FP64 parity engine running each job alone from its initial state."""
     from gpumdpd_b200 import inputs
     rates = [float(x) for x in args.rates.split(",")]
     sweep = []
@@ -459,27 +617,53 @@ def run_served(args):
     # the same jobs one at a time on the plain engine (job contents do not depend on the rate)
     plain_s = 0.0
     for (_, s), r in zip(ids, res):
-        ms, _ = plain_step_ms(s, min(args.plain_steps, r["steps"]))
+        ms = plain_step_ms(s, min(args.plain_steps, r["steps"]))
         plain_s += ms / 1000.0 * r["steps"]
     plain = sweep[-1]["particle_steps"] / plain_s
     head = max(sweep, key=lambda x: x["value"])
-    return {"workload": f"{len(ids)}_job_poisson_stream", "jobs": len(ids), "value": head["value"],
-            "unit": "particle-steps/s", "rate_jobs_per_s": head["rate_jobs_per_s"],
-            "p50_latency_s": head["p50_latency_s"], "p99_latency_s": head["p99_latency_s"],
-            "plain_one_at_a_time": plain, "speedup_vs_plain": head["value"] / plain, "rate_sweep": sweep,
-            "hbm_budget_bytes": 120e9, "chunk_steps": args.chunk,
-            "admission_window": {"max_wait_s": args.max_wait, "min_jobs": args.min_jobs},
-            "plain_timing": f"device time per step over min({args.plain_steps}, steps) steps x steps, per job"}
+    cheap = sorted(range(len(ids)), key=lambda k: ids[k][1].n * res[k]["steps"])[:4]
+    acc = []
+    for k in cheap:
+        s = ids[k][1]
+        r = res[k]
+        t64 = run_alone(s, "fp64")
+        rec = {"job": k, "n": s.n, "steps": r["steps"]}
+        for f, fm, fs in (("temp", "mean_temp", "stderr_temp"), ("pressure", "mean_pressure", "stderr_pressure")):
+            m64, s64 = block_stats(t64[f][1:])
+            se = math.sqrt(r[fs] ** 2 + s64 ** 2)
+            rec[f] = {"served": round(r[fm], 6), "fp64": round(m64, 6), "err": round(r[fm] - m64, 6),
+                      "stderr": round(se, 6), "z": round((r[fm] - m64) / se, 2) if se > 0 else None}
+        acc.append(rec)
+
+    def worst(f):
+        r = max(acc, key=lambda a: abs(a[f]["z"] or 0.0))
+        c = r[f]
+        return {"job": r["job"], "err": c["err"], "stderr": c["stderr"], "z": c["z"],
+                "rel_err": round(c["err"] / c["fp64"], 6) if c["fp64"] else None}
+
+    summary = {"workload": f"{len(ids)}_job_poisson_stream", "jobs": len(ids), "value": head["value"],
+               "unit": "particle-steps/s", "rate_jobs_per_s": head["rate_jobs_per_s"],
+               "p50_latency_s": head["p50_latency_s"], "p99_latency_s": head["p99_latency_s"],
+               "plain_one_at_a_time": plain, "speedup_vs_plain": head["value"] / plain,
+               "rates": [{k: x[k] for k in ("rate_jobs_per_s", "value", "p50_latency_s", "p99_latency_s")}
+                         for x in sweep],
+               "hbm_budget_bytes": 120e9, "chunk_steps": args.chunk,
+               "admission_window": {"max_wait_s": args.max_wait, "min_jobs": args.min_jobs},
+               "err_vs_fp64": {"jobs_checked": len(acc), "worst_temp": worst("temp"),
+                               "worst_pressure": worst("pressure")}}
+    return summary, {"rate_sweep": sweep, "accuracy": acc}
 
 
-def time_reference_binary(binary, system, K):
-    """Runs a reference executable on `system` for 2K steps with thermo every K steps and
-    times steps K..2K on the host clock between its thermo lines (setup and file I/O
-    excluded).  Returns (seconds, None) or (None, the end of its output)."""
+def time_reference_binary(binary, system, W, K, every):
+    """Runs a reference executable on `system` for W+K steps with a thermo line every
+    `every` steps (a divisor of W and K) and times steps W..W+K on the host clock between
+    its thermo lines at W and W+K (setup and file I/O excluded; the reference flushes each
+    line after the device work of its step).  Returns (seconds, None) or (None, the end
+    of its output)."""
     import tempfile
     with tempfile.TemporaryDirectory() as td:
         lines = [ln for ln in system.run_in.splitlines() if not ln.startswith(("run ", "thermo ", "read_data "))]
-        lines += [f"run {2 * K}", f"thermo {K}", "read_data system.data"]
+        lines += [f"run {W + K}", f"thermo {every}", "read_data system.data"]
         open(os.path.join(td, "run.in"), "w").write("\n".join(lines) + "\n")
         system.write_data(os.path.join(td, "system.data"))
         p = subprocess.Popen([binary], cwd=td, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, bufsize=1)
@@ -487,13 +671,15 @@ def time_reference_binary(binary, system, K):
         log = []
         for line in p.stdout:
             log.append(line)
+            if len(log) > 50:
+                log.pop(0)
             tok = line.split()
             if tok and tok[0].isdigit() and len(tok) >= 5:
                 stamps[int(tok[0])] = time.perf_counter()
         rc = p.wait()
-    if rc != 0 or K not in stamps or 2 * K not in stamps:
+    if rc != 0 or W not in stamps or W + K not in stamps:
         return None, f"rc={rc}: " + "".join(log[-3:]).strip().replace("\n", " | ")
-    return stamps[2 * K] - stamps[K], None
+    return stamps[W + K] - stamps[W], None
 
 
 def run_fp64(args):
@@ -511,26 +697,26 @@ def run_fp64(args):
            "value": s.n / (ms / 1000.0), "unit": "particle-steps/s", "dtype": "f64"}
     binary = os.path.join(ROOT, "oracle", "_ref", "gpudpd_double")
     if os.path.exists(binary):
-        dt, why = time_reference_binary(binary, s, K)
+        dt, why = time_reference_binary(binary, s, 1000, K, 1000)
         if dt is not None:
             out["reference_double_ms_per_step"] = dt * 1000 / K
             out["speedup_vs_reference_double"] = out["reference_double_ms_per_step"] / ms
         else:
             out["reference_double"] = f"failed {why}"
-    return out
+    return out, {}
 
 
 def run_reference(args, world, rank):
     """The reference's own CUDA build (oracle/_ref/gpudpd_single, built from its sources by
-    oracle/build_ref.sh) on the same system: it reads run.in + a data file in its own
-    format; K steps are timed on the host clock between its thermo lines at steps K and 2K
-    (thermo every K steps, so setup and file I/O are excluded)."""
+    oracle/build_ref.sh) on the same system and thermo cadence: it reads run.in + a data
+    file in its own format; after W warm-up steps, K steps are timed on the host clock
+    between its thermo lines at steps W and W+K (setup and file I/O excluded)."""
     if rank != 0:
         return
-    from gpumdpd_b200 import inputs  # noqa: F401
+    every = thermo_every(args)
+    system = make_system(args, thermo=every)
+    K, W = args.steps, args.warmup
     binary = os.path.join(ROOT, "oracle", "_ref", "gpudpd_single")
-    system = make_system(args)
-    K = args.steps
     if not os.path.exists(binary):
         # no reference build: time the FP64 port on the host cores instead
         cb = cpu_baseline(system, os.cpu_count() or 1)
@@ -540,20 +726,20 @@ def run_reference(args, world, rank):
                           "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": 0}}))
         return
-    dt, why = time_reference_binary(binary, system, K)
+    dt, why = time_reference_binary(binary, system, W, K, every)
     if dt is None:
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed {why}"}))
         return
     value = system.n * K / dt
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
-           "steps": K, "warmup": K, "ms_per_step": dt * 1000 / K, "higher_is_better": True,
+           "steps": K, "warmup": W, "ms_per_step": dt * 1000 / K, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (same generator and seed)",
            "config": {"workload": workload_name(args), "n_particles": system.n, "skin": args.skin,
-                      "parallelism": "single GPU, rank 0 only"},
+                      "thermo_every": every, "parallelism": "single GPU, rank 0 only"},
            "impl": "reference",
            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": 1, "kind": "reference",
                             "sample": f"reference CUDA build (-DSINGLE, sm_100a) on one B200 driven by one host "
-                                      f"thread; steps {K}..{2 * K} timed between its thermo lines"},
+                                      f"thread; steps {W}..{W + K} timed between its thermo lines"},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -572,9 +758,15 @@ def main():
                     help="pair-kernel schedule (default: the engine's choice)")
     ap.add_argument("--build-variant", type=int, default=0,
                     help="list-build kernel (0: ranges in registers; 1, 2: in shared memory)")
+    ap.add_argument("--tile", type=int, default=0,
+                    help="pair schedule 11: home cells per tile edge (0: the engine's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched and served lines")
+    ap.add_argument("--no-extras", action="store_true", help="skip the slab, batched, served and fp64 objects")
+    ap.add_argument("--detail", default="bench_detail.json",
+                    help="file for the per-replica records, density profile and rate sweep ('' = none)")
+    ap.add_argument("--acc-steps", type=int, default=300, help="FP32-vs-FP64 window of the headline system")
     ap.add_argument("--slab-steps", type=int, default=20000)
+    ap.add_argument("--slab-acc-steps", type=int, default=1000)
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5000)
     ap.add_argument("--batch-skin", type=float, default=0.0)

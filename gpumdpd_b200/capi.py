@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libdpd_b200.so")
 DPD_ERRORS = {
     -1: "DPD_E_ARG", -2: "DPD_E_IO", -3: "DPD_E_CUDA", -4: "DPD_E_NOMEM",
     -5: "DPD_E_OVERFLOW", -6: "DPD_E_STATE", -7: "DPD_E_NUMERIC", -8: "DPD_E_NODEV",
+    -9: "DPD_E_CANCELLED",
 }
 
 # every symbol declared in include/dpd_b200.h
@@ -25,7 +26,7 @@ EXPORTED = [
     "dpd_write_data", "dpd_time_steps", "dpd_get_list_stats", "dpd_last_error", "dpd_destroy", "dpd_pair_compute_aos",
     "dpd_batch_create", "dpd_batch_n", "dpd_batch_get_thermo", "dpd_batch_get_state",
     "dpd_batch_rdf_result", "dpd_server_create", "dpd_server_submit", "dpd_server_set_policy", "dpd_server_step",
-    "dpd_server_result", "dpd_server_job_state", "dpd_server_job_rdf", "dpd_server_stats",
+    "dpd_server_result", "dpd_server_cancel", "dpd_server_job_state", "dpd_server_job_rdf", "dpd_server_stats",
     "dpd_server_last_error", "dpd_server_destroy", "dpd_pair_forces_noalloc", "dpd_version",
 ]
 
@@ -65,7 +66,8 @@ class dpd_thermo(ctypes.Structure):
 class dpd_tuning(ctypes.Structure):
     _fields_ = [
         ("pair_block", ctypes.c_int), ("pair_variant", ctypes.c_int), ("cell_order", ctypes.c_int),
-        ("build_variant", ctypes.c_int), ("launch_mode", ctypes.c_int), ("reserved", ctypes.c_int * 3),
+        ("build_variant", ctypes.c_int), ("launch_mode", ctypes.c_int), ("tile", ctypes.c_int),
+        ("tile_capacity", ctypes.c_int), ("reserved", ctypes.c_int),
     ]
 
 
@@ -75,6 +77,7 @@ class dpd_job_result(ctypes.Structure):
         ("mean_temp", ctypes.c_double), ("mean_pressure", ctypes.c_double),
         ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double),
         ("last", dpd_thermo),
+        ("stderr_temp", ctypes.c_double), ("stderr_pressure", ctypes.c_double),
     ]
 
 
@@ -143,6 +146,7 @@ def load():
         "dpd_server_set_policy": (i, [vp, d, i]),
         "dpd_server_step": (i, [vp, P(i), P(i)]),
         "dpd_server_result": (i, [vp, i64, P(dpd_job_result)]),
+        "dpd_server_cancel": (i, [vp, i64]),
         "dpd_server_job_state": (i, [vp, i64, vp, vp]),
         "dpd_server_job_rdf": (i, [vp, i64, vp, P(i64)]),
         "dpd_server_stats": (i, [vp, P(i64), P(d), P(i64)]),

@@ -16,6 +16,7 @@
 #include "kernels.cuh"
 #include "kernels_aos.cuh"
 #include "kernels_step.cuh"
+#include "kernels_tile.cuh"
 
 namespace dpd {
 
@@ -281,6 +282,10 @@ int Engine::alloc_and_upload()
     DA(b_.build_flag, 2);
     DA(b_.phase, 1);
     DA(b_.limit, nrep);
+    if (!any_mdpd_) {  // pair schedule 11: at most one tile per cell
+        DA(b_.tile_rep, C_);
+        DA(b_.tile_code, C_);
+    }
 #undef DA
     {
         std::vector<uint32_t> lim(nrep, 0xFFFFFFFFu);
@@ -542,6 +547,13 @@ int Engine::upload_particles()
             float o[3];
             for (int k = 0; k < 3; k++) {
                 double x = R.sys.x[3 * (size_t)i + k] - d.lo[k];
+                if (!std::isfinite(x)) {
+                    // kept non-finite: the first list build flags the replica
+                    // (DPD_E_NUMERIC) instead of binning garbage
+                    c[k] = 0;
+                    o[k] = NAN;
+                    continue;
+                }
                 const double L = R.box_len[k];
                 if (x >= L || x < 0) x -= L * std::floor(x / L);
                 int cc = (int)std::floor(x / (double)d.w[k]);
@@ -709,6 +721,24 @@ static void pdl_launch(void (*kern)(KArgs...), int grid, int block, cudaStream_t
     cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// the same with dynamic shared memory
+template <typename... KArgs, typename... Args>
+static void pdl_launch_smem(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t s,
+                            Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <int STYLE, bool BONDS>
 static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -740,7 +770,8 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
 // the list build fused into it (DPD; mDPD falls back to 4); 7 and 8 (the default): the
 // flattened schedule as two launches, non-log steps without FP64 sums at 6 (7) or 5 (8)
 // blocks/SM, log steps at 4; 9: as 8 with the i-side forces summed per owner in the warp;
-// 10: one thread per list entry (small grids)
+// 10: one thread per list entry (small grids); 11 (DPD engines): no list, the cell-tile
+// kernel (kernels_tile.cuh) after the counting sort
 template <int STYLE>
 static void launch_pair(int variant, bool bonds, int grid, cudaStream_t s, const StepArgs& a)
 {
@@ -791,13 +822,26 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     // engine that shares the GPU with others (a server's cohorts) gains more from leaving
     // SMs to them than from spreading its own few pairs
     const bool tiny = small && gp <= 148 && tune_.launch_mode != 3;
-    const int variant = small && tune_.pair_variant == 8 ? (tiny ? 10 : 4) : tune_.pair_variant;
+    // schedule 11: no neighbour list, the cell-tile kernel after the counting sort
+    const bool tile = use_tile();
+    const int variant = tile ? 11 : (small && tune_.pair_variant == 8 ? (tiny ? 10 : 4) : tune_.pair_variant);
     // schedule 6: the DPD list build runs inside the pair kernel
     const bool fused = variant == 6 && !any_mdpd_;
-    enqueue_build(s, !fused, (tiny && tune_.build_variant == 0) || tune_.build_variant == 3);
+    enqueue_build(s, !fused && !tile, (tiny && tune_.build_variant == 0) || tune_.build_variant == 3);
     if (any_mdpd_) pdl_launch(k_density, gp, 256, s, sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
-    if (fused) {
+    if (tile) {
+        const TileArgs ta{b_.tile_rep, b_.tile_code, ntiles_, tile_edge_, tile_smax_};
+        const size_t sm = tile_smem_bytes(tile_smax_);
+        const int glog = std::min(ntiles_, 148 * 2);
+        if (bonds_) {
+            pdl_launch_smem(k_tile<true, 4>, ntiles_, 256, sm, s, sa, ta);
+            pdl_launch_smem(k_tile_logsteps<true>, glog, 256, sm, s, sa, ta);
+        } else {
+            pdl_launch_smem(k_tile<false, 4>, ntiles_, 256, sm, s, sa, ta);
+            pdl_launch_smem(k_tile_logsteps<false>, glog, 256, sm, s, sa, ta);
+        }
+    } else if (fused) {
         const BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
         if (bonds_) pdl_launch(k_build_pair<true, 4>, gp, 256, s, sa, ba);
         else pdl_launch(k_build_pair<false, 4>, gp, 256, s, sa, ba);
@@ -859,11 +903,96 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
     if (any_twowall_) enqueue_two_wall(s, sa);
 }
 
+// The tile table of pair schedule 11: the tiles of every replica (edge^3 home cells,
+// fewer at a grid's edge), each replica's tiles in Morton order of their coordinates
+// (the order of the slots), and the staging capacity of a CTA: 1.75 times the mean
+// particle count of a tile's neighbourhood (plus 64) in the densest replica.  Edge 0
+// (the default) takes the largest edge up to 4 that still gives at least 8 tiles per
+// SM, else 1.
+int Engine::prepare_tiles()
+{
+    ntiles_ = 0;
+    if (!use_tile()) return DPD_OK;
+    auto count = [&](int E) {
+        int64_t n = 0;
+        for (auto& R : reps_) {
+            const RepDesc& d = R.desc;
+            n += (int64_t)((d.nc[0] + E - 1) / E) * ((d.nc[1] + E - 1) / E) * ((d.nc[2] + E - 1) / E);
+        }
+        return n;
+    };
+    int E = tune_.tile;
+    if (E <= 0) {
+        E = 1;
+        for (int e = 4; e >= 2; e--)
+            if (count(e) >= 148 * 8) {
+                E = e;
+                break;
+            }
+    }
+    E = std::min(E, TILE_MAX_EDGE);
+    std::vector<int> trep, tcode;
+    int smax = 128;
+    for (int r = 0; r < (int)reps_.size(); r++) {
+        const RepDesc& d = reps_[r].desc;
+        const int nt[3] = {(d.nc[0] + E - 1) / E, (d.nc[1] + E - 1) / E, (d.nc[2] + E - 1) / E};
+        std::vector<std::pair<uint32_t, int>> order;
+        for (int x = 0; x < nt[0]; x++)
+            for (int y = 0; y < nt[1]; y++)
+                for (int z = 0; z < nt[2]; z++) order.push_back({morton3(x, y, z), x | (y << 10) | (z << 20)});
+        std::sort(order.begin(), order.end());
+        for (auto& o : order) {
+            trep.push_back(r);
+            tcode.push_back(o.second);
+        }
+        const double mean_cell = (double)d.n_real / std::max(d.ncell, 1);
+        const int region = (std::min(E, d.nc[0]) + 2) * (std::min(E, d.nc[1]) + 2) * (std::min(E, d.nc[2]) + 1);
+        smax = std::max(smax, (int)std::ceil(1.75 * mean_cell * region) + 64);
+    }
+    if (tune_.tile_capacity > 0) smax = tune_.tile_capacity;
+    smax = (smax + 31) / 32 * 32;
+    // at most 200 KB of shared memory a CTA (a neighbourhood beyond it takes its home
+    // cells one at a time)
+    while (smax > 32 && tile_smem_bytes(smax) > 200 * 1024) smax -= 32;
+    if ((int64_t)trep.size() > C_) {
+        err = "tile table larger than the cell count";
+        return DPD_E_STATE;
+    }
+    ntiles_ = (int)trep.size();
+    tile_edge_ = E;
+    tile_smax_ = smax;
+    CK(cudaMemcpyAsync(b_.tile_rep, trep.data(), sizeof(int) * trep.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.tile_code, tcode.data(), sizeof(int) * tcode.size(), cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    const int bytes = (int)tile_smem_bytes(smax);
+    CK(cudaFuncSetAttribute(k_tile<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile_logsteps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile_logsteps<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return DPD_OK;
+}
+
+// the half list of the current state (cells of the last build), for get_neighbors and
+// list_stats of an engine whose steps build none
+int Engine::refresh_list()
+{
+    if (!use_tile()) return DPD_OK;
+    const BuildArgs ba = build_args(b_, P_, C_, nmax_, maxb_);
+    k_build_nlist_now<<<(P_ + 255) / 256, 256, 0, stream_>>>(ba);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
 int Engine::build_graph()
 {
     if (graph_) {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
+    }
+    {
+        const int e = prepare_tiles();
+        if (e) return e;
     }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -970,7 +1099,7 @@ int Engine::status_error(int s, int r)
         return DPD_E_OVERFLOW;
     }
     if (s & ST_NONFINITE) {
-        err = "non-finite position or velocity in replica " + std::to_string(r);
+        err = "non-finite (or runaway) position or velocity in replica " + std::to_string(r);
         return DPD_E_NUMERIC;
     }
     if (s & ST_FENE_BROKEN) {
@@ -1041,6 +1170,19 @@ int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64
     if (pair_ms) *pair_ms = pair;
     if (launches) *launches = (int64_t)nsteps * ((any_dpd_ ? 1 : 0) + (any_mdpd_ ? 1 : 0));
     return sync_and_check();
+}
+
+__global__ void k_freeze(uint32_t* limit, int r)
+{
+    if (threadIdx.x == 0) limit[r] = 0u;
+}
+
+int Engine::freeze_async(int rep)
+{
+    if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    k_freeze<<<1, 32, 0, stream_>>>(b_.limit, rep);
+    CK(cudaGetLastError());
+    return DPD_OK;
 }
 
 int Engine::set_limits(const std::vector<uint32_t>& limit)
@@ -1383,6 +1525,10 @@ int Engine::get_cells(int rep, int* cell, float* off, int* nc, float* w, float* 
 int Engine::get_neighbors(int rep, int* pairs, int64_t cap, int64_t* n_pairs)
 {
     if (rep < 0 || rep >= (int)reps_.size()) return DPD_E_ARG;
+    {
+        const int e = refresh_list();
+        if (e) return e;
+    }
     const RepDesc& d = reps_[rep].desc;
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<int> cnt(ns), lst((size_t)ns * nmax_);
@@ -1477,6 +1623,10 @@ int Engine::write_data(int rep, const std::string& path)
 
 int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 {
+    {
+        const int e = refresh_list();
+        if (e) return e;
+    }
     const RepDesc& d = reps_[0].desc;
     const int ns = d.p_cap_end - d.p_begin;
     std::vector<int> cnt(ns);
@@ -1493,10 +1643,12 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 10 || t->cell_order < 0 || t->cell_order > 1 ||
+    if (t->pair_variant < 0 || t->pair_variant > 11 || t->cell_order < 0 || t->cell_order > 1 ||
         t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 3 || t->launch_mode < 0 ||
-        t->launch_mode > 3) {
-        err = "dpd_set_tuning: pair_variant must be 0..10, build_variant 0..3, cell_order 0 or 1, launch_mode 0..3";
+        t->launch_mode > 3 || t->tile < 0 || t->tile > TILE_MAX_EDGE || t->tile_capacity < 0 ||
+        t->tile_capacity > 4096) {
+        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..3, cell_order 0 or 1, "
+              "launch_mode 0..3, tile edge 0..6, tile capacity 0..4096";
         return DPD_E_ARG;
     }
     tune_ = *t;
@@ -1637,12 +1789,14 @@ int Engine::pair_compute_aos(const float* d_pos, const float* d_vel, const int* 
     enqueue_build(stream_, true, tune_.build_variant == 3);
     if (any_mdpd_) k_density<<<gp, 256, 0, stream_>>>(sa);
     const bool peratom = d_pe || d_virial;
+    // this entry builds the list itself: schedule 11 (no list) runs as the default 8
+    const int pv = tune_.pair_variant == 11 ? 8 : tune_.pair_variant;
     if (d.style == 0) {
         if (peratom) k_pair_peratom<0><<<gp, 256, 0, stream_>>>(sa, pe_slot_, vir_slot_);
-        else launch_pair<0>(tune_.pair_variant, false, gp, stream_, sa);
+        else launch_pair<0>(pv, false, gp, stream_, sa);
     } else {
         if (peratom) k_pair_peratom<1><<<gp, 256, 0, stream_>>>(sa, pe_slot_, vir_slot_);
-        else launch_pair<1>(tune_.pair_variant, false, gp, stream_, sa);
+        else launch_pair<1>(pv, false, gp, stream_, sa);
     }
     k_aos_out<<<gp, 256, 0, stream_>>>(sa, d_force, d_pe, d_virial, pe_slot_, vir_slot_);
     k_aos_done<<<1, 1, 0, stream_>>>(b_.build_flag, b_.phase);

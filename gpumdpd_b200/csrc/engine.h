@@ -74,6 +74,8 @@ struct DeviceBuffers {
     double* gc_ring = nullptr;
     int* gc_count = nullptr;
     int* wall_ext = nullptr;        // wall extents (fix two_wall, compute wall_contact)
+    int* tile_rep = nullptr;        // pair schedule 11: replica and coordinates of each tile
+    int* tile_code = nullptr;
 };
 
 class Engine {
@@ -139,6 +141,9 @@ public:
 
     // per-replica step limits: replica r evaluates no step beyond limit[r]
     int set_limits(const std::vector<uint32_t>& limit);
+    // stop replica r after the work already enqueued on the engine's stream: its limit
+    // becomes 0, so the next run segment leaves it inactive (no host wait)
+    int freeze_async(int rep);
     int read_rstate(std::vector<RepState>& st);
     // enqueue a copy of every replica's state word into host memory (pinned, n_rep entries)
     // on the engine's stream, after the work enqueued so far
@@ -157,6 +162,12 @@ private:
     void enqueue_build(cudaStream_t s, bool list = true, bool wide = false);
     void enqueue_integrate_initial(cudaStream_t s);
     int build_graph();
+    // pair schedule 11 (the cell-tile kernel, DPD engines): the tile table and staging
+    // capacity for the current tuning; refresh_list() builds the neighbour list of the
+    // current state on demand (that schedule builds none in its steps)
+    bool use_tile() const { return tune_.pair_variant == 11 && !any_mdpd_; }
+    int prepare_tiles();
+    int refresh_list();
     int dump_frame(DumpWriter* w, uint32_t step);
     int dump_start(std::unique_ptr<DumpWriter> w);
     static bool dump_due(const DumpWriter* w, uint32_t step);
@@ -198,6 +209,7 @@ private:
     bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
+    int ntiles_ = 0, tile_edge_ = 0, tile_smax_ = 0;
     std::vector<std::unique_ptr<DumpWriter>> dumps_;
 };
 

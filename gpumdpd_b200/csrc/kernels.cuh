@@ -173,7 +173,9 @@ __device__ __forceinline__ bool build_on(const BuildArgs& a)
 }
 
 // Re-bin a particle: move whole cell widths from the offset into the cell index,
-// wrapping the cell grid and counting images.  Returns false for a non-finite offset.
+// wrapping the cell grid and counting images.  Returns false for a non-finite offset
+// and for a runaway one (a million cell widths or more since the last build, which no
+// finite-temperature trajectory reaches: its offset is clamped into the new cell).
 __device__ __forceinline__ bool rebin(const RepDesc& d, float4& p, int dimg[3])
 {
     int code = __float_as_int(p.w);
@@ -190,6 +192,7 @@ __device__ __forceinline__ bool rebin(const RepDesc& d, float4& p, int dimg[3])
                 continue;
             }
             float q = floorf(o[k] * d.inv_w[k]);
+            if (!(fabsf(q) < 1.0e6f)) ok = false;
             q = fminf(fmaxf(q, -1.0e6f), 1.0e6f);
             o[k] = __fmaf_rn(-q, d.w[k], o[k]);
             int cc = c[k] + (int)q;
@@ -394,14 +397,15 @@ __constant__ int8_t c_half[13][3] = {
 // r2 = fma(dz,dz,fma(dy,dy,dx*dx)) <= (global_cut+skin)^2 in float with
 // d = (o_i - o_j) + (c_i - c_j) w, the reference's test (src/force/neigh_list.cu:373-382)
 // on the cell-offset representation.  Entries store j and the shift code of the pair.
+template <bool ALL = false>
 __device__ __forceinline__ void build_nlist_slot(const BuildArgs& a, const int s)
 {
     if (s >= a.P) return;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
     // ghosts, and replicas past their last step (a finished job of a server cohort),
-    // get no list
-    if (s >= d.p_end || a.rstate[r].step > a.rstate[r].target) {
+    // get no list (ALL: every replica's list, for an on-demand build between runs)
+    if (s >= d.p_end || (!ALL && a.rstate[r].step > a.rstate[r].target)) {
         a.ncount[s] = 0;
         return;
     }
@@ -471,6 +475,13 @@ __global__ void __launch_bounds__(256, 4) k_build_nlist(BuildArgs a)
     griddep_wait();
     if (!build_on(a)) return;
     build_nlist_slot(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the same list of the current state, whatever the build flag (on demand, for engines
+// whose steps build no list)
+__global__ void __launch_bounds__(256, 4) k_build_nlist_now(BuildArgs a)
+{
+    build_nlist_slot<true>(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Small grids, where one thread per particle leaves most of the GPU idle and each thread's

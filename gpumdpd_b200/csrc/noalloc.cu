@@ -14,11 +14,18 @@
 // rejected with DPD_E_ARG before anything is launched.  The scratch array is shared by
 // every call in the process (each device that loads the library holds its own copy until
 // exit) and keeps the last call's contents: each call clears what must start at zero.
-// Calls that overlap on the GPU (different streams or threads) race on the array.  The
-// first call on a device resolves the array's device address with that device current;
-// it should come before any stream capture.
+// Calls that overlap on the GPU (different streams or threads) race on the array.
+//
+// Set-up: CUDA loads a library's device code lazily, so the first call on a device
+// loads this module, and with it the array (the driver reserves its device memory then,
+// not when the library is loaded).  That first call also resolves the array's device
+// address with the device current; the address is kept per device and CUDA context, and
+// resolved again when the context changes (after a cudaDeviceReset, for instance).  Make
+// that first call at start-up, before any stream capture.  Every call waits for its own
+// work on `stream` before it returns (it reads back a status word).
 #include <algorithm>
 #include <cmath>
+#include <cuda.h>
 #include <mutex>
 
 #include "../../include/dpd_b200.h"
@@ -79,11 +86,25 @@ __device__ __forceinline__ int na_cell(const NaParams& p, const float* x, int i)
     return (c[0] * p.nc[1] + c[1]) * p.nc[2] + c[2];
 }
 
+// a position more than a thousandth of a cell outside [lo, hi) (or not finite): the
+// cell stencil would miss some of its pairs
+__device__ __forceinline__ bool na_outside(const NaParams& p, const float* x, int i)
+{
+    bool out = false;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float q = (x[3 * i + k] - p.lo[k]) * p.inv_w[k];
+        out = out || !(q >= -1.0e-3f && q < (float)p.nc[k] + 1.0e-3f);
+    }
+    return out;
+}
+
 __global__ void k_na_count(NaParams p, int* scratch, const float* x, const int* id, const int* type, int n)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (type[i] < 1 || type[i] > p.ntypes || id[i] < 1) atomicOr(&scratch[kOffStatus], 1);
+    if (na_outside(p, x, i)) atomicOr(&scratch[kOffStatus], 2);
     const int c = na_cell(p, x, i);
     scratch[kOffCellOf + i] = c;
     atomicAdd(&scratch[kOffCount + c], 1);
@@ -189,21 +210,59 @@ __global__ void __launch_bounds__(256) k_na_force(NaParams p, const int* scratch
 }
 
 std::mutex g_mu;
-int* g_ptr[64] = {nullptr};
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;  // CUDA context the address belongs to (0: none yet)
+    int* ptr = nullptr;
+};
+ScratchAddr g_addr[64];
 
-// Per-device set-up: the device address of the scratch array, resolved once per device
-// with that device current.
+// the unique id of the calling thread's current CUDA context (driver entry points looked
+// up through the runtime, so the library needs no link to libcuda); 0 when unavailable
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            get_current = (GetCurrent)a;
+            get_id = (GetId)b;
+        }
+        looked_up = true;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Set-up: the device address of the scratch array, resolved with the device current
+// once per device and CUDA context (again after the context changes; on every call when
+// the context id cannot be read).  cudaSetDevice makes the device's primary context
+// current, so the context read here is the one the kernels will run in.
 int scratch_ptr(int** out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DPD_E_NODEV;
+    if (cudaSetDevice(dev) != cudaSuccess) return DPD_E_CUDA;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_ptr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    ScratchAddr& a = g_addr[dev];
+    if (!a.ptr || ctx == 0 || a.ctx_id != ctx) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DPD_E_CUDA;
-        g_ptr[dev] = (int*)p;
+        a.ptr = (int*)p;
+        a.ctx_id = ctx;
     }
-    *out = g_ptr[dev];
+    *out = a.ptr;
     return DPD_OK;
 }
 

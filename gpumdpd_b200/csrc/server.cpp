@@ -15,6 +15,8 @@
 //      last job has finished.
 // Each job keeps its own tags, seed, step counter and step limit inside its cohort, so
 // its trajectory is the one it has alone, up to the FP32 summation order of forces.
+// A job whose replica reports an error (its own status word) fails alone: the replica
+// is frozen and its cohort mates run on.  Cancelling a job freezes it the same way.
 // A server is used from one host thread at a time.
 #include <algorithm>
 #include <chrono>
@@ -128,7 +130,20 @@ struct dpd_server {
     int make_cohort(const std::vector<int64_t>& ids);
     int advance();
     void retire_job(Cohort& c, int r, int64_t id);
+    // end a running job of cohort c (replica r) with an error status; its cohort mates
+    // run on
+    void fail_job(Cohort& c, int r, int code, const std::string& msg);
 };
+
+void dpd_server::fail_job(Cohort& c, int r, int code, const std::string& msg)
+{
+    Job& j = jobs[c.jobs[r]];
+    j.status = code;
+    j.finish_s = now();
+    c.finished[r] = true;
+    err = "job " + std::to_string(j.id) + ": " + msg;
+    if (c.eng->freeze_async(r) != DPD_OK) err += " (and its replica could not be frozen)";
+}
 
 // Admission: one new cohort from the queued jobs that fit the budget together.  The
 // estimate of a set is the sum of the jobs' own estimates, corrected for the set's
@@ -283,19 +298,23 @@ int dpd_server::advance()
             if (q == cudaErrorNotReady) break;
             c.pending.pop_front();
             progressed = true;
-            int rc = DPD_OK;
             if (q != cudaSuccess) {
+                // a CUDA error ends the whole cohort (it is sticky for the context)
                 c.eng->err = std::string("CUDA error in a chunk: ") + cudaGetErrorString(q);
-                rc = DPD_E_CUDA;
-            }
-            for (size_t r = 0; r < c.jobs.size() && !rc; r++)
-                if (!c.finished[r]) rc = c.eng->status_error(k.rs[r].status, (int)r);
-            if (rc) {
-                fail_cohort(c, rc);
+                fail_cohort(c, DPD_E_CUDA);
                 cudaStreamSynchronize(c.eng->stream());
                 c.pending.clear();
                 failed = true;
                 break;
+            }
+            // a replica's own status word fails its job alone
+            for (size_t r = 0; r < c.jobs.size(); r++) {
+                if (c.finished[r]) continue;
+                const int rc = c.eng->status_error(k.rs[r].status, (int)r);
+                if (rc) {
+                    fail_job(c, (int)r, rc, c.eng->err);
+                    if (!first_err) first_err = rc;
+                }
             }
             for (size_t r = 0; r < c.jobs.size(); r++) {
                 if (c.finished[r]) continue;
@@ -432,8 +451,56 @@ int dpd_server_result(dpd_server* srv, int64_t job_id, dpd_job_result* res)
     }
     res->mean_temp = n ? st / n : (j.thermo.empty() ? 0.0 : j.thermo[0].temp);
     res->mean_pressure = n ? sp / n : (j.thermo.empty() ? 0.0 : j.thermo[0].pressure);
+    // standard errors of the means from block averages (rows after the first, in up to
+    // 10 consecutive blocks of equal length; the last rows that do not fill a block
+    // are left out of this estimate)
+    res->stderr_temp = res->stderr_pressure = NAN;
+    if (n >= 4) {
+        const int nb = std::min(10, n / 2), len = n / nb;
+        double mt = 0, mp = 0, vt = 0, vp = 0;
+        std::vector<double> bt(nb), bp(nb);
+        for (int b = 0; b < nb; b++) {
+            double a = 0, c = 0;
+            for (int k = 0; k < len; k++) {
+                a += j.thermo[1 + b * len + k].temp;
+                c += j.thermo[1 + b * len + k].pressure;
+            }
+            bt[b] = a / len;
+            bp[b] = c / len;
+            mt += bt[b] / nb;
+            mp += bp[b] / nb;
+        }
+        for (int b = 0; b < nb; b++) {
+            vt += (bt[b] - mt) * (bt[b] - mt);
+            vp += (bp[b] - mp) * (bp[b] - mp);
+        }
+        res->stderr_temp = std::sqrt(vt / (nb - 1) / nb);
+        res->stderr_pressure = std::sqrt(vp / (nb - 1) / nb);
+    }
     if (!j.thermo.empty()) res->last = j.thermo.back();
     return DPD_OK;
+}
+
+int dpd_server_cancel(dpd_server* srv, int64_t job_id)
+{
+    if (!srv) return DPD_E_ARG;
+    auto it = srv->jobs.find(job_id);
+    if (it == srv->jobs.end()) return srv->fail(DPD_E_ARG, "unknown job id");
+    Job& j = it->second;
+    if (j.status == JOB_QUEUED) {
+        srv->queue.erase(std::find(srv->queue.begin(), srv->queue.end(), job_id));
+        j.status = DPD_E_CANCELLED;
+        j.finish_s = srv->now();
+        return DPD_OK;
+    }
+    if (j.status != JOB_RUNNING) return srv->fail(DPD_E_STATE, "job " + std::to_string(job_id) + " has already ended");
+    for (auto& c : srv->cohorts)
+        for (size_t r = 0; r < c->jobs.size(); r++)
+            if (c->jobs[r] == job_id && !c->finished[r]) {
+                srv->fail_job(*c, (int)r, DPD_E_CANCELLED, "cancelled");
+                return DPD_OK;
+            }
+    return srv->fail(DPD_E_STATE, "job " + std::to_string(job_id) + " is not in a running batch");
 }
 
 int dpd_server_job_state(dpd_server* srv, int64_t job_id, double* x, double* v)

@@ -218,10 +218,13 @@ class Engine:
         _check(self.lib.dpd_pair_compute_aos(self.h, d_pos, d_vel, d_id, d_type, int(n), int(step), d_force,
                                              d_pe, d_virial), self.lib, self.h)
 
-    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0):
+    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0, tile=0,
+                   tile_capacity=0):
         t = capi.dpd_tuning()
         t.pair_block, t.pair_variant, t.cell_order, t.build_variant = pair_block, pair_variant, cell_order, build_variant
         t.launch_mode = launch_mode
+        t.tile = tile
+        t.tile_capacity = tile_capacity
         _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
 
 
@@ -265,10 +268,13 @@ class Batch:
     def run(self, nsteps):
         _check(self.lib.dpd_run(self.h, int(nsteps)), self.lib, self.h)
 
-    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0):
+    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0, tile=0,
+                   tile_capacity=0):
         t = capi.dpd_tuning()
         t.pair_block, t.pair_variant, t.cell_order, t.build_variant = pair_block, pair_variant, cell_order, build_variant
         t.launch_mode = launch_mode
+        t.tile = tile
+        t.tile_capacity = tile_capacity
         _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
 
     def thermo(self, rep, max_rows=4096):

@@ -71,11 +71,17 @@ class Server:
     def result(self, job_id):
         r = capi.dpd_job_result()
         self._check(self.lib.dpd_server_result(self.h, int(job_id), ctypes.byref(r)))
-        status = {0: "done", 1: "queued", 2: "running"}.get(r.status, f"error {r.status}")
-        return {"job_id": r.job_id, "status": status, "steps": r.steps, "mean_temp": r.mean_temp,
-                "mean_pressure": r.mean_pressure, "submit_s": r.submit_s, "start_s": r.start_s,
+        status = {0: "done", 1: "queued", 2: "running", -9: "cancelled"}.get(r.status, f"error {r.status}")
+        return {"job_id": r.job_id, "status": status, "code": r.status, "steps": r.steps,
+                "mean_temp": r.mean_temp, "mean_pressure": r.mean_pressure,
+                "stderr_temp": r.stderr_temp, "stderr_pressure": r.stderr_pressure,
+                "submit_s": r.submit_s, "start_s": r.start_s,
                 "finish_s": r.finish_s, "latency_s": r.finish_s - r.submit_s if r.finish_s >= 0 else None,
                 "last_temp": r.last.temp, "last_pressure": r.last.pressure, "last_step": r.last.step}
+
+    def cancel(self, job_id):
+        """Cancel a queued or running job (its status becomes "cancelled")."""
+        self._check(self.lib.dpd_server_cancel(self.h, int(job_id)))
 
     def state(self, job_id):
         n = self.n_atoms[job_id]

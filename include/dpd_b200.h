@@ -37,6 +37,7 @@ extern "C" {
 #define DPD_E_STATE -6     /* call not valid in the engine's current state          */
 #define DPD_E_NUMERIC -7   /* non-finite position/velocity, or a FENE bond broke    */
 #define DPD_E_NODEV -8     /* no CUDA device: there is no CPU fallback               */
+#define DPD_E_CANCELLED -9 /* a served job was cancelled before it finished          */
 
 typedef struct dpd_engine dpd_engine;
 
@@ -87,7 +88,11 @@ typedef struct dpd_tuning {
                               7-8 = flattened, log and non-log steps split (8 is
                               the default), 9 = as 8 with the i-side forces summed
                               per owner in the warp before the reduction,
-                              10 = one thread per list entry                     */
+                              10 = one thread per list entry, 11 = no neighbour
+                              list: a CTA per tile of cells stages the tile's
+                              neighbourhood in shared memory and evaluates its
+                              pairs straight from the cell ranges (DPD engines;
+                              mDPD runs 8)                                        */
     int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
     int build_variant;     /* list build: 0 = cell ranges in registers, 4
                               blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
@@ -103,7 +108,13 @@ typedef struct dpd_tuning {
                               1 = never; 2 = always; 3 = as 0 without the tiny-grid
                               kernels (the server's cohorts: engines that share
                               the GPU run better on fewer, fuller blocks)         */
-    int reserved[3];
+    int tile;              /* pair_variant 11: home cells per tile edge, 1..6 (0 = the
+                              engine's choice)                                    */
+    int tile_capacity;     /* pair_variant 11: particles a CTA stages (0 = 1.75 times
+                              the mean of a tile's neighbourhood, plus 64); a
+                              neighbourhood beyond it is taken a home cell at a
+                              time                                                */
+    int reserved;
 } dpd_tuning;
 
 /* ---- plain engine: replaces main()/read_info/preprocess/zero_step/simulation
@@ -289,12 +300,15 @@ int dpd_create_fp64(const char* run_in_text, const char* data_path, const char* 
                     const dpd_system* sys, dpd_engine** out);
 
 /* ---- serving: continuous batching of DPD jobs -----------------------------------
+ * No counterpart in the reference (one run.in per process, src/main/main.cu:15-72).
  * A server owns a device-memory budget.  Jobs are submitted at any time; at each
  * scheduling point (every `chunk` steps) finished jobs are retired, their memory is
  * released, and queued jobs are admitted while they fit the budget; all admitted
  * jobs advance together in one packed batch.  Each job keeps its own tags, seed and
  * step counter, so its trajectory does not depend on which other jobs share the
- * batch. */
+ * batch.  A job that fails (a non-finite state, a broken bond, a list overflow) fails
+ * alone: its replica is frozen and the other jobs of its batch run on (the reference
+ * exits the process on any such error, src/main/common.cuh:46-60). */
 typedef struct dpd_server dpd_server;
 
 typedef struct dpd_job_result {
@@ -305,6 +319,8 @@ typedef struct dpd_job_result {
     double mean_pressure;
     double submit_s, start_s, finish_s; /* host clock seconds since server creation */
     dpd_thermo last;
+    double stderr_temp;    /* standard errors of the two means: block averages over  */
+    double stderr_pressure;/* up to 10 blocks of those rows (NaN with fewer than 4)   */
 } dpd_job_result;
 
 /* `tune` (NULL: the engine defaults) applies to every cohort; its launch_mode 0 runs
@@ -326,6 +342,12 @@ int dpd_server_set_policy(dpd_server* srv, double max_wait_s, int min_jobs);
  * after the pass. */
 int dpd_server_step(dpd_server* srv, int* n_active, int* n_queued);
 int dpd_server_result(dpd_server* srv, int64_t job_id, dpd_job_result* res);
+/* Cancel a queued or running job: a queued job leaves the queue; a running job's replica
+ * is frozen at the end of the chunks already in flight and the other jobs of its batch
+ * run on; when it was the last running job of its batch, the batch's device memory
+ * returns to the budget at the next scheduling point.  The job's status becomes
+ * DPD_E_CANCELLED.  DPD_E_STATE for a job that has already finished or failed. */
+int dpd_server_cancel(dpd_server* srv, int64_t job_id);
 int dpd_server_job_state(dpd_server* srv, int64_t job_id, double* x, double* v);
 int dpd_server_job_rdf(dpd_server* srv, int64_t job_id, double* g, int64_t* nsamples);
 int dpd_server_stats(dpd_server* srv, int64_t* particle_steps, double* busy_s,
@@ -346,13 +368,18 @@ int dpd_server_destroy(dpd_server* srv);
  * library holds until exit.  Limits: n <= DPD_NOALLOC_MAX_ATOMS, at most
  * DPD_NOALLOC_MAX_CELLS cells of edge >= max rc with at least 3 per dimension,
  * ntypes <= DPD_NOALLOC_MAX_TYPES; larger inputs return DPD_E_ARG before any launch.
- * Positions must lie in [lo, hi).  The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress, with that device current); make that first
- * call before any stream capture.  All calls share the array and it keeps the last
- * call's contents (each call clears what must start at zero), so calls that overlap on
- * the GPU -- other streams, other threads -- race and must be serialized by the caller.
- * Work goes on `stream` (a cudaStream_t, NULL = legacy default stream) and the call
- * returns after the forces are written; d_force is overwritten. */
+ * Positions must lie in [lo, hi): one more than a thousandth of a cell outside, an id
+ * below 1 or a type out of range returns DPD_E_ARG (after the launches).  CUDA loads
+ * device code lazily, so the first call on a device loads the library's kernels and
+ * the array with them (the driver reserves the array's device memory at that moment)
+ * and resolves the array's device address (cudaGetSymbolAddress, with that device
+ * current; again whenever the device's CUDA context has changed).  Make that first call
+ * at start-up, as a warm-up, and before any stream capture.  All calls share the array
+ * and it keeps the last call's contents (each call clears what must start at zero), so
+ * calls that overlap on the GPU -- other streams, other threads -- race and must be
+ * serialized by the caller.  Work goes on `stream` (a cudaStream_t, NULL = legacy default
+ * stream); the call waits for that work (it reads back a status word) and returns after
+ * the forces are written; d_force is overwritten. */
 #define DPD_NOALLOC_MAX_ATOMS 262144
 #define DPD_NOALLOC_MAX_CELLS 262144
 #define DPD_NOALLOC_MAX_TYPES 8

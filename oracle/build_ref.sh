@@ -8,7 +8,9 @@
 # thrust::max_element/min_element without including <thrust/extrema.h>; the header is
 # force-included on the command line instead of editing any source.
 #
-# Usage: oracle/build_ref.sh [SINGLE|DOUBLE|SHIM]   (default SINGLE, the reference's default)
+# Usage: oracle/build_ref.sh [SINGLE|DOUBLE|SHIM] [REF_SRC]
+#   (mode default SINGLE, the reference's default; REF_SRC is the reference's src/
+#   directory, from the second argument or the environment variable REF_SRC)
 #   SHIM: the SINGLE build plus the plugins of gpumdpd_b200/shim/ (pair_style dpd/b200 and
 #   mdpd/b200, bond_style harmonic/b200, fix nve/b200, which hand the reference's device
 #   buffers to libdpd_b200), linked against the in-tree libdpd_b200.so
@@ -17,7 +19,11 @@ set -euo pipefail
 MODE="${1:-SINGLE}"
 PREC="$MODE"
 [ "$MODE" = "SHIM" ] && PREC=SINGLE
-REF_SRC="${REF_SRC:-/root/reference/src}"
+REF_SRC="${2:-${REF_SRC:-}}"
+if [ -z "$REF_SRC" ]; then
+    echo "usage: $0 [SINGLE|DOUBLE|SHIM] REF_SRC   (the reference's src/ directory)" >&2
+    exit 2
+fi
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj_${PREC}"

@@ -825,8 +825,10 @@ int oracle_rdf(int n, const int* type, const double* x, const double* lo, const 
 /* CPU baseline timing path: the reference's algorithm (half Verlet list with
  * skin, rebuilt on the reference's displacement criterion, src/force/neigh_list.cu
  * :322-393 and :483-514) over a DPD system, in FP64, split over nthreads POSIX
- * threads with thread-private force buffers.  Advances nsteps after a step-0
- * force evaluation and returns the number of list builds.                     */
+ * threads with thread-private force buffers, plus the bond forces
+ * (src/force/bond_harmonic.cu:275-351) on one thread.  Advances nsteps after a
+ * step-0 force evaluation and returns the number of list builds (-3 when a bond
+ * names a tag outside 1..n).                                                    */
 typedef struct {
     int i0, i1, n, nmax;
     const int *tag, *type, *nl, *nn;
@@ -927,7 +929,6 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
                        const int* bonds, uint32_t first_step, int nsteps, double skin,
                        int nthreads)
 {
-    (void)nbonds; (void)bonds;
     double cut = max_rc(ff) + skin;
     double cut2 = cut * cut;
     int nc[3];
@@ -948,6 +949,13 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
     pthread_t th[256];
     bench_task task[256];
     double sig_scale = sqrt(2.0 * ff->kT) / sqrt(ff->dt);
+    int* tag_to_idx = NULL;
+    if (nbonds > 0 && bonds) {
+        tag_to_idx = (int*)malloc(sizeof(int) * n);
+        for (int i = 0; i < n; i++) tag_to_idx[i] = 0;
+        for (int i = 0; i < n; i++)
+            if (tag[i] >= 1 && tag[i] <= n) tag_to_idx[tag[i] - 1] = i;
+    }
     int builds = 0;
     int need = 1;
     for (int s = -1; s < nsteps; s++) {
@@ -1022,6 +1030,10 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
             bench_reduce_range(&rt[0]);
             for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
         }
+        if (tag_to_idx) {
+            double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+            if (bond_forces(n, tag_to_idx, n, x, lo, L, ff, nbonds, bonds, f, &pe, vir) == -1) builds = -3;
+        }
         if (s >= 0) {
             for (int i = 0; i < n; i++) {
                 double dtm = 0.5 * ff->dt / ff->mass[type[i] - 1];
@@ -1030,6 +1042,7 @@ int oracle_bench_steps(int n, const int* tag, const int* type, double* x, double
         }
     }
     free(nl); free(nn); free(xlast); free(f); free(head); free(next); free(cid); free(fpriv);
+    free(tag_to_idx);
     return builds;
 }
 

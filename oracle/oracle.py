@@ -327,13 +327,18 @@ def rdf(types, x, lo, L, ta, tb, rmax, nbins):
     return g
 
 
-def bench_steps(ff, tags, types, x, v, lo, L, first_step, nsteps, skin, nthreads):
-    """The reference algorithm (half Verlet list + skin) in FP64 on nthreads host threads."""
+def bench_steps(ff, tags, types, x, v, lo, L, first_step, nsteps, skin, nthreads, bonds=None):
+    """The reference algorithm (half Verlet list + skin) in FP64 on nthreads host threads;
+    bonds (rows type, tag_i, tag_j) add their forces on one thread."""
     lib = load()
     tags = np.ascontiguousarray(tags, dtype=np.int32)
     types = np.ascontiguousarray(types, dtype=np.int32)
     x = np.array(x, dtype=np.float64, order="C")
     v = np.array(v, dtype=np.float64, order="C")
+    nb, bp = 0, None
+    if bonds is not None and len(bonds):
+        bonds = np.ascontiguousarray(bonds, dtype=np.int32)
+        nb, bp = len(bonds), _p(bonds)
     return lib.oracle_bench_steps(len(types), _p(tags), _p(types), _p(x), _p(v),
                                   _p(np.asarray(lo, dtype=np.float64)), _p(np.asarray(L, dtype=np.float64)),
-                                  ctypes.byref(ff), 0, None, first_step, nsteps, skin, nthreads)
+                                  ctypes.byref(ff), nb, bp, first_step, nsteps, skin, nthreads)

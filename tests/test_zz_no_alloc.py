@@ -5,9 +5,11 @@ its cell binning in a fixed static device array instead of engine buffers.
 
 Each test calls it through the C ABI on two calls in a row (different positions and
 step, so the second call sees the first call's leftovers in the shared array) and
-compares with dpd_pair_compute_aos, the engine-backed entry point, within the force
-tolerance the other force tests use: max |dF| / F_rms < 1e-5.  The file is named to run
-last, after every other GPU test has used the device."""
+compares with dpd_pair_compute_aos, the engine-backed entry point, and with the FP64
+oracle on the same inputs, within the force tolerance the other force tests use:
+max |dF| / F_rms < 1e-5.  The device's free memory is the same before and after the
+second call.  The file is named to run last, after every other GPU test has used the
+device."""
 import ctypes
 
 import numpy as np
@@ -55,7 +57,7 @@ def _cases():
 
 
 @pytest.mark.parametrize("name", ["one_type_L8", "two_types_L10"])
-def test_noalloc_matches_engine_entry_point(name):
+def test_noalloc_matches_engine_entry_point(name, oracle_mod):
     import torch
     from gpumdpd_b200 import Engine, capi
     s = _cases()[name]
@@ -83,13 +85,20 @@ def test_noalloc_matches_engine_entry_point(name):
                            f_ref.data_ptr())
         f_na = torch.full((3 * s.n,), float("nan"), device=dev)
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         code = lib.dpd_pair_forces_noalloc(ctypes.byref(params), xd.data_ptr(), vd.data_ptr(), ids.data_ptr(),
                                            types.data_ptr(), s.n, step, f_na.data_ptr(), stream)
         assert code == 0
+        if call == 1:  # after the first call has loaded the module: no device memory taken
+            assert torch.cuda.mem_get_info()[0] == free0
         a = f_na.cpu().numpy().reshape(-1, 3).astype(np.float64)
         b = f_ref.cpu().numpy().reshape(-1, 3).astype(np.float64)
         assert np.isfinite(a).all()
         assert force_err(a, b) < TOL, (name, call)
+        ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+        o = oracle_mod.forces(ff, np.arange(1, s.n + 1), s.types, x.astype(np.float64), v.astype(np.float64),
+                              s.lo, L.astype(np.float64), step)
+        assert force_err(a, o["f"]) < TOL, (name, call)
         np.testing.assert_allclose(a.sum(axis=0), 0.0, atol=1e-3 * np.sqrt(np.mean(b * b)) * np.sqrt(s.n))
     e.close()
 
@@ -126,6 +135,10 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
     bad = ids.clone()
     bad[7] = 0                                           # ids start at 1
     assert lib.dpd_pair_forces_noalloc(ctypes.byref(p), xd.data_ptr(), vd.data_ptr(), bad.data_ptr(),
+                                       types.data_ptr(), s.n, 0, fd.data_ptr(), None) == -1
+    far = xd.clone()
+    far[3 * 11 + 1] = 9.5                                # a cell and a half beyond hi = 8
+    assert lib.dpd_pair_forces_noalloc(ctypes.byref(p), far.data_ptr(), vd.data_ptr(), ids.data_ptr(),
                                        types.data_ptr(), s.n, 0, fd.data_ptr(), None) == -1
     # a valid call still works after the rejected ones
     assert call(p, s.n) == 0
