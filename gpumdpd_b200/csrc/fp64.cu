@@ -6,9 +6,10 @@
 // summation order is fixed), the mDPD density pass (src/force/pair_mdpd.cu:253-297), the
 // force pass, the final half kick (src/fix/fix_nve.cu:131-149) and on logged steps a
 // fixed-order reduction of the thermo sums (src/compute/thermo.cu:240-246,301-303,422-434,
-// 506-517).  The force pass gives one warp per atom all its pairs from both sides (a lane
-// per cell of the 27), its bonds and its angles, summed by a fixed butterfly, so no
-// atomics touch the forces and runs repeat bit for bit.
+// 506-517).  The force pass gives one warp per atom all its pairs from both sides (the
+// 27 cells' candidates filtered 32 at a time, the pairs inside the cutoff evaluated 32 at
+// a time), its bonds and its angles, summed by a fixed butterfly, so no atomics touch the
+// forces and runs repeat bit for bit.
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -160,57 +161,142 @@ __global__ void __launch_bounds__(256) k64_density(F64Args a)
     if (lane == 0) a.rho[i] = rho;
 }
 
-// Forces on atom i, one warp per atom: lane c takes the DPD / mDPD pairs of the c-th of
-// the 27 cells (src/force/pair_dpd.cu:292-403, pair_mdpd.cu:399-521), the lanes share out
-// the atom's bonds (src/force/bond_harmonic.cu:208-268; FENE + WCA as the FP32 engine)
-// and harmonic angles (src/force/angle_harmonic.cu:187-270), and a fixed butterfly sums
-// the lanes.  On logged steps the atom's share of the energies and of the virial: half of
-// each pair and bond, a third of each angle, as the reference splits them.
+// Forces on atom i, one warp per atom.  The records of the 27 cells around the atom
+// (src/force/pair_dpd.cu:292-403, pair_mdpd.cu:399-521) are taken 32 at a time as one
+// sequence, cell by cell in a fixed order and each cell's records in index order: each
+// lane tests one candidate, the pairs inside the largest cutoff are queued in the warp's
+// shared ring in ballot order, and whenever 32 are queued every lane evaluates one (the
+// Saru random force, the FP64 force) into its own partial sums -- a fixed assignment of
+// pairs to lanes, so the sums repeat bit for bit.  The lanes also share out the atom's
+// bonds (src/force/bond_harmonic.cu:208-268; FENE + WCA as the FP32 engine) and harmonic
+// angles (src/force/angle_harmonic.cu:187-270), and a fixed butterfly sums the lanes.  On
+// logged steps the atom's share of the energies and of the virial: half of each pair and
+// bond, a third of each angle, as the reference splits them.
+#define F64_Q 64  // per-warp ring of queued pairs (power of two, >= 63)
+
+template <bool LOG>
+__device__ __forceinline__ void f64_pairs(const F64Args& a, int i, int ti, double rho_i, uint32_t step,
+                                          const double4* qd, const int* qj, uint32_t head, int cnt, int lane,
+                                          double& fx, double& fy, double& fz, double& pe, double (&vir)[6])
+{
+    if (lane >= cnt) return;
+    const uint32_t e = (head + lane) & (F64_Q - 1);
+    const double4 d = qd[e];
+    const int j = qj[e];
+    const double dx = d.x, dy = d.y, dz = d.z, r2 = d.w;
+    const double* c = a.coeff + NC * tri(ti, a.type[j], a.ntypes);
+    if (!(r2 <= c[8])) return;
+    const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4], sigma = c[5];
+    // 1/r by rsqrt and r/rc as r * (1/rc): within an ulp of the divisions
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv;
+    if (r < 1.0e-10) return;
+    const double dot = dx * (a.v[3 * i] - a.v[3 * j]) + dy * (a.v[3 * i + 1] - a.v[3 * j + 1]) +
+                       dz * (a.v[3 * i + 2] - a.v[3 * j + 2]);
+    const double wc = 1.0 - r * c[6];
+    const uint32_t t1 = (uint32_t)min(i, j) + 1u, t2 = (uint32_t)max(i, j) + 1u;
+    const double theta = saru_theta_f64(t1, t2, a.seed, step);
+    double fpair, e2;
+    if (a.style == 0) {
+        fpair = A * wc - gamma * wc * wc * dot * rinv + sigma * wc * theta;
+        e2 = 0.5 * A * rc * wc * wc;
+    } else {
+        double wd = 1.0 - r * c[7];
+        if (wd < 0.0) wd = 0.0;
+        const double rs = rho_i + a.rho[j];
+        fpair = A * wc + B * rs * wd - gamma * wc * wc * dot * rinv + sigma * wc * theta;
+        e2 = 0.5 * A * rc * wc * wc + 0.25 * B * rd * rs * wd * wd;
+    }
+    fpair *= rinv;
+    const double gx = dx * fpair, gy = dy * fpair, gz = dz * fpair;
+    fx += gx;
+    fy += gy;
+    fz += gz;
+    if (LOG) {
+        pe += 0.5 * e2;
+        vir[0] += 0.5 * dx * gx; vir[1] += 0.5 * dx * gy; vir[2] += 0.5 * dx * gz;
+        vir[3] += 0.5 * dy * gy; vir[4] += 0.5 * dy * gz; vir[5] += 0.5 * dz * gz;
+    }
+}
+
 template <bool LOG>
 __global__ void __launch_bounds__(256) k64_force(F64Args a, uint32_t step)
 {
+    __shared__ double4 s_qd[8][F64_Q];
+    __shared__ int s_qj[8][F64_Q];
+    const int warp = threadIdx.x >> 5;
     const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (i >= a.n) return;  // warp-uniform
     const int ti = a.type[i];
-    const double vxi = a.v[3 * i], vyi = a.v[3 * i + 1], vzi = a.v[3 * i + 2];
     double fx = 0.0, fy = 0.0, fz = 0.0, pe = 0.0, bpe = 0.0, ape = 0.0;
     double vir[6] = {0, 0, 0, 0, 0, 0};
     const double rho_i = a.style == 1 ? a.rho[i] : 0.0;
-    if (lane < 27)
-        for_cell(a, i, lane, [&](int j, double dx, double dy, double dz, double r2) {
-            const double* c = a.coeff + NC * tri(ti, a.type[j], a.ntypes);
-            const double A = c[0], B = c[1], gamma = c[2], rc = c[3], rd = c[4], sigma = c[5];
-            if (!(r2 <= c[8])) return;
-            // 1/r by rsqrt and r/rc as r * (1/rc): within an ulp of the divisions
-            const double rinv = rsqrt(r2);
-            const double r = r2 * rinv;
-            if (r < 1.0e-10) return;
-            const double dot = dx * (vxi - a.v[3 * j]) + dy * (vyi - a.v[3 * j + 1]) + dz * (vzi - a.v[3 * j + 2]);
-            const double wc = 1.0 - r * c[6];
-            const uint32_t t1 = (uint32_t)min(i, j) + 1u, t2 = (uint32_t)max(i, j) + 1u;
-            const double theta = saru_theta_f64(t1, t2, a.seed, step);
-            double fpair, e;
-            if (a.style == 0) {
-                fpair = A * wc - gamma * wc * wc * dot * rinv + sigma * wc * theta;
-                e = 0.5 * A * rc * wc * wc;
-            } else {
-                double wd = 1.0 - r * c[7];
-                if (wd < 0.0) wd = 0.0;
-                const double rs = rho_i + a.rho[j];
-                fpair = A * wc + B * rs * wd - gamma * wc * wc * dot * rinv + sigma * wc * theta;
-                e = 0.5 * A * rc * wc * wc + 0.25 * B * rd * rs * wd * wd;
-            }
-            fpair *= rinv;
-            const double gx = dx * fpair, gy = dy * fpair, gz = dz * fpair;
-            fx += gx;
-            fy += gy;
-            fz += gz;
-            if (LOG) {
-                pe += 0.5 * e;
-                vir[0] += 0.5 * dx * gx; vir[1] += 0.5 * dx * gy; vir[2] += 0.5 * dx * gz;
-                vir[3] += 0.5 * dy * gy; vir[4] += 0.5 * dy * gz; vir[5] += 0.5 * dz * gz;
-            }
-        });
+    const double xi = a.x[3 * i], yi = a.x[3 * i + 1], zi = a.x[3 * i + 2];
+    // lane c < 27: the c-th cell around the atom (c = 9 (ox+1) + 3 (oy+1) + (oz+1); nc >= 3
+    // per dimension, so no cell is visited twice) and its record count
+    int cell = 0, m = 0;
+    if (lane < 27) {
+        const int code = a.ccode[i];
+        int cx = (code & 1023) + lane / 9 - 1, cy = ((code >> 10) & 1023) + (lane / 3) % 3 - 1,
+            cz = (code >> 20) + lane % 3 - 1;
+        cx += cx < 0 ? a.nc[0] : 0; cx -= cx >= a.nc[0] ? a.nc[0] : 0;
+        cy += cy < 0 ? a.nc[1] : 0; cy -= cy >= a.nc[1] ? a.nc[1] : 0;
+        cz += cz < 0 ? a.nc[2] : 0; cz -= cz >= a.nc[2] ? a.nc[2] : 0;
+        cell = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+        m = min(a.cnt[cell], a.cap);
+    }
+    int incl = m;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int excl = incl - m;
+    const int M = __shfl_sync(0xffffffffu, incl, 31);
+    const unsigned lt = (1u << lane) - 1u;
+    uint32_t head = 0, tail = 0;
+    for (int cb = 0; cb < M; cb += 32) {
+        const int t = cb + lane;
+        // the candidate's cell: the last of the 27 whose first record is at or before t
+        // (an empty cell shares its start with the next one, which then wins)
+        int c = 0;
+#pragma unroll
+        for (int stp = 16; stp >= 1; stp >>= 1) {
+            const int probe = min(c + stp, 26);
+            const int pstart = __shfl_sync(0xffffffffu, excl, probe);
+            if (c + stp <= 26 && pstart <= t) c += stp;
+        }
+        const int cc = __shfl_sync(0xffffffffu, cell, c);
+        const int c0 = __shfl_sync(0xffffffffu, excl, c);
+        bool hit = false;
+        double dx = 0.0, dy = 0.0, dz = 0.0, r2 = 0.0;
+        int j = 0;
+        if (t < M) {
+            const double4 rj = a.crec[(size_t)cc * a.cap + (t - c0)];
+            j = (int)rj.w;
+            dx = min_image(xi - rj.x, a.L[0]);
+            dy = min_image(yi - rj.y, a.L[1]);
+            dz = min_image(zi - rj.z, a.L[2]);
+            r2 = dx * dx + dy * dy + dz * dz;
+            hit = j != i && r2 <= a.maxrc2;
+        }
+        const unsigned bm = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const uint32_t e = (tail + __popc(bm & lt)) & (F64_Q - 1);
+            s_qd[warp][e] = make_double4(dx, dy, dz, r2);
+            s_qj[warp][e] = j;
+        }
+        tail += __popc(bm);
+        __syncwarp();
+        if (tail - head >= 32u) {
+            f64_pairs<LOG>(a, i, ti, rho_i, step, s_qd[warp], s_qj[warp], head, 32, lane, fx, fy, fz, pe, vir);
+            head += 32;
+            __syncwarp();
+        }
+    }
+    if (tail != head)
+        f64_pairs<LOG>(a, i, ti, rho_i, step, s_qd[warp], s_qj[warp], head, (int)(tail - head), lane, fx, fy, fz,
+                       pe, vir);
     for (int b = a.bstart[i] + lane; b < a.bstart[i + 1]; b += 32) {
         const int2 e2 = a.bent[b];
         const int j = e2.x;
