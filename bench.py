@@ -121,6 +121,17 @@ def compare(a, b, nblocks=10):
             "stderr": round(se, 6), "z": round((ma - mb) / se, 2) if se > 0 else None}
 
 
+def compact(x, sig=4):
+    """Floats of a nested summary rounded to `sig` significant digits (the printed line)."""
+    if isinstance(x, float):
+        return float(f"{x:.{sig}g}") if math.isfinite(x) else None
+    if isinstance(x, dict):
+        return {k: compact(v, sig) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [compact(v, sig) for v in x]
+    return x
+
+
 def with_thermo(run_in, every):
     import re
     return re.sub(r"(?m)^thermo \d+$", f"thermo {int(every)}", run_in)
@@ -337,7 +348,8 @@ def run_ours(args, world, rank, local):
     # end to end through the C ABI with host buffers: the state (x, v in FP64) goes host
     # -> device, K steps run (a zero-step force evaluation and list build first), the
     # final x, v come back device -> host with the thermo rows
-    chunk = args.steps
+    # (chunks of at least 1000 steps: a production call runs many steps per upload)
+    chunk = max(args.steps, 1000)
     st = eng.state(forces=False, images=False)
     x = np.ascontiguousarray(st["x"])
     v = np.ascontiguousarray(st["v"])
@@ -363,9 +375,8 @@ def run_ours(args, world, rank, local):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     # state (two parity buffers of position, velocity, image and bond partners) + half list
     foot = n * (2 * (48 + 8 * maxb) + 4 * 48 + 16)
-    l2 = (f"inputs larger than L2 (state+list ~{foot / 1e9:.2f} GB)" if foot > 126e6 else
-          f"inputs smaller than L2 (state+list ~{foot / 1e6:.1f} MB): L2-resident, no flush; "
-          "a latency-bound small system, not the headline workload")
+    l2 = (f"inputs > L2 ({foot / 1e9:.2f} GB)" if foot > 126e6 else
+          f"inputs < L2 ({foot / 1e6:.1f} MB), no flush: small latency-bound system")
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
@@ -386,17 +397,17 @@ def run_ours(args, world, rank, local):
                    "mean_half_list": round(ls["mean_half_list"], 3),
                    "list_builds_per_step": builds_per_step, "pair_variant": pair_variant,
                    "tile": args.tile if pair_variant == 11 else None,
-                   "tuned": tuned if isinstance(tuned, str) else "bench --tune",
+                   "tuned": "defaults (tune.py)" if isinstance(tuned, str) else "bench --tune",
                    "parallelism": f"replicas{world}", "l2": l2},
         "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "chunk_steps": chunk, "path": "dpd_set_state + dpd_run + dpd_get_state (C ABI, host buffers)"},
+                "chunk_steps": chunk, "path": "dpd_set_state+dpd_run+dpd_get_state"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": pair_kernel_name(system, pair_variant),
                      "bytes_per_particle": bpp, "pair_ms_per_launch": per_launch_ms,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      # the kernel is issue-bound, not HBM-bound: the Saru chain's integer
                      # operations per pair inside rc set the compute-side ceiling
-                     "binding": "instruction issue (Saru integer chain + gathers), not HBM",
+                     "binding": "issue (Saru integer chain), not HBM",
                      "pairs_per_step": pairs_per_step,
                      "saru_int_ops_per_pair": 130},
         "clocks": clk.summary(),
@@ -409,9 +420,14 @@ def run_ours(args, world, rank, local):
     }
     if world == 1 and not args.no_extras:
         # T and P of the headline system: the FP32 engine against the FP64 parity engine
-        # from the same (timed-run) state over the same window
-        out["accuracy"] = fp32_fp64_window(system, st2["x"], st2["v"], args.acc_steps, 5,
-                                           tuning={"pair_variant": pair_variant, "cell_order": 1})
+        # from the same state over the same window, after the melt's bonds have relaxed
+        # (2000 more steps of the FP32 engine)
+        eng.run(args.acc_equil)
+        st3 = eng.state(forces=False, images=False)
+        out["accuracy"] = compact(fp32_fp64_window(system, st3["x"], st3["v"], args.acc_steps, 5,
+                                                   tuning={"pair_variant": pair_variant, "cell_order": 1}))
+        out["accuracy"]["from_step"] = args.warmup + args.steps + chunk + args.acc_equil
+        del st3
     eng.close()
     del st, st2
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -422,7 +438,7 @@ def run_ours(args, world, rank, local):
         for name, fn in (("slab", run_slab), ("batched", run_batched), ("served", run_served),
                          ("fp64", run_fp64)):
             summary, det = fn(args)
-            out[name] = summary
+            out[name] = compact(summary)
             detail[name] = det
     if rank == 0:
         if detail and args.detail:
@@ -460,14 +476,12 @@ def run_slab(args):
     acc = fp32_fp64_window(s, st["x"], st["v"], args.slab_acc_steps, 10,
                            extra={"surface_tension": lambda t: 0.5 * lz * (t["p"][:, 5] - 0.5 * (t["p"][:, 0] + t["p"][:, 3]))})
     value = s.n * args.slab_steps / (total_ms / 1000.0)
-    summary = {"workload": f"mdpd_slab_40x40x120_N{s.n}_skin{args.batch_skin}", "particles": s.n,
-               "steps": args.slab_steps, "value": value, "unit": "particle-steps/s",
-               "ms_per_step": total_ms / args.slab_steps, "liquid_density": round(liq, 4),
-               "vapour_density": round(vap, 4), "surface_tension": round(g, 4),
-               "surface_tension_stderr": round(gerr, 4),
-               "mean_temp_second_half": round(float(np.mean(th["temp"][half:])), 5),
-               "err_vs_fp64": acc}
-    return summary, {"density_profile_z0.5": [round(float(x), 4) for x in rho]}
+    window = acc.pop("window")
+    summary = {"workload": f"mdpd_slab_N{s.n}", "value": value, "ms_per_step": total_ms / args.slab_steps,
+               "liquid_density": liq, "vapour_density": vap, "surface_tension": g,
+               "surface_tension_stderr": gerr, "err_vs_fp64": acc}
+    return summary, {"steps": args.slab_steps, "density_profile_z0.5": [round(float(x), 4) for x in rho],
+                     "mean_temp_second_half": float(np.mean(th["temp"][half:])), "fp64_window": window}
 
 
 def plain_step_ms(system, steps):
@@ -554,19 +568,16 @@ def run_batched(args):
     def worst(f, key):
         r = max(acc, key=lambda a: abs(a[f][key]["z"] or 0.0))
         c = r[f][key]
-        return {"replica": r["replica"], "err": c["err"], "stderr": c["stderr"], "z": c["z"],
-                "rel_err": round(c["err"] / c["fp64"], 6) if c["fp64"] else None}
+        return {"rep": r["replica"], "err": c["err"], "stderr": c["stderr"], "z": c["z"],
+                "rel": c["err"] / c["fp64"] if c["fp64"] else None}
 
-    summary = {"workload": f"{R}_replica_AB_sweep_L8-24_skin{args.batch_skin}", "replicas": R,
-               "particles": n_tot, "value": batched, "unit": "particle-steps/s", "steps": K,
+    summary = {"workload": f"{R}_replica_AB_sweep_N{n_tot}", "value": batched,
                "plain_one_at_a_time": plain, "speedup_vs_plain": batched / plain,
-               "plain_steps_per_replica": args.plain_steps,
-               "err_vs_fp64": {"replicas_checked": len(sel), "steps": K, "thermo_every": 10,
-                               "worst_temp": worst("temp", "batched_vs_fp64"),
-                               "worst_pressure": worst("pressure", "batched_vs_fp64")},
-               "batched_vs_plain": {"worst_temp": worst("temp", "batched_vs_plain"),
-                                    "worst_pressure": worst("pressure", "batched_vs_plain")}}
-    return summary, {"per_replica": per_rep, "accuracy": acc}
+               "err_vs_fp64": {"replicas": len(sel), "T": worst("temp", "batched_vs_fp64"),
+                               "P": worst("pressure", "batched_vs_fp64")},
+               "vs_plain": {"T": worst("temp", "batched_vs_plain"), "P": worst("pressure", "batched_vs_plain")}}
+    return summary, {"steps": K, "thermo_every": 10, "plain_steps_per_replica": args.plain_steps,
+                     "per_replica": per_rep, "accuracy": acc}
 
 
 def served_run(jobs, args, rate_label):
@@ -639,19 +650,15 @@ def run_served(args):
         r = max(acc, key=lambda a: abs(a[f]["z"] or 0.0))
         c = r[f]
         return {"job": r["job"], "err": c["err"], "stderr": c["stderr"], "z": c["z"],
-                "rel_err": round(c["err"] / c["fp64"], 6) if c["fp64"] else None}
+                "rel": c["err"] / c["fp64"] if c["fp64"] else None}
 
-    summary = {"workload": f"{len(ids)}_job_poisson_stream", "jobs": len(ids), "value": head["value"],
-               "unit": "particle-steps/s", "rate_jobs_per_s": head["rate_jobs_per_s"],
-               "p50_latency_s": head["p50_latency_s"], "p99_latency_s": head["p99_latency_s"],
+    summary = {"workload": f"{len(ids)}_job_poisson_stream", "value": head["value"],
                "plain_one_at_a_time": plain, "speedup_vs_plain": head["value"] / plain,
-               "rates": [{k: x[k] for k in ("rate_jobs_per_s", "value", "p50_latency_s", "p99_latency_s")}
-                         for x in sweep],
-               "hbm_budget_bytes": 120e9, "chunk_steps": args.chunk,
-               "admission_window": {"max_wait_s": args.max_wait, "min_jobs": args.min_jobs},
-               "err_vs_fp64": {"jobs_checked": len(acc), "worst_temp": worst("temp"),
-                               "worst_pressure": worst("pressure")}}
-    return summary, {"rate_sweep": sweep, "accuracy": acc}
+               "rates": [[x["rate_jobs_per_s"], x["value"], x["p50_latency_s"], x["p99_latency_s"]] for x in sweep],
+               "rates_cols": "jobs/s, particle-steps/s, p50 s, p99 s",
+               "err_vs_fp64": {"jobs": len(acc), "T": worst("temp"), "P": worst("pressure")}}
+    return summary, {"rate_sweep": sweep, "accuracy": acc, "hbm_budget_bytes": 120e9, "chunk_steps": args.chunk,
+                     "admission_window": {"max_wait_s": args.max_wait, "min_jobs": args.min_jobs}}
 
 
 def time_reference_binary(binary, system, W, K, every):
@@ -683,26 +690,32 @@ def time_reference_binary(binary, system, W, K, every):
 
 
 def run_fp64(args):
-    """The FP64 parity mode on C1 (plain DPD, 3000 particles): the FP64 engine's device time
-    per step (CUDA events) against the reference's -DDOUBLE build on the same input (host
-    clock between its thermo lines, as the reference arm)."""
+    """The FP64 parity mode against the reference's -DDOUBLE build on the same inputs: C1
+    (plain DPD, 3000 particles, 2000 timed steps) and the 3M A5B5 melt (20 timed steps after
+    10): the FP64 engine's device time per step (CUDA events) and the reference's host clock
+    between its thermo lines (as the reference arm)."""
     from gpumdpd_b200 import Engine, inputs
-    s = inputs.plain_dpd(L=10.0, seed=2024, nsteps=10 ** 6, thermo=1000, skin=0.0)
-    e = Engine(s.run_in, system=s.c_system(), precision="fp64")
-    e.run(0)
-    e.run(50)
-    K = 2000
-    ms = e.time_steps(K)["total_ms"] / K
-    out = {"workload": f"plain_L10_N{s.n}_fp64", "particles": s.n, "ms_per_step": ms,
-           "value": s.n / (ms / 1000.0), "unit": "particle-steps/s", "dtype": "f64"}
     binary = os.path.join(ROOT, "oracle", "_ref", "gpudpd_double")
-    if os.path.exists(binary):
-        dt, why = time_reference_binary(binary, s, 1000, K, 1000)
-        if dt is not None:
-            out["reference_double_ms_per_step"] = dt * 1000 / K
-            out["speedup_vs_reference_double"] = out["reference_double_ms_per_step"] / ms
-        else:
-            out["reference_double"] = f"failed {why}"
+    out = {"dtype": "f64"}
+    cases = [("c1", inputs.plain_dpd(L=10.0, seed=2024, nsteps=10 ** 6, thermo=1000, skin=0.0), 50, 2000, 1000)]
+    if not args.no_fp64_melt:
+        cases.append(("melt_3M", inputs.diblock_melt(L=100.0, seed=7, nsteps=10 ** 6, thermo=10, skin=0.0),
+                      10, 20, 10))
+    for name, s, W, K, every in cases:
+        e = Engine(s.run_in, system=s.c_system(), precision="fp64")
+        e.run(0)
+        e.run(W)
+        ms = e.time_steps(K)["total_ms"] / K
+        e.close()
+        rec = {"particles": s.n, "ms_per_step": ms, "value": s.n / (ms / 1000.0)}
+        if os.path.exists(binary):
+            dt, why = time_reference_binary(binary, s, max(W, every), K, every)
+            if dt is not None:
+                rec["reference_double_ms_per_step"] = dt * 1000 / K
+                rec["speedup_vs_reference_double"] = rec["reference_double_ms_per_step"] / ms
+            else:
+                rec["reference_double"] = f"failed {why}"[:120]
+        out[name] = rec
     return out, {}
 
 
@@ -765,6 +778,9 @@ def main():
     ap.add_argument("--detail", default="bench_detail.json",
                     help="file for the per-replica records, density profile and rate sweep ('' = none)")
     ap.add_argument("--acc-steps", type=int, default=300, help="FP32-vs-FP64 window of the headline system")
+    ap.add_argument("--acc-equil", type=int, default=2000,
+                    help="FP32 steps before the headline system's FP32-vs-FP64 window")
+    ap.add_argument("--no-fp64-melt", action="store_true", help="skip the 3M melt in the fp64 object")
     ap.add_argument("--slab-steps", type=int, default=20000)
     ap.add_argument("--slab-acc-steps", type=int, default=1000)
     ap.add_argument("--replicas", type=int, default=256)

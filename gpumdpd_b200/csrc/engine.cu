@@ -226,7 +226,7 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
     }
     int st = layout();
     if (st) return st;
-    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, stream_priority_));
     st = alloc_and_upload();
     if (st) return st;
     host_target_.assign(reps_.size(), 0);

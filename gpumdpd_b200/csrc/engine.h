@@ -136,6 +136,9 @@ public:
     int64_t steps_done(int r) const;
     int64_t n_builds();
     int64_t device_bytes() const { return dev_bytes_; }
+    // priority of the engine's stream (CUDA stream priority: lower is served first); set
+    // before init().  A server gives its longest jobs the highest priority.
+    void set_stream_priority(int p) { stream_priority_ = p; }
     int64_t total_atoms() const;
     std::string err;
 
@@ -210,6 +213,7 @@ private:
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
     int ntiles_ = 0, tile_edge_ = 0, tile_smax_ = 0;
+    int stream_priority_ = 0;
     std::vector<std::unique_ptr<DumpWriter>> dumps_;
 };
 

@@ -208,35 +208,71 @@ long oracle_pairs_f64(int n, const int* tag, const double* x, const double* lo, 
  * r2 <= cut2 (float).  Same predicate as the engine's list builder; it restates
  * the reference's r2 <= (global_cut+skin)^2 test (src/force/neigh_list.cu:373-382)
  * on the cell-offset representation.  Returns unordered tag pairs.            */
+static int pair_f32(int i, int j, const int* cell, const float* off, const int* nc, const float* w,
+                    float cut2)
+{
+    float d[3];
+    for (int k = 0; k < 3; k++) {
+        int dc = cell[3 * i + k] - cell[3 * j + k];
+        if (dc > nc[k] / 2) dc -= nc[k];
+        if (dc < -(nc[k] / 2)) dc += nc[k];
+        if (dc > 1 || dc < -1) return 0;
+        volatile float diff = off[3 * i + k] - off[3 * j + k];
+        d[k] = fmaf((float)dc, w[k], diff);
+    }
+    volatile float r2 = d[0] * d[0];
+    r2 = fmaf(d[1], d[1], r2);
+    r2 = fmaf(d[2], d[2], r2);
+    return r2 <= cut2;
+}
+
+static long emit_pair(const int* tag, int i, int j, int* out, long cap, long cnt)
+{
+    if (cnt < cap) {
+        int a = tag[i], b = tag[j];
+        out[2 * cnt] = a < b ? a : b;
+        out[2 * cnt + 1] = a < b ? b : a;
+    }
+    return cnt + 1;
+}
+
+/* With at least 3 cells per dimension the candidates of i are the particles of the 27
+ * cells around its own (each visited once), taken once per pair (j > i); any pair whose
+ * wrapped cell difference exceeds 1 fails the predicate anyway, so the set is the one
+ * of the all-pairs loop used for smaller grids. */
 long oracle_pairs_f32(int n, const int* tag, const int* cell /*3n*/, const float* off /*3n*/,
                       const int* nc, const float* w, float cut2, int* out, long cap)
 {
     long cnt = 0;
+    if (nc[0] < 3 || nc[1] < 3 || nc[2] < 3) {
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++)
+                if (pair_f32(i, j, cell, off, nc, w, cut2)) cnt = emit_pair(tag, i, j, out, cap, cnt);
+        return cnt;
+    }
+    long ncell = (long)nc[0] * nc[1] * nc[2];
+    int* head = (int*)malloc(sizeof(int) * ncell);
+    int* next = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (long c = 0; c < ncell; c++) head[c] = -1;
+    for (int i = n - 1; i >= 0; i--) {
+        long c = ((long)cell[3 * i] * nc[1] + cell[3 * i + 1]) * nc[2] + cell[3 * i + 2];
+        next[i] = head[c];
+        head[c] = i;
+    }
     for (int i = 0; i < n; i++)
-        for (int j = i + 1; j < n; j++) {
-            float d[3];
-            int near = 1;
-            for (int k = 0; k < 3; k++) {
-                int dc = cell[3 * i + k] - cell[3 * j + k];
-                if (dc > nc[k] / 2) dc -= nc[k];
-                if (dc < -(nc[k] / 2)) dc += nc[k];
-                if (dc > 1 || dc < -1) { near = 0; break; }
-                volatile float diff = off[3 * i + k] - off[3 * j + k];
-                d[k] = fmaf((float)dc, w[k], diff);
-            }
-            if (!near) continue;
-            volatile float r2 = d[0] * d[0];
-            r2 = fmaf(d[1], d[1], r2);
-            r2 = fmaf(d[2], d[2], r2);
-            if (r2 <= cut2) {
-                if (cnt < cap) {
-                    int a = tag[i], b = tag[j];
-                    out[2 * cnt] = a < b ? a : b;
-                    out[2 * cnt + 1] = a < b ? b : a;
+        for (int ox = -1; ox <= 1; ox++)
+            for (int oy = -1; oy <= 1; oy++)
+                for (int oz = -1; oz <= 1; oz++) {
+                    int cx = (cell[3 * i] + ox + nc[0]) % nc[0];
+                    int cy = (cell[3 * i + 1] + oy + nc[1]) % nc[1];
+                    int cz = (cell[3 * i + 2] + oz + nc[2]) % nc[2];
+                    long c = ((long)cx * nc[1] + cy) * nc[2] + cz;
+                    for (int j = head[c]; j >= 0; j = next[j])
+                        if (j > i && pair_f32(i, j, cell, off, nc, w, cut2))
+                            cnt = emit_pair(tag, i, j, out, cap, cnt);
                 }
-                cnt++;
-            }
-        }
+    free(head);
+    free(next);
     return cnt;
 }
 
