@@ -831,8 +831,8 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     if (any_mdpd_) pdl_launch(k_density, gp, 256, s, sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
     if (tile) {
-        const TileArgs ta{b_.tile_rep, b_.tile_code, ntiles_, tile_edge_, tile_smax_};
-        const size_t sm = tile_smem_bytes(tile_smax_);
+        const TileArgs ta{b_.tile_rep, b_.tile_code, ntiles_, tile_edge_, tile_smax_, tile_hc_};
+        const size_t sm = tile_smem_bytes(tile_smax_, tile_hc_);
         const int glog = std::min(ntiles_, 148 * 2);
         if (bonds_) {
             pdl_launch_smem(k_tile<true, 4>, ntiles_, 256, sm, s, sa, ta);
@@ -905,8 +905,9 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
 
 // The tile table of pair schedule 11: the tiles of every replica (edge^3 home cells,
 // fewer at a grid's edge), each replica's tiles in Morton order of their coordinates
-// (the order of the slots), and the staging capacity of a CTA: 1.75 times the mean
-// particle count of a tile's neighbourhood (plus 64) in the densest replica.  Edge 0
+// (the order of the slots), the staging capacity of a CTA: 1.5 times the mean particle
+// count of a tile's neighbourhood (plus 64) in the densest replica, and the pairs a
+// particle may have (from the list capacity's max_rho, 16..64).  Edge 0
 // (the default) takes the largest edge up to 4 that still gives at least 8 tiles per
 // SM, else 1.
 int Engine::prepare_tiles()
@@ -932,7 +933,7 @@ int Engine::prepare_tiles()
     }
     E = std::min(E, TILE_MAX_EDGE);
     std::vector<int> trep, tcode;
-    int smax = 128;
+    int smax = 128, hc = 0;
     for (int r = 0; r < (int)reps_.size(); r++) {
         const RepDesc& d = reps_[r].desc;
         const int nt[3] = {(d.nc[0] + E - 1) / E, (d.nc[1] + E - 1) / E, (d.nc[2] + E - 1) / E};
@@ -947,13 +948,18 @@ int Engine::prepare_tiles()
         }
         const double mean_cell = (double)d.n_real / std::max(d.ncell, 1);
         const int region = (std::min(E, d.nc[0]) + 2) * (std::min(E, d.nc[1]) + 2) * (std::min(E, d.nc[2]) + 1);
-        smax = std::max(smax, (int)std::ceil(1.75 * mean_cell * region) + 64);
+        smax = std::max(smax, (int)std::ceil(1.5 * mean_cell * region) + 64);
+        // pairs a particle may have inside the largest cutoff: 1.5 times half the
+        // neighbours of the list capacity's density (`neighbor ... max_rho`)
+        const double rcm = std::sqrt((double)d.rcmax2);
+        hc = std::max(hc, (int)std::ceil(0.75 * reps_[r].in.max_rho * 4.0 / 3.0 * M_PI * rcm * rcm * rcm));
     }
+    hc = std::min(64, std::max(16, (hc + 7) / 8 * 8));
     if (tune_.tile_capacity > 0) smax = tune_.tile_capacity;
     smax = (smax + 31) / 32 * 32;
     // at most 200 KB of shared memory a CTA (a neighbourhood beyond it takes its home
     // cells one at a time)
-    while (smax > 32 && tile_smem_bytes(smax) > 200 * 1024) smax -= 32;
+    while (smax > 32 && tile_smem_bytes(smax, hc) > 200 * 1024) smax -= 32;
     if ((int64_t)trep.size() > C_) {
         err = "tile table larger than the cell count";
         return DPD_E_STATE;
@@ -961,10 +967,11 @@ int Engine::prepare_tiles()
     ntiles_ = (int)trep.size();
     tile_edge_ = E;
     tile_smax_ = smax;
+    tile_hc_ = hc;
     CK(cudaMemcpyAsync(b_.tile_rep, trep.data(), sizeof(int) * trep.size(), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.tile_code, tcode.data(), sizeof(int) * tcode.size(), cudaMemcpyHostToDevice, stream_));
     CK(cudaStreamSynchronize(stream_));
-    const int bytes = (int)tile_smem_bytes(smax);
+    const int bytes = (int)tile_smem_bytes(smax, hc);
     CK(cudaFuncSetAttribute(k_tile<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile_logsteps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));

@@ -212,7 +212,7 @@ private:
     bool aos_built_ = false;
     int64_t dev_bytes_ = 0;
     std::vector<uint32_t> host_target_;
-    int ntiles_ = 0, tile_edge_ = 0, tile_smax_ = 0;
+    int ntiles_ = 0, tile_edge_ = 0, tile_smax_ = 0, tile_hc_ = 32;
     int stream_priority_ = 0;
     std::vector<std::unique_ptr<DumpWriter>> dumps_;
 };

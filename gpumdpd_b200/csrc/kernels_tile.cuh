@@ -10,28 +10,30 @@
 //   R1: cells (x-1..x+1, y+1, z)                       (the row dz = 0, dy = +1)
 //   R2..R4: cells (x-1..x+1, y-1..y+1, z+1)             (the three rows dz = +1)
 // -- the half stencil of src/force/neigh_list.cu:322-393 (every unordered cell pair
-// once; at least 3 cells per dimension).  Its warps take home cells one at a time
-// (a shared counter hands them out): the lanes take the home cell's candidates j, 32 at
-// a time, and each lane tests its j against every particle i of the home cell in turn
-// (i broadcast from shared memory), with the list predicate of the list build:
+// once; at least 3 cells per dimension).  The warps take the home particles 32 at a time
+// (a shared counter hands them out); each lane walks its particle's five ranges as one
+// sequence with the list predicate of the list build,
 //   d = (o_i - o_j) + (c_i - c_j) w,  r2 = fma(dz,dz, fma(dy,dy, dx*dx)) <= rc_max^2,
-// so the pairs evaluated are exactly the list path's.  Pairs inside the cutoff go to a
-// per-warp ring queue; whenever 32 are pending, the lanes evaluate them together (Saru
-// random force, src/force/pair_dpd.cu:468-558), each with the float4 reductions of both
-// sides into the force array.  The home particles' bonds follow (bond_loop).  Log steps
-// add the FP64 energy and virial sums, flushed per warp.
+// so the pairs evaluated are exactly the list path's, and keeps its hits in its own
+// column of a shared buffer.  The warp then takes its 32 lanes' hits as one sequence,
+// 32 pairs at a time (the owner lane of each found by a binary search over the scanned
+// counts), and evaluates them with every lane busy (Saru random force,
+// src/force/pair_dpd.cu:468-558), each with the float4 reductions of both sides into the
+// force array.  The home particles' bonds follow (bond_loop).  Log steps add the FP64
+// energy and virial sums, flushed per warp.
 //
 // When a tile's neighbourhood holds more particles than the staging capacity (a local
 // density far above the mean), the CTA takes its home cells one at a time with the
-// smaller neighbourhood of one cell; only if that does not fit either is the replica's
-// ST_LIST_OVERFLOW raised (the pairs of that cell are then missing, and the run fails
-// with DPD_E_OVERFLOW).
+// smaller neighbourhood of one cell; only if that does not fit either, or a particle has
+// more pairs than the hit buffer holds (the list capacity of `neighbor ... max_rho`), is
+// the replica's ST_LIST_OVERFLOW raised (pairs are then missing, and the run fails with
+// DPD_E_OVERFLOW).
 #pragma once
 #include "kernels_step.cuh"
 
 #define TILE_MAX_EDGE 6
 #define TILE_MAX_REGION ((TILE_MAX_EDGE + 2) * (TILE_MAX_EDGE + 2) * (TILE_MAX_EDGE + 1))
-#define TILE_Q 64  // per-warp ring queue of pairs (power of two, >= 63)
+#define TILE_THREADS 256
 
 struct TileArgs {
     const int* tile_rep;   // [ntiles] replica of each tile
@@ -39,25 +41,27 @@ struct TileArgs {
     int ntiles;
     int edge;              // home cells per tile edge
     int smax;              // staging capacity (particles) of a CTA
+    int hc;                // pairs a home particle may have (hit buffer column)
 };
 
 // dynamic shared memory of a CTA: staged positions, velocities, slots; region cell
-// starts (+1) and global starts; per-warp pair queues
-__host__ __device__ inline size_t tile_smem_bytes(int smax)
+// starts (+1) and global starts; home rows; the hit buffer
+__host__ __device__ inline size_t tile_smem_bytes(int smax, int hc)
 {
-    return (size_t)smax * (16 + 16 + 4) + (size_t)(2 * TILE_MAX_REGION + 32) * 4 +
-           (size_t)8 * TILE_Q * (16 + 4);
+    return (size_t)smax * (16 + 16 + 4) + (size_t)(2 * TILE_MAX_REGION + 32) * 4 + 128 * 4 +
+           (size_t)hc * TILE_THREADS * 2;
 }
 
 struct TileSmem {
-    float4* pos;   // [smax] {o.x, o.y, o.z, region cell code rx | ry << 8 | rz << 16}
-    float4* vel;   // [smax] as in the particle arrays (tag and type in .w)
-    int* slot;     // [smax] particle slot
-    int* rstart;   // [TILE_MAX_REGION + 16] first staged index of each region cell, the
-                   // total after the last one; [TILE_MAX_REGION + 8 + w]: warp totals
-    int* gstart;   // [TILE_MAX_REGION] first slot of each region cell
-    float4* qd;    // [8][TILE_Q] {dx, dy, dz, r2} of a queued pair
-    uint32_t* qij; // [8][TILE_Q] i | j << 16 (staged indices)
+    float4* pos;    // [smax] {o.x, o.y, o.z, region cell code rx | ry << 8 | rz << 16}
+    float4* vel;    // [smax] as in the particle arrays (tag and type in .w)
+    int* slot;      // [smax] particle slot
+    int* rstart;    // [TILE_MAX_REGION + 16] first staged index of each region cell, the
+                    // total after the last one; [TILE_MAX_REGION + 8 + w]: warp totals
+    int* gstart;    // [TILE_MAX_REGION] first slot of each region cell
+    int* rowpre;    // [64] home particles before each home row (y, z), the total after
+    int* rowbeg;    // [64] first staged index of each home row
+    uint16_t* hits; // [hc][TILE_THREADS] staged index j of each pair found, a column a thread
 };
 
 __device__ __forceinline__ TileSmem tile_smem(unsigned char* base, int smax)
@@ -68,30 +72,78 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* base, int smax)
     t.slot = (int*)(t.vel + smax);
     t.rstart = t.slot + smax;
     t.gstart = t.rstart + TILE_MAX_REGION + 16;
-    t.qd = (float4*)(t.gstart + TILE_MAX_REGION + 16);
-    t.qij = (uint32_t*)(t.qd + 8 * TILE_Q);
+    t.rowpre = t.gstart + TILE_MAX_REGION + 16;
+    t.rowbeg = t.rowpre + 64;
+    t.hits = (uint16_t*)(t.rowbeg + 64);
     return t;
 }
 
-// Evaluate `cnt` (<= 32) queued pairs from the warp's ring position `head`.
+// One staged pair (i, j): the displacement again from the offsets and the region cells
+// (bit for bit the walk's), then the DPD force into both sides.
 template <bool LOG>
-__device__ __forceinline__ void tile_eval(const StepArgs& a, const RepDesc& d, const TileSmem& sm, int warp,
-                                          int lane, uint32_t head, int cnt, uint32_t step, double (&accv)[8])
+__device__ __forceinline__ void tile_pair(const StepArgs& a, const RepDesc& d, const TileSmem& sm, int i, int j,
+                                          uint32_t step, double (&accv)[8])
 {
-    if (lane < cnt) {
-        const uint32_t e = (head + lane) & (TILE_Q - 1);
-        const float4 dd = sm.qd[warp * TILE_Q + e];
-        const uint32_t ij = sm.qij[warp * TILE_Q + e];
-        const int i = ij & 0xffff, j = ij >> 16;
-        const float4 vi = sm.vel[i], vj = sm.vel[j];
-        const float4* crow = a.coeff + d.coeff_off + type0_of(vi.w) * d.ntypes * 3;
-        float fx, fy, fz;
-        if (pair_force<0, LOG>(crow, dd.w, dd.x, dd.y, dd.z, vi, vj, 0.0f, 0.0f, d.seed, step, fx, fy, fz, accv)) {
-            atomicAdd(&a.force4[sm.slot[i]], make_float4(fx, fy, fz, 0.0f));
-            atomicAdd(&a.force4[sm.slot[j]], make_float4(-fx, -fy, -fz, 0.0f));
-        }
+    const float4 pi = sm.pos[i], pj = sm.pos[j];
+    const int ci = __float_as_int(pi.w), cj = __float_as_int(pj.w);
+    const float sx = __int2float_rn((ci & 0xff) - (cj & 0xff)) * d.w[0];
+    const float sy = __int2float_rn(((ci >> 8) & 0xff) - ((cj >> 8) & 0xff)) * d.w[1];
+    const float sz = __int2float_rn((ci >> 16) - (cj >> 16)) * d.w[2];
+    const float dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sx);
+    const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
+    const float dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sz);
+    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    const float4 vi = sm.vel[i], vj = sm.vel[j];
+    const float4* crow = a.coeff + d.coeff_off + type0_of(vi.w) * d.ntypes * 3;
+    float fx, fy, fz;
+    if (pair_force<0, LOG>(crow, r2, dx, dy, dz, vi, vj, 0.0f, 0.0f, d.seed, step, fx, fy, fz, accv)) {
+        atomicAdd(&a.force4[sm.slot[i]], make_float4(fx, fy, fz, 0.0f));
+        atomicAdd(&a.force4[sm.slot[j]], make_float4(-fx, -fy, -fz, 0.0f));
     }
-    __syncwarp();
+}
+
+// The pairs of staged home particle i inside rc_max: its five candidate ranges walked as
+// one sequence; the staged index of each hit goes to the thread's column of the hit
+// buffer (the first hc of them).  Returns the number of hits.
+__device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int RY, float wx, float wy, float wz,
+                                         float rcmax2, uint16_t* col, int hc)
+{
+    const float4 pi = sm.pos[i];
+    const int code = __float_as_int(pi.w);
+    const int rx = code & 0xff, ry = (code >> 8) & 0xff, rz = code >> 16;
+    int cnt = 0, k = 0;
+    // range 0: the rest of the own cell (sx = 0), then cell x+1 (sx = -w); b1 = 0: no
+    // cell x-1 part
+    const int cr = (rz * RY + ry) * RX + rx + 1;
+    int j = i + 1, b1 = 0, b2 = sm.rstart[cr], end = sm.rstart[cr + 1];
+    float sy = 0.0f, sz = 0.0f;
+    for (;;) {
+        if (j >= end) {
+            if (++k == 5) break;
+            // ranges 1..4: the rows (x-1..x+1) at (y+1, z), (y-1, z+1), (y, z+1), (y+1, z+1)
+            const int yy = k == 1 ? ry + 1 : ry + k - 3, zz = k == 1 ? rz : rz + 1;
+            const int c0 = (zz * RY + yy) * RX + rx - 1;
+            j = sm.rstart[c0];
+            b1 = sm.rstart[c0 + 1];
+            b2 = sm.rstart[c0 + 2];
+            end = sm.rstart[c0 + 3];
+            sy = __int2float_rn(ry - yy) * wy;
+            sz = __int2float_rn(rz - zz) * wz;
+            continue;
+        }
+        const float4 pj = sm.pos[j];
+        const float sx = j < b1 ? wx : (j < b2 ? 0.0f : -wx);
+        const float dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sx);
+        const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
+        const float dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sz);
+        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        if (r2 <= rcmax2) {
+            if (cnt < hc) col[cnt * TILE_THREADS] = (uint16_t)j;
+            cnt++;
+        }
+        j++;
+    }
+    return cnt;
 }
 
 // Stage the neighbourhood of the home box [hx0, hx0+ex) x [hy0, hy0+ey) x [hz0, hz0+ez)
@@ -168,87 +220,88 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
         }
     }
     __syncthreads();
-    // 3. home cells, handed out one at a time to the warps
+    // 3. home rows (the home cells of one (y, z), contiguous in staged order) and the
+    //    count of home particles before each
+    auto rc_idx = [&](int x, int y, int z) { return (z * RY + y) * RX + x; };
+    const int NROW = ey * ez;  // <= 36
+    if (warp == 0) {
+        int sz0 = 0, sz1 = 0, bg0 = 0, bg1 = 0;
+        if (lane < NROW) {
+            bg0 = sm.rstart[rc_idx(1, lane % ey + 1, lane / ey)];
+            sz0 = sm.rstart[rc_idx(ex, lane % ey + 1, lane / ey) + 1] - bg0;
+        }
+        if (lane + 32 < NROW) {
+            const int r2w = lane + 32;
+            bg1 = sm.rstart[rc_idx(1, r2w % ey + 1, r2w / ey)];
+            sz1 = sm.rstart[rc_idx(ex, r2w % ey + 1, r2w / ey) + 1] - bg1;
+        }
+        int i0 = sz0, i1 = sz1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t0 = __shfl_up_sync(0xffffffffu, i0, o), t1 = __shfl_up_sync(0xffffffffu, i1, o);
+            if (lane >= o) {
+                i0 += t0;
+                i1 += t1;
+            }
+        }
+        const int tot0 = __shfl_sync(0xffffffffu, i0, 31), tot1 = __shfl_sync(0xffffffffu, i1, 31);
+        if (lane < NROW) {
+            sm.rowpre[lane] = i0 - sz0;
+            sm.rowbeg[lane] = bg0;
+        }
+        if (lane + 32 < NROW) {
+            sm.rowpre[lane + 32] = tot0 + i1 - sz1;
+            sm.rowbeg[lane + 32] = bg1;
+        }
+        if (lane == 0) sm.rowpre[NROW] = tot0 + tot1;
+    }
+    __syncthreads();
+    // 4. home particles, handed out 32 at a time to the warps: each lane walks its
+    //    particle's candidates, then the warp evaluates the pairs its lanes found
     const float wx = d.w[0], wy = d.w[1], wz = d.w[2];
     const float rcmax2 = d.rcmax2;
-    const int nhome = ex * ey * ez;
-    const unsigned lt = (1u << lane) - 1u;
-    uint32_t head = 0, tail = 0;
-    auto rc_idx = [&](int x, int y, int z) { return (z * RY + y) * RX + x; };
+    const int H = sm.rowpre[NROW];
+    const int hc = ta.hc;
+    uint16_t* col = sm.hits + tid;
     for (;;) {
-        int h = 0;
-        if (lane == 0) h = atomicAdd(&s_next, 1);
-        h = __shfl_sync(0xffffffffu, h, 0);
-        if (h >= nhome) break;
-        const int hx = h % ex, hy = (h / ex) % ey, hz = h / (ex * ey);
-        const int ch = rc_idx(hx + 1, hy + 1, hz);
-        const int ia = sm.rstart[ch], ib = sm.rstart[ch + 1];
-        if (ia == ib) continue;
-        // lanes 0..4 hold the five candidate ranges {start, length}
-        int rs = 0, rl = 0;
-        if (lane < 5) {
-            int c0, c1;
-            if (lane == 0) {
-                c0 = 0;  // unused: R0 starts at the home cell's first particle
-                c1 = rc_idx(hx + 2, hy + 1, hz);
-            } else if (lane == 1) {
-                c0 = rc_idx(hx, hy + 2, hz);
-                c1 = rc_idx(hx + 2, hy + 2, hz);
-            } else {
-                c0 = rc_idx(hx, hy + lane - 2, hz + 1);
-                c1 = rc_idx(hx + 2, hy + lane - 2, hz + 1);
-            }
-            rs = lane == 0 ? ia : sm.rstart[c0];
-            rl = sm.rstart[c1 + 1] - rs;
-        }
-        int rp = rl;  // inclusive prefix of the lengths over lanes 0..4
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&s_next, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= H) break;
+        const int t = base + lane;
+        int cnt = 0, i = 0;
+        if (t < H) {
+            int rr = 0;  // the last row whose first home particle is at or before t
 #pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, rp, o);
-            if (lane >= o) rp += t;
+            for (int stp = 32; stp >= 1; stp >>= 1)
+                if (rr + stp < NROW && sm.rowpre[rr + stp] <= t) rr += stp;
+            i = sm.rowbeg[rr] + (t - sm.rowpre[rr]);
+            cnt = tile_walk(sm, i, RX, RY, wx, wy, wz, rcmax2, col, hc);
         }
-        const int M = __shfl_sync(0xffffffffu, rp, 4);
-        const int p1 = __shfl_sync(0xffffffffu, rp, 0), p2 = __shfl_sync(0xffffffffu, rp, 1),
-                  p3 = __shfl_sync(0xffffffffu, rp, 2), p4 = __shfl_sync(0xffffffffu, rp, 3);
-        for (int cb = 0; cb < M; cb += 32) {
-            const int t = cb + lane;
-            const bool valid = t < M;
-            const int k = (t >= p1) + (t >= p2) + (t >= p3) + (t >= p4);
-            const int kstart = __shfl_sync(0xffffffffu, rs, k);
-            const int kpre = __shfl_sync(0xffffffffu, rp - rl, k);  // exclusive prefix
-            const int j = valid ? kstart + (t - kpre) : 0;
-            const float4 pj = sm.pos[j];
-            const int code = __float_as_int(pj.w);
-            // (c_i - c_j) w: exact multiples of w (differences in {-1, 0, 1})
-            const float sx = __int2float_rn(hx + 1 - (code & 0xff)) * wx;
-            const float sy = __int2float_rn(hy + 1 - ((code >> 8) & 0xff)) * wy;
-            const float sz = __int2float_rn(hz - (code >> 16)) * wz;
-            for (int i = ia; i < ib; i++) {
-                const float4 pi = sm.pos[i];
-                const float dx = __fadd_rn(__fsub_rn(pi.x, pj.x), sx);
-                const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
-                const float dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sz);
-                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-                const bool hit = valid && j > i && r2 <= rcmax2;
-                const unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (m) {
-                    if (hit) {
-                        const uint32_t e = (tail + __popc(m & lt)) & (TILE_Q - 1);
-                        sm.qd[warp * TILE_Q + e] = make_float4(dx, dy, dz, r2);
-                        sm.qij[warp * TILE_Q + e] = (uint32_t)i | ((uint32_t)j << 16);
-                    }
-                    tail += __popc(m);
-                    __syncwarp();
-                    if (tail - head >= 32u) {
-                        tile_eval<LOG>(a, d, sm, warp, lane, head, 32, step, accv);
-                        head += 32;
-                    }
-                }
-            }
+        if (__any_sync(0xffffffffu, cnt > hc) && lane == 0) atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+        const int c = min(cnt, hc);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
+        const int excl = incl - c;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();  // the lanes' hits are written
+        for (int b = 0; b < total; b += 32) {
+            const int f = b + lane;
+            int o = 0;  // owner lane: the last lane whose first hit is at or before f
+#pragma unroll
+            for (int stp = 16; stp >= 1; stp >>= 1)
+                if (__shfl_sync(0xffffffffu, excl, o + stp) <= f) o += stp;
+            const int io = __shfl_sync(0xffffffffu, i, o);
+            const int q = f - __shfl_sync(0xffffffffu, excl, o);
+            if (f < total) tile_pair<LOG>(a, d, sm, io, sm.hits[q * TILE_THREADS + warp * 32 + o], step, accv);
+        }
+        __syncwarp();  // the hits are read before the next walk writes the columns again
     }
-    if (tail != head) tile_eval<LOG>(a, d, sm, warp, lane, head, (int)(tail - head), step, accv);
-    // 4. bonds of the home particles (each takes its own side of its bonds)
+    // 5. bonds of the home particles (each takes its own side of its bonds)
     if (BONDS && d.bond_style) {
         const int par = *a.parity;
         const float4* pos = a.buf.pos[par];

@@ -110,7 +110,7 @@ typedef struct dpd_tuning {
                               the GPU run better on fewer, fuller blocks)         */
     int tile;              /* pair_variant 11: home cells per tile edge, 1..6 (0 = the
                               engine's choice)                                    */
-    int tile_capacity;     /* pair_variant 11: particles a CTA stages (0 = 1.75 times
+    int tile_capacity;     /* pair_variant 11: particles a CTA stages (0 = 1.5 times
                               the mean of a tile's neighbourhood, plus 64); a
                               neighbourhood beyond it is taken a home cell at a
                               time                                                */
