@@ -834,11 +834,15 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
         const TileArgs ta{b_.tile_rep, b_.tile_code, ntiles_, tile_edge_, tile_smax_, tile_hc_};
         const size_t sm = tile_smem_bytes(tile_smax_, tile_hc_);
         const int glog = std::min(ntiles_, 148 * 2);
+        // pair_block 3: the kernel compiled for 3 CTAs per SM (more registers), else 4
+        const bool b3 = tune_.pair_block == 3;
         if (bonds_) {
-            pdl_launch_smem(k_tile<true, 4>, ntiles_, 256, sm, s, sa, ta);
+            if (b3) pdl_launch_smem(k_tile<true, 3>, ntiles_, 256, sm, s, sa, ta);
+            else pdl_launch_smem(k_tile<true, 4>, ntiles_, 256, sm, s, sa, ta);
             pdl_launch_smem(k_tile_logsteps<true>, glog, 256, sm, s, sa, ta);
         } else {
-            pdl_launch_smem(k_tile<false, 4>, ntiles_, 256, sm, s, sa, ta);
+            if (b3) pdl_launch_smem(k_tile<false, 3>, ntiles_, 256, sm, s, sa, ta);
+            else pdl_launch_smem(k_tile<false, 4>, ntiles_, 256, sm, s, sa, ta);
             pdl_launch_smem(k_tile_logsteps<false>, glog, 256, sm, s, sa, ta);
         }
     } else if (fused) {
@@ -907,7 +911,7 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
 // fewer at a grid's edge), each replica's tiles in Morton order of their coordinates
 // (the order of the slots), the staging capacity of a CTA: 1.5 times the mean particle
 // count of a tile's neighbourhood (plus 64) in the densest replica, and the pairs a
-// particle may have (from the list capacity's max_rho, 16..64).  Edge 0
+// particle may have (the list capacity max_rho implies at the largest cutoff, 16..96).  Edge 0
 // (the default) takes the largest edge up to 4 that still gives at least 8 tiles per
 // SM, else 1.
 int Engine::prepare_tiles()
@@ -949,12 +953,12 @@ int Engine::prepare_tiles()
         const double mean_cell = (double)d.n_real / std::max(d.ncell, 1);
         const int region = (std::min(E, d.nc[0]) + 2) * (std::min(E, d.nc[1]) + 2) * (std::min(E, d.nc[2]) + 1);
         smax = std::max(smax, (int)std::ceil(1.5 * mean_cell * region) + 64);
-        // pairs a particle may have inside the largest cutoff: 1.5 times half the
-        // neighbours of the list capacity's density (`neighbor ... max_rho`)
+        // pairs a particle may have inside the largest cutoff: the reference's list
+        // capacity rule (src/force/neigh_list.cu:14-17) at that cutoff
         const double rcm = std::sqrt((double)d.rcmax2);
-        hc = std::max(hc, (int)std::ceil(0.75 * reps_[r].in.max_rho * 4.0 / 3.0 * M_PI * rcm * rcm * rcm));
+        hc = std::max(hc, ((int)(reps_[r].in.max_rho * 4.0 / 3.0 * M_PI * rcm * rcm * rcm) + 1 + 15) / 16 * 16);
     }
-    hc = std::min(64, std::max(16, (hc + 7) / 8 * 8));
+    hc = std::min(96, std::max(16, hc));
     if (tune_.tile_capacity > 0) smax = tune_.tile_capacity;
     smax = (smax + 31) / 32 * 32;
     // at most 200 KB of shared memory a CTA (a neighbourhood beyond it takes its home
@@ -974,6 +978,8 @@ int Engine::prepare_tiles()
     const int bytes = (int)tile_smem_bytes(smax, hc);
     CK(cudaFuncSetAttribute(k_tile<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile_logsteps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile_logsteps<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return DPD_OK;

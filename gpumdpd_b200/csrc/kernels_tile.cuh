@@ -2,7 +2,7 @@
 // with no neighbour list: the list build and the list-driven pair pass as one kernel.
 //
 // A CTA takes a tile of home cells (T x T x T, fewer at the grid's edge) of one replica
-// and stages the particles of the cells its half stencil reaches -- x in [x0-1, x0+T],
+// and stages the positions of the particles of the cells its half stencil reaches -- x in [x0-1, x0+T],
 // y in [y0-1, y0+T], z in [z0, z0+T] -- into shared memory, cell by cell with x fastest,
 // so that the 13 forward cells of a home cell plus the rest of its own cell form five
 // contiguous ranges of staged particles:
@@ -44,17 +44,16 @@ struct TileArgs {
     int hc;                // pairs a home particle may have (hit buffer column)
 };
 
-// dynamic shared memory of a CTA: staged positions, velocities, slots; region cell
-// starts (+1) and global starts; home rows; the hit buffer
+// dynamic shared memory of a CTA: staged positions and slots; region cell starts (+1)
+// and global starts; home rows; the hit buffer
 __host__ __device__ inline size_t tile_smem_bytes(int smax, int hc)
 {
-    return (size_t)smax * (16 + 16 + 4) + (size_t)(2 * TILE_MAX_REGION + 32) * 4 + 128 * 4 +
+    return (size_t)smax * (16 + 4) + (size_t)(2 * TILE_MAX_REGION + 32) * 4 + 128 * 4 +
            (size_t)hc * TILE_THREADS * 2;
 }
 
 struct TileSmem {
     float4* pos;    // [smax] {o.x, o.y, o.z, region cell code rx | ry << 8 | rz << 16}
-    float4* vel;    // [smax] as in the particle arrays (tag and type in .w)
     int* slot;      // [smax] particle slot
     int* rstart;    // [TILE_MAX_REGION + 16] first staged index of each region cell, the
                     // total after the last one; [TILE_MAX_REGION + 8 + w]: warp totals
@@ -68,8 +67,7 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* base, int smax)
 {
     TileSmem t;
     t.pos = (float4*)base;
-    t.vel = t.pos + smax;
-    t.slot = (int*)(t.vel + smax);
+    t.slot = (int*)(t.pos + smax);
     t.rstart = t.slot + smax;
     t.gstart = t.rstart + TILE_MAX_REGION + 16;
     t.rowpre = t.gstart + TILE_MAX_REGION + 16;
@@ -79,11 +77,13 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* base, int smax)
 }
 
 // One staged pair (i, j): the displacement again from the offsets and the region cells
-// (bit for bit the walk's), then the DPD force into both sides.
+// (bit for bit the walk's), the velocities (tag and type in .w) through L1, then the DPD
+// force into both sides.
 template <bool LOG>
-__device__ __forceinline__ void tile_pair(const StepArgs& a, const RepDesc& d, const TileSmem& sm, int i, int j,
-                                          uint32_t step, double (&accv)[8])
+__device__ __forceinline__ void tile_pair(const StepArgs& a, const RepDesc& d, const TileSmem& sm,
+                                          const float4* vel, int i, int j, uint32_t step, double (&accv)[8])
 {
+    const int si = sm.slot[i], sj = sm.slot[j];
     const float4 pi = sm.pos[i], pj = sm.pos[j];
     const int ci = __float_as_int(pi.w), cj = __float_as_int(pj.w);
     const float sx = __int2float_rn((ci & 0xff) - (cj & 0xff)) * d.w[0];
@@ -93,12 +93,12 @@ __device__ __forceinline__ void tile_pair(const StepArgs& a, const RepDesc& d, c
     const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
     const float dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sz);
     const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-    const float4 vi = sm.vel[i], vj = sm.vel[j];
+    const float4 vi = __ldg(vel + si), vj = __ldg(vel + sj);
     const float4* crow = a.coeff + d.coeff_off + type0_of(vi.w) * d.ntypes * 3;
     float fx, fy, fz;
     if (pair_force<0, LOG>(crow, r2, dx, dy, dz, vi, vj, 0.0f, 0.0f, d.seed, step, fx, fy, fz, accv)) {
-        atomicAdd(&a.force4[sm.slot[i]], make_float4(fx, fy, fz, 0.0f));
-        atomicAdd(&a.force4[sm.slot[j]], make_float4(-fx, -fy, -fz, 0.0f));
+        atomicAdd(&a.force4[si], make_float4(fx, fy, fz, 0.0f));
+        atomicAdd(&a.force4[sj], make_float4(-fx, -fy, -fz, 0.0f));
     }
 }
 
@@ -205,7 +205,6 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
     {
         const int par = *a.parity;
         const float4* pos = a.buf.pos[par];
-        const float4* vel = a.buf.vel[par];
         for (int c = tid; c < NR; c += blockDim.x) {
             const int lx = c % RX, ly = (c / RX) % RY, lz = c / (RX * RY);
             const float code = __int_as_float(lx | (ly << 8) | (lz << 16));
@@ -214,7 +213,6 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
                 const int s = g0 + (k - k0);
                 const float4 p = pos[s];
                 sm.pos[k] = make_float4(p.x, p.y, p.z, code);
-                sm.vel[k] = vel[s];
                 sm.slot[k] = s;
             }
         }
@@ -263,6 +261,7 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
     const int H = sm.rowpre[NROW];
     const int hc = ta.hc;
     uint16_t* col = sm.hits + tid;
+    const float4* vel = a.buf.vel[*a.parity];
     for (;;) {
         int base = 0;
         if (lane == 0) base = atomicAdd(&s_next, 32);
@@ -297,7 +296,7 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
                 if (__shfl_sync(0xffffffffu, excl, o + stp) <= f) o += stp;
             const int io = __shfl_sync(0xffffffffu, i, o);
             const int q = f - __shfl_sync(0xffffffffu, excl, o);
-            if (f < total) tile_pair<LOG>(a, d, sm, io, sm.hits[q * TILE_THREADS + warp * 32 + o], step, accv);
+            if (f < total) tile_pair<LOG>(a, d, sm, vel, io, sm.hits[q * TILE_THREADS + warp * 32 + o], step, accv);
         }
         __syncwarp();  // the hits are read before the next walk writes the columns again
     }

@@ -81,7 +81,8 @@ typedef struct dpd_thermo {
 /* Launch/tuning knobs chosen by the autotuner (gpumdpd_b200/tune.py); zero fields
  * mean "engine default". */
 typedef struct dpd_tuning {
-    int pair_block;        /* threads per block of the pair kernel               */
+    int pair_block;        /* pair_variant 11: 3 = the tile kernel compiled for 3
+                              CTAs per SM (more registers), else 4                */
     int pair_variant;      /* 0 = thread per particle, 1-3 = warp pair-queue,
                               4-5 = flattened warp schedule (small skins),
                               6 = flattened with the list build fused (DPD),
