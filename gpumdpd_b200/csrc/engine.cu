@@ -802,7 +802,11 @@ void Engine::enqueue_build(cudaStream_t s, bool list, bool wide)
         pdl_launch(k_flip, (nrep + 255) / 256, 256, s, ba, nrep);
     }
     if (list) {
-        if (wide && gp <= 148 * 8) pdl_launch(k_build_wide, (14 * P_ + 255) / 256, 256, s, ba);
+        if (tile_build()) {
+            const StepArgs sa = step_args(b_, P_, nmax_, maxb_, nrep);
+            const TileArgs ta{b_.tile_rep, b_.tile_code, ntiles_, tile_edge_, tile_smax_, 0};
+            pdl_launch_smem(k_tile_build<5>, ntiles_, 256, tile_smem_bytes(tile_smax_, 0), s, sa, ta, ba);
+        } else if (wide && gp <= 148 * 8) pdl_launch(k_build_wide, (14 * P_ + 255) / 256, 256, s, ba);
         else if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
         else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);
         else pdl_launch(k_build_nlist, gp, 256, s, ba);
@@ -917,7 +921,7 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
 int Engine::prepare_tiles()
 {
     ntiles_ = 0;
-    if (!use_tile()) return DPD_OK;
+    if (!use_tile() && !tile_build()) return DPD_OK;
     auto count = [&](int E) {
         int64_t n = 0;
         for (auto& R : reps_) {
@@ -980,6 +984,8 @@ int Engine::prepare_tiles()
     CK(cudaFuncSetAttribute(k_tile<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile<true, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile<false, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_tile_build<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tile_smem_bytes(smax, 0)));
     CK(cudaFuncSetAttribute(k_tile_logsteps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     CK(cudaFuncSetAttribute(k_tile_logsteps<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return DPD_OK;
@@ -1657,10 +1663,10 @@ int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
     if (t->pair_variant < 0 || t->pair_variant > 11 || t->cell_order < 0 || t->cell_order > 1 ||
-        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 3 || t->launch_mode < 0 ||
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 4 || t->launch_mode < 0 ||
         t->launch_mode > 3 || t->tile < 0 || t->tile > TILE_MAX_EDGE || t->tile_capacity < 0 ||
         t->tile_capacity > 4096) {
-        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..3, cell_order 0 or 1, "
+        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..4, cell_order 0 or 1, "
               "launch_mode 0..3, tile edge 0..6, tile capacity 0..4096";
         return DPD_E_ARG;
     }

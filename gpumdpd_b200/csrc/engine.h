@@ -169,6 +169,8 @@ private:
     // capacity for the current tuning; refresh_list() builds the neighbour list of the
     // current state on demand (that schedule builds none in its steps)
     bool use_tile() const { return tune_.pair_variant == 11 && !any_mdpd_; }
+    // list-build variant 4: the list built from the same tiles (DPD engines)
+    bool tile_build() const { return tune_.build_variant == 4 && !any_mdpd_ && !use_tile(); }
     int prepare_tiles();
     int refresh_list();
     int dump_frame(DumpWriter* w, uint32_t step);

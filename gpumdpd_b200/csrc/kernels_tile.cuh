@@ -102,11 +102,12 @@ __device__ __forceinline__ void tile_pair(const StepArgs& a, const RepDesc& d, c
     }
 }
 
-// The pairs of staged home particle i inside rc_max: its five candidate ranges walked as
-// one sequence; the staged index of each hit goes to the thread's column of the hit
-// buffer (the first hc of them).  Returns the number of hits.
+// The candidates of staged home particle i: its five ranges walked as one sequence with
+// the list predicate r2 <= cut2; hit(count, j, code) is called for each pair found, code =
+// 9 (dcx+1) + 3 (dcy+1) + (dcz+1) of the cell difference c_i - c_j.  Returns the count.
+template <class Hit>
 __device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int RY, float wx, float wy, float wz,
-                                         float rcmax2, uint16_t* col, int hc)
+                                         float cut2, Hit&& hit)
 {
     const float4 pi = sm.pos[i];
     const int code = __float_as_int(pi.w);
@@ -117,6 +118,7 @@ __device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int 
     const int cr = (rz * RY + ry) * RX + rx + 1;
     int j = i + 1, b1 = 0, b2 = sm.rstart[cr], end = sm.rstart[cr + 1];
     float sy = 0.0f, sz = 0.0f;
+    int cyz = 4;  // 3 (dcy+1) + (dcz+1) of the current range
     for (;;) {
         if (j >= end) {
             if (++k == 5) break;
@@ -129,6 +131,7 @@ __device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int 
             end = sm.rstart[c0 + 3];
             sy = __int2float_rn(ry - yy) * wy;
             sz = __int2float_rn(rz - zz) * wz;
+            cyz = 3 * (ry - yy + 1) + (rz - zz + 1);
             continue;
         }
         const float4 pj = sm.pos[j];
@@ -137,8 +140,8 @@ __device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int 
         const float dy = __fadd_rn(__fsub_rn(pi.y, pj.y), sy);
         const float dz = __fadd_rn(__fsub_rn(pi.z, pj.z), sz);
         const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-        if (r2 <= rcmax2) {
-            if (cnt < hc) col[cnt * TILE_THREADS] = (uint16_t)j;
+        if (r2 <= cut2) {
+            hit(cnt, j, (j < b1 ? 18 : (j < b2 ? 9 : 0)) + cyz);
             cnt++;
         }
         j++;
@@ -150,9 +153,13 @@ __device__ __forceinline__ int tile_walk(const TileSmem& sm, int i, int RX, int 
 // (global cell coordinates) of replica r and evaluate its pairs and its home particles'
 // bonds.  Returns false (having done nothing) when the neighbourhood does not fit the
 // staging capacity.  Called by the whole CTA; begins and ends with a barrier.
-template <bool LOG, bool BONDS>
-__device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& sm, const RepDesc& d, int r,
-                         int hx0, int hy0, int hz0, int ex, int ey, int ez, uint32_t step, double (&accv)[8])
+// LIST: instead of the forces, the half list of the list schedules: each home particle's
+// pairs within (global_cut + skin) as entries j | code << 27 of its warp-interleaved list
+// (the list build's entries, src/force/neigh_list.cu:322-393).
+template <bool LOG, bool BONDS, bool LIST = false>
+__device__ __forceinline__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& sm, const RepDesc& d, int r,
+                         int hx0, int hy0, int hz0, int ex, int ey, int ez, uint32_t step, double (&accv)[8],
+                         int* nlist = nullptr, int* ncount = nullptr)
 {
     __shared__ int s_total, s_next;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -259,6 +266,27 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
     const float wx = d.w[0], wy = d.w[1], wz = d.w[2];
     const float rcmax2 = d.rcmax2;
     const int H = sm.rowpre[NROW];
+    if (LIST) {
+        for (int t = tid; t < H; t += blockDim.x) {
+            int rr = 0;
+#pragma unroll
+            for (int stp = 32; stp >= 1; stp >>= 1)
+                if (rr + stp < NROW && sm.rowpre[rr + stp] <= t) rr += stp;
+            const int i = sm.rowbeg[rr] + (t - sm.rowpre[rr]);
+            const int s = sm.slot[i];
+            int* out = nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+            const int nmax = a.nmax;
+            int cnt = tile_walk(sm, i, RX, RY, wx, wy, wz, d.cut2, [&](int c, int j, int code) {
+                if (c < nmax) out[(size_t)c * 32] = sm.slot[j] | (code << DPD_CODE_SHIFT);
+            });
+            if (cnt > nmax) {
+                atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+                cnt = nmax;
+            }
+            ncount[s] = cnt;
+        }
+        return true;
+    }
     const int hc = ta.hc;
     uint16_t* col = sm.hits + tid;
     const float4* vel = a.buf.vel[*a.parity];
@@ -275,7 +303,9 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
             for (int stp = 32; stp >= 1; stp >>= 1)
                 if (rr + stp < NROW && sm.rowpre[rr + stp] <= t) rr += stp;
             i = sm.rowbeg[rr] + (t - sm.rowpre[rr]);
-            cnt = tile_walk(sm, i, RX, RY, wx, wy, wz, rcmax2, col, hc);
+            cnt = tile_walk(sm, i, RX, RY, wx, wy, wz, rcmax2, [&](int c, int j, int) {
+                if (c < hc) col[c * TILE_THREADS] = (uint16_t)j;
+            });
         }
         if (__any_sync(0xffffffffu, cnt > hc) && lane == 0) atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
         const int c = min(cnt, hc);
@@ -318,10 +348,10 @@ __device__ bool tile_box(const StepArgs& a, const TileArgs& ta, const TileSmem& 
 }
 
 // One tile: the whole home box, or (when its neighbourhood does not fit) its home cells
-// one at a time.
-template <bool LOG, bool BONDS>
+// one at a time (a single call site, so that the box code is inlined once).
+template <bool LOG, bool BONDS, bool LIST = false>
 __device__ __forceinline__ void tile_run(const StepArgs& a, const TileArgs& ta, const TileSmem& sm, int t,
-                                         double (&accv)[8])
+                                         double (&accv)[8], int* nlist = nullptr, int* ncount = nullptr)
 {
     const int r = ta.tile_rep[t];
     const RepDesc& d = a.reps[r];
@@ -330,11 +360,25 @@ __device__ __forceinline__ void tile_run(const StepArgs& a, const TileArgs& ta, 
     const int E = ta.edge;
     const int x0 = (code & 1023) * E, y0 = ((code >> 10) & 1023) * E, z0 = (code >> 20) * E;
     const int ex = min(E, d.nc[0] - x0), ey = min(E, d.nc[1] - y0), ez = min(E, d.nc[2] - z0);
-    if (tile_box<LOG, BONDS>(a, ta, sm, d, r, x0, y0, z0, ex, ey, ez, st.step, accv)) return;
-    for (int h = 0; h < ex * ey * ez; h++) {
-        const int hx = x0 + h % ex, hy = y0 + (h / ex) % ey, hz = z0 + h / (ex * ey);
-        if (!tile_box<LOG, BONDS>(a, ta, sm, d, r, hx, hy, hz, 1, 1, 1, st.step, accv) && threadIdx.x == 0)
+    bool whole = true;
+    int nbox = 1;
+    for (int b = 0; b < nbox; b++) {
+        int bx = x0, by = y0, bz = z0, bex = ex, bey = ey, bez = ez;
+        if (!whole) {
+            bx = x0 + b % ex;
+            by = y0 + (b / ex) % ey;
+            bz = z0 + b / (ex * ey);
+            bex = bey = bez = 1;
+        }
+        const bool ok = tile_box<LOG, BONDS, LIST>(a, ta, sm, d, r, bx, by, bz, bex, bey, bez, st.step, accv, nlist,
+                                                   ncount);
+        if (!ok && whole) {  // CTA-uniform: the home cells one at a time instead
+            whole = false;
+            nbox = ex * ey * ez;
+            b = -1;
+        } else if (!ok && threadIdx.x == 0) {
             atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+        }
     }
 }
 
@@ -384,4 +428,22 @@ __global__ void __launch_bounds__(256, 2) k_tile_logsteps(StepArgs a, TileArgs t
                                ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
         acc_flush_warp<8>(accv, fields, ta.tile_rep[t], a.acc);
     }
+}
+
+// The half list of the list schedules built from the tiles (list-build variant 4): a CTA
+// per tile stages its neighbourhood's positions and walks each home particle's candidates
+// in shared memory, instead of a thread per particle gathering its 14 cell ranges from
+// global memory.  The same entries as the list build; their order within a particle's list
+// is the walk's.  Runs only when a list build is due.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_tile_build(StepArgs a, TileArgs ta, BuildArgs b)
+{
+    griddep_wait();
+    extern __shared__ __align__(16) unsigned char tile_dyn[];
+    if (!build_on(b)) return;  // grid-uniform
+    const int t = blockIdx.x;
+    if (t >= ta.ntiles || !rep_active(a.rstate[ta.tile_rep[t]])) return;  // a finished replica gets no list
+    const TileSmem sm = tile_smem(tile_dyn, ta.smax);
+    double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    tile_run<false, false, true>(a, ta, sm, t, accv, b.nlist, b.ncount);
 }

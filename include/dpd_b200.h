@@ -98,7 +98,9 @@ typedef struct dpd_tuning {
     int build_variant;     /* list build: 0 = cell ranges in registers, 4
                               blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
                               8 blocks/SM; 3 = a thread per (slot, stencil cell)
-                              (grids up to 1184 blocks; larger ones use 0)        */
+                              (grids up to 1184 blocks; larger ones use 0); 4 = a
+                              CTA per tile of cells walking the candidates staged
+                              in shared memory (DPD engines; mDPD runs 0)        */
     int launch_mode;       /* 0 = small grids (up to 1184 blocks of 256 slots) run the
                               pair pass as one launch (schedule 4 in place of 8) and
                               the integrate as one, the step's bookkeeping in the

@@ -177,3 +177,35 @@ def test_tile_matches_list_schedule_over_steps():
     assert force_err(sa["f"], sb["f"]) < 1e-3
     ta, tb = a.thermo(), b.thermo()
     assert ta["temp"][-1] == pytest.approx(tb["temp"][-1], rel=1e-3)
+
+
+@pytest.mark.parametrize("name", ["dpd_skin0", "dpd_skin03", "melt_skin0", "box3", "box4"])
+def test_tile_list_build_matches_oracle(oracle_mod, name):
+    """List-build variant 4 (the half list written from the tiles): the neighbour set equals
+    the oracle's FP32-predicate set, and the list schedule's step-0 forces and the forces of
+    the next 5 steps on the engine's own state are the oracle's."""
+    from gpumdpd_b200 import Engine
+    s = _systems()[name]
+    s.run_in = re.sub(r"(?m)^thermo \d+$", "thermo 1000", s.run_in)
+    e = Engine(s.run_in, system=s.c_system())
+    e.set_tuning(pair_variant=8, cell_order=1, build_variant=4)
+    e.run(0)
+    c = e.cells()
+    got = e.neighbors()
+    ref = oracle_mod.pairs_f32(np.arange(1, s.n + 1), c["cell"], c["offset"], c["nc"], c["w"], c["cut2"])
+    assert len(got) == len(set(map(tuple, got.tolist())))
+    assert set(map(tuple, got.tolist())) == set(map(tuple, ref.tolist()))
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    tags = np.arange(1, s.n + 1)
+    st = e.state()
+    o = oracle_mod.forces(ff, tags, s.types, st["x"], st["v"], s.lo, _box(e), 0, bonds=s.bonds)
+    assert force_err(st["f"], o["f"]) < TOL
+    dt = float(re.search(r"(?m)^timestep (\S+)$", s.run_in).group(1))
+    m = np.asarray(s.masses)[np.asarray(s.types) - 1][:, None]
+    for k in range(1, 6):
+        e.run(1)
+        got = e.state()
+        vh = got["v"] - 0.5 * dt * got["f"] / m
+        o = oracle_mod.forces(ff, tags, s.types, got["x"], vh, s.lo, _box(e), k, bonds=s.bonds)
+        assert force_err(got["f"], o["f"]) < TOL, k
+    e.close()
