@@ -753,10 +753,10 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 1, 4>, grid, 256, s, a);
     } else if (variant == 8) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5>, grid, 256, s, a);
-        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 4), 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 3), 256, s, a);
     } else if (variant == 9) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5, true>, grid, 256, s, a);
-        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 4), 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 3), 256, s, a);
     } else if (variant == 10) {
         pdl_launch(k_pair_entry<STYLE, BONDS>, (a.nmax * (a.P >> 5) + 7) / 8, 256, s, a);
     }
@@ -890,7 +890,7 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
         pdl_launch(k_integrate_logsteps<false>, std::min(gp, 148 * 4), 256, s, sa);
     }
     if (any_twowall_) enqueue_two_wall(s, sa);
-    pdl_launch(k_advance, gr, 256, s, sa);
+    pdl_launch(k_advance, (nrep * 32 + 255) / 256, 256, s, sa);
 }
 
 // fix two_wall after a drift: wall extents, then the reflection of the group

@@ -609,8 +609,39 @@ __global__ void __launch_bounds__(256, MINB) k_pair_q(StepArgs a)
 // SEG: the i-side forces of an iteration are summed per owner in registers first (the flat
 // entries of one owner sit in consecutive lanes: a segmented warp scan), so one float4
 // reduction per owner and iteration reaches L2 instead of one per pair.
+// Warp-level FP64 sums of a replica kept across several calls (grid-stride loops): added
+// to `tot` while the replica stays the same, flushed to the spread accumulators (one
+// atomic per field and warp) when it changes and at the end.
+template <int NV>
+struct WarpAcc {
+    double tot[NV];
+    int rep = -1;
+    __device__ __forceinline__ WarpAcc()
+    {
+#pragma unroll
+        for (int k = 0; k < NV; k++) tot[k] = 0.0;
+    }
+    // warp-uniform r
+    __device__ __forceinline__ void add(const double (&v)[NV], int r, const int* fields, double* acc)
+    {
+        if (r != rep) {
+            flush(fields, acc);
+            rep = r;
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) tot[k] += v[k];
+    }
+    __device__ __forceinline__ void flush(const int* fields, double* acc)
+    {
+        if (rep >= 0) acc_flush_warp<NV>(tot, fields, rep, acc);
+#pragma unroll
+        for (int k = 0; k < NV; k++) tot[k] = 0.0;
+        rep = -1;
+    }
+};
+
 template <int STYLE, bool BONDS, int LOGM = 2, bool SEG = false>
-__device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
+__device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s, WarpAcc<8>* keep = nullptr)
 {
     __shared__ int s_start[8][33];
     __shared__ float4 s_pi[8][32];
@@ -738,7 +769,8 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s)
     if (log) {
         const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
                                ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
-        acc_flush_warp<8>(accv, fields, r, a.acc);
+        if (keep) keep->add(accv, r, fields, a.acc);
+        else acc_flush_warp<8>(accv, fields, r, a.acc);
     }
 }
 
@@ -760,7 +792,7 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 // first checks whether any replica logs this step (the common answer is no, and then the
 // launch costs one wave of tiny blocks instead of a full grid of early exits).
 template <int STYLE, bool BONDS, bool SEG = false>
-__global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
+__global__ void __launch_bounds__(256, 3) k_pair_flat_logsteps(StepArgs a)
 {
     griddep_wait();
     int any = 0;
@@ -770,10 +802,15 @@ __global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
     }
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
+    // the warp's sums over its virtual blocks, flushed once per replica
+    WarpAcc<8> keep;
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-        pair_flat_warp<STYLE, BONDS, 1, SEG>(a, vb * 256 + threadIdx.x);
+        pair_flat_warp<STYLE, BONDS, 1, SEG>(a, vb * 256 + threadIdx.x, &keep);
         __syncwarp();  // the warp's shared slots are reused by the next virtual block
     }
+    const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
+                           ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+    keep.flush(fields, a.acc);
 }
 
 // List build fused with the flattened pair force (DPD only: mDPD needs every density
@@ -803,7 +840,7 @@ __global__ void __launch_bounds__(256, MINB) k_build_pair(StepArgs a, BuildArgs 
 // A step is logged when the thermo or (EXT) a group compute is due.  EXT adds the group
 // fixes and the group computes.
 template <int LOGM, bool EXT>
-__device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
+__device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s, WarpAcc<10>* keep = nullptr)
 {
     int r = -1;
     bool log = false;
@@ -813,15 +850,21 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
     if (EXT && LOGM != 0)
         for (int k = 0; k < 3 * DPD_MAX_GC; k++) gv[k] = 0.0;
     if (s < a.P) {
-        // the particle's three streams are requested first (every slot < P is valid
-        // memory), so their latency overlaps the replica-state reads
+        // the particle's three streams are requested before the replica-state reads (every
+        // slot < P is valid memory), so their latency overlaps them -- except in the
+        // non-log kernel of a logged step, which leaves the slot to the log-step kernel and
+        // reads nothing else
+        r = a.warp_rep[s >> 5];
+        if (LOGM == 0) {
+            const RepState st0 = a.rstate[r];
+            if (a.mode == 0 && rep_active(st0) && (st0.step % (uint32_t)a.reps[r].log_f) == 0u) return;
+        }
         const int par = *a.parity;
         float4* posp = a.buf.pos[par];
         float4* velp = a.buf.vel[par];
         float4 v = velp[s];
         const float4 f = a.force4[s];
         float4 p = posp[s];
-        r = a.warp_rep[s >> 5];
         const RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
         const bool active = rep_active(st);
@@ -1009,7 +1052,8 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s)
     if (a.mode == 0 && log) {
         const int fields[10] = {ACC_KE, ACC_KIN + 0, ACC_KIN + 1, ACC_KIN + 2, ACC_KIN + 3,
                                 ACC_KIN + 4, ACC_KIN + 5, ACC_MOM + 0, ACC_MOM + 1, ACC_MOM + 2};
-        acc_flush_warp<10>(accv, fields, r, a.acc);
+        if (keep) keep->add(accv, r, fields, a.acc);
+        else acc_flush_warp<10>(accv, fields, r, a.acc);
     }
     if (EXT && LOGM != 0 && gcd) {
         int fields[3 * DPD_MAX_GC];
@@ -1048,7 +1092,12 @@ __global__ void __launch_bounds__(256) k_integrate_logsteps(StepArgs a)
     }
     if (!__syncthreads_or(any)) return;
     const int nvb = (a.P + 255) / 256;
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, EXT>(a, vb * 256 + threadIdx.x);
+    // the warp's sums over its virtual blocks, flushed once per replica
+    WarpAcc<10> keep;
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) integrate_slot<1, EXT>(a, vb * 256 + threadIdx.x, &keep);
+    const int fields[10] = {ACC_KE, ACC_KIN + 0, ACC_KIN + 1, ACC_KIN + 2, ACC_KIN + 3,
+                            ACC_KIN + 4, ACC_KIN + 5, ACC_MOM + 0, ACC_MOM + 1, ACC_MOM + 2};
+    keep.flush(fields, a.acc);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1398,7 +1447,12 @@ __global__ void __launch_bounds__(256) k_angle(StepArgs a, const int4* __restric
 // ---------------------------------------------------------------------------------
 // End of step bookkeeping, one thread per replica: thermo row of a logged step
 // (src/compute/thermo.cu:274-306, 479-520), step counter, build flag of this phase.
-__device__ __forceinline__ void advance_rep(const StepArgs& a, const int r)
+// The step's bookkeeping of replica r by one warp (lane = spread slot: DPD_ACC_SLOTS is
+// 32): on a logged step the lanes take the 32 spread slots of the thermo sums and a fixed
+// butterfly adds them (the row then repeats bit for bit); lane 0 writes the thermo row and
+// does the rest.
+static_assert(DPD_ACC_SLOTS == 32, "advance_rep gives each lane of a warp one spread slot");
+__device__ __forceinline__ void advance_rep(const StepArgs& a, const int r, const int lane)
 {
     {
         RepState st = a.rstate[r];
@@ -1406,13 +1460,16 @@ __device__ __forceinline__ void advance_rep(const StepArgs& a, const int r)
         if (rep_active(st)) {
             if ((st.step % (uint32_t)d.log_f) == 0u) {
                 double sum[DPD_NACC_THERMO];
-                for (int k = 0; k < DPD_NACC_THERMO; k++) sum[k] = 0.0;
-                double* base = a.acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC;
-                for (int sl = 0; sl < DPD_ACC_SLOTS; sl++)
-                    for (int k = 0; k < DPD_NACC_THERMO; k++) {
-                        sum[k] += base[sl * DPD_NACC + k];
-                        base[sl * DPD_NACC + k] = 0.0;
-                    }
+                double* base = a.acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC + (size_t)lane * DPD_NACC;
+#pragma unroll
+                for (int k = 0; k < DPD_NACC_THERMO; k++) sum[k] = base[k];
+#pragma unroll
+                for (int k = 0; k < DPD_NACC_THERMO; k++) base[k] = 0.0;
+#pragma unroll
+                for (int k = 0; k < DPD_NACC_THERMO; k++)
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+                if (lane != 0) return;
                 double* row = a.ring + ((size_t)r * DPD_RING_ROWS + (st.nlog % DPD_RING_ROWS)) *
                                            DPD_THERMO_FIELDS;
                 const double vol = d.volume;
@@ -1431,6 +1488,7 @@ __device__ __forceinline__ void advance_rep(const StepArgs& a, const int r)
                 row[16] = sum[ACC_ANGLE_PE];
                 st.nlog++;
             }
+            if (lane != 0) return;
             if (a.gc && d.gc_n) {
                 const int due = gc_due(a, d, st, r);
                 double* base = a.acc + (size_t)r * DPD_ACC_SLOTS * DPD_NACC;
@@ -1471,12 +1529,14 @@ __device__ __forceinline__ void advance_phase(const StepArgs& a)
     *a.phase = ph + 1u;
 }
 
+// a warp per replica
 __global__ void k_advance(StepArgs a)
 {
     griddep_wait();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < a.nrep) advance_rep(a, r);
-    if (r == 0) advance_phase(a);
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = g >> 5;
+    if (r < a.nrep) advance_rep(a, r, threadIdx.x & 31);
+    if (g == 0) advance_phase(a);
 }
 
 // Small grids, where a launch costs more than the work: the whole velocity-Verlet step
@@ -1497,7 +1557,7 @@ __global__ void __launch_bounds__(256) k_integrate_adv(StepArgs a)
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) advance_rep(a, r);
+    for (int r = threadIdx.x >> 5; r < a.nrep; r += blockDim.x >> 5) advance_rep(a, r, threadIdx.x & 31);
     __syncthreads();
     if (threadIdx.x == 0) {
         advance_phase(a);

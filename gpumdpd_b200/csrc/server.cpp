@@ -116,7 +116,7 @@ struct dpd_server {
     int64_t used_bytes = 0;
     double max_wait_s = 0.0;  // admission window (see dpd_server_set_policy)
     int min_jobs = 1;
-    bool prio_by_length = true;  // cohort stream priority by job length (DPD_B200_FLAT_PRIORITY=1: off)
+
     int64_t particle_steps = 0;
     double busy_s = 0;
     Clock::time_point t0 = Clock::now();
@@ -219,7 +219,7 @@ int dpd_server::make_cohort(const std::vector<int64_t>& ids)
     // nearly their alone speed while shorter cohorts fill the rest of the GPU
     {
         int least = 0, greatest = 0;
-        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess && prio_by_length) {
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) {
             int k = 0;
             while ((c->max_steps >> (k + 1)) != 0u) k++;
             c->eng->set_stream_priority(std::max(greatest, least - std::max(0, k - 9)));
@@ -384,7 +384,6 @@ int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning
     if (!s) return DPD_E_NOMEM;
     s->budget = hbm_budget_bytes;
     s->chunk = chunk_steps;
-    if (const char* fp = std::getenv("DPD_B200_FLAT_PRIORITY")) s->prio_by_length = std::atoi(fp) == 0;
     if (tune) {
         s->tune = *tune;
     } else {  // the engine defaults
