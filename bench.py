@@ -378,14 +378,16 @@ def run_ours(args, world, rank, local):
     foot = n * (2 * (48 + 8 * maxb) + 4 * 48 + 16)
     l2 = (f"inputs > L2 ({foot / 1e9:.2f} GB)" if foot > 126e6 else
           f"inputs < L2 ({foot / 1e6:.1f} MB), no flush: small latency-bound system")
-    traffic = None
+    traffic, wipp = None, None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
         t = prof.get(args.workload)
-        if t:
+        if t and pair_variant == 8:
             traffic = t["dram_bytes_per_launch"]
+            wipp = t.get("warp_instr_per_particle")
     except Exception:
         pass
+    clk_summary = clk.summary()
     pairs_per_step = ls["pairs"]
     out = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -411,7 +413,7 @@ def run_ours(args, world, rank, local):
                      "binding": "issue (Saru integer chain), not HBM",
                      "pairs_per_step": pairs_per_step,
                      "saru_int_ops_per_pair": 130},
-        "clocks": clk.summary(),
+        "clocks": clk_summary,
         # per step: the list-build kernels (counting pass, 1 or 3 scan launches, permutation,
         # list; each returns at once unless a build is flagged), the pair kernel(s), the
         # integrate pair (non-log steps + log steps), advance; plus 2 before the graph
@@ -419,6 +421,12 @@ def run_ours(args, world, rank, local):
                                           step_launches(system, pair_variant)) + 2),
         "impl": "ours",
     }
+    if wipp and clk_summary.get("sm_mhz"):
+        # the instruction-issue ceiling of the pair kernel: its warp instructions (ncu count per
+        # particle) at one instruction per clock on each of the 4 schedulers of 148 SMs
+        ceil_ms = n * wipp / (148 * 4 * clk_summary["sm_mhz"] * 1e6) * 1e3
+        out["roofline"]["issue"] = {"warp_instr_per_particle": wipp, "ceiling_ms": ceil_ms,
+                                    "frac": ceil_ms / per_launch_ms, "sm_mhz": clk_summary["sm_mhz"]}
     if world == 1 and not args.no_extras:
         # T and P of the headline system: the FP32 engine against the FP64 parity engine
         # from the same state over the same window, after the melt's bonds have relaxed
