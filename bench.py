@@ -186,50 +186,91 @@ def fp32_fp64_window(s, x, v, steps, every, fields=("temp", "pressure"), extra=N
 
 
 class ClockSampler:
-    """nvidia-smi clocks sampled every 200 ms while the timed region runs."""
+    """SM clocks and clock-event reasons read through NVML every 2 ms while the timed
+    region runs (read-only queries: nothing about the GPU is changed).  A first sample is
+    taken on entry, so a region of a few milliseconds still has samples; nvidia-smi's
+    200 ms loop is the fallback when NVML cannot be loaded."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
-        self.gpu = str(gpu_index)
-        self.rows = []
+        self.gpu = int(gpu_index)
+        self.rows = []  # (sm_mhz, max_mhz, {reason names})
         self.proc = None
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _nvml_loop(self, nv, h):
+        while True:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.rows.append((float(sm), float(mx), {n for n, a in self.REASONS if bits & getattr(nv, a)}))
+            if self.stop.wait(0.002):
+                break
+
+    def _smi_read(self):
+        for line in self.proc.stdout:
+            r = [c.strip() for c in line.split(",")]
+            try:
+                names = {n for k, (n, _) in enumerate(self.REASONS) if len(r) > 5 + k and r[5 + k].lower() == "active"}
+                self.rows.append((float(r[1]), float(r[2]), names))
+            except ValueError:
+                pass
 
     def __enter__(self):
         try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:  # the CUDA device itself (NVML numbers devices regardless of CUDA_VISIBLE_DEVICES)
+                import torch
+                u = str(torch.cuda.get_device_properties(self.gpu).uuid)
+                h = nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            while not self.rows:  # the first sample before the timed region starts
+                time.sleep(0.0005)
+            return self
+        except Exception:
+            self.thread = None
+        try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", self.gpu], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+                 "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._smi_read, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
-
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4)
-                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted(set().union(*[r[2] for r in self.rows]))
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": reasons, "samples": len(self.rows),
+                "source": "nvml" if self.proc is None else "nvidia-smi"}
 
 
 def dist_setup(args, backend="nccl"):

@@ -850,21 +850,17 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s, W
     if (EXT && LOGM != 0)
         for (int k = 0; k < 3 * DPD_MAX_GC; k++) gv[k] = 0.0;
     if (s < a.P) {
-        // the particle's three streams are requested before the replica-state reads (every
-        // slot < P is valid memory), so their latency overlaps them -- except in the
-        // non-log kernel of a logged step, which leaves the slot to the log-step kernel and
-        // reads nothing else
-        r = a.warp_rep[s >> 5];
-        if (LOGM == 0) {
-            const RepState st0 = a.rstate[r];
-            if (a.mode == 0 && rep_active(st0) && (st0.step % (uint32_t)a.reps[r].log_f) == 0u) return;
-        }
+        // the particle's three streams are requested first (every slot < P is valid
+        // memory), so their latency overlaps the replica-state reads; on a logged step the
+        // non-log kernel's loads are wasted, which costs less than putting the state read
+        // before them on every other step
         const int par = *a.parity;
         float4* posp = a.buf.pos[par];
         float4* velp = a.buf.vel[par];
         float4 v = velp[s];
         const float4 f = a.force4[s];
         float4 p = posp[s];
+        r = a.warp_rep[s >> 5];
         const RepState st = a.rstate[r];
         const RepDesc& d = a.reps[r];
         const bool active = rep_active(st);
