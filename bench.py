@@ -370,8 +370,8 @@ def run_ours(args, world, rank, local):
     system = make_system(args, thermo=every)
     eng = Engine(system.run_in, system=system.c_system())
     pair_variant = 8 if args.pair_variant is None else args.pair_variant
-    eng.set_tuning(pair_variant=pair_variant, cell_order=1, build_variant=args.build_variant, tile=args.tile,
-                   pair_block=args.pair_block)
+    eng.set_tuning(pair_variant=pair_variant, cell_order=args.cell_order, build_variant=args.build_variant,
+                   tile=args.tile, pair_block=args.pair_block)
     eng.run(0)
     st0 = eng.state(images=False) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     eng.run(args.warmup)
@@ -820,7 +820,10 @@ def main():
     ap.add_argument("--pair-variant", type=int, default=None,
                     help="pair-kernel schedule (default: the engine's choice)")
     ap.add_argument("--build-variant", type=int, default=0,
-                    help="list-build kernel (0: ranges in registers; 1, 2: in shared memory)")
+                    help="list-build kernel (0: ranges in registers; 1, 2: in shared memory; 4: cell tiles; "
+                         "5: column ranges, with --cell-order 2)")
+    ap.add_argument("--cell-order", type=int, default=1,
+                    help="cell order of the slots (0: linear, 1: Morton, 2: x-y columns in Morton order)")
     ap.add_argument("--pair-block", type=int, default=0,
                     help="pair schedule 11: 3 = the tile kernel at 3 CTAs per SM (default 4)")
     ap.add_argument("--tile", type=int, default=0,

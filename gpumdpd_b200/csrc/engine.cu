@@ -73,6 +73,57 @@ static uint32_t morton3(uint32_t x, uint32_t y, uint32_t z)
     return spread(x) | (spread(y) << 1) | (spread(z) << 2);
 }
 
+static uint32_t morton2(uint32_t x, uint32_t y)
+{
+    auto spread = [](uint32_t v) {
+        v &= 0x3ff;
+        v = (v | (v << 8)) & 0x00FF00FF;
+        v = (v | (v << 4)) & 0x0F0F0F0F;
+        v = (v | (v << 2)) & 0x33333333;
+        v = (v | (v << 1)) & 0x55555555;
+        return v;
+    };
+    return spread(x) | (spread(y) << 1);
+}
+
+// The order of a replica's cells in the slot array: 0 = linear (z fastest), 1 = Morton,
+// 2 = the x-y columns in Morton order with the cells of a column consecutive (z
+// fastest), so that cells z-1..z+1 of a column are one slot range (list build 5).
+void Engine::rank_cells(Replica& R) const
+{
+    const RepDesc& d = R.desc;
+    R.crank.resize(d.ncell);
+    std::vector<std::pair<uint32_t, int>> order(d.ncell);
+    for (int cx = 0; cx < d.nc[0]; cx++)
+        for (int cy = 0; cy < d.nc[1]; cy++)
+            for (int cz = 0; cz < d.nc[2]; cz++) {
+                const int lin = (cx * d.nc[1] + cy) * d.nc[2] + cz;
+                uint32_t key = (uint32_t)lin;
+                if (tune_.cell_order == 1) key = morton3(cx, cy, cz);
+                else if (tune_.cell_order == 2) key = morton2(cx, cy) * (uint32_t)d.nc[2] + (uint32_t)cz;
+                order[lin] = {key, lin};
+            }
+    std::sort(order.begin(), order.end());
+    for (int k = 0; k < d.ncell; k++) R.crank[order[k].second] = k;
+}
+
+// the device copies of the cell ranks and of their inverse
+int Engine::upload_ranks()
+{
+    std::vector<int> crank(C_, 0), cell_lin(C_, -1);
+    for (const Replica& R : reps_) {
+        const RepDesc& d = R.desc;
+        for (int c = 0; c < d.ncell; c++) {
+            crank[d.c_begin + c] = R.crank[c];
+            cell_lin[d.c_begin + R.crank[c]] = c;
+        }
+    }
+    CK(cudaMemcpyAsync(b_.crank, crank.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(b_.cell_lin, cell_lin.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return DPD_OK;
+}
+
 int Engine::layout()
 {
     P_ = 0;
@@ -173,18 +224,7 @@ int Engine::layout()
             for (int i = 0; i < n; i++) R.maxb = std::max(R.maxb, deg[i]);
             maxb_ = std::max(maxb_, R.maxb);
         }
-        // cell order
-        R.crank.resize(d.ncell);
-        std::vector<std::pair<uint32_t, int>> order(d.ncell);
-        for (int cx = 0; cx < d.nc[0]; cx++)
-            for (int cy = 0; cy < d.nc[1]; cy++)
-                for (int cz = 0; cz < d.nc[2]; cz++) {
-                    int lin = (cx * d.nc[1] + cy) * d.nc[2] + cz;
-                    uint32_t key = tune_.cell_order == 1 ? morton3(cx, cy, cz) : (uint32_t)lin;
-                    order[lin] = {key, lin};
-                }
-        std::sort(order.begin(), order.end());
-        for (int k = 0; k < d.ncell; k++) R.crank[order[k].second] = k;
+        rank_cells(R);
     }
     if (maxb_ > 16) {
         err = "an atom has more than 16 bonds";
@@ -294,7 +334,7 @@ int Engine::alloc_and_upload()
     }
     // tables
     std::vector<RepDesc> hd(nrep);
-    std::vector<int> wrep(P_ / 32), crank(C_, 0), cell_rep(C_, 0), cell_lin(C_, -1);
+    std::vector<int> wrep(P_ / 32), cell_rep(C_, 0);
     std::vector<float4> coeff(ncoeff);
     std::vector<float2> mass(nmass);
     std::vector<float4> bondc(nbond);
@@ -303,10 +343,6 @@ int Engine::alloc_and_upload()
         const RepDesc& d = R.desc;
         hd[r] = d;
         for (int wv = d.p_begin / 32; wv < d.p_cap_end / 32; wv++) wrep[wv] = r;
-        for (int c = 0; c < d.ncell; c++) {
-            crank[d.c_begin + c] = R.crank[c];
-            cell_lin[d.c_begin + R.crank[c]] = c;
-        }
         for (int c = 0; c <= d.ncell; c++) cell_rep[d.c_begin + c] = r;
         const int nt = d.ntypes;
         const double sig_scale = std::sqrt(2.0 * R.ff.temp) / std::sqrt(R.in.dt);
@@ -335,9 +371,8 @@ int Engine::alloc_and_upload()
     }
     CK(cudaMemcpyAsync(b_.reps, hd.data(), sizeof(RepDesc) * nrep, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.warp_rep, wrep.data(), sizeof(int) * wrep.size(), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.crank, crank.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.cell_rep, cell_rep.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.cell_lin, cell_lin.data(), sizeof(int) * C_, cudaMemcpyHostToDevice, stream_));
+    if ((st = upload_ranks())) return st;
     CK(cudaMemcpyAsync(b_.coeff, coeff.data(), sizeof(float4) * ncoeff, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.mass, mass.data(), sizeof(float2) * nmass, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.bondc, bondc.data(), sizeof(float4) * nbond, cudaMemcpyHostToDevice, stream_));
@@ -809,6 +844,8 @@ void Engine::enqueue_build(cudaStream_t s, bool list, bool wide)
         } else if (wide && gp <= 148 * 8) pdl_launch(k_build_wide, (14 * P_ + 255) / 256, 256, s, ba);
         else if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
         else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);
+        else if (tune_.build_variant == 5) pdl_launch(k_build_cols<false, 4>, gp, 256, s, ba);
+        else if (tune_.build_variant == 6) pdl_launch(k_build_cols<true, 5>, gp, 256, s, ba);
         else pdl_launch(k_build_nlist, gp, 256, s, ba);
     }
 }
@@ -1054,6 +1091,11 @@ int Engine::run_async(uint32_t nsteps)
     for (;;) {
         uint32_t end = last;
         for (auto& w : dumps_) end = std::min(end, next_dump(w.get(), s));
+        if (ranks_dirty_) {
+            const int e = upload_ranks();
+            if (e) return e;
+            ranks_dirty_ = false;
+        }
         k_set_target<<<g, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, end, zero ? 1 : 0,
                                              zero || force_build_ ? 1 : 0, b_.build_flag, b_.phase);
         force_build_ = false;
@@ -1155,7 +1197,15 @@ int Engine::time_steps(uint32_t nsteps, double* total_ms, double* pair_ms, int64
     std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 2);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     const uint32_t target = next_step_ - 1 + nsteps;
-    k_set_target<<<(nrep + 255) / 256, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 0, 0, b_.build_flag, b_.phase);
+    if (ranks_dirty_) {
+        const int e = upload_ranks();
+        if (e) return e;
+        ranks_dirty_ = false;
+    }
+    // a pending list build (new cell ranks, a restart) comes first, as in a run
+    k_set_target<<<(nrep + 255) / 256, 256, 0, stream_>>>(b_.rstate, b_.limit, nrep, target, 0, force_build_ ? 1 : 0,
+                                                          b_.build_flag, b_.phase);
+    force_build_ = false;
     enqueue_integrate_initial(stream_);
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1662,15 +1712,24 @@ int Engine::list_stats(int64_t* n_pairs, int64_t* n_atoms, int64_t* n_builds)
 int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
-    if (t->pair_variant < 0 || t->pair_variant > 11 || t->cell_order < 0 || t->cell_order > 1 ||
-        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 4 || t->launch_mode < 0 ||
+    if (t->pair_variant < 0 || t->pair_variant > 11 || t->cell_order < 0 || t->cell_order > 2 ||
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 6 || t->launch_mode < 0 ||
         t->launch_mode > 3 || t->tile < 0 || t->tile > TILE_MAX_EDGE || t->tile_capacity < 0 ||
         t->tile_capacity > 4096) {
-        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..4, cell_order 0 or 1, "
+        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..6, cell_order 0..2, "
               "launch_mode 0..3, tile edge 0..6, tile capacity 0..4096";
         return DPD_E_ARG;
     }
+    const bool reorder = t->cell_order != tune_.cell_order;
     tune_ = *t;
+    if (reorder) {
+        // the slots stay sorted in the old order (and the device keeps the old ranks, so
+        // that the list and cell ranges stay consistent) until the next run, which uploads
+        // the new ranks and starts with a list build
+        for (Replica& R : reps_) rank_cells(R);
+        ranks_dirty_ = true;
+        force_build_ = true;
+    }
     return build_graph();
 }
 

@@ -159,6 +159,8 @@ public:
 
 private:
     int layout();
+    void rank_cells(Replica& R) const;
+    int upload_ranks();
     int alloc_and_upload();
     int upload_particles();
     void enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1);
@@ -198,6 +200,7 @@ private:
     std::vector<int> gc_ring_base_;               // first compute ring of each replica
     bool zero_pending_ = true;
     bool force_build_ = false;  // the next run starts with a list build (after a restart)
+    bool ranks_dirty_ = false;  // new cell ranks (a changed cell order) wait for the next run
     uint32_t next_step_ = 0;
     std::vector<void*> allocs_;
     float4 *h_pos_ = nullptr, *h_vel_ = nullptr, *h_frc_ = nullptr;  // pinned staging

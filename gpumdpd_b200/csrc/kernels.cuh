@@ -605,3 +605,162 @@ __global__ void __launch_bounds__(256, MINB) k_build_nlist_s(BuildArgs a)
     }
     a.ncount[s] = count;
 }
+
+// ---------------------------------------------------------------------------------
+// The list build over x-y columns (build variant 5).  The half stencil with x outermost,
+// (ox > 0) | (ox == 0 & oy > 0) | (ox == 0 & oy == 0 & oz > 0), is the rest of the own
+// cell, cell z+1 of the own column, and cells z-1..z+1 of the columns (x, y+1),
+// (x+1, y-1), (x+1, y), (x+1, y+1).  When the cells of a column are consecutive in the
+// cell order (cell order 0, linear with z fastest, or 2, columns in Morton order), each of
+// these five groups is one contiguous slot range, walked 4 slots at a time with the z
+// shift of each slot taken from the range's two cell boundaries: five ranges of about
+// nine candidates in place of fourteen cells of about three, so fewer idle lanes at the
+// ends of short ranges.  At the ends of a column (z = 0 or z = nc-1) the cell across the
+// periodic boundary is not next to the other two: the group is its two contiguous cells
+// plus that one cell, walked after the five ranges.  A particle whose groups are not
+// contiguous otherwise (every particle under the Morton order) walks the same 13 cells one
+// at a time.  The predicate and the pair set are those of the other builds; which particle
+// of a pair holds it follows this stencil's orientation.
+__constant__ int8_t c_half_x[13][3] = {
+    {0, 0, 1}, {0, 1, -1}, {0, 1, 0}, {0, 1, 1}, {1, -1, -1}, {1, -1, 0}, {1, -1, 1},
+    {1, 0, -1}, {1, 0, 0}, {1, 0, 1}, {1, 1, -1}, {1, 1, 0}, {1, 1, 1}};
+
+// slots [jb, je) of one column group: cell z-1 below b1, cell z in [b1, b2), cell z+1
+// from b2; sx, sy the group's shifts (c_i - c_j) w in x and y, cxy its 9 (dcx+1) + 3 (dcy+1)
+__device__ __forceinline__ void column_walk(const float4* __restrict__ pos, const float4 pi, const int jb,
+                                            const int je, const int b1, const int b2, const float sx,
+                                            const float sy, const float wz, const int cxy, const float cut2,
+                                            int* out, const int nmax, int& count)
+{
+    for (int j0 = jb; j0 < je; j0 += 4) {
+        float4 pj[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (j0 + u < je) pj[u] = pos[j0 + u];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int j = j0 + u;
+            if (j < je) {
+                const bool below = j < b1, mid = j < b2;
+                const float sz = below ? wz : (mid ? 0.0f : -wz);
+                const float dx = __fadd_rn(__fsub_rn(pi.x, pj[u].x), sx);
+                const float dy = __fadd_rn(__fsub_rn(pi.y, pj[u].y), sy);
+                const float dz = __fadd_rn(__fsub_rn(pi.z, pj[u].z), sz);
+                float r2 = __fmul_rn(dx, dx);
+                r2 = __fmaf_rn(dy, dy, r2);
+                r2 = __fmaf_rn(dz, dz, r2);
+                if (r2 <= cut2) {
+                    if (count < nmax)
+                        out[(size_t)count * 32] = j | ((cxy + (below ? 2 : (mid ? 1 : 0))) << DPD_CODE_SHIFT);
+                    count++;
+                }
+            }
+        }
+    }
+}
+
+// SMR: the five ranges kept in shared memory ([group][thread], conflict-free) rather than
+// in registers, for MINB blocks per SM within the register budget
+template <bool SMR, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_build_cols(BuildArgs a)
+{
+    __shared__ int4 s_rng[SMR ? 5 : 1][256];
+    griddep_wait();
+    if (!build_on(a)) return;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.P) return;
+    const int r = a.warp_rep[s >> 5];
+    const RepDesc& d = a.reps[r];
+    if (s >= d.p_end || a.rstate[r].step > a.rstate[r].target) {
+        a.ncount[s] = 0;
+        return;
+    }
+    const float4* pos = a.buf.pos[*a.parity];
+    const float4 pi = pos[s];
+    const int code = __float_as_int(pi.w);
+    const int cx = cell_x(code), cy = cell_y(code), cz = cell_z(code);
+    const int ncx = d.nc[0], ncy = d.nc[1], ncz = d.nc[2];
+    const float cut2 = d.cut2;
+    const float wx = d.w[0], wy = d.w[1], wz = d.w[2];
+    const int* crank = a.crank + d.c_begin;
+    const int* cstart = a.cstart + d.c_begin;
+    int* out = a.nlist + ((size_t)(s >> 5) * a.nmax) * 32 + (s & 31);
+    int count = 0;
+    // z = 0: cell z-1 lies across the periodic boundary; z = nc-1: cell z+1 does
+    const bool wlo = cz == 0, whi = cz == ncz - 1;
+    const int zm = wlo ? ncz - 1 : cz - 1, zp = whi ? 0 : cz + 1;
+    // ranks of cells z-1, z, z+1 of the five columns (group 0: the own column, whose
+    // z-1 cell is not in the stencil)
+    int rl[5], rm[5], rh[5];
+#pragma unroll
+    for (int g = 0; g < 5; g++) {
+        const int ox = g < 2 ? 0 : 1, oy = g == 0 ? 0 : (g == 1 ? 1 : g - 3);
+        int nx = cx + ox; nx -= nx >= ncx ? ncx : 0;
+        int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
+        const int base = (nx * ncy + ny) * ncz;
+        rl[g] = g ? __ldg(crank + base + zm) : 0;
+        rm[g] = __ldg(crank + base + cz);
+        rh[g] = __ldg(crank + base + zp);
+    }
+    // the cells of each group on this side of the periodic boundary are consecutive
+    bool contiguous = true;
+#pragma unroll
+    for (int g = 0; g < 5; g++)
+        contiguous &= (whi || rh[g] == rm[g] + 1) && (wlo || g == 0 || rm[g] == rl[g] + 1);
+    if (contiguous) {
+        // main range of a group: from cell z-1 (cell z at z = 0) to the end of cell z+1
+        // (of cell z at z = nc-1); the end of cell z is the start of cell z+1 in between
+        int jb[5], b1[5], b2[5], je[5];
+#pragma unroll
+        for (int g = 0; g < 5; g++) {
+            jb[g] = g ? __ldg(cstart + (wlo ? rm[g] : rl[g])) : s + 1;
+            b1[g] = g ? __ldg(cstart + rm[g]) : s + 1;
+            b2[g] = __ldg(cstart + rm[g] + 1);
+            je[g] = __ldg(cstart + (whi ? rm[g] : rh[g]) + 1);
+            if constexpr (SMR) s_rng[g][threadIdx.x] = make_int4(jb[g], b1[g], b2[g], je[g]);
+        }
+#pragma unroll
+        for (int g = 0; g < 5; g++) {
+            const int ox = g < 2 ? 0 : 1, oy = g == 0 ? 0 : (g == 1 ? 1 : g - 3);
+            if constexpr (SMR) {
+                const int4 q = s_rng[g][threadIdx.x];
+                jb[g] = q.x, b1[g] = q.y, b2[g] = q.z, je[g] = q.w;
+            }
+            column_walk(pos, pi, jb[g], je[g], b1[g], b2[g], __int2float_rn(-ox) * wx, __int2float_rn(-oy) * wy,
+                        wz, (1 - ox) * 9 + (1 - oy) * 3, cut2, out, a.nmax, count);
+        }
+        if (wlo || whi) {
+            // the cell across the boundary of each group: z-1 below, z+1 above both bounds
+#pragma unroll 1
+            for (int g = wlo ? 1 : 0; g < 5; g++) {
+                const int ox = g < 2 ? 0 : 1, oy = g == 0 ? 0 : (g == 1 ? 1 : g - 3);
+                int nx = cx + ox; nx -= nx >= ncx ? ncx : 0;
+                int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
+                const int key = __ldg(crank + (nx * ncy + ny) * ncz + (wlo ? zm : zp));
+                const int b = __ldg(cstart + key), e = __ldg(cstart + key + 1);
+                column_walk(pos, pi, b, e, wlo ? e : b, wlo ? e : b, __int2float_rn(-ox) * wx,
+                            __int2float_rn(-oy) * wy, wz, (1 - ox) * 9 + (1 - oy) * 3, cut2, out, a.nmax, count);
+            }
+        }
+    } else {
+#pragma unroll 1
+        for (int st = 0; st < 14; st++) {
+            const int ox = st ? c_half_x[st - 1][0] : 0, oy = st ? c_half_x[st - 1][1] : 0,
+                      oz = st ? c_half_x[st - 1][2] : 0;
+            int nx = cx + ox; nx -= nx >= ncx ? ncx : 0;
+            int ny = cy + oy; ny += ny < 0 ? ncy : 0; ny -= ny >= ncy ? ncy : 0;
+            int nz = cz + oz; nz += nz < 0 ? ncz : 0; nz -= nz >= ncz ? ncz : 0;
+            const int key = __ldg(crank + (nx * ncy + ny) * ncz + nz);
+            const int b = st ? __ldg(cstart + key) : s + 1, e = __ldg(cstart + key + 1);
+            // the whole cell on one side of both boundaries: below b1 for z-1, in [b1, b2)
+            // for z, from b2 for z+1
+            column_walk(pos, pi, b, e, oz < 0 ? e : b, oz > 0 ? b : e, __int2float_rn(-ox) * wx,
+                        __int2float_rn(-oy) * wy, wz, (1 - ox) * 9 + (1 - oy) * 3, cut2, out, a.nmax, count);
+        }
+    }
+    if (count > a.nmax) {
+        atomicOr(&a.rstate[r].status, ST_LIST_OVERFLOW);
+        count = a.nmax;
+    }
+    a.ncount[s] = count;
+}

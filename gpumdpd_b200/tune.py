@@ -107,7 +107,7 @@ def tune_system(system, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MO
                 table.append({"skin": skin, "nl_f": nl_f, "error": str(e)})
                 continue
             for c in _candidates(schedules, launch_modes):
-                eng.set_tuning(cell_order=1, **c)
+                eng.set_tuning(**{"cell_order": 1, **c})
                 table.append(dict(c, skin=skin, nl_f=nl_f, ms_per_step=_time(eng, steps, warmup)))
             eng.close()
     ok = [t for t in table if "ms_per_step" in t]
@@ -129,7 +129,7 @@ def tune_batch(systems, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MO
             table.append({"skin": skin, "error": str(e)})
             continue
         for c in _candidates(schedules, launch_modes):
-            b.set_tuning(cell_order=1, **c)
+            b.set_tuning(**{"cell_order": 1, **c})
             table.append(dict(c, skin=skin, nl_f=1, ms_per_step=_time(b, steps, warmup)))
         b.close()
     ok = [t for t in table if "ms_per_step" in t]

@@ -94,13 +94,19 @@ typedef struct dpd_tuning {
                               neighbourhood in shared memory and evaluates its
                               pairs straight from the cell ranges (DPD engines;
                               mDPD runs 8)                                        */
-    int cell_order;        /* 0 = linear cells, 1 = Morton-ordered cells           */
+    int cell_order;        /* 0 = linear cells (z fastest), 1 = Morton-ordered cells,
+                              2 = x-y columns in Morton order, the cells of a column
+                              consecutive (z fastest).  A change between runs takes
+                              effect at the next run, which starts with a list build */
     int build_variant;     /* list build: 0 = cell ranges in registers, 4
                               blocks/SM; 1, 2 = cell ranges in shared memory, 6 or
                               8 blocks/SM; 3 = a thread per (slot, stencil cell)
                               (grids up to 1184 blocks; larger ones use 0); 4 = a
                               CTA per tile of cells walking the candidates staged
-                              in shared memory (DPD engines; mDPD runs 0)        */
+                              in shared memory (DPD engines; mDPD runs 0); 5 = a
+                              thread per slot walking five column ranges of slots
+                              (cells z-1..z+1 of a column, contiguous under cell
+                              order 0 or 2; cell by cell where they are not)      */
     int launch_mode;       /* 0 = small grids (up to 1184 blocks of 256 slots) run the
                               pair pass as one launch (schedule 4 in place of 8) and
                               the integrate as one, the step's bookkeeping in the

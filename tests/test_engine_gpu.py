@@ -528,6 +528,60 @@ def test_build_variants_give_the_same_list(oracle_mod, name, build_variant, laun
     assert force_err(b.state()["f"], a.state()["f"]) < 1e-4
 
 
+@pytest.mark.parametrize("cell_order,build_variant", [(0, 5), (1, 5), (2, 5), (0, 6), (2, 6)])
+@pytest.mark.parametrize("name", ["dpd", "diblock", "small_box"])
+def test_column_build_gives_the_oracle_pairs(oracle_mod, name, cell_order, build_variant):
+    """The list build over x-y columns (build variant 5: five contiguous slot ranges per
+    particle where the cells of a column are consecutive, the 13 cells one at a time
+    elsewhere; 6: the same with the ranges in shared memory, 5 blocks per SM) gives the oracle's FP32-predicate pair set under every cell order -- linear
+    and column order (contiguous groups, cell by cell at the column ends where z wraps),
+    Morton (cell by cell throughout) -- and step-0 forces within 1e-5 of the RMS force."""
+    s = _systems()[name]
+    e = _engine_from(s)
+    e.set_tuning(pair_variant=8, cell_order=cell_order, build_variant=build_variant, launch_mode=1)
+    e.run(0)
+    c = e.cells()
+    tags = np.arange(1, s.n + 1)
+    got = e.neighbors()
+    assert len(got) == len(set(map(tuple, got.tolist())))  # no duplicates
+    ref = oracle_mod.pairs_f32(tags, c["cell"], c["offset"], c["nc"], c["w"], c["cut2"])
+    assert set(map(tuple, got.tolist())) == set(map(tuple, ref.tolist()))
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    o = oracle_mod.forces(ff, tags, s.types, st["x"], st["v"], s.lo, _box(e), 0, bonds=s.bonds)
+    assert force_err(st["f"], o["f"]) < FORCE_TOL
+    e.close()
+
+
+def test_cell_order_change_between_runs(oracle_mod):
+    """A cell order changed between runs leaves the current list in place until the next
+    run (the neighbour set read back right after the change is the old one), and the next
+    run starts with a list build in the new order even at skin 0.3, where the list would
+    otherwise be kept: the build count rises at its first step, and the forces of every
+    later step equal the oracle's on the engine's state."""
+    from gpumdpd_b200 import inputs
+    s = inputs.binary_mixture(10.0, 30.0, seed=41, nsteps=0, skin=0.3)
+    e = _engine_from(s)
+    e.set_tuning(pair_variant=8, cell_order=1, launch_mode=1)
+    e.run(0)
+    e.run(1)
+    before = set(map(tuple, e.neighbors().tolist()))
+    b0 = e.info()["builds"]
+    e.set_tuning(pair_variant=8, cell_order=2, build_variant=5, launch_mode=1)
+    assert set(map(tuple, e.neighbors().tolist())) == before
+    e.run(1)
+    assert e.info()["builds"] == b0 + 1
+    ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
+    tags = np.arange(1, s.n + 1)
+    for k in range(3):
+        if k:
+            e.run(1)
+        got = e.state()
+        o = oracle_mod.forces(ff, tags, s.types, got["x"], half_step_velocities(got, s), s.lo, _box(e), 2 + k)
+        assert force_err(got["f"], o["f"]) < FORCE_TOL, k
+    e.close()
+
+
 @pytest.mark.parametrize("skin,nl_f", [(0.0, 1), (0.3, 1), (0.3, 2)])
 def test_rdf_samples_over_a_run_vs_oracle(oracle_mod, skin, nl_f):
     """The RDF accumulated over samples every 2 steps equals the mean of the oracle's RDFs

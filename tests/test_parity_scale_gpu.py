@@ -1,9 +1,11 @@
 """Parity on the headline configurations at full size, through the C ABI.
 
 - The A5B5 diblock melt (L = 100, N = 3.0M, 2.7M harmonic bonds, skin 0: the
-  configuration the headline throughput is measured on): step-0 forces within 1e-5 of the
-  RMS force against the FP64 oracle on the engine's own state, and the neighbour set equal
-  to the oracle's FP32-predicate set (src/force/neigh_list.cu:360-389) as tag pairs.
+  configuration the headline throughput is measured on), with the Morton cell order and
+  the default list build, and with the column cell order and the column-range build:
+  step-0 forces within 1e-5 of the RMS force against the FP64 oracle on the engine's own
+  state, and the neighbour set equal to the oracle's FP32-predicate set
+  (src/force/neigh_list.cu:360-389) as tag pairs.
 - The packed 256-replica A/B sweep (3.16M slots, L log-uniform over 8..24, a_AB over
   25..45, skin 0): for 8 replicas (smallest, largest, a_AB extremes and four between),
   step-0 forces and the forces of each of steps 1-10 on the engine's own state within
@@ -40,12 +42,14 @@ def _half_v(st, masses, types, dt):
     return st["v"] - 0.5 * dt * st["f"] / m
 
 
-def test_melt_3M_step0_forces_and_neighbor_set(oracle_mod):
+@pytest.mark.parametrize("tuning", [{"cell_order": 1}, {"cell_order": 2, "build_variant": 5}],
+                         ids=["morton", "columns"])
+def test_melt_3M_step0_forces_and_neighbor_set(oracle_mod, tuning):
     from gpumdpd_b200 import Engine, inputs
     s = inputs.diblock_melt(L=100.0, seed=7, nsteps=10, thermo=1000, skin=0.0)
     assert s.n == 3_000_000
     e = Engine(s.run_in, system=s.c_system())
-    e.set_tuning(pair_variant=8, cell_order=1)
+    e.set_tuning(pair_variant=8, **tuning)
     e.run(0)
     st = e.state()
     c = e.cells()
