@@ -370,8 +370,7 @@ def run_ours(args, world, rank, local):
     system = make_system(args, thermo=every)
     eng = Engine(system.run_in, system=system.c_system())
     pair_variant = 8 if args.pair_variant is None else args.pair_variant
-    eng.set_tuning(pair_variant=pair_variant, cell_order=args.cell_order, build_variant=args.build_variant,
-                   tile=args.tile, pair_block=args.pair_block)
+    eng.set_tuning(pair_variant=pair_variant, tile=args.tile, pair_block=args.pair_block, **list_tuning(args))
     eng.run(0)
     st0 = eng.state(images=False) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     eng.run(args.warmup)
@@ -475,7 +474,7 @@ def run_ours(args, world, rank, local):
         eng.run(args.acc_equil)
         st3 = eng.state(forces=False, images=False)
         out["accuracy"] = compact(fp32_fp64_window(system, st3["x"], st3["v"], args.acc_steps, 5,
-                                                   tuning={"pair_variant": pair_variant, "cell_order": 1}))
+                                                   tuning={"pair_variant": pair_variant, **list_tuning(args)}))
         out["accuracy"]["from_step"] = args.warmup + args.steps + chunk + args.acc_equil
         del st3
     eng.close()
@@ -508,7 +507,7 @@ def run_slab(args):
     s = inputs.mdpd_slab(nsteps=args.slab_steps, thermo=100)
     s.run_in = tune.with_skin(s.run_in, args.batch_skin)
     eng = Engine(s.run_in, system=s.c_system())
-    eng.set_tuning(pair_variant=8, cell_order=1)
+    eng.set_tuning(pair_variant=8, **list_tuning(args))
     eng.run(0)
     total_ms, done = 0.0, 0
     while done < args.slab_steps:  # timed in graphs of at most 500 steps
@@ -532,6 +531,11 @@ def run_slab(args):
                "surface_tension_stderr": gerr, "err_vs_fp64": acc}
     return summary, {"steps": args.slab_steps, "density_profile_z0.5": [round(float(x), 4) for x in rho],
                      "mean_temp_second_half": float(np.mean(th["temp"][half:])), "fp64_window": window}
+
+
+def list_tuning(args):
+    """Cell order and list build of every engine the bench creates."""
+    return {"cell_order": args.cell_order, "build_variant": args.build_variant}
 
 
 def plain_step_ms(system, steps):
@@ -573,7 +577,7 @@ def run_batched(args):
         s.run_in = tune.with_skin(s.run_in, args.batch_skin)
     n_tot = sum(s.n for s in systems)
     b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
-              tuning={"pair_variant": 8, "cell_order": 1})
+              tuning={"pair_variant": 8, **list_tuning(args)})
     b.run(0)
     K = args.batch_steps
     total_ms, done = 0.0, 0
@@ -633,7 +637,7 @@ def run_batched(args):
 def served_run(jobs, args, rate_label):
     """One pass of a job stream through the server; returns (summary, results, ids)."""
     from gpumdpd_b200.server import Server, latency_percentiles
-    srv = Server(120e9, chunk_steps=args.chunk)
+    srv = Server(120e9, chunk_steps=args.chunk, tuning={"pair_variant": 8, **list_tuning(args)})
     srv.set_policy(args.max_wait, args.min_jobs)
     pending = list(jobs)
     ids = []
@@ -819,11 +823,12 @@ def main():
     ap.add_argument("--tune", action="store_true", help="run the autotuner first (skin and pair schedule)")
     ap.add_argument("--pair-variant", type=int, default=None,
                     help="pair-kernel schedule (default: the engine's choice)")
-    ap.add_argument("--build-variant", type=int, default=0,
-                    help="list-build kernel (0: ranges in registers; 1, 2: in shared memory; 4: cell tiles; "
-                         "5: column ranges, with --cell-order 2)")
-    ap.add_argument("--cell-order", type=int, default=1,
-                    help="cell order of the slots (0: linear, 1: Morton, 2: x-y columns in Morton order)")
+    ap.add_argument("--build-variant", type=int, default=5,
+                    help="list-build kernel of every engine (0: cell ranges in registers; 1, 2: in shared memory; "
+                         "4: cell tiles; 5: column ranges, contiguous under --cell-order 0 or 2)")
+    ap.add_argument("--cell-order", type=int, default=0,
+                    help="cell order of the slots of every engine (0: linear, 1: Morton, 2: x-y columns in "
+                         "Morton order)")
     ap.add_argument("--pair-block", type=int, default=0,
                     help="pair schedule 11: 3 = the tile kernel at 3 CTAs per SM (default 4)")
     ap.add_argument("--tile", type=int, default=0,

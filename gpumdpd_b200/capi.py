@@ -71,6 +71,20 @@ class dpd_tuning(ctypes.Structure):
     ]
 
 
+# the engine's knobs when none are given (pair schedule 8, linear cells, column-range build)
+DEFAULT_TUNING = {"pair_variant": 8, "cell_order": 0, "build_variant": 5}
+
+
+def tuning(**knobs):
+    """A dpd_tuning of the engine defaults with the given knobs replaced."""
+    t = dpd_tuning()
+    for k, v in {**DEFAULT_TUNING, **knobs}.items():
+        if not hasattr(t, k) or k == "reserved":
+            raise TypeError(f"unknown tuning knob {k!r}")
+        setattr(t, k, int(v))
+    return t
+
+
 class dpd_job_result(ctypes.Structure):
     _fields_ = [
         ("job_id", ctypes.c_int64), ("status", ctypes.c_int), ("steps", ctypes.c_int64),

@@ -259,11 +259,7 @@ int Engine::init(std::vector<Replica>&& reps, const dpd_tuning* tune)
         err = "no replicas";
         return DPD_E_ARG;
     }
-    if (tune) tune_ = *tune;
-    if (!tune) {
-        tune_.cell_order = 1;
-        tune_.pair_variant = 8;
-    }
+    tune_ = tune ? *tune : engine_default_tuning();
     int st = layout();
     if (st) return st;
     CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, stream_priority_));
@@ -844,8 +840,7 @@ void Engine::enqueue_build(cudaStream_t s, bool list, bool wide)
         } else if (wide && gp <= 148 * 8) pdl_launch(k_build_wide, (14 * P_ + 255) / 256, 256, s, ba);
         else if (tune_.build_variant == 1) pdl_launch(k_build_nlist_s<6>, gp, 256, s, ba);
         else if (tune_.build_variant == 2) pdl_launch(k_build_nlist_s<8>, gp, 256, s, ba);
-        else if (tune_.build_variant == 5) pdl_launch(k_build_cols<false, 4>, gp, 256, s, ba);
-        else if (tune_.build_variant == 6) pdl_launch(k_build_cols<true, 5>, gp, 256, s, ba);
+        else if (tune_.build_variant == 5) pdl_launch(k_build_cols, gp, 256, s, ba);
         else pdl_launch(k_build_nlist, gp, 256, s, ba);
     }
 }
@@ -868,7 +863,8 @@ void Engine::enqueue_step(cudaStream_t s, cudaEvent_t ev0, cudaEvent_t ev1)
     const int variant = tile ? 11 : (small && tune_.pair_variant == 8 ? (tiny ? 10 : 4) : tune_.pair_variant);
     // schedule 6: the DPD list build runs inside the pair kernel
     const bool fused = variant == 6 && !any_mdpd_;
-    enqueue_build(s, !fused && !tile, (tiny && tune_.build_variant == 0) || tune_.build_variant == 3);
+    enqueue_build(s, !fused && !tile,
+                  (tiny && (tune_.build_variant == 0 || tune_.build_variant == 5)) || tune_.build_variant == 3);
     if (any_mdpd_) pdl_launch(k_density, gp, 256, s, sa);
     if (ev0) cudaEventRecordWithFlags(ev0, s, cudaEventRecordExternal);
     if (tile) {
@@ -1713,10 +1709,10 @@ int Engine::set_tuning(const dpd_tuning* t)
 {
     if (!t) return DPD_E_ARG;
     if (t->pair_variant < 0 || t->pair_variant > 11 || t->cell_order < 0 || t->cell_order > 2 ||
-        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 6 || t->launch_mode < 0 ||
+        t->pair_block < 0 || t->build_variant < 0 || t->build_variant > 5 || t->launch_mode < 0 ||
         t->launch_mode > 3 || t->tile < 0 || t->tile > TILE_MAX_EDGE || t->tile_capacity < 0 ||
         t->tile_capacity > 4096) {
-        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..6, cell_order 0..2, "
+        err = "dpd_set_tuning: pair_variant must be 0..11, build_variant 0..5, cell_order 0..2, "
               "launch_mode 0..3, tile edge 0..6, tile capacity 0..4096";
         return DPD_E_ARG;
     }

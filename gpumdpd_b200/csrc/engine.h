@@ -78,6 +78,17 @@ struct DeviceBuffers {
     int* tile_code = nullptr;
 };
 
+// the knobs of an engine created without tuning: pair schedule 8, linear cells (z
+// fastest), the list build over column ranges
+inline dpd_tuning engine_default_tuning()
+{
+    dpd_tuning t{};
+    t.pair_variant = 8;
+    t.cell_order = 0;
+    t.build_variant = 5;
+    return t;
+}
+
 class Engine {
 public:
     Engine() = default;

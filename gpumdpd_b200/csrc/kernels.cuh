@@ -659,12 +659,8 @@ __device__ __forceinline__ void column_walk(const float4* __restrict__ pos, cons
     }
 }
 
-// SMR: the five ranges kept in shared memory ([group][thread], conflict-free) rather than
-// in registers, for MINB blocks per SM within the register budget
-template <bool SMR, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_build_cols(BuildArgs a)
+__global__ void __launch_bounds__(256, 4) k_build_cols(BuildArgs a)
 {
-    __shared__ int4 s_rng[SMR ? 5 : 1][256];
     griddep_wait();
     if (!build_on(a)) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -717,15 +713,10 @@ __global__ void __launch_bounds__(256, MINB) k_build_cols(BuildArgs a)
             b1[g] = g ? __ldg(cstart + rm[g]) : s + 1;
             b2[g] = __ldg(cstart + rm[g] + 1);
             je[g] = __ldg(cstart + (whi ? rm[g] : rh[g]) + 1);
-            if constexpr (SMR) s_rng[g][threadIdx.x] = make_int4(jb[g], b1[g], b2[g], je[g]);
         }
 #pragma unroll
         for (int g = 0; g < 5; g++) {
             const int ox = g < 2 ? 0 : 1, oy = g == 0 ? 0 : (g == 1 ? 1 : g - 3);
-            if constexpr (SMR) {
-                const int4 q = s_rng[g][threadIdx.x];
-                jb[g] = q.x, b1[g] = q.y, b2[g] = q.z, je[g] = q.w;
-            }
             column_walk(pos, pi, jb[g], je[g], b1[g], b2[g], __int2float_rn(-ox) * wx, __int2float_rn(-oy) * wy,
                         wz, (1 - ox) * 9 + (1 - oy) * 3, cut2, out, a.nmax, count);
         }

@@ -386,9 +386,8 @@ int dpd_server_create(double hbm_budget_bytes, int chunk_steps, const dpd_tuning
     s->chunk = chunk_steps;
     if (tune) {
         s->tune = *tune;
-    } else {  // the engine defaults
-        s->tune.cell_order = 1;
-        s->tune.pair_variant = 8;
+    } else {
+        s->tune = dpd::engine_default_tuning();
     }
     // cohorts run side by side: no tiny-grid kernels (launch_mode 3 for 0)
     if (s->tune.launch_mode == 0) s->tune.launch_mode = 3;

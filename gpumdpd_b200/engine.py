@@ -218,13 +218,10 @@ class Engine:
         _check(self.lib.dpd_pair_compute_aos(self.h, d_pos, d_vel, d_id, d_type, int(n), int(step), d_force,
                                              d_pe, d_virial), self.lib, self.h)
 
-    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0, tile=0,
-                   tile_capacity=0):
-        t = capi.dpd_tuning()
-        t.pair_block, t.pair_variant, t.cell_order, t.build_variant = pair_block, pair_variant, cell_order, build_variant
-        t.launch_mode = launch_mode
-        t.tile = tile
-        t.tile_capacity = tile_capacity
+    def set_tuning(self, **knobs):
+        """Launch knobs (the fields of dpd_tuning); those not named take the engine defaults
+        (capi.DEFAULT_TUNING, zero for the rest)."""
+        t = capi.tuning(**knobs)
         _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
 
 
@@ -246,9 +243,8 @@ class Batch:
         self._keep.append(structs)
         tune = None
         if tuning is not None:
-            tune = capi.dpd_tuning()
-            for k, v in tuning.items():
-                setattr(tune, k, v)
+            tune = capi.tuning(**tuning)
+            self._keep.append(tune)
             tune = ctypes.byref(tune)
         code = self.lib.dpd_batch_create(n, texts, structs, tune, ctypes.byref(self.h))
         _check(code, self.lib, None)
@@ -268,13 +264,10 @@ class Batch:
     def run(self, nsteps):
         _check(self.lib.dpd_run(self.h, int(nsteps)), self.lib, self.h)
 
-    def set_tuning(self, pair_block=0, pair_variant=0, cell_order=0, build_variant=0, launch_mode=0, tile=0,
-                   tile_capacity=0):
-        t = capi.dpd_tuning()
-        t.pair_block, t.pair_variant, t.cell_order, t.build_variant = pair_block, pair_variant, cell_order, build_variant
-        t.launch_mode = launch_mode
-        t.tile = tile
-        t.tile_capacity = tile_capacity
+    def set_tuning(self, **knobs):
+        """Launch knobs (the fields of dpd_tuning); those not named take the engine defaults
+        (capi.DEFAULT_TUNING, zero for the rest)."""
+        t = capi.tuning(**knobs)
         _check(self.lib.dpd_set_tuning(self.h, ctypes.byref(t)), self.lib, self.h)
 
     def thermo(self, rep, max_rows=4096):

@@ -21,9 +21,7 @@ class Server:
         self.h = ctypes.c_void_p()
         tune = None
         if tuning is not None:
-            t = capi.dpd_tuning()
-            for k, v in tuning.items():
-                setattr(t, k, v)
+            t = capi.tuning(**tuning)
             tune = ctypes.byref(t)
         code = self.lib.dpd_server_create(float(hbm_budget_bytes), int(chunk_steps), tune, ctypes.byref(self.h))
         if code:

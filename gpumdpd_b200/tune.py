@@ -16,7 +16,10 @@ src/force/pair_dpd.cu:613-616 eight threads per particle):
 - the pair schedule and its work split: a thread per particle (0), the warp pair queue
   (1), the flattened warp schedule (4, 8, 9), and the cell-tile kernel without a list
   (11) with 1, 2 or 4 home cells per tile edge (or the engine's choice);
-- the launch mode (0: the fused small-grid launches where they apply; 1: never).
+- the launch mode (0: the fused small-grid launches where they apply; 1: never);
+- the cell order of the slots and the list build that goes with it: linear cells with the
+  build over column ranges (five contiguous slot ranges per particle), or Morton-ordered
+  cells with the build cell by cell.
 
 Candidates are timed with CUDA events over whole steps (list builds included) after a
 short warm-up; the fastest is returned with the table of every candidate.
@@ -32,6 +35,7 @@ SCHEDULES = ({"pair_variant": 8}, {"pair_variant": 4}, {"pair_variant": 1}, {"pa
              {"pair_variant": 11, "tile": 0}, {"pair_variant": 11, "tile": 2}, {"pair_variant": 11, "tile": 4})
 LAUNCH_MODES = (0, 1)
 INTERVALS = (1, 2, 5)
+LISTS = ({"cell_order": 0, "build_variant": 5}, {"cell_order": 1, "build_variant": 0})
 VARIANTS = tuple(sorted({s["pair_variant"] for s in SCHEDULES}))
 
 
@@ -76,14 +80,15 @@ def safe_intervals(skin, dmax, intervals=INTERVALS, margin=1.5):
     return tuple(k for k in intervals if k == 1 or k * dmax * margin < 0.5 * skin)
 
 
-def _candidates(schedules, launch_modes):
+def _candidates(schedules, launch_modes, lists):
     for sc in schedules:
         for lm in launch_modes:
-            yield dict(sc, launch_mode=lm)
+            for li in lists:
+                yield dict(sc, launch_mode=lm, **li)
 
 
 def tune_system(system, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MODES, intervals=INTERVALS,
-                steps=20, warmup=5, variants=None):
+                steps=20, warmup=5, variants=None, lists=LISTS):
     """Best knobs for one system; returns (best, table of ms/step).  `variants` (pair
     schedules without tile options) narrows `schedules`."""
     if variants is not None:
@@ -106,8 +111,8 @@ def tune_system(system, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MO
             except Exception as e:  # box too small for this skin's cells, for example
                 table.append({"skin": skin, "nl_f": nl_f, "error": str(e)})
                 continue
-            for c in _candidates(schedules, launch_modes):
-                eng.set_tuning(**{"cell_order": 1, **c})
+            for c in _candidates(schedules, launch_modes, lists):
+                eng.set_tuning(**c)
                 table.append(dict(c, skin=skin, nl_f=nl_f, ms_per_step=_time(eng, steps, warmup)))
             eng.close()
     ok = [t for t in table if "ms_per_step" in t]
@@ -116,20 +121,19 @@ def tune_system(system, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MO
 
 
 def tune_batch(systems, skins=SKINS, schedules=SCHEDULES, launch_modes=LAUNCH_MODES, steps=10, warmup=3,
-               variants=None):
+               variants=None, lists=LISTS):
     """Best knobs for a packed batch of systems (one skin for all; check interval 1)."""
     if variants is not None:
         schedules = tuple({"pair_variant": v} for v in variants)
     table = []
     for skin in skins:
         try:
-            b = Batch([with_skin(s.run_in, skin) for s in systems], [s.c_system() for s in systems],
-                      tuning={"pair_variant": 8, "cell_order": 1})
+            b = Batch([with_skin(s.run_in, skin) for s in systems], [s.c_system() for s in systems])
         except Exception as e:
             table.append({"skin": skin, "error": str(e)})
             continue
-        for c in _candidates(schedules, launch_modes):
-            b.set_tuning(**{"cell_order": 1, **c})
+        for c in _candidates(schedules, launch_modes, lists):
+            b.set_tuning(**c)
             table.append(dict(c, skin=skin, nl_f=1, ms_per_step=_time(b, steps, warmup)))
         b.close()
     ok = [t for t in table if "ms_per_step" in t]

@@ -78,8 +78,9 @@ typedef struct dpd_thermo {
     double angle_pe;    /* atom_style angle: the angle_pe column */
 } dpd_thermo;
 
-/* Launch/tuning knobs chosen by the autotuner (gpumdpd_b200/tune.py); zero fields
- * mean "engine default". */
+/* Launch/tuning knobs chosen by the autotuner (gpumdpd_b200/tune.py).  An engine,
+ * batch or server created without a dpd_tuning runs pair_variant 8, cell_order 0 and
+ * build_variant 5, with every other field zero. */
 typedef struct dpd_tuning {
     int pair_block;        /* pair_variant 11: 3 = the tile kernel compiled for 3
                               CTAs per SM (more registers), else 4                */
@@ -112,7 +113,7 @@ typedef struct dpd_tuning {
                               the integrate as one, the step's bookkeeping in the
                               integrate's last block; tiny ones (up to 148 blocks)
                               also build the list with a thread per (slot, stencil
-                              cell) (in place of build variant 0) and run the pair
+                              cell) (in place of build variant 0 or 5) and run the pair
                               pass with a thread per list entry (schedule 10);
                               1 = never; 2 = always; 3 = as 0 without the tiny-grid
                               kernels (the server's cohorts: engines that share

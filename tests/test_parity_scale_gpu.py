@@ -1,9 +1,9 @@
 """Parity on the headline configurations at full size, through the C ABI.
 
 - The A5B5 diblock melt (L = 100, N = 3.0M, 2.7M harmonic bonds, skin 0: the
-  configuration the headline throughput is measured on), with the Morton cell order and
-  the default list build, and with the column cell order and the column-range build:
-  step-0 forces within 1e-5 of the RMS force against the FP64 oracle on the engine's own
+  configuration the headline throughput is measured on) under the default knobs (linear
+  cell order, column-range list build), the column cell order, and the Morton cell order
+  with the cell-by-cell build: step-0 forces within 1e-5 of the RMS force against the FP64 oracle on the engine's own
   state, and the neighbour set equal to the oracle's FP32-predicate set
   (src/force/neigh_list.cu:360-389) as tag pairs.
 - The packed 256-replica A/B sweep (3.16M slots, L log-uniform over 8..24, a_AB over
@@ -42,8 +42,8 @@ def _half_v(st, masses, types, dt):
     return st["v"] - 0.5 * dt * st["f"] / m
 
 
-@pytest.mark.parametrize("tuning", [{"cell_order": 1}, {"cell_order": 2, "build_variant": 5}],
-                         ids=["morton", "columns"])
+@pytest.mark.parametrize("tuning", [{}, {"cell_order": 2}, {"cell_order": 1, "build_variant": 0}],
+                         ids=["linear_columns", "columns", "morton"])
 def test_melt_3M_step0_forces_and_neighbor_set(oracle_mod, tuning):
     from gpumdpd_b200 import Engine, inputs
     s = inputs.diblock_melt(L=100.0, seed=7, nsteps=10, thermo=1000, skin=0.0)
@@ -76,7 +76,7 @@ def test_packed_sweep_replicas_every_step(oracle_mod):
     for s in systems:
         s.run_in = tune.with_skin(s.run_in, 0.0)
     b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
-              tuning={"pair_variant": 8, "cell_order": 1})
+              tuning={"pair_variant": 8})
     assert sum(s.n for s in systems) > 3_000_000
     ns = np.array([s.n for s in systems])
     sel = sorted({int(np.argmin(ns)), int(np.argmax(ns)), 0, 255} | {int(k) for k in np.linspace(0, 255, 6)[1:-1]})

@@ -49,7 +49,7 @@ def _golden(name):
 def _engine(s, **tuning):
     from gpumdpd_b200 import Engine
     e = Engine(s.run_in, system=s.c_system())
-    e.set_tuning(pair_variant=11, cell_order=1, **tuning)
+    e.set_tuning(pair_variant=11, **tuning)
     return e
 
 
@@ -145,7 +145,7 @@ def test_tile_batch_of_uneven_replicas(oracle_mod):
     for s in systems:
         s.run_in = tune.with_skin(s.run_in, 0.0)
     b = Batch([s.run_in for s in systems], [s.c_system() for s in systems],
-              tuning={"pair_variant": 11, "cell_order": 1})
+              tuning={"pair_variant": 11})
     b.run(0)
     for k, s in enumerate(systems):
         st = b.state(k)
@@ -166,7 +166,7 @@ def test_tile_matches_list_schedule_over_steps():
     s = _systems()["melt_skin0"]
     a = _engine(s)
     b = Engine(s.run_in, system=s.c_system())
-    b.set_tuning(pair_variant=8, cell_order=1)
+    b.set_tuning(pair_variant=8)
     a.run(20)
     b.run(20)
     sa, sb = a.state(), b.state()
@@ -188,7 +188,7 @@ def test_tile_list_build_matches_oracle(oracle_mod, name):
     s = _systems()[name]
     s.run_in = re.sub(r"(?m)^thermo \d+$", "thermo 1000", s.run_in)
     e = Engine(s.run_in, system=s.c_system())
-    e.set_tuning(pair_variant=8, cell_order=1, build_variant=4)
+    e.set_tuning(pair_variant=8, build_variant=4)
     e.run(0)
     c = e.cells()
     got = e.neighbors()

@@ -1,5 +1,5 @@
 """The autotuner: it times every candidate (skin = cell size, safe rebuild check interval,
-pair schedule, tile edge, launch mode) over whole steps and returns the fastest; every
+pair schedule, tile edge, launch mode, cell order with its list build) over whole steps and returns the fastest; every
 candidate it may return is a valid configuration of the same system (its step-0 forces
 are the FP64 oracle's within 1e-5 of the RMS force)."""
 import numpy as np
@@ -22,12 +22,13 @@ def test_tune_system_picks_the_fastest_exact_candidate(oracle_mod):
     assert {t["skin"] for t in timed} == {0.0, 0.3}
     assert {t["launch_mode"] for t in timed} == {0, 1}
     assert {(t["pair_variant"], t.get("tile")) for t in timed} == {(8, None), (11, 0), (11, 2)}
+    assert {(t["cell_order"], t["build_variant"]) for t in timed} == {(0, 5), (1, 0)}
     assert all(t["nl_f"] == 1 for t in timed if t["skin"] == 0.0)
     ff = oracle_mod.ff_from_run_in(s.run_in, s.masses)
     for t in timed:
-        knobs = {k: t[k] for k in ("pair_variant", "launch_mode", "tile") if k in t}
+        knobs = {k: t[k] for k in ("pair_variant", "launch_mode", "tile", "cell_order", "build_variant") if k in t}
         e = Engine(tune.with_skin(s.run_in, t["skin"], t["nl_f"]), system=s.c_system())
-        e.set_tuning(cell_order=1, **knobs)
+        e.set_tuning(**knobs)
         e.run(0)
         st = e.state()
         c = e.cells()
