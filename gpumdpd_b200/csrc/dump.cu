@@ -15,10 +15,11 @@
 
 namespace dpd {
 
-// Copy replica 0's current slots (the parity buffer of this step) and the fix results
-// into a snapshot slot.  One thread per particle slot.
+// Copy replica 0's current slots (the parity buffer of this step), its image counters
+// (kept by tag, copied in tag order) and the fix results into a snapshot slot.  One
+// thread per particle slot.
 __global__ void k_snapshot(const int* parity, const float4* pos0, const float4* pos1, const float4* vel0,
-                           const float4* vel1, const int4* img0, const int4* img1, const float4* force4,
+                           const float4* vel1, const int4* img, int nimg, const float4* force4,
                            const FixOut* fixo, int p0, int ns, float4* opos, float4* ovel, int4* oimg,
                            float4* ofrc, FixOut* ofo)
 {
@@ -28,7 +29,7 @@ __global__ void k_snapshot(const int* parity, const float4* pos0, const float4* 
     const int par = *parity & 1;
     opos[s] = (par ? pos1 : pos0)[p0 + s];
     ovel[s] = (par ? vel1 : vel0)[p0 + s];
-    oimg[s] = (par ? img1 : img0)[p0 + s];
+    if (s < nimg) oimg[s] = img[s];  // in tag order
     ofrc[s] = force4[p0 + s];
 }
 
@@ -253,7 +254,8 @@ int Engine::dump_frame(DumpWriter* w, uint32_t step)
     }
     const int p0 = reps_[0].desc.p_begin;
     k_snapshot<<<(w->ns + 255) / 256, 256, 0, stream_>>>(b_.parity, b_.pos[0], b_.pos[1], b_.vel[0], b_.vel[1],
-                                                        b_.img[0], b_.img[1], b_.force4, b_.fixo, p0, w->ns,
+                                                        b_.img + reps_[0].desc.tag_base, reps_[0].desc.n_real,
+                                                        b_.force4, b_.fixo, p0, w->ns,
                                                         w->dpos[slot], w->dvel[slot], w->dimg[slot],
                                                         w->dfrc[slot], w->dfo[slot]);
     cudaError_t e = cudaGetLastError();

@@ -291,7 +291,6 @@ int Engine::alloc_and_upload()
     for (int q = 0; q < 2; q++) {
         DA(b_.pos[q], P_);
         DA(b_.vel[q], P_);
-        DA(b_.img[q], P_);
         DA(b_.bonds[q], (size_t)std::max(maxb_, 1) * P_);
     }
     DA(b_.parity, 1);
@@ -309,6 +308,7 @@ int Engine::alloc_and_upload()
     int64_t ntag = 0;
     for (auto& R : reps_) ntag += R.sys.n_atoms;
     DA(b_.tag2idx, ntag);
+    DA(b_.img, ntag);
     DA(b_.ncount, P_);
     DA(b_.nlist, (size_t)P_ * nmax_);
     DA(b_.blocksum, (C_ + 4095) / 4096 + 1);
@@ -564,7 +564,6 @@ int Engine::upload_particles()
     if (st) return st;
     float4* pos = h_pos_;
     float4* vel = h_vel_;
-    int4* img = h_img_;
     const bool first = !bonds_tag_;
     std::vector<int2> bonds;
     if (first) bonds.assign((size_t)std::max(maxb_, 1) * P_, make_int2(0, 0));
@@ -605,7 +604,6 @@ int Engine::upload_particles()
             memcpy(&tagf, &tagw, 4);
             vel[s] = make_float4((float)R.sys.v[3 * (size_t)i], (float)R.sys.v[3 * (size_t)i + 1],
                                  (float)R.sys.v[3 * (size_t)i + 2], tagf);
-            img[s] = make_int4(0, 0, 0, 0);
         }
         });
         if (first && d.bond_style) {
@@ -622,7 +620,6 @@ int Engine::upload_particles()
         for (int s = d.p_end; s < d.p_cap_end; s++) {
             pos[s] = make_float4(0, 0, 0, 0);
             vel[s] = make_float4(0, 0, 0, 0);
-            img[s] = make_int4(0, 0, 0, 0);
         }
     }
     // the state goes into buffer 0, which becomes the current one
@@ -633,7 +630,11 @@ int Engine::upload_particles()
     }
     CK(cudaMemcpyAsync(b_.pos[0], pos, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.vel[0], vel, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.img[0], img, sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
+    {
+        int64_t ntag = 0;
+        for (auto& R : reps_) ntag += R.sys.n_atoms;
+        CK(cudaMemsetAsync(b_.img, 0, sizeof(int4) * ntag, stream_));
+    }
     CK(cudaMemcpyAsync(b_.bonds[0], bonds_tag_, sizeof(int2) * nb, cudaMemcpyDeviceToDevice, stream_));
     CK(cudaMemsetAsync(b_.parity, 0, sizeof(int), stream_));
     // slots are in tag order until the first build
@@ -670,9 +671,9 @@ static BuildArgs build_args(const DeviceBuffers& b, int P, int C, int nmax, int 
     for (int q = 0; q < 2; q++) {
         a.buf.pos[q] = b.pos[q];
         a.buf.vel[q] = b.vel[q];
-        a.buf.img[q] = b.img[q];
         a.buf.bonds[q] = b.bonds[q];
     }
+    a.buf.img = b.img;
     a.last4 = b.last4;
     a.cnt = b.cnt;
     a.cstart = b.cstart;
@@ -702,9 +703,9 @@ static StepArgs step_args(const DeviceBuffers& b, int P, int nmax, int maxb, int
     for (int q = 0; q < 2; q++) {
         a.buf.pos[q] = b.pos[q];
         a.buf.vel[q] = b.vel[q];
-        a.buf.img[q] = b.img[q];
         a.buf.bonds[q] = b.bonds[q];
     }
+    a.buf.img = b.img;
     a.parity = b.parity;
     a.force4 = b.force4;
     a.rho = b.rho;
@@ -1438,7 +1439,7 @@ int Engine::get_state(int rep, double* x, double* v, int* image, double* f)
     CK(cudaMemcpyAsync(vel, b_.vel[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     if (x || image) {
         CK(cudaMemcpyAsync(pos, b_.pos[par] + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
-        CK(cudaMemcpyAsync(img, b_.img[par] + d.p_begin, sizeof(int4) * ns, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(img, b_.img + d.tag_base, sizeof(int4) * d.n_real, cudaMemcpyDeviceToHost, stream_));
     }
     if (f) CK(cudaMemcpyAsync(frc, b_.force4 + d.p_begin, sizeof(float4) * ns, cudaMemcpyDeviceToHost, stream_));
     // a spring's share of the force (post_force adds it to the force array the reference
@@ -1489,7 +1490,8 @@ bool Engine::slots_to_tags(int rep, const float4* pos, const float4* vel, const 
                 f[o + q] = q == 0 ? frc[k].x : (q == 1 ? frc[k].y : frc[k].z);
                 if (spring_a && ((R.ff.spring.mask >> t0) & 1u)) f[o + q] += (double)spring_a[q] * R.sys.masses[t0];
             }
-            if (image) image[o + q] = (q == 0 ? img[k].x : (q == 1 ? img[k].y : img[k].z)) + (int)wrap;
+            const int4& im = img[tag - 1];
+            if (image) image[o + q] = (q == 0 ? im.x : (q == 1 ? im.y : im.z)) + (int)wrap;
         }
     }
     });

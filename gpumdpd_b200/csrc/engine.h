@@ -51,7 +51,7 @@ struct DeviceBuffers {
     float4* bondc = nullptr;
     float4* pos[2] = {nullptr, nullptr};  // double-buffered by *parity
     float4* vel[2] = {nullptr, nullptr};
-    int4* img[2] = {nullptr, nullptr};
+    int4* img = nullptr;  // [tags] image counters by tag index, not permuted
     int2* bonds[2] = {nullptr, nullptr};
     int* parity = nullptr;
     float4 *force4 = nullptr, *last4 = nullptr;
@@ -131,7 +131,8 @@ public:
     // into an engine made from the same run.in and system (restart.cu)
     int write_restart(const std::string& path);
     int read_restart(const std::string& path);
-    // FP32 slots of a replica (host copies) to FP64 arrays in tag order; false on a bad tag
+    // FP32 slots of a replica (host copies; the image counters already in tag order) to
+    // FP64 arrays in tag order; false on a bad tag
     bool slots_to_tags(int rep, const float4* pos, const float4* vel, const int4* img, const float4* frc,
                        const float* spring_a, double* x, double* v, int* image, double* f) const;
     int pair_compute_aos(const float* d_pos, const float* d_vel, const int* d_id, const int* d_type,

@@ -9,7 +9,9 @@
 //              [0,w) in between; a build re-bins every particle.
 //   vel[s]   = {vx, vy, vz, tag<<5 | (type-1)}
 //   force4[s]= {fx, fy, fz, 0}           accumulated with vector atomics
-//   img[s]   = image counters (updated when a build re-bins across the box)
+//   img[t]   = image counters, by tag (tag_base + tag - 1), single-buffered: a build that
+//              re-bins a particle across the box updates its counters in place, so the
+//              permutation does not move them
 // Slots are sorted by cell (counting sort at every build; cells in linear or Morton
 // order; within a cell in the order the counting pass's atomics drew).  The half neighbour list is warp-chunked,
 //   nlist[((s>>5)*nmax + k)*32 + (s&31)] = j | code<<27,
@@ -128,11 +130,12 @@ __device__ __forceinline__ void acc_flush_warp(double (&val)[NV], const int* fie
 }
 
 // ---------------------------------------------------------------------------------
-// Double-buffered particle arrays; `par` selects the current buffer.
+// Double-buffered particle arrays; `par` selects the current buffer.  The image counters
+// are indexed by tag and not permuted.
 struct PBuf {
     float4* pos[2];
     float4* vel[2];
-    int4* img[2];
+    int4* img;
     int2* bonds[2];
 };
 
@@ -328,19 +331,25 @@ __device__ __forceinline__ void permute_slot(const BuildArgs& a, const int s)
     }
     float4 p = a.buf.pos[par][s];
     float4 v = a.buf.vel[par][s];
-    int4 im = a.buf.img[par][s];
     if (s < d.p_end) {
         int dimg[3];
         if (!rebin(d, p, dimg)) atomicOr(&a.rstate[r].status, ST_NONFINITE);
-        im.x += dimg[0];
-        im.y += dimg[1];
-        im.z += dimg[2];
         int t = tag_of(v.w);
-        if (t >= 1 && t <= d.n_real) a.tag2idx[d.tag_base + t - 1] = dst;
+        if (t >= 1 && t <= d.n_real) {
+            a.tag2idx[d.tag_base + t - 1] = dst;
+            // across the box: the particle's own counters (one slot per tag, no race)
+            if (dimg[0] | dimg[1] | dimg[2]) {
+                int4* ip = a.buf.img + d.tag_base + t - 1;
+                int4 im = *ip;
+                im.x += dimg[0];
+                im.y += dimg[1];
+                im.z += dimg[2];
+                *ip = im;
+            }
+        }
     }
     a.buf.pos[nxt][dst] = p;
     a.buf.vel[nxt][dst] = v;
-    a.buf.img[nxt][dst] = im;
     if (!d.skin_zero) a.last4[dst] = p;  // skin 0 rebuilds unconditionally: no skin check
     for (int k = 0; k < a.maxb; k++)
         a.buf.bonds[nxt][(size_t)k * a.P + dst] = a.buf.bonds[par][(size_t)k * a.P + s];

@@ -971,8 +971,9 @@ __device__ __forceinline__ void integrate_slot(const StepArgs& a, const int s, W
                             }
                             gv[3 * k] = in ? 1.0 : 0.0;
                         } else {
-                            const int4 im = a.buf.img[par][s];
-                            const float4 x0 = a.uw0[d.tag_base + (int)((uint32_t)__float_as_int(v.w) >> DPD_TYPE_BITS) - 1];
+                            const int ti = d.tag_base + (int)((uint32_t)__float_as_int(v.w) >> DPD_TYPE_BITS) - 1;
+                            const int4 im = a.buf.img[ti];
+                            const float4 x0 = a.uw0[ti];
                             const double dx = d.lo[0] + xa[0] + (double)im.x * g.L[0] - x0.x;
                             const double dy = d.lo[1] + xa[1] + (double)im.y * g.L[1] - x0.y;
                             const double dz = d.lo[2] + xa[2] + (double)im.z * g.L[2] - x0.z;
@@ -1285,7 +1286,7 @@ __global__ void __launch_bounds__(256) k_fix_sums(StepArgs a)
         const uint32_t gm = PH == 0 ? fd.spring_mask : ((eos & 2) ? fd.recenter_mask : 0u);
         if ((gm >> t0) & 1u) {
             const float4 p = a.buf.pos[par][s];
-            const int4 im = a.buf.img[par][s];
+            const int4 im = a.buf.img[d.tag_base + tag_of(v.w) - 1];
             const int code = __float_as_int(p.w);
             const int base = PH == 0 ? 0 : 3;
             accv[base + 0] = (double)m.x * unwrapped(d, fd, code, p.x, im.x, 0);

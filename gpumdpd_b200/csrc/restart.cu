@@ -60,7 +60,7 @@ int Engine::write_restart(const std::string& path)
         if (b_.fixo) CK(cudaMemcpy(&fo, b_.fixo + r, sizeof(FixOut), cudaMemcpyDeviceToHost));
         CK(cudaMemcpyAsync(h_pos_, b_.pos[par] + d.p_begin, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream_));
         CK(cudaMemcpyAsync(h_vel_, b_.vel[par] + d.p_begin, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream_));
-        CK(cudaMemcpyAsync(h_img_, b_.img[par] + d.p_begin, sizeof(int4) * n, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(h_img_, b_.img + d.tag_base, sizeof(int4) * n, cudaMemcpyDeviceToHost, stream_));
         CK(cudaMemcpyAsync(h_frc_, b_.force4 + d.p_begin, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
         // slots to tag order
@@ -77,7 +77,7 @@ int Engine::write_restart(const std::string& path)
             }
             pos[tag - 1] = h_pos_[k];
             vel[tag - 1] = h_vel_[k];
-            img[tag - 1] = h_img_[k];
+            img[k] = h_img_[k];  // already in tag order
             frc[tag - 1] = h_frc_[k];
         }
         const int32_t na = n;
@@ -181,7 +181,9 @@ int Engine::read_restart(const std::string& path)
     const size_t nb = (size_t)std::max(maxb_, 1) * P_;
     CK(cudaMemcpyAsync(b_.pos[0], h_pos_, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.vel[0], h_vel_, sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(b_.img[0], h_img_, sizeof(int4) * P_, cudaMemcpyHostToDevice, stream_));
+    for (const auto& R : reps_)
+        CK(cudaMemcpyAsync(b_.img + R.desc.tag_base, h_img_ + R.desc.p_begin, sizeof(int4) * R.desc.n_real,
+                           cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.force4, frc_all.data(), sizeof(float4) * P_, cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(b_.bonds[0], bonds_tag_, sizeof(int2) * nb, cudaMemcpyDeviceToDevice, stream_));
     CK(cudaMemsetAsync(b_.parity, 0, sizeof(int), stream_));
