@@ -375,14 +375,16 @@ int Engine::alloc_and_upload()
     // harmonic angles (atom_style angle): a static table in global tag indices
     {
         std::vector<int4> tbl;
-        std::vector<float2> acoef;
+        std::vector<float4> acoef;
         std::vector<int> awrep;
         for (int r = 0; r < nrep; r++) {
             const Replica& R = reps_[r];
             if (R.ff.angle_style != 1 || R.sys.angles.empty()) continue;
             const int off = (int)acoef.size();
-            for (const auto& c : R.ff.angle_coeff)
-                acoef.push_back(make_float2((float)c[0], (float)(c[1] * (M_PI / 180.0))));
+            for (const auto& c : R.ff.angle_coeff) {
+                const double th0 = c[1] * (M_PI / 180.0);
+                acoef.push_back(make_float4((float)c[0], (float)th0, (float)std::cos(th0), (float)std::sin(th0)));
+            }
             const int tb = R.desc.tag_base;
             for (size_t q = 0; q < R.sys.angles.size() / 4; q++) {
                 const int* a = &R.sys.angles[4 * q];
@@ -397,7 +399,7 @@ int Engine::alloc_and_upload()
             if ((st = dalloc(&angle_coef_, acoef.size()))) return st;
             if ((st = dalloc(&angle_wrep_, awrep.size()))) return st;
             CK(cudaMemcpyAsync(angle_tbl_, tbl.data(), sizeof(int4) * tbl.size(), cudaMemcpyHostToDevice, stream_));
-            CK(cudaMemcpyAsync(angle_coef_, acoef.data(), sizeof(float2) * acoef.size(), cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(angle_coef_, acoef.data(), sizeof(float4) * acoef.size(), cudaMemcpyHostToDevice, stream_));
             CK(cudaMemcpyAsync(angle_wrep_, awrep.data(), sizeof(int) * awrep.size(), cudaMemcpyHostToDevice, stream_));
             CK(cudaStreamSynchronize(stream_));
         }

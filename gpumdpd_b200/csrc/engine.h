@@ -219,7 +219,7 @@ private:
     int4* h_img_ = nullptr;
     int2* bonds_tag_ = nullptr;  // bond partner table in tag order (device)
     int4* angle_tbl_ = nullptr;   // angles: {coef index or -1, global tags i, j, k}
-    float2* angle_coef_ = nullptr;  // {k, theta0 in radians} per replica and angle type
+    float4* angle_coef_ = nullptr;  // {k, theta0 in radians, cos, sin theta0} per replica and angle type
     int* angle_wrep_ = nullptr;   // replica of each warp of the angle table
     int nang_ = 0;                // angle table length (padded to whole warps per replica)
     float *pe_slot_ = nullptr, *vir_slot_ = nullptr;  // per-atom PE/virial of the AoS entry

@@ -1385,8 +1385,18 @@ __global__ void k_fix_reduce(StepArgs a)
 // float4 reductions.  The table is in global tag indices (it never moves); each
 // replica's range is padded to whole warps (entries with coef < 0 are padding), so a
 // warp's FP64 sums belong to one replica.
+// a*b - c*d with about one rounding (Kahan's form with fma): the cross product of two
+// nearly parallel vectors without cancellation
+__device__ __forceinline__ float diff_of_products(float a, float b, float c, float d)
+{
+    const float w = c * d;
+    const float e = __fmaf_rn(-c, d, w);
+    const float f = __fmaf_rn(a, b, -w);
+    return f + e;
+}
+
 __global__ void __launch_bounds__(256) k_angle(StepArgs a, const int4* __restrict__ tbl,
-                                               const float2* __restrict__ coef, const int* awarp_rep, int nang)
+                                               const float4* __restrict__ coef, const int* awarp_rep, int nang)
 {
     griddep_wait();
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1410,12 +1420,21 @@ __global__ void __launch_bounds__(256) k_angle(StepArgs a, const int4* __restric
             disp3(d, __float_as_int(pk.w), pk, pj, d2x, d2y, d2z);
             const float rsq1 = d1x * d1x + d1y * d1y + d1z * d1z;
             const float rsq2 = d2x * d2x + d2y * d2y + d2z * d2z;
-            const float r1 = sqrtf(rsq1), r2 = sqrtf(rsq2);
-            float c = (d1x * d2x + d1y * d2y + d1z * d2z) / (r1 * r2);
+            const float r1 = sqrtf(rsq1), r2 = sqrtf(rsq2), r12 = r1 * r2;
+            float c = (d1x * d2x + d1y * d2y + d1z * d2z) / r12;
             c = fminf(fmaxf(c, -1.0f), 1.0f);
-            const float sn = fmaxf(sqrtf(1.0f - c * c), 0.001f);
-            const float2 kc = coef[e.x];  // {k, theta0 in radians}
-            const float dth = acosf(c) - kc.y;
+            // The reference's harmonic angle (src/force/angle_harmonic.cu), kept accurate in
+            // FP32 near straight triples: sin(theta) from the cross product rather than
+            // sqrt(1 - c^2), and theta - theta0 as atan2 of its sine and cosine (cos and sin
+            // of theta0 precomputed in double) rather than acos(c) - theta0, which near
+            // c = -1 resolves the angle only to about 3e-4 rad
+            const float cpx = diff_of_products(d1y, d2z, d1z, d2y);
+            const float cpy = diff_of_products(d1z, d2x, d1x, d2z);
+            const float cpz = diff_of_products(d1x, d2y, d1y, d2x);
+            const float st = sqrtf(cpx * cpx + cpy * cpy + cpz * cpz) / r12;
+            const float sn = fmaxf(st, 0.001f);
+            const float4 kc = coef[e.x];  // {k, theta0 in radians, cos theta0, sin theta0}
+            const float dth = atan2f(st * kc.z - c * kc.w, c * kc.z + st * kc.w);
             const float aa = -2.0f * kc.x * dth / sn;
             const float a11 = aa * c / rsq1, a12 = -aa / (r1 * r2), a22 = aa * c / rsq2;
             const float fix = a11 * d1x + a12 * d2x, fiy = a11 * d1y + a12 * d2y, fiz = a11 * d1z + a12 * d2z;

@@ -153,6 +153,43 @@ def test_forces_every_step_on_engine_state(oracle_mod, name):
         assert force_err(got["f"], o["f"]) < FORCE_TOL, k
 
 
+def test_angle_forces_near_straight_triples(oracle_mod):
+    """Harmonic angles at theta0 = 180 on chains laid out almost straight (each bead off the
+    chain's line by 1e-4 to 1e-2, log-uniform): the step-0 forces, angle energy included,
+    equal the oracle's within 1e-5 of the RMS force.  In FP32, acos(c) - theta0 and
+    sqrt(1 - c^2) lose the angle near c = -1 (the float spacing of c there is 6e-8, about
+    3e-4 rad of angle); the kernel takes sin(theta) from the cross product and
+    theta - theta0 from atan2 instead."""
+    from gpumdpd_b200 import inputs
+    s = inputs.angle_chains(L=8.0, seed=29, nsteps=10, angle_k=3.0, theta0=180.0)
+    rng = np.random.default_rng(3)
+    chain = 10
+    x = np.empty_like(s.x)
+    L = np.asarray(s.box, dtype=np.float64)
+    for c in range(s.n // chain):
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        p = rng.normal(size=3)
+        p -= u * (p @ u)
+        p /= np.linalg.norm(p)
+        x0 = rng.uniform(0.0, 1.0, 3) * L
+        off = 10.0 ** rng.uniform(-4.0, -2.0, chain)
+        x[c * chain:(c + 1) * chain] = x0 + np.outer(np.arange(chain) * 0.9, u) + np.outer(off, p)
+    x = s.lo + np.mod(x, L)
+    t = inputs.System(s.lo, s.hi, s.masses, s.types, x, s.v, bonds=s.bonds, n_bondtypes=s.n_bondtypes,
+                      mol=s.mol, run_in=s.run_in, atom_style=s.atom_style, angles=s.angles,
+                      n_angletypes=s.n_angletypes)
+    e = _engine_from(t)
+    e.run(0)
+    st = e.state()
+    ff = oracle_mod.ff_from_run_in(t.run_in, t.masses)
+    o = oracle_mod.forces(ff, np.arange(1, t.n + 1), t.types, st["x"], st["v"], t.lo, _box(e), 0,
+                          bonds=t.bonds, angles=t.angles)
+    assert force_err(st["f"], o["f"]) < FORCE_TOL
+    assert e.thermo()["angle_pe"][0] == pytest.approx(o["angle_pe"], rel=1e-5, abs=1e-9)
+    e.close()
+
+
 @pytest.mark.parametrize("name", ["dpd", "mdpd", "diblock", "angles"])
 def test_trajectory_10_steps(oracle_mod, name):
     """Drift diagnostic: after equilibrating 100 steps on the GPU, 10 steps of engine and
