@@ -787,10 +787,10 @@ static void launch_pair2(int variant, int grid, cudaStream_t s, const StepArgs& 
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 1, 4>, grid, 256, s, a);
     } else if (variant == 8) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5>, grid, 256, s, a);
-        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 3), 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS>, std::min(grid, 148 * 4), 256, s, a);
     } else if (variant == 9) {
         pdl_launch(k_pair_flat_split<STYLE, BONDS, 0, 5, true>, grid, 256, s, a);
-        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 3), 256, s, a);
+        pdl_launch(k_pair_flat_logsteps<STYLE, BONDS, true>, std::min(grid, 148 * 4), 256, s, a);
     } else if (variant == 10) {
         pdl_launch(k_pair_entry<STYLE, BONDS>, (a.nmax * (a.P >> 5) + 7) / 8, 256, s, a);
     }

@@ -659,7 +659,16 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s, W
     const bool log_step = (step % (uint32_t)d.log_f) == 0u;
     if ((LOGM == 0 && log_step) || (LOGM == 1 && !log_step)) return;  // warp-uniform
     const bool log = LOGM == 2 ? log_step : LOGM == 1;
-    double accv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
+                           ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
+    // FP64 sums: with `keep` (grid-stride calls) straight into the warp's kept sums, which
+    // are flushed when the warp moves to another replica; else this call's own
+    double own[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (keep && keep->rep != r) {
+        keep->flush(fields, a.acc);
+        keep->rep = r;
+    }
+    double (&accv)[8] = keep ? keep->tot : own;
     const int par = *a.parity;
     const float4* pos = a.buf.pos[par];
     const float4* vel = a.buf.vel[par];
@@ -766,12 +775,7 @@ __device__ __forceinline__ void pair_flat_warp(const StepArgs& a, const int s, W
         else bond_loop<false>(a, d, pos, a.buf.bonds[par], r, s, pi, fx, fy, fz, accv);
         atomicAdd(&a.force4[s], make_float4(fx, fy, fz, 0.0f));
     }
-    if (log) {
-        const int fields[8] = {ACC_PAIR_PE, ACC_BOND_PE, ACC_VIR + 0, ACC_VIR + 1,
-                               ACC_VIR + 2, ACC_VIR + 3, ACC_VIR + 4, ACC_VIR + 5};
-        if (keep) keep->add(accv, r, fields, a.acc);
-        else acc_flush_warp<8>(accv, fields, r, a.acc);
-    }
+    if (log && !keep) acc_flush_warp<8>(accv, fields, r, a.acc);
 }
 
 template <int STYLE, bool BONDS, int MINB>
@@ -792,7 +796,7 @@ __global__ void __launch_bounds__(256, MINB) k_pair_flat_split(StepArgs a)
 // first checks whether any replica logs this step (the common answer is no, and then the
 // launch costs one wave of tiny blocks instead of a full grid of early exits).
 template <int STYLE, bool BONDS, bool SEG = false>
-__global__ void __launch_bounds__(256, 3) k_pair_flat_logsteps(StepArgs a)
+__global__ void __launch_bounds__(256, 4) k_pair_flat_logsteps(StepArgs a)
 {
     griddep_wait();
     int any = 0;
