@@ -324,16 +324,24 @@ __device__ __forceinline__ void permute_slot(const BuildArgs& a, const int s)
     const int par = *a.parity, nxt = par ^ 1;
     const int r = a.warp_rep[s >> 5];
     const RepDesc& d = a.reps[r];
-    const int dst = a.cstart[a.skey[s]] + a.srank[s];
+    // the slot's own records first: their loads do not wait on the destination, which takes
+    // a dependent gather (the cell start of the slot's key)
+    float4 p = a.buf.pos[par][s];
+    const float4 v = a.buf.vel[par][s];
+    int2 b01[2] = {make_int2(0, 0), make_int2(0, 0)};  // the first two bond records
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+        if (k < a.maxb) b01[k] = a.buf.bonds[par][(size_t)k * a.P + s];
+    const int key = a.skey[s], rank = a.srank[s];
+    int dimg[3] = {0, 0, 0};
+    const bool real = s < d.p_end;
+    if (real && !rebin(d, p, dimg)) atomicOr(&a.rstate[r].status, ST_NONFINITE);
+    const int dst = a.cstart[key] + rank;
     if (dst < d.p_begin || dst >= d.p_cap_end) {  // cannot happen: keys stay in the replica
         atomicOr(&a.rstate[r].status, ST_BAD_INPUT);
         return;
     }
-    float4 p = a.buf.pos[par][s];
-    float4 v = a.buf.vel[par][s];
-    if (s < d.p_end) {
-        int dimg[3];
-        if (!rebin(d, p, dimg)) atomicOr(&a.rstate[r].status, ST_NONFINITE);
+    if (real) {
         int t = tag_of(v.w);
         if (t >= 1 && t <= d.n_real) {
             a.tag2idx[d.tag_base + t - 1] = dst;
@@ -351,7 +359,10 @@ __device__ __forceinline__ void permute_slot(const BuildArgs& a, const int s)
     a.buf.pos[nxt][dst] = p;
     a.buf.vel[nxt][dst] = v;
     if (!d.skin_zero) a.last4[dst] = p;  // skin 0 rebuilds unconditionally: no skin check
-    for (int k = 0; k < a.maxb; k++)
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+        if (k < a.maxb) a.buf.bonds[nxt][(size_t)k * a.P + dst] = b01[k];
+    for (int k = 2; k < a.maxb; k++)
         a.buf.bonds[nxt][(size_t)k * a.P + dst] = a.buf.bonds[par][(size_t)k * a.P + s];
 }
 
