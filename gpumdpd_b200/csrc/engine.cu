@@ -949,7 +949,7 @@ void Engine::enqueue_integrate_initial(cudaStream_t s)
 
 // The tile table of pair schedule 11: the tiles of every replica (edge^3 home cells,
 // fewer at a grid's edge), each replica's tiles in Morton order of their coordinates
-// (the order of the slots), the staging capacity of a CTA: 1.5 times the mean particle
+// (neighbouring tiles run close in time, whatever the cell order of the slots), the staging capacity of a CTA: 1.5 times the mean particle
 // count of a tile's neighbourhood (plus 64) in the densest replica, and the pairs a
 // particle may have (the list capacity max_rho implies at the largest cutoff, 16..96).  Edge 0
 // (the default) takes the largest edge up to 4 that still gives at least 8 tiles per

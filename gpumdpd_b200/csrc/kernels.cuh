@@ -12,8 +12,10 @@
 //   img[t]   = image counters, by tag (tag_base + tag - 1), single-buffered: a build that
 //              re-bins a particle across the box updates its counters in place, so the
 //              permutation does not move them
-// Slots are sorted by cell (counting sort at every build; cells in linear or Morton
-// order; within a cell in the order the counting pass's atomics drew).  The half neighbour list is warp-chunked,
+// Slots are sorted by cell (counting sort at every build; cells in the engine's cell order:
+// linear with z fastest, Morton, or x-y columns in Morton order with z fastest; within a
+// cell in the order the counting pass's atomics drew).  The half neighbour list is
+// warp-chunked,
 //   nlist[((s>>5)*nmax + k)*32 + (s&31)] = j | code<<27,
 // where code = 9(dcx+1)+3(dcy+1)+(dcz+1) encodes the cell difference c_i - c_j in
 // {-1,0,1}^3 of the pair at build time; the displacement is (o_i - o_j) + code*w.
