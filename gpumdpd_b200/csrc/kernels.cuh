@@ -641,8 +641,9 @@ __global__ void __launch_bounds__(256, MINB) k_build_nlist_s(BuildArgs a)
 // periodic boundary is not next to the other two: the group is its two contiguous cells
 // plus that one cell, walked after the five ranges.  A particle whose groups are not
 // contiguous otherwise (every particle under the Morton order) walks the same 13 cells one
-// at a time.  The predicate and the pair set are those of the other builds; which particle
-// of a pair holds it follows this stencil's orientation.
+// at a time.  The predicate and the pair set are those of the other builds (the half list
+// of src/force/neigh_list.cu:322-393); which particle of a pair holds it follows this
+// stencil's orientation.
 __constant__ int8_t c_half_x[13][3] = {
     {0, 0, 1}, {0, 1, -1}, {0, 1, 0}, {0, 1, 1}, {1, -1, -1}, {1, -1, 0}, {1, -1, 1},
     {1, 0, -1}, {1, 0, 0}, {1, 0, 1}, {1, 1, -1}, {1, 1, 0}, {1, 1, 1}};
